@@ -1,0 +1,155 @@
+/*
+ * spooky_b200.h -- C ABI of the B200-native SPOOKY hot path.
+ *
+ * The library advances incompressible HD / MHD / Boussinesq fields (with
+ * field-aligned anisotropic conduction) in a triply periodic box with the
+ * low-storage RK3 integrator and RKL2 super-time-stepping, on one B200.
+ *
+ * State layout (the reference's): U[f][i][j][k], k < NZ/2+1, complex FP64
+ * interleaved (re, im), fields in the order vx vy vz [bx by bz] [th]
+ * (heat-equation mode: th only).  i runs over x (slowest), k over z.
+ *
+ * Every entry point returns an int status (SPK_OK == 0).  A context is not
+ * thread safe; all of its GPU work is issued on the one CUDA stream given at
+ * creation (NULL = the legacy default stream).  No entry point allocates
+ * device memory after spk_ctx_create, and spk_advance issues no host
+ * synchronisation.
+ *
+ * Reference interfaces replaced (paths inside LorenzoLMP/spooky-git):
+ *   spk_ctx_create       Supervisor::Supervisor + Fields::allocate_and_move_to_gpu
+ *                        + Wavevector::Wavevector + init_plan
+ *                        (src/supervisor/supervisor.cu:19-66, src/fields/fields.cu:297-363,
+ *                         src/fields/wavevector.cu:22-112, src/cuda/cufft_routines.cu:84-96)
+ *   spk_set_state /      the device mega-array d_all_fields (src/fields/fields.hpp:64-68)
+ *   spk_get_state
+ *   spk_clean_divergence Fields::CleanFieldDivergence (src/fields/symmetries.cu:114-130)
+ *   spk_compute_dt       TimeStepping::compute_dt (src/timestepping/compute_dt.cu:15-309)
+ *   spk_compute_dfield   TimeStepping::compute_dfield (src/timestepping/compute_dfield.cu:11-90)
+ *   spk_advance          Supervisor::executeMainLoop body: CleanFieldDivergence +
+ *                        TimeStepping::HydroMHDAdvance (src/supervisor/supervisor.cu:179-192,
+ *                        src/timestepping/hydro_mhd_advance.cu:18-189)
+ *   spk_rkl_cycle        RKLegendre::compute_cycle (src/rkl/rkl.cu:187-204, 437-591)
+ *   spk_to_real          Supervisor::Complex2RealFields (src/supervisor/supervisor.cu:261-272)
+ *   spk_budgets          computeEnergy (src/io/spooky_output_functions.cu:23-55)
+ */
+#ifndef SPOOKY_B200_H
+#define SPOOKY_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SPK_OK                 0
+#define SPK_ERR_ARG            1   /* bad argument (null pointer, bad size)          */
+#define SPK_ERR_UNSUPPORTED    2   /* configuration outside what the kernels cover    */
+#define SPK_ERR_CUDA           3   /* a CUDA runtime call failed                      */
+#define SPK_ERR_ALLOC          4   /* device allocation failed at context creation    */
+#define SPK_ERR_NONFINITE      5   /* dt reduction saw NaN/Inf in the real fields     */
+#define SPK_ERR_CONFIG         6   /* inconsistent modules (Parameters::checkParameters) */
+
+/* ---- arithmetic forms --------------------------------------------------- */
+#define SPK_FORM_PLAIN  0   /* FFT passes and products in FP64 (reference precision)   */
+#define SPK_FORM_FP32   1   /* FFT passes and products in FP32, FP64 state and RK/RKL  */
+
+/* ---- super-time-stepping algorithms (Parameters::sts_algorithm) ---------- */
+#define SPK_STS_RKL2    3
+
+/* ---- integrators --------------------------------------------------------- */
+#define SPK_INT_RK3     0   /* TimeStepping::RungeKutta3 (default)                       */
+#define SPK_INT_EULER   1   /* TimeStepping::ForwardEuler (the reference's STS test build) */
+
+/* Parameters: the subset of spooky.cfg that the hot path reads
+ * (src/parameters/parameters.cu:77-505).  Diffusivities are the inverses of
+ * the cfg's reynolds* keys, as the reference computes them (:205-219). */
+typedef struct spk_params {
+    /* physics.gridsize, physics.boxsize */
+    int    nx, ny, nz;
+    double lx, ly, lz;
+    /* modules */
+    int    incompressible, heat_equation, mhd, boussinesq;
+    int    stratification, strat_direction;      /* 0=x 1=y 2=z            */
+    int    anisotropic_diffusion;
+    int    supertimestepping, sts_algorithm;     /* SPK_STS_*              */
+    unsigned sts_vars_mask;                      /* bit f: field f is STS  */
+    int    with2d, antialiasing;
+    /* physics */
+    double nu, nu_m, nu_th;                      /* 1/reynolds, 1/reynolds_magnetic, 1/reynolds_thermic */
+    double reynolds_ani;                         /* chi_parallel = 1/reynolds_ani */
+    double N2, OmegaT2;                          /* brunt_vaissala_squared, mti_frequency_squared */
+    /* code */
+    double cfl, cfl_par, cfl_sts, safety_source;
+    int    safety_sts;
+    double t_initial, t_final, toutput_flow;
+    /* extensions (not in the reference cfg) */
+    double fixed_dt;        /* > 0: use this dt instead of the CFL dt (then clamped like the CFL dt) */
+    int    integrator;      /* SPK_INT_RK3 or SPK_INT_EULER                                        */
+    int    sts_every_step;  /* 1: RKL cycle after the integrator on every step (the STS test build) */
+    int    form;            /* SPK_FORM_PLAIN or SPK_FORM_FP32                                     */
+} spk_params_t;
+
+/* Fill *p with the reference's defaults (parameters.cu:77-505). */
+void spk_params_default(spk_params_t* p);
+
+typedef struct spk_ctx spk_ctx;
+
+/* Create a context: validates the modules (checkParameters), builds the
+ * wavevector tables and the FFT twiddles, allocates every device buffer.
+ * cuda_stream: a cudaStream_t (NULL = default stream). */
+int spk_ctx_create(const spk_params_t* p, void* cuda_stream, spk_ctx** out);
+int spk_ctx_destroy(spk_ctx* ctx);
+
+/* Number of fields F and complex modes Nc = NX*NY*(NZ/2+1) per field. */
+int spk_sizes(const spk_ctx* ctx, int* num_fields, size_t* n_complex);
+
+/* where: 0 = device pointer, 1 = host pointer (copied through pinned staging). */
+int spk_set_state(spk_ctx* ctx, const double* U, int where);
+int spk_get_state(spk_ctx* ctx, double* U, int where);
+
+int spk_set_time(spk_ctx* ctx, double t, int step, double t_lastsnap);
+int spk_get_time(spk_ctx* ctx, double* t, double* dt, int* step);
+
+/* Fields::CleanFieldDivergence on the context state. */
+int spk_clean_divergence(spk_ctx* ctx);
+
+/* TimeStepping::compute_dt on the context state (no divergence cleaning).
+ * Outputs may be NULL.  dt_current is the clamped step the integrator uses. */
+int spk_compute_dt(spk_ctx* ctx, double* dt_hyp, double* dt_par, double* dt_sts, double* dt_current);
+
+/* TimeStepping::compute_dfield: dU = RHS(U), real buffer = C2R(U).
+ * U, dU: device pointers in the state layout ([F][Nc] complex FP64). */
+int spk_compute_dfield(spk_ctx* ctx, const double* U, double* dU);
+
+/* nsteps x { CleanFieldDivergence; HydroMHDAdvance } on the context state.
+ * Asynchronous on the context stream; captured once into a CUDA graph. */
+int spk_advance(spk_ctx* ctx, int nsteps);
+
+/* One RKLegendre::compute_cycle on the context state with the last dt
+ * (uses the real-space B of the last compute_dt / to_real). *s_out may be NULL. */
+int spk_rkl_cycle(spk_ctx* ctx, int* s_out);
+
+/* Supervisor::Complex2RealFields: real fields R[f][i][j][z] (unpadded, FP64)
+ * of the context state into a device buffer of F*NX*NY*NZ doubles. */
+int spk_to_real(spk_ctx* ctx, double* R);
+
+/* Wait for the context stream; returns the first asynchronous error seen. */
+int spk_synchronize(spk_ctx* ctx);
+
+/* Energy budgets in FP64 with the reference's half-spectrum weighting
+ * (computeEnergy: (2*sum|q|^2 - sum_{kz=0}|q|^2) / (2 N^6)) per field. */
+typedef struct spk_budgets {
+    double energy[8];        /* per field: 0.5 <q^2>                       */
+    double dissipation[8];   /* per field: <|grad q|^2> (k^2-weighted)     */
+} spk_budgets_t;
+int spk_budgets(spk_ctx* ctx, spk_budgets_t* out);
+
+/* Human-readable text of the last error on this context (or of the last
+ * failed spk_ctx_create when ctx is NULL). */
+const char* spk_last_error(const spk_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPOOKY_B200_H */

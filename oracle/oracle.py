@@ -1,0 +1,157 @@
+"""ctypes wrapper of the CPU FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the product path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle not built: {path} (run `make -C oracle`)")
+        L = ctypes.CDLL(path)
+        vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [vp]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_num_fields.argtypes = [vp]
+        L.orc_num_fields.restype = ctypes.c_int
+        L.orc_ncomplex.argtypes = [vp]
+        L.orc_ncomplex.restype = ctypes.c_size_t
+        for name in ("orc_set_state", "orc_get_state", "orc_compute_dt", "orc_to_real"):
+            getattr(L, name).argtypes = [vp, dp]
+        L.orc_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        L.orc_get_time.argtypes = [vp, dp, dp, ip]
+        L.orc_kgrid.argtypes = [vp, dp, dp, dp]
+        L.orc_clean_divergence.argtypes = [vp]
+        L.orc_compute_dfield.argtypes = [vp, dp, dp]
+        L.orc_step.argtypes = [vp, ctypes.c_int]
+        L.orc_rkl_cycle.argtypes = [vp]
+        L.orc_rkl_cycle.restype = ctypes.c_int
+        L.orc_budgets.argtypes = [vp, dp, dp]
+        L.orc_r2c.argtypes = [vp, dp, dp]
+        L.orc_c2r.argtypes = [vp, dp, dp]
+        L.orc_fft1d.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        _LIB = L
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def fft1d(x, sign=-1):
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(x)
+    lib().orc_fft1d(len(x), _dp(x), _dp(out), sign)
+    return out
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+class Oracle:
+    """CPU restatement of the reference's Fields/TimeStepping/RKLegendre path."""
+
+    def __init__(self, params):
+        self.params = params.copy()
+        self._h = lib().orc_create(ctypes.byref(self.params))
+        if not self._h:
+            raise RuntimeError("orc_create failed")
+        self.F = lib().orc_num_fields(self._h)
+        self.nc = lib().orc_ncomplex(self._h)
+        p = self.params
+        self.shape_c = (self.F, p.nx, p.ny, p.nz // 2 + 1)
+        self.shape_r = (self.F, p.nx, p.ny, p.nz)
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
+        lib().orc_set_state(self._h, _dp(U))
+
+    def get_state(self):
+        U = np.empty(self.shape_c, dtype=np.complex128)
+        lib().orc_get_state(self._h, _dp(U))
+        return U
+
+    def set_time(self, t, step=0, t_lastsnap=0.0):
+        lib().orc_set_time(self._h, t, step, t_lastsnap)
+
+    def get_time(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        lib().orc_get_time(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st))
+        return t.value, dt.value, st.value
+
+    def kgrid(self):
+        p = self.params
+        kvec = np.empty((3, p.nx, p.ny, p.nz // 2 + 1))
+        mask = np.empty((p.nx, p.ny, p.nz // 2 + 1))
+        km = np.empty(4)
+        lib().orc_kgrid(self._h, _dp(kvec), _dp(mask), _dp(km))
+        return kvec, mask, km
+
+    def clean_divergence(self):
+        lib().orc_clean_divergence(self._h)
+
+    def compute_dt(self):
+        out = np.empty(4)
+        lib().orc_compute_dt(self._h, _dp(out))
+        return out
+
+    def compute_dfield(self, U):
+        U = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
+        dU = np.empty_like(U)
+        lib().orc_compute_dfield(self._h, _dp(U), _dp(dU))
+        return dU
+
+    def step(self, n=1):
+        lib().orc_step(self._h, int(n))
+
+    def rkl_cycle(self):
+        return lib().orc_rkl_cycle(self._h)
+
+    def to_real(self):
+        R = np.empty(self.shape_r)
+        lib().orc_to_real(self._h, _dp(R))
+        return R
+
+    def budgets(self):
+        e = np.empty(self.F)
+        d = np.empty(self.F)
+        lib().orc_budgets(self._h, _dp(e), _dp(d))
+        return e, d
+
+    def r2c(self, R):
+        p = self.params
+        R = np.ascontiguousarray(R, dtype=np.float64).reshape(p.nx, p.ny, p.nz)
+        C = np.empty((p.nx, p.ny, p.nz // 2 + 1), dtype=np.complex128)
+        lib().orc_r2c(self._h, _dp(R), _dp(C))
+        return C
+
+    def c2r(self, C):
+        p = self.params
+        C = np.ascontiguousarray(C, dtype=np.complex128).reshape(p.nx, p.ny, p.nz // 2 + 1)
+        R = np.empty((p.nx, p.ny, p.nz))
+        lib().orc_c2r(self._h, _dp(C), _dp(R))
+        return R
