@@ -1,0 +1,319 @@
+"""Benchmark: 256^3 incompressible MHD, low-storage RK3 steps per second on B200.
+
+Workload (the reference's headline metric, BASELINE "256^3 MHD RK3 steps/s,
+FP32 form vs plain"): 256^3 box [0, 2 pi)^3, u and B independent random
+solenoidal Gaussian fields with shell spectrum E(k) ~ k^4 exp(-2 (k/4)^2),
+rms 1 per component, B0 = 0.1 z added to the k=0 mode of B, nu = eta = 1e-3,
+CFL 1.5, 2/3 dealiasing, dt from the reference's CFL rule every step.
+
+A step = one main-loop iteration (CleanFieldDivergence + HydroMHDAdvance:
+compute_dt, three RK3 stages), run through the C ABI on a CUDA graph.
+
+Arms:
+  default            this library (value = FP32 form; the plain FP64 form,
+                     the FP32-vs-FP64 error, the per-pass roofline, the
+                     end-to-end host-buffer run and a CPU baseline are reported
+                     in the same JSON line)
+  --impl reference   the CPU FP64 oracle (restatement of the reference's
+                     algorithm; the reference itself has no CPU path) on all
+                     host cores, same workload
+
+Multi-GPU: one independent box per rank (the single-box path does not shard
+without a distributed FFT); value = box-steps/s summed over ranks, timed as
+the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "spooky-git_b200"))
+
+from spooky_b200.initial import mhd_random_state  # noqa: E402
+from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, default_params  # noqa: E402
+
+METRIC = "256^3 MHD RK3 steps/s, FP32 form vs plain, 1xB200, at <=1e-5 rel L2 vs FP64"
+HBM_FALLBACK = 6650.0
+
+
+def workload_params(n, form):
+    L = 2 * np.pi
+    return default_params(incompressible=1, mhd=1, gridsize=(n, n, n), boxsize=(L, L, L),
+                          reynolds=1e3, reynolds_magnetic=1e3, cfl=1.5, form=form,
+                          t_final=1e30, toutput_flow=1e30)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def config_dict(n, world):
+    return {"workload": f"incompressible MHD {n}^3, box 2pi, nu=eta=1e-3, B0=0.1z, CFL 1.5, random solenoidal "
+                        f"E(k)~k^4 exp(-2(k/4)^2) u,B (seeds 1,2)",
+            "grid": [n, n, n], "fields": 6, "integrator": "low-storage RK3 (3 stages/step)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single box",
+            "l2_flush": "not needed: working set (state 0.8 GB + pass buffers) >> 126 MB L2"}
+
+
+class ClockSampler:
+    def __init__(self, gpu_index, path):
+        self.path = path
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args):
+    """CPU FP64 oracle on all host cores (the reference arm)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    p = workload_params(args.n, SPK_FORM_PLAIN)
+    U0 = mhd_random_state(p)
+    o = O.Oracle(p)
+    o.set_state(U0)
+    t0 = time.perf_counter()
+    o.step(1)                      # warm-up (one step regardless of --warmup: a step is seconds of CPU)
+    t_step = time.perf_counter() - t0
+    budget = 150.0
+    k = max(1, min(args.steps, int(budget / max(t_step, 1e-3))))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    v = k / el
+    sample = (f"{k} of the requested {args.steps} RK3 steps at {args.n}^3 MHD after 1 warm-up step "
+              f"(steps capped so the run stays within ~{int(budget)} s)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": k, "warmup": 1, "ms_per_step": 1e3 * el / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(args.n, 1),
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU path; this arm is the project's FP64 C restatement of its "
+                    "algorithm (oracle/), OpenMP over pencils"}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(n):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    p = workload_params(n, SPK_FORM_PLAIN)
+    o = O.Oracle(p)
+    o.set_state(mhd_random_state(p))
+    steps, el = 0, 0.0
+    while el < 10.0 and steps < 20:
+        t0 = time.perf_counter()
+        o.step(1)
+        el += time.perf_counter() - t0
+        steps += 1
+    return {"value": steps / el, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} RK3 step(s) of {n}^3 MHD from the same initial state (FP64 C oracle, OpenMP)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import spooky_b200 as S
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    U0 = mhd_random_state(workload_params(n, SPK_FORM_PLAIN))
+    stream = torch.cuda.Stream()
+
+    def timed_run(form, sampler_path=None):
+        ctx = S.Context(workload_params(n, form), stream=stream.cuda_stream)
+        ctx.set_state(U0)
+        ctx.advance(args.warmup)
+        ctx.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local_rank, sampler_path) if sampler_path else None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        ctx.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        return ctx, max_over_ranks(ms), clocks
+
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    clk_path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_rank{rank}.csv")
+    ctx32, ms32, clocks = timed_run(SPK_FORM_FP32, clk_path)
+    kps, bytes_step = ctx32.step_info()
+    ctx64, ms64, _ = timed_run(SPK_FORM_PLAIN)
+    _, bytes_step64 = ctx64.step_info()
+
+    # FP32 form vs the FP64 plain form after the same steps from the same state
+    U32 = ctx32.get_state()
+    U64 = ctx64.get_state()
+    rel = float(np.linalg.norm((U32 - U64).ravel()) / np.linalg.norm(U64.ravel()))
+    t32 = ctx32.get_time()
+    del ctx64
+    torch.cuda.empty_cache()
+
+    # end to end through the public API with host buffers: initial state H2D
+    # from pinned memory, per step an energy-budget read-back (D2H), final
+    # state D2H into pinned memory
+    hostU = torch.from_numpy(U0.view(np.float64).copy()).pin_memory()
+    hostOut = torch.empty_like(hostU).pin_memory()
+    state_bytes = hostU.numel() * 8
+    ctxe = S.Context(workload_params(n, SPK_FORM_FP32), stream=stream.cuda_stream)
+    ctxe.set_state(hostU)
+    ctxe.advance(args.warmup)
+    ctxe.budgets()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctxe.set_state(hostU)
+    for _ in range(args.steps):
+        ctxe.advance(1)
+        ctxe.budgets()
+    ctxe.get_state(hostOut)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    del ctxe
+
+    # per-pass roofline on the FP32 context (its state is no longer needed)
+    prof = ctx32.profile_passes(reps=5)
+    peak, peak_kind = peaks()
+    for pz in prof:
+        pz["gbs"] = pz["bytes"] / (pz["ms"] * 1e-3) / 1e9
+        pz["frac_of_peak"] = pz["gbs"] / peak
+        pz["share_of_step"] = pz["ms"] * pz["launches_per_step"] / ms32
+    dom = max(prof, key=lambda d: d["ms"] * d["launches_per_step"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom["name"], {}).get("dram_bytes_per_launch_256")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(n)
+
+    if rank == 0:
+        value = world * 1000.0 / ms32
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 passes, fp64 state", "data": "synthetic (seeded random fields)",
+            "config": config_dict(n, world),
+            "plain_fp64": {"value": world * 1000.0 / ms64, "unit": "steps/s", "ms_per_step": ms64,
+                           "bytes_per_step": bytes_step64,
+                           "step_hbm_frac": bytes_step64 / (ms64 * 1e-3) / 1e9 / peak},
+            "fp32_vs_fp64_rel_l2": rel, "fp32_vs_fp64_after_steps": args.warmup + args.steps,
+            "sim_time": t32[0], "last_dt": t32[1],
+            "mmode_steps_per_s": value * n ** 3 / 1e6,
+            "step_bytes": bytes_step, "step_hbm_frac": bytes_step / (ms32 * 1e-3) / 1e9 / peak,
+            "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": dom["gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": dom["gbs"] / peak, "traffic": traffic,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                         "algorithmic_bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]},
+            "passes": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in pz.items()} for pz in prof],
+            "clocks": clocks,
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s",
+                    "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": state_bytes / args.steps + 128,
+                    "what": "C ABI with host pinned buffers: state H2D at start, per-step spk_advance + "
+                            "spk_budgets read-back (128 B), state D2H at end"},
+            "gpu_launches": kps * args.steps,
+            "kernels_per_step": kps,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -11,7 +11,8 @@
  *
  * Every entry point returns an int status (SPK_OK == 0).  A context is not
  * thread safe; all of its GPU work is issued on the one CUDA stream given at
- * creation (NULL = the legacy default stream).  No entry point allocates
+ * creation (NULL: the context creates its own non-blocking stream, since a
+ * CUDA graph cannot be captured on the legacy default stream).  No entry point allocates
  * device memory after spk_ctx_create, and spk_advance issues no host
  * synchronisation.
  *
@@ -97,14 +98,16 @@ typedef struct spk_ctx spk_ctx;
 
 /* Create a context: validates the modules (checkParameters), builds the
  * wavevector tables and the FFT twiddles, allocates every device buffer.
- * cuda_stream: a cudaStream_t (NULL = default stream). */
+ * cuda_stream: a cudaStream_t (NULL: a stream owned by the context). */
 int spk_ctx_create(const spk_params_t* p, void* cuda_stream, spk_ctx** out);
 int spk_ctx_destroy(spk_ctx* ctx);
 
 /* Number of fields F and complex modes Nc = NX*NY*(NZ/2+1) per field. */
 int spk_sizes(const spk_ctx* ctx, int* num_fields, size_t* n_complex);
 
-/* where: 0 = device pointer, 1 = host pointer (copied through pinned staging). */
+/* where: 0 = device pointer, 1 = host pointer (one cudaMemcpyAsync; pinned
+ * host memory gives full PCIe/C2C bandwidth).  Work queued earlier on other
+ * streams that produced a device U must be complete before the call. */
 int spk_set_state(spk_ctx* ctx, const double* U, int where);
 int spk_get_state(spk_ctx* ctx, double* U, int where);
 
@@ -144,6 +147,26 @@ typedef struct spk_budgets {
     double dissipation[8];   /* per field: <|grad q|^2> (k^2-weighted)     */
 } spk_budgets_t;
 int spk_budgets(spk_ctx* ctx, spk_budgets_t* out);
+
+/* Launch accounting of one recorded main-loop step: kernels launched per
+ * step (RKL stages counted at their recorded bound) and the algorithmic HBM
+ * bytes of one RK3 step of this pass design (every array a pass must touch,
+ * read once and written once; dealiased regions excluded).  No reference
+ * counterpart: it reports on the B200 pipeline. */
+int spk_step_info(spk_ctx* ctx, int* kernels_per_step, double* bytes_per_step);
+
+/* Per-pass timing of one RK3 stage: each pass of stage 2 (no cleaning, no
+ * dt reduction) is launched `reps` times between CUDA events on the context
+ * stream.  out[i]: pass name, average ms per launch, algorithmic bytes per
+ * launch.  The passes update the context state (stage-2 RK updates), so call
+ * it on a context whose state may change.  No reference counterpart. */
+typedef struct spk_pass_stat {
+    char   name[24];
+    double ms;
+    double bytes;
+    int    launches_per_step;
+} spk_pass_stat_t;
+int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out, int* n_out);
 
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */

@@ -1,0 +1,1074 @@
+// spk_api.cu -- context, pipelines and the C ABI of include/spooky_b200.h.
+//
+// Reference = LorenzoLMP/spooky-git.  The host logic mirrors
+// Supervisor/Fields/TimeStepping/RKLegendre; every step is recorded once
+// into a CUDA graph (two graphs when RKL2 alternates before/after RK3) and
+// replayed without host synchronisation.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/spooky_b200.h"
+#include "spk_kernels.cuh"
+
+#include "spk_kernels.cu"
+
+using namespace spk;
+
+static std::string g_create_error;
+
+#define EPT_AXIS_F 16
+#define EPT_AXIS_D 8
+#define EPT_Z_F 16
+#define EPT_Z_D 8
+#define MAXT 256
+
+struct spk_ctx {
+    spk_params_t p;
+    cudaStream_t stream;
+    bool own_stream;
+    bool fp32;
+    int F, VX, VY, VZ, BX, BY, BZ, TH, VEL, MAG;
+    int nx, ny, nz, nzh;
+    size_t nc, nr;
+    std::vector<double> kx, ky, kz, mx, my, mz;
+    double kxmax, kymax, kzmax, kmax;
+    int kz_keep;
+    unsigned sts_mask;
+    int nsts, sts_fields[8], sts_kind[8];
+    bool sts_aniso, sts_iso, aniso_rhs;
+    int rkl_smax;
+    // device memory
+    double* d_tab;                 // kx ky kz mx my mz
+    void* d_tw;                    // twiddles x, y, z in pass precision
+    FftPlan plan_x, plan_y, plan_z;
+    double2 *U, *S;
+    void *bufA, *bufB;
+    int nbuf_ch;
+    void *rA, *rB, *breal;
+    double2 *Uc0, *Uc1, *dU0;
+    DevScalars* sc;
+    DevScalars* h_sc;              // pinned mirror
+    double* d_sums;
+    double* h_sums;
+    DevGrid g;
+    // pipeline layout
+    int nin, nout, ch_u, ch_b, ch_th, ch_gx, ch_gy;
+    int out_T, out_E, out_F, out_Q;
+    // graphs
+    cudaGraphExec_t gexec[2];
+    bool have_graph[2];
+    int h_step;
+    std::string err;
+    int sticky;
+    long launches;                 // kernels issued (counted by the launch helpers)
+    bool bad_job;                  // a pass was built with an out-of-range channel
+    const void* user_U;            // caller's state array during spk_compute_dfield
+    int kernels_per_step[2];
+};
+
+static int fail(spk_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg; else g_create_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            return fail(c, SPK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// buffer addressing
+// ---------------------------------------------------------------------------
+static size_t csize(const spk_ctx* c) { return c->fp32 ? sizeof(float2) : sizeof(double2); }
+// Channel ch of a pass buffer; channels outside the buffer abort the launch
+// (add_job / zpass refuse null pointers) instead of addressing other memory.
+static void* chan(const spk_ctx* c, void* base, int ch) {
+    const int nch = (base == c->rA || base == c->rB) ? 3 : c->nbuf_ch;
+    if (!base || ch < 0 || ch >= nch) return nullptr;
+    return (char*)base + (size_t)ch * c->nc * csize(c);
+}
+
+static AxisArgs axis_args(spk_ctx* c, int ax) {
+    AxisArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->g;
+    a.plan = ax == 0 ? c->plan_x : c->plan_y;
+    a.axis = ax;
+    a.kcols = c->nzh;
+    a.cs_in = a.cs_out = c->nc;
+    a.scale = 1.0;
+    return a;
+}
+
+// True when [p, p + nch channels) lies inside one of the context's arrays.
+static bool span_ok(const spk_ctx* c, const void* p, int nch, bool state) {
+    if (!p || nch < 1) return false;
+    const char* q = (const char*)p;
+    const size_t cb = state ? c->nc * sizeof(double2) : c->nc * csize(c);
+    const size_t need = (size_t)nch * cb;
+    auto inside = [&](const void* base, size_t bytes) {
+        const char* b = (const char*)base;
+        return b && q >= b && q + need <= b + bytes;
+    };
+    if (state) return inside(c->U, (size_t)c->F * c->nc * sizeof(double2)) ||
+                      inside(c->user_U, (size_t)c->F * c->nc * sizeof(double2));
+    return inside(c->bufA, (size_t)c->nbuf_ch * cb) || inside(c->bufB, (size_t)c->nbuf_ch * cb) ||
+           inside(c->rA, 3 * cb) || inside(c->rB, 3 * cb);
+}
+
+
+// ---------------------------------------------------------------------------
+// FFT plans: radices from {16 (FP32 only), 8, 4, 2, 3, 5}; twiddles in long double.
+// ---------------------------------------------------------------------------
+static bool make_plan(int n, int maxr, FftPlan* pl) {
+    pl->n = n;
+    pl->nst = 0;
+    int r = n;
+    const int cands[] = {16, 8, 4, 2, 3, 5};
+    for (int cnd : cands) {
+        if (cnd > maxr) continue;
+        while (r % cnd == 0 && pl->nst < 12) { pl->radix[pl->nst++] = cnd; r /= cnd; }
+    }
+    return r == 1;
+}
+
+static void twiddles(int n, std::vector<double>& out) {
+    const long double PI = 3.141592653589793238462643383279502884L;
+    out.resize(2 * (size_t)n);
+    for (int k = 0; k < n; k++) {
+        long double a = 2.0L * PI * (long double)k / (long double)n;
+        out[2 * k] = (double)cosl(a);
+        out[2 * k + 1] = -(double)sinl(a);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static inline int rup32(long x) { return (int)(((x + 31) / 32) * 32); }
+
+struct AxisCfg { int kt; int nthr; size_t smem; };
+
+static AxisCfg axis_cfg(const spk_ctx* c, int N) {
+    AxisCfg a;
+    const int ept = c->fp32 ? EPT_AXIS_F : EPT_AXIS_D;
+    int kt = c->fp32 ? 16 : 8;
+    while (kt > 1 && (long)N * kt > (long)MAXT * ept) kt /= 2;
+    kt = std::min(kt, c->nzh);
+    a.kt = kt;
+    a.nthr = std::max(32, std::min(MAXT, rup32(((long)N * kt + ept - 1) / ept)));
+    a.smem = (size_t)N * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
+    return a;
+}
+
+static AxisCfg xfwd_cfg(const spk_ctx* c) {
+    AxisCfg a;
+    const int ept = c->fp32 ? 8 : 4;
+    int kt = c->fp32 ? 16 : 8;
+    while (kt > 1 && (long)c->nx * kt > (long)MAXT * ept) kt /= 2;
+    kt = std::min(kt, c->nzh);
+    a.kt = kt;
+    a.nthr = std::max(32, std::min(MAXT, rup32(((long)c->nx * kt + ept - 1) / ept)));
+    a.smem = (size_t)c->nx * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
+    return a;
+}
+
+struct ZCfg { int lines; int nthr; size_t smem; };
+
+static ZCfg z_cfg(const spk_ctx* c, int nin_all, int nout) {
+    ZCfg z;
+    const int npin = (nin_all + 1) / 2, npout = (nout + 1) / 2;
+    const int maxp = std::max(npin, std::max(npout, 1));
+    const size_t csz = c->fp32 ? sizeof(float2) : sizeof(double2);
+    const size_t per_line = (size_t)(npin + npout) * c->nz * csz;
+    int L = (int)std::max<size_t>(1, 65536 / std::max<size_t>(per_line, 1));
+    L = std::min(L, 64);
+    const int ept = c->fp32 ? EPT_Z_F : EPT_Z_D;
+    L = std::min(L, std::max(1, MAXT * ept / (maxp * c->nz)));
+    L = std::min<long>(L, (long)c->nx * c->ny);
+    z.lines = L;
+    z.nthr = std::max(32, std::min(MAXT, rup32(((long)L * maxp * c->nz + ept - 1) / ept)));
+    // input pairs, output pairs, then 6 x 32 values of block-max scratch
+    z.smem = (size_t)L * (npin + npout) * c->nz * csz + 6 * 32 * (c->fp32 ? sizeof(float) : sizeof(double));
+    return z;
+}
+
+template <typename T>
+static void launch_axis(spk_ctx* c, AxisArgs& a, int dir, int outer) {
+    const AxisCfg cf = axis_cfg(c, a.plan.n);
+    a.kt = cf.kt;
+    dim3 grid((a.kcols + cf.kt - 1) / cf.kt, outer, a.njobs);
+    constexpr int ept = sizeof(T) == 4 ? EPT_AXIS_F : EPT_AXIS_D;
+    c->launches++;
+    if (dir > 0) k_axis<T, +1, ept><<<grid, cf.nthr, cf.smem, c->stream>>>(a);
+    else k_axis<T, -1, ept><<<grid, cf.nthr, cf.smem, c->stream>>>(a);
+}
+
+static void axis(spk_ctx* c, AxisArgs& a, int dir) {
+    if (c->bad_job) { c->err = "internal: a pass job addressed a channel outside its buffer"; c->sticky = SPK_ERR_ARG; return; }
+    if (a.njobs == 0) return;
+    const int outer = a.axis == 0 ? c->ny : c->nx;
+    if (c->fp32) launch_axis<float>(c, a, dir, outer);
+    else launch_axis<double>(c, a, dir, outer);
+}
+
+static void zpass(spk_ctx* c, ZArgs& z) {
+    if (!span_ok(c, z.in, std::max(z.nin, 1), false) || (z.nout > 0 && !span_ok(c, z.out, z.nout, false)) ||
+        ((z.store_breal || z.load_breal) && !c->breal)) {
+        c->err = "internal: a z pass addressed channels outside its buffers";
+        c->sticky = SPK_ERR_ARG;
+        return;
+    }
+    const int nin_all = z.nin + (z.derive_gz == 1 ? 1 : 0);
+    const ZCfg cf = z_cfg(c, nin_all, z.nout);
+    z.lines = cf.lines;
+    const int nblk = (int)(((size_t)c->nx * c->ny + cf.lines - 1) / cf.lines);
+    c->launches++;
+    if (c->fp32) k_zpass<float, EPT_Z_F><<<nblk, cf.nthr, cf.smem, c->stream>>>(z);
+    else k_zpass<double, EPT_Z_D><<<nblk, cf.nthr, cf.smem, c->stream>>>(z);
+}
+
+static void xfwd(spk_ctx* c, XfArgs& x) {
+    const AxisCfg cf = xfwd_cfg(c);
+    x.kt = cf.kt;
+    dim3 grid((c->nzh + cf.kt - 1) / cf.kt, c->ny);
+    c->launches++;
+    if (c->fp32) k_xfwd<float, 8><<<grid, cf.nthr, cf.smem, c->stream>>>(x);
+    else k_xfwd<double, 4><<<grid, cf.nthr, cf.smem, c->stream>>>(x);
+}
+
+static int ew_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+// ---------------------------------------------------------------------------
+// argument builders
+// ---------------------------------------------------------------------------
+static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch, int in_state, int deriv, int clean) {
+    if (!span_ok(c, in, nch, in_state != 0) || !span_ok(c, out, nch, false) || a.njobs >= SPK_MAXJOBS) {
+        c->bad_job = true;
+        return;
+    }
+    AxisJob& j = a.job[a.njobs++];
+    j.in = in; j.out = out; j.nch = nch; j.in_state = in_state; j.deriv = deriv; j.clean = clean;
+}
+
+// first inverse pass over the state: fields in order, cleaning u and B when asked
+static void pass_x_inverse(spk_ctx* c, const double2* U, bool clean, bool with_gx) {
+    AxisArgs a = axis_args(c, 0);
+    a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);   // scaleKernel factor
+    if (c->p.incompressible) add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_u), 3, 1, 0, clean ? 1 : 0);
+    if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, clean ? 1 : 0);
+    if (c->p.boussinesq) {
+        add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_th), 1, 1, 0, 0);
+        if (with_gx && c->aniso_rhs) add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_gx), 1, 1, 1, 0);
+    }
+    axis(c, a, +1);
+}
+
+static void pass_y_inverse(spk_ctx* c, bool with_g) {
+    AxisArgs a = axis_args(c, 1);
+    const int n = with_g ? c->nin : (c->nin - (c->aniso_rhs ? 2 : 0));
+    // channels 0..n-1 one to one (gx included when present)
+    add_job(c, a, c->bufA, c->bufB, with_g ? (c->aniso_rhs ? c->ch_gx + 1 : n) : n, 0, 0, 0);
+    if (with_g && c->aniso_rhs) add_job(c, a, chan(c, c->bufA, c->ch_th), chan(c, c->bufB, c->ch_gy), 1, 0, 1, 0);
+    axis(c, a, +1);
+}
+
+static ZArgs z_args(spk_ctx* c) {
+    ZArgs z;
+    memset(&z, 0, sizeof(z));
+    z.g = c->g;
+    z.plan = c->plan_z;
+    z.in = c->bufB; z.cs_in = c->nc;
+    z.out = c->bufA; z.cs_out = c->nc;
+    z.ch_u = z.ch_b = z.ch_th = z.ch_gx = z.ch_gy = -1;
+    z.maxbits = c->sc->maxbits;
+    z.nonfinite = &c->sc->nonfinite;
+    z.breal = c->breal;
+    z.sd = c->p.strat_direction;
+    z.chi = 1.0 / c->p.reynolds_ani;
+    z.omegaT2 = c->p.OmegaT2;
+    return z;
+}
+
+static void set_inputs(spk_ctx* c, ZArgs& z, bool with_g) {
+    z.nin = with_g ? c->nin : c->nin - (c->aniso_rhs ? 2 : 0);
+    z.ch_u = c->ch_u; z.ch_b = c->ch_b; z.ch_th = c->ch_th;
+    if (with_g && c->aniso_rhs) { z.ch_gx = c->ch_gx; z.ch_gy = c->ch_gy; z.derive_gz = 1; }
+}
+
+static void pass_z_products(spk_ctx* c, bool do_max) {
+    ZArgs z = z_args(c);
+    z.mode = ZM_PRODUCTS;
+    set_inputs(c, z, true);
+    z.nout = c->nout;
+    z.hydro = 1;
+    z.mhd = c->p.mhd; z.bous = c->p.boussinesq; z.aniso = c->aniso_rhs ? 1 : 0;
+    z.do_max = do_max ? 1 : 0;
+    zpass(c, z);
+}
+
+static void pass_z_inverse_only(spk_ctx* c, bool do_max, bool store_b) {
+    ZArgs z = z_args(c);
+    z.mode = ZM_INVERSE_ONLY;
+    set_inputs(c, z, false);
+    z.nout = 0;
+    z.do_max = do_max ? 1 : 0;
+    z.store_breal = store_b ? 1 : 0;
+    zpass(c, z);
+}
+
+static void pass_y_forward(spk_ctx* c, int nch, void* in, void* out) {
+    AxisArgs a = axis_args(c, 1);
+    a.kcols = c->kz_keep;
+    a.row_filter = 1;
+    add_job(c, a, in, out, nch, 0, 0, 0);
+    if (a.kcols > 0) axis(c, a, -1);
+}
+
+static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
+    XfArgs x;
+    memset(&x, 0, sizeof(x));
+    x.g = c->g;
+    x.plan = c->plan_x;
+    x.nl = c->bufB; x.cs_nl = c->nc;
+    x.nl_T = c->out_T; x.nl_E = c->out_E; x.nl_F = c->out_F; x.nl_Q = c->out_Q;
+    x.U = U; x.S = c->S; x.out = nullptr;
+    x.F = c->F; x.VEL = c->VEL; x.MAG = c->MAG; x.TH = c->TH;
+    x.incompressible = c->p.incompressible; x.mhd = c->p.mhd; x.bous = c->p.boussinesq;
+    x.heat = c->p.heat_equation; x.strat = c->p.stratification; x.sd = c->p.strat_direction;
+    x.aniso_rhs = c->aniso_rhs ? 1 : 0;
+    x.sts_mask = c->sts_mask;
+    x.nu = c->p.nu; x.nu_m = c->p.nu_m; x.nu_th = c->p.nu_th; x.N2 = c->p.N2;
+    x.mode = mode; x.clean = clean ? 1 : 0;
+    x.sc = c->sc;
+    return x;
+}
+
+static DtArgs dt_args(spk_ctx* c, bool advance) {
+    DtArgs d;
+    memset(&d, 0, sizeof(d));
+    const spk_params_t& p = c->p;
+    d.incompressible = p.incompressible; d.heat = p.heat_equation; d.mhd = p.mhd; d.bous = p.boussinesq;
+    d.aniso = p.anisotropic_diffusion; d.sts = p.supertimestepping && c->nsts > 0; d.with_fixed = p.fixed_dt > 0.0;
+    d.kxmax = c->kxmax; d.kymax = c->kymax; d.kzmax = c->kzmax;
+    d.nu = p.nu; d.nu_m = p.nu_m; d.nu_th = p.nu_th; d.reynolds_ani = p.reynolds_ani; d.N2 = p.N2; d.OmegaT2 = p.OmegaT2;
+    d.cfl = p.cfl; d.cfl_par = p.cfl_par; d.cfl_sts = p.cfl_sts; d.safety_source = p.safety_source; d.safety_sts = p.safety_sts;
+    d.t_final = p.t_final; d.toutput_flow = p.toutput_flow; d.fixed_dt = p.fixed_dt;
+    d.sts_pos_mask = c->sts_mask;
+    d.VX = c->VX; d.VY = c->VY; d.VZ = c->VZ; d.BX = c->BX; d.BY = c->BY; d.BZ = c->BZ; d.TH = c->TH;
+    d.advance = advance ? 1 : 0;
+    d.rkl_smax = c->rkl_smax;
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// RKL2 cycle (RKLegendre::compute_cycle_RKL2, rkl.cu:437-591); stages beyond
+// the device-computed count exit immediately.
+// ---------------------------------------------------------------------------
+static RklArgs rkl_args(spk_ctx* c, int stage) {
+    RklArgs r;
+    memset(&r, 0, sizeof(r));
+    r.g = c->g;
+    r.plan = c->plan_x;
+    r.nl = c->rB; r.cs_nl = c->nc;
+    r.Uc0 = c->Uc0; r.Uc1 = c->Uc1; r.dU0 = c->dU0;
+    r.stage = stage;
+    r.nsts = c->nsts;
+    for (int v = 0; v < c->nsts; v++) { r.fields[v] = c->sts_fields[v]; r.kind[v] = c->sts_kind[v]; }
+    r.nu = c->p.nu; r.nu_m = c->p.nu_m; r.nu_th = c->p.nu_th;
+    r.sc = c->sc;
+    return r;
+}
+
+static void record_rkl_cycle(spk_ctx* c) {
+    for (int st = 1; st <= c->rkl_smax; st++) {
+        if (c->sts_iso) {
+            RklArgs r = rkl_args(c, st);
+            c->launches++;
+            k_rkl_spectral<<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U);
+        }
+        if (c->sts_aniso) {
+            // theta and i*kx*theta, x inverse
+            AxisArgs a = axis_args(c, 0);
+            a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);
+            a.gate = c->sc; a.gate_stage = st;
+            add_job(c, a, c->U + (size_t)c->TH * c->nc, chan(c, c->rA, 0), 1, 1, 0, 0);
+            add_job(c, a, c->U + (size_t)c->TH * c->nc, chan(c, c->rA, 1), 1, 1, 1, 0);
+            axis(c, a, +1);
+            // y inverse: theta (for i*kz theta), i*ky theta, i*kx theta
+            AxisArgs b = axis_args(c, 1);
+            b.gate = c->sc; b.gate_stage = st;
+            add_job(c, b, chan(c, c->rA, 0), chan(c, c->rB, 0), 1, 0, 0, 0);
+            add_job(c, b, chan(c, c->rA, 0), chan(c, c->rB, 1), 1, 0, 1, 0);
+            add_job(c, b, chan(c, c->rA, 1), chan(c, c->rB, 2), 1, 0, 0, 0);
+            axis(c, b, +1);
+            // z: gradient, real B, heat flux, R2C
+            ZArgs z = z_args(c);
+            z.gate = c->sc; z.gate_stage = st;
+            z.mode = ZM_RKL_FLUX;
+            z.in = c->rB; z.out = c->rA;
+            z.nin = 3; z.ch_th = 0; z.ch_gy = 1; z.ch_gx = 2; z.derive_gz = 2;
+            z.load_breal = 1; z.aniso = 1; z.nout = 3;
+            zpass(c, z);
+            AxisArgs f = axis_args(c, 1);
+            f.gate = c->sc; f.gate_stage = st;
+            f.kcols = c->kz_keep; f.row_filter = 1;
+            add_job(c, f, c->rA, c->rB, 3, 0, 0, 0);
+            if (f.kcols > 0) axis(c, f, -1);
+            RklArgs r = rkl_args(c, st);
+            const AxisCfg cf = xfwd_cfg(c);
+            r.kt = cf.kt;
+            dim3 grid((c->nzh + cf.kt - 1) / cf.kt, c->ny);
+            int vslot = 0;
+            for (int v = 0; v < c->nsts; v++) if (c->sts_kind[v] == 3) vslot = v;
+            c->launches++;
+            if (c->fp32) k_xfwd_rkl<float, 8><<<grid, cf.nthr, cf.smem, c->stream>>>(r, c->U, vslot);
+            else k_xfwd_rkl<double, 4><<<grid, cf.nthr, cf.smem, c->stream>>>(r, c->U, vslot);
+        }
+    }
+}
+
+// real-space B of the current state for the anisotropic STS flux
+static void record_breal(spk_ctx* c) {
+    AxisArgs a = axis_args(c, 0);
+    a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);
+    add_job(c, a, c->U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, 0);
+    axis(c, a, +1);
+    AxisArgs b = axis_args(c, 1);
+    add_job(c, b, chan(c, c->bufA, c->ch_b), chan(c, c->bufB, c->ch_b), 3, 0, 0, 0);
+    axis(c, b, +1);
+    ZArgs z = z_args(c);
+    z.mode = ZM_INVERSE_ONLY;
+    z.nin = c->ch_b + 3;   // channels before B are unused zeros of the pair layout
+    z.ch_b = c->ch_b;
+    z.store_breal = 1;
+    zpass(c, z);
+}
+
+// ---------------------------------------------------------------------------
+// one main-loop iteration (CleanFieldDivergence + HydroMHDAdvance)
+// ---------------------------------------------------------------------------
+static void record_step(spk_ctx* c, int parity) {
+    const spk_params_t& p = c->p;
+    const bool sts = p.supertimestepping && c->nsts > 0;
+    const bool sts_before = sts && !p.sts_every_step && parity == 1;
+    const bool sts_after = sts && (p.sts_every_step || parity == 0);
+    const bool euler = p.integrator == SPK_INT_EULER;
+    const int nst = euler ? 1 : 3;
+    if (p.heat_equation) {
+        DtArgs d = dt_args(c, true);
+        k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+        c->launches++;
+        if (sts_before) record_rkl_cycle(c);
+        for (int s = 0; s < nst; s++) {
+            XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, false);
+            k_heat<<<ew_blocks(c->nc), 256, 0, c->stream>>>(x);
+            c->launches++;
+        }
+        if (sts_after) record_rkl_cycle(c);
+        return;
+    }
+    k_reset_max<<<1, 32, 0, c->stream>>>(c->sc);
+    c->launches++;
+    for (int s = 0; s < nst; s++) {
+        const bool first = s == 0;
+        pass_x_inverse(c, c->U, first, true);
+        pass_y_inverse(c, true);
+        if (first) {
+            if (sts_before) {
+                pass_z_inverse_only(c, true, c->sts_aniso);
+                DtArgs d = dt_args(c, true);
+                k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+                c->launches++;
+                record_rkl_cycle(c);
+                pass_z_products(c, false);
+            } else {
+                pass_z_products(c, true);
+                DtArgs d = dt_args(c, true);
+                k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+                c->launches++;
+            }
+        } else {
+            pass_z_products(c, false);
+        }
+        pass_y_forward(c, c->nout, c->bufA, c->bufB);
+        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, first);
+        xfwd(c, x);
+    }
+    if (sts_after) {
+        if (c->sts_aniso) record_breal(c);
+        record_rkl_cycle(c);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// context creation
+// ---------------------------------------------------------------------------
+extern "C" void spk_params_default(spk_params_t* p) {
+    memset(p, 0, sizeof(*p));
+    p->nx = p->ny = p->nz = 32;
+    p->lx = p->ly = p->lz = 1.0;
+    p->strat_direction = 2;
+    p->sts_algorithm = SPK_STS_RKL2;
+    p->antialiasing = 1;
+    p->nu = p->nu_m = p->nu_th = 1.0;
+    p->reynolds_ani = 1.0;
+    p->cfl = 1.5; p->cfl_par = 1.0; p->cfl_sts = 1.0; p->safety_source = 0.2;
+    p->safety_sts = 1;
+    p->t_initial = 0.0; p->t_final = 1.0; p->toutput_flow = 1.0;
+    p->integrator = SPK_INT_RK3;
+    p->form = SPK_FORM_PLAIN;
+}
+
+static int check_params(const spk_params_t* p, std::string& why) {
+    // Parameters::checkParameters (parameters.cu:511-566)
+    if (p->incompressible && p->heat_equation) { why = "incompressible and heat_equation modules are mutually exclusive"; return SPK_ERR_CONFIG; }
+    if (!p->incompressible && !p->heat_equation) { why = "choose either the incompressible or the heat_equation module"; return SPK_ERR_CONFIG; }
+    if (p->boussinesq && !p->incompressible) { why = "Boussinesq requires incompressible module"; return SPK_ERR_CONFIG; }
+    if (p->stratification && !p->boussinesq) { why = "stratification requires Boussinesq module"; return SPK_ERR_CONFIG; }
+    if (p->mhd && !p->incompressible) { why = "mhd requires incompressible module"; return SPK_ERR_CONFIG; }
+    if (p->anisotropic_diffusion && !(p->mhd && p->boussinesq)) { why = "anisotropic_diffusion requires mhd and boussinesq module"; return SPK_ERR_CONFIG; }
+    if (p->nx < 2 || p->ny < 2 || p->nz < 2) { why = "grid sizes must be >= 2"; return SPK_ERR_ARG; }
+    if (p->nz % 2) { why = "NZ must be even"; return SPK_ERR_UNSUPPORTED; }
+    if (p->nx > 1024 || p->ny > 1024 || p->nz > 1024) { why = "axis lengths above 1024 are not supported"; return SPK_ERR_UNSUPPORTED; }
+    if (p->supertimestepping && p->sts_algorithm != SPK_STS_RKL2) { why = "only the rkl2 super-time-stepping algorithm is implemented"; return SPK_ERR_UNSUPPORTED; }
+    if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
+    if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
+    return SPK_OK;
+}
+
+static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
+    c->p = *pin;
+    const spk_params_t& p = c->p;
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    if (!c->stream) {
+        // graph capture needs a non-legacy stream: create one
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(nullptr, SPK_ERR_CUDA, "cudaStreamCreateWithFlags failed");
+        c->own_stream = true;
+    }
+    c->fp32 = p.form == SPK_FORM_FP32;
+    // Parameters::popVariablesGrid (parameters.cu:568-654)
+    c->F = 0; c->VX = c->VY = c->VZ = c->BX = c->BY = c->BZ = c->TH = c->VEL = c->MAG = 0;
+    if (p.heat_equation) { c->TH = 0; c->F = 1; }
+    else {
+        c->VX = 0; c->VY = 1; c->VZ = 2; c->F = 3;
+        if (p.mhd) { c->BX = 3; c->BY = 4; c->BZ = 5; c->MAG = 3; c->F += 3; if (p.boussinesq) { c->TH = 6; c->F += 1; } }
+        else if (p.boussinesq) { c->TH = 3; c->F += 1; }
+    }
+    c->nx = p.nx; c->ny = p.ny; c->nz = p.nz; c->nzh = p.nz / 2 + 1;
+    c->nc = (size_t)c->nx * c->ny * c->nzh;
+    c->nr = (size_t)c->nx * c->ny * c->nz;
+    // Wavevector::Wavevector (wavevector.cu:50-112): host FP64, exact expressions
+    c->kx.resize(c->nx); c->ky.resize(c->ny); c->kz.resize(c->nzh);
+    c->mx.assign(c->nx, 1.0); c->my.assign(c->ny, 1.0); c->mz.assign(c->nzh, 1.0);
+    volatile double twopi = 2.0 * M_PI;
+    for (int i = 0; i < c->nx; i++) c->kx[i] = twopi / p.lx * (fmod((double)i + ((double)c->nx / 2), c->nx) - (double)c->nx / 2);
+    for (int j = 0; j < c->ny; j++) c->ky[j] = twopi / p.ly * (fmod((double)j + ((double)c->ny / 2), c->ny) - (double)c->ny / 2);
+    for (int k = 0; k < c->nzh; k++) c->kz[k] = p.with2d ? 0.0 : twopi / p.lz * (double)k;
+    c->kxmax = 2.0 * M_PI / p.lx * ((c->nx / 2) - 1);
+    c->kymax = 2.0 * M_PI / p.ly * ((c->ny / 2) - 1);
+    c->kzmax = 2.0 * M_PI / p.lz * ((c->nz / 2) - 1);
+    if (p.with2d) c->kzmax = 0.0;
+    if (p.antialiasing) {
+        volatile double two3 = 2.0 / 3.0;
+        const double tx = two3 * c->kxmax, ty = two3 * c->kymax, tz = two3 * c->kzmax;
+        for (int i = 0; i < c->nx; i++) if (fabs(c->kx[i]) > tx) c->mx[i] = 0.0;
+        for (int j = 0; j < c->ny; j++) if (fabs(c->ky[j]) > ty) c->my[j] = 0.0;
+        for (int k = 0; k < c->nzh; k++) if (fabs(c->kz[k]) > tz) c->mz[k] = 0.0;
+        c->kxmax = (2.0 / 3.0) * c->kxmax;
+        c->kymax = (2.0 / 3.0) * c->kymax;
+        c->kzmax = (2.0 / 3.0) * c->kzmax;
+    }
+    c->kmax = pow(c->kxmax * c->kxmax + c->kymax * c->kymax + c->kzmax * c->kzmax, 0.5);
+    c->kz_keep = 0;
+    while (c->kz_keep < c->nzh && c->mz[c->kz_keep] != 0.0) c->kz_keep++;
+    for (int k = c->kz_keep; k < c->nzh; k++)
+        if (c->mz[k] != 0.0) return fail(nullptr, SPK_ERR_UNSUPPORTED, "kz mask is not a prefix");
+
+    // STS variables (RKLegendre ctor, rkl.cu:40-58)
+    c->sts_mask = 0; c->nsts = 0; c->sts_aniso = c->sts_iso = false;
+    if (p.supertimestepping) {
+        for (int f = 0; f < c->F; f++) {
+            if ((p.sts_vars_mask >> f) & 1u) {
+                c->sts_mask |= 1u << f;
+                int kind;
+                if (p.heat_equation || (p.boussinesq && f == c->TH)) kind = (p.anisotropic_diffusion ? 3 : 2);
+                else if (p.mhd && f >= c->MAG && f < c->MAG + 3) kind = 1;
+                else kind = 0;
+                c->sts_fields[c->nsts] = f;
+                c->sts_kind[c->nsts] = kind;
+                c->nsts++;
+                if (kind == 3) c->sts_aniso = true; else c->sts_iso = true;
+            }
+        }
+        if (c->sts_aniso && p.mhd && (c->sts_mask >> c->MAG & 7u))
+            return fail(nullptr, SPK_ERR_UNSUPPORTED, "super-time-stepping of B together with anisotropic conduction is not supported");
+    }
+    c->aniso_rhs = p.anisotropic_diffusion && p.boussinesq && !((c->sts_mask >> c->TH) & 1u);
+    // RKL2 stage bound
+    c->rkl_smax = 0;
+    if (c->nsts > 0) {
+        double r;
+        if (p.heat_equation) {
+            const double gam = (c->kxmax * c->kxmax + c->kymax * c->kymax + c->kzmax * c->kzmax) * p.nu_th;
+            const double dts = p.cfl_par / gam;
+            double dtm = p.fixed_dt > 0.0 ? p.fixed_dt : p.t_final - p.t_initial;
+            r = std::max(1.0, dtm / dts);
+        } else {
+            r = std::max(1.0, (double)p.safety_sts);
+        }
+        const double s_str = 4.0 * (1.0 + 2.0 * r) / (1.0 + sqrt(9.0 + 16.0 * r));
+        c->rkl_smax = std::min(SPK_RKL_MAX - 1, 2 + (int)s_str);
+    }
+
+    // channel layout of the main pipeline
+    int ch = 0;
+    c->ch_u = c->ch_b = c->ch_th = c->ch_gx = c->ch_gy = -1;
+    if (p.incompressible) { c->ch_u = ch; ch += 3; }
+    if (p.mhd) { c->ch_b = ch; ch += 3; }
+    if (p.boussinesq) { c->ch_th = ch; ch += 1; }
+    if (c->aniso_rhs) { c->ch_gx = ch; c->ch_gy = ch + 1; ch += 2; }
+    c->nin = ch;
+    int oc = 0;
+    c->out_T = c->out_E = c->out_F = c->out_Q = -1;
+    if (p.incompressible) { c->out_T = oc; oc += 5; }
+    if (p.mhd) { c->out_E = oc; oc += 3; }
+    if (p.boussinesq) { c->out_F = oc; oc += 3; }
+    if (c->aniso_rhs) { c->out_Q = oc; oc += 3; }
+    c->nout = oc;
+    c->nbuf_ch = std::max(std::max(c->nin + 1, c->nout), 3);
+
+    // FFT plans (lengths the device decomposition covers)
+    const int rf = c->fp32 ? 16 : 8;
+    if (!fft_supported(c->nx, rf) || !fft_supported(c->ny, rf) || !fft_supported(c->nz, rf))
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be (16 or 8)^k times {1,2,4,8} x {1,3,9} x {1,5}");
+    make_plan(c->nx, 16, &c->plan_x);
+    make_plan(c->ny, 16, &c->plan_y);
+    make_plan(c->nz, 16, &c->plan_z);
+    return SPK_OK;
+}
+
+static int ctx_alloc(spk_ctx* c) {
+    const size_t nc = c->nc;
+    const size_t cs = csize(c);
+    // tables
+    CK(cudaMalloc(&c->d_tab, sizeof(double) * (2 * ((size_t)c->nx + c->ny + c->nzh))));
+    double* t = c->d_tab;
+    CK(cudaMemcpy(t, c->kx.data(), sizeof(double) * c->nx, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t + c->nx, c->ky.data(), sizeof(double) * c->ny, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t + c->nx + c->ny, c->kz.data(), sizeof(double) * c->nzh, cudaMemcpyHostToDevice));
+    double* m = t + c->nx + c->ny + c->nzh;
+    CK(cudaMemcpy(m, c->mx.data(), sizeof(double) * c->nx, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m + c->nx, c->my.data(), sizeof(double) * c->ny, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m + c->nx + c->ny, c->mz.data(), sizeof(double) * c->nzh, cudaMemcpyHostToDevice));
+    c->g.nx = c->nx; c->g.ny = c->ny; c->g.nz = c->nz; c->g.nzh = c->nzh;
+    c->g.kz_keep = c->kz_keep; c->g.nc = nc;
+    c->g.kx = t; c->g.ky = t + c->nx; c->g.kz = t + c->nx + c->ny;
+    c->g.mx = m; c->g.my = m + c->nx; c->g.mz = m + c->nx + c->ny;
+    // twiddles
+    const size_t ntw = (size_t)c->nx + c->ny + c->nz;
+    CK(cudaMalloc(&c->d_tw, cs * ntw));
+    std::vector<double> tw;
+    size_t off = 0;
+    FftPlan* pls[3] = {&c->plan_x, &c->plan_y, &c->plan_z};
+    for (int a = 0; a < 3; a++) {
+        const int n = pls[a]->n;
+        twiddles(n, tw);
+        void* dst = (char*)c->d_tw + off * cs;
+        if (c->fp32) {
+            std::vector<float> tf(tw.begin(), tw.end());
+            CK(cudaMemcpy(dst, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(dst, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice));
+        }
+        pls[a]->tw = dst;
+        off += n;
+    }
+    // state and buffers
+    CK(cudaMalloc(&c->U, sizeof(double2) * nc * c->F));
+    CK(cudaMalloc(&c->S, sizeof(double2) * nc * c->F));
+    CK(cudaMemset(c->U, 0, sizeof(double2) * nc * c->F));
+    CK(cudaMemset(c->S, 0, sizeof(double2) * nc * c->F));
+    if (c->p.incompressible) {
+        CK(cudaMalloc(&c->bufA, cs * nc * c->nbuf_ch));
+        CK(cudaMalloc(&c->bufB, cs * nc * c->nbuf_ch));
+        CK(cudaMemset(c->bufA, 0, cs * nc * c->nbuf_ch));
+        CK(cudaMemset(c->bufB, 0, cs * nc * c->nbuf_ch));
+    }
+    if (c->nsts > 0) {
+        CK(cudaMalloc(&c->Uc0, sizeof(double2) * nc * c->nsts));
+        CK(cudaMalloc(&c->Uc1, sizeof(double2) * nc * c->nsts));
+        CK(cudaMalloc(&c->dU0, sizeof(double2) * nc * c->nsts));
+        CK(cudaMemset(c->Uc0, 0, sizeof(double2) * nc * c->nsts));
+        CK(cudaMemset(c->Uc1, 0, sizeof(double2) * nc * c->nsts));
+        CK(cudaMemset(c->dU0, 0, sizeof(double2) * nc * c->nsts));
+    }
+    if (c->sts_aniso) {
+        CK(cudaMalloc(&c->rA, cs * nc * 3));
+        CK(cudaMalloc(&c->rB, cs * nc * 3));
+        CK(cudaMemset(c->rA, 0, cs * nc * 3));
+        CK(cudaMemset(c->rB, 0, cs * nc * 3));
+        CK(cudaMalloc(&c->breal, (c->fp32 ? sizeof(float) : sizeof(double)) * c->nr * 3));
+    }
+    CK(cudaMalloc(&c->sc, sizeof(DevScalars)));
+    CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
+    memset(c->h_sc, 0, sizeof(DevScalars));
+    c->h_sc->t = c->p.t_initial;
+    CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
+    CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
+    // shared-memory limits of the instantiations used
+    const int big = 200 * 1024;
+    CK(cudaFuncSetAttribute(k_zpass<float, EPT_Z_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_zpass<double, EPT_Z_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<float, 1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<float, -1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<double, 1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<double, -1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd_rkl<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd_rkl<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    return SPK_OK;
+}
+
+static void ctx_free(spk_ctx* c) {
+    for (int i = 0; i < 2; i++) if (c->have_graph[i]) cudaGraphExecDestroy(c->gexec[i]);
+    cudaFree(c->d_tab); cudaFree(c->d_tw); cudaFree(c->U); cudaFree(c->S);
+    cudaFree(c->bufA); cudaFree(c->bufB); cudaFree(c->rA); cudaFree(c->rB); cudaFree(c->breal);
+    cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
+    if (c->h_sums) cudaFreeHost(c->h_sums);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+}
+
+static int launch_status(spk_ctx* c) {
+    if (c->sticky) return c->sticky;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, SPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return SPK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int spk_ctx_create(const spk_params_t* p, void* stream, spk_ctx** out) {
+    if (!p || !out) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    int rc = check_params(p, why);
+    if (rc != SPK_OK) return fail(nullptr, rc, why);
+    spk_ctx* c = new spk_ctx();
+    memset(c->have_graph, 0, sizeof(c->have_graph));
+    c->d_tab = nullptr; c->d_tw = nullptr; c->U = c->S = nullptr; c->bufA = c->bufB = nullptr;
+    c->rA = c->rB = c->breal = nullptr; c->Uc0 = c->Uc1 = c->dU0 = nullptr; c->sc = nullptr;
+    c->h_sc = nullptr; c->d_sums = nullptr; c->h_sums = nullptr; c->h_step = 0; c->sticky = 0;
+    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->user_U = nullptr;
+    rc = ctx_init(c, p, stream);
+    if (rc != SPK_OK) { delete c; return rc; }
+    rc = ctx_alloc(c);
+    if (rc != SPK_OK) {
+        g_create_error = c->err;
+        ctx_free(c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return SPK_OK;
+}
+
+extern "C" int spk_ctx_destroy(spk_ctx* c) {
+    if (!c) return SPK_ERR_ARG;
+    cudaStreamSynchronize(c->stream);
+    ctx_free(c);
+    delete c;
+    return SPK_OK;
+}
+
+extern "C" int spk_sizes(const spk_ctx* c, int* nf, size_t* ncx) {
+    if (!c) return SPK_ERR_ARG;
+    if (nf) *nf = c->F;
+    if (ncx) *ncx = c->nc;
+    return SPK_OK;
+}
+
+extern "C" int spk_set_state(spk_ctx* c, const double* U, int where) {
+    if (!c || !U) return SPK_ERR_ARG;
+    CK(cudaMemcpyAsync(c->U, U, sizeof(double2) * c->nc * c->F, where ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
+    return SPK_OK;
+}
+
+extern "C" int spk_get_state(spk_ctx* c, double* U, int where) {
+    if (!c || !U) return SPK_ERR_ARG;
+    CK(cudaMemcpyAsync(U, c->U, sizeof(double2) * c->nc * c->F, where ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c->stream));
+    if (where) CK(cudaStreamSynchronize(c->stream));
+    return SPK_OK;
+}
+
+extern "C" int spk_set_time(spk_ctx* c, double t, int step, double t_lastsnap) {
+    if (!c) return SPK_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(c->h_sc, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
+    c->h_sc->t = t; c->h_sc->step = step; c->h_sc->t_lastsnap = t_lastsnap;
+    CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice));
+    c->h_step = step;
+    return SPK_OK;
+}
+
+static int pull_scalars(spk_ctx* c) {
+    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SPK_OK;
+}
+
+extern "C" int spk_get_time(spk_ctx* c, double* t, double* dt, int* step) {
+    if (!c) return SPK_ERR_ARG;
+    int rc = pull_scalars(c);
+    if (rc) return rc;
+    if (t) *t = c->h_sc->t;
+    if (dt) *dt = c->h_sc->dt;
+    if (step) *step = c->h_sc->step;
+    return SPK_OK;
+}
+
+extern "C" int spk_clean_divergence(spk_ctx* c) {
+    if (!c) return SPK_ERR_ARG;
+    if (c->p.incompressible) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc);
+    if (c->p.mhd) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc);
+    return launch_status(c);
+}
+
+extern "C" int spk_compute_dt(spk_ctx* c, double* dt_hyp, double* dt_par, double* dt_sts, double* dt_cur) {
+    if (!c) return SPK_ERR_ARG;
+    if (c->p.incompressible) {
+        k_reset_max<<<1, 32, 0, c->stream>>>(c->sc);
+        pass_x_inverse(c, c->U, false, false);
+        pass_y_inverse(c, false);
+        pass_z_inverse_only(c, true, c->sts_aniso);
+    }
+    DtArgs d = dt_args(c, false);
+    k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+    int rc = launch_status(c);
+    if (rc) return rc;
+    rc = pull_scalars(c);
+    if (rc) return rc;
+    if (dt_hyp) *dt_hyp = c->h_sc->dt_hyp;
+    if (dt_par) *dt_par = c->h_sc->dt_par;
+    if (dt_sts) *dt_sts = c->h_sc->dt_sts;
+    if (dt_cur) *dt_cur = c->h_sc->dt;
+    if (c->h_sc->nonfinite) return fail(c, SPK_ERR_NONFINITE, "non-finite value in the real-space fields");
+    return SPK_OK;
+}
+
+extern "C" int spk_compute_dfield(spk_ctx* c, const double* Uin, double* dUout) {
+    if (!c || !Uin || !dUout) return SPK_ERR_ARG;
+    double2* U = (double2*)Uin;
+    if (c->p.heat_equation) {
+        XfArgs x = xf_args(c, U, XM_DFIELD, false);
+        x.out = (double2*)dUout;
+        k_heat<<<ew_blocks(c->nc), 256, 0, c->stream>>>(x);
+        return launch_status(c);
+    }
+    c->user_U = U;
+    pass_x_inverse(c, U, false, true);
+    c->user_U = nullptr;
+    pass_y_inverse(c, true);
+    pass_z_products(c, false);
+    pass_y_forward(c, c->nout, c->bufA, c->bufB);
+    XfArgs x = xf_args(c, U, XM_DFIELD, false);
+    x.out = (double2*)dUout;
+    xfwd(c, x);
+    return launch_status(c);
+}
+
+extern "C" int spk_advance(spk_ctx* c, int nsteps) {
+    if (!c || nsteps < 0) return SPK_ERR_ARG;
+    const bool alternate = c->p.supertimestepping && c->nsts > 0 && !c->p.sts_every_step;
+    for (int it = 0; it < nsteps; it++) {
+        const int par = alternate ? (c->h_step & 1) : 0;
+        if (!c->have_graph[par]) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            const long l0 = c->launches;
+            record_step(c, par);
+            c->kernels_per_step[par] = (int)(c->launches - l0);
+            if (c->sticky) {
+                cudaGraph_t gbad;
+                cudaStreamEndCapture(c->stream, &gbad);
+                if (gbad) cudaGraphDestroy(gbad);
+                return c->sticky;
+            }
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (e != cudaSuccess) return fail(c, SPK_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            CK(cudaGraphInstantiate(&c->gexec[par], g, 0));
+            cudaGraphDestroy(g);
+            c->have_graph[par] = true;
+        }
+        CK(cudaGraphLaunch(c->gexec[par], c->stream));
+        c->h_step++;
+    }
+    return SPK_OK;
+}
+
+extern "C" int spk_rkl_cycle(spk_ctx* c, int* s_out) {
+    if (!c) return SPK_ERR_ARG;
+    if (c->nsts == 0) { if (s_out) *s_out = 0; return SPK_OK; }
+    record_rkl_cycle(c);
+    int rc = launch_status(c);
+    if (rc) return rc;
+    rc = pull_scalars(c);
+    if (rc) return rc;
+    if (s_out) *s_out = c->h_sc->s_rkl;
+    return SPK_OK;
+}
+
+extern "C" int spk_to_real(spk_ctx* c, double* R) {
+    if (!c || !R) return SPK_ERR_ARG;
+    if (!c->p.incompressible) {
+        // heat equation: transform the single field through a temporary pipeline
+        return fail(c, SPK_ERR_UNSUPPORTED, "spk_to_real needs the incompressible module");
+    }
+    pass_x_inverse(c, c->U, false, false);
+    pass_y_inverse(c, false);
+    ZArgs z = z_args(c);
+    z.mode = ZM_TO_REAL;
+    set_inputs(c, z, false);
+    z.real_out = R;
+    zpass(c, z);
+    return launch_status(c);
+}
+
+extern "C" int spk_synchronize(spk_ctx* c) {
+    if (!c) return SPK_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    int rc = pull_scalars(c);
+    if (rc) return rc;
+    if (c->h_sc->err) return fail(c, SPK_ERR_ARG, "RKL2 stage count exceeded the recorded bound");
+    if (c->h_sc->nonfinite) return fail(c, SPK_ERR_NONFINITE, "non-finite value in the real-space fields");
+    return SPK_OK;
+}
+
+extern "C" int spk_budgets(spk_ctx* c, spk_budgets_t* out) {
+    if (!c || !out) return SPK_ERR_ARG;
+    CK(cudaMemsetAsync(c->d_sums, 0, sizeof(double) * 16, c->stream));
+    k_budgets<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->F, c->d_sums);
+    CK(cudaMemcpyAsync(c->h_sums, c->d_sums, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double n2 = (double)c->nr * (double)c->nr;
+    memset(out, 0, sizeof(*out));
+    for (int f = 0; f < c->F && f < 8; f++) {
+        out->energy[f] = 0.5 * c->h_sums[2 * f] / n2;
+        out->dissipation[f] = c->h_sums[2 * f + 1] / n2;
+    }
+    return SPK_OK;
+}
+
+extern "C" const char* spk_last_error(const spk_ctx* c) {
+    return c ? c->err.c_str() : g_create_error.c_str();
+}
+
+// ---------------------------------------------------------------------------
+// accounting and per-pass timing
+// ---------------------------------------------------------------------------
+struct PassBytes { double x_inv, y_inv, z, y_fwd, x_fwd[3]; };
+
+// Algorithmic HBM bytes of each pass: every array the pass must read or
+// write, once; products only where the 2/3 mask keeps them.
+static PassBytes pass_bytes(const spk_ctx* c) {
+    PassBytes b;
+    const double nc = (double)c->nc, b_t = (double)csize(c), s16 = 16.0;
+    int ny_keep = 0;
+    for (int j = 0; j < c->ny; j++) ny_keep += c->my[j] != 0.0;
+    const double nkz = (double)c->nx * c->ny * c->kz_keep;          // after the z R2C
+    const double nkyz = (double)c->nx * ny_keep * c->kz_keep;       // after the y forward
+    const int nx_in = c->F + (c->aniso_rhs ? 1 : 0);                // x inverse outputs (gx extra)
+    b.x_inv = c->F * nc * s16 + nx_in * nc * b_t;
+    b.y_inv = nx_in * nc * b_t + c->nin * nc * b_t;
+    b.z = c->nin * nc * b_t + c->nout * nkz * b_t;
+    b.y_fwd = c->nout * nkz * b_t + c->nout * nkyz * b_t;
+    const double nl = c->nout * nkyz * b_t;
+    const double strat = c->p.stratification ? 2.0 * nc * s16 : 0.0;   // theta and u_strat re-read
+    b.x_fwd[0] = nl + 3.0 * c->F * nc * s16 + strat;    // U r, U w, S w
+    b.x_fwd[1] = nl + 4.0 * c->F * nc * s16 + strat;    // U r, S r, U w, S w
+    b.x_fwd[2] = nl + 3.0 * c->F * nc * s16 + strat;    // U r, S r, U w
+    return b;
+}
+
+extern "C" int spk_step_info(spk_ctx* c, int* kps, double* bytes) {
+    if (!c) return SPK_ERR_ARG;
+    if (kps) {
+        if (!c->have_graph[0] && !c->have_graph[1]) {
+            // record (and discard) one step to count its launches
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            const long l0 = c->launches;
+            record_step(c, c->h_step & 1);
+            c->kernels_per_step[c->h_step & 1] = (int)(c->launches - l0);
+            CK(cudaStreamEndCapture(c->stream, &g));
+            cudaGraphDestroy(g);
+        }
+        *kps = std::max(c->kernels_per_step[0], c->kernels_per_step[1]);
+    }
+    if (bytes) {
+        if (c->p.heat_equation) {
+            *bytes = 3.0 * 3.0 * c->F * (double)c->nc * 16.0;
+        } else {
+            const PassBytes b = pass_bytes(c);
+            *bytes = 3.0 * (b.x_inv + b.y_inv + b.z + b.y_fwd) + b.x_fwd[0] + b.x_fwd[1] + b.x_fwd[2];
+        }
+    }
+    return SPK_OK;
+}
+
+extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, int max_out, int* n_out) {
+    if (!c || !out || reps < 1) return SPK_ERR_ARG;
+    if (!c->p.incompressible) return fail(c, SPK_ERR_UNSUPPORTED, "pass profiling needs the incompressible module");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const PassBytes pb = pass_bytes(c);
+    const char* names[5] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward_rhs_rk"};
+    const double bytes[5] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd[2]};
+    int n = 0;
+    // one warm pipeline so every buffer holds stage data
+    pass_x_inverse(c, c->U, false, true);
+    pass_y_inverse(c, true);
+    pass_z_products(c, false);
+    pass_y_forward(c, c->nout, c->bufA, c->bufB);
+    for (int k = 0; k < 5 && n < max_out; k++) {
+        CK(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < reps; r++) {
+            switch (k) {
+                case 0: pass_x_inverse(c, c->U, false, true); break;
+                case 1: pass_y_inverse(c, true); break;
+                case 2: pass_z_products(c, false); break;
+                case 3: pass_y_forward(c, c->nout, c->bufA, c->bufB); break;
+                default: { XfArgs x = xf_args(c, c->U, XM_RK2, false); xfwd(c, x); } break;
+            }
+        }
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        memset(out[n].name, 0, sizeof(out[n].name));
+        strncpy(out[n].name, names[k], sizeof(out[n].name) - 1);
+        out[n].ms = ms / reps;
+        out[n].bytes = bytes[k];
+        out[n].launches_per_step = 3;
+        n++;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_out) *n_out = n;
+    return launch_status(c);
+}

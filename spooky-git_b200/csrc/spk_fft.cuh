@@ -1,0 +1,209 @@
+// spk_fft.cuh -- shared-memory mixed-radix FFT for the SPOOKY passes (sm_100a).
+//
+// A CTA transforms `ncol` independent sequences of length N held in shared
+// memory; element (n, col) lives at buf[n*es + col*cs].  The transform is a
+// Stockham decimation-in-frequency FFT written from the DFT definition
+//     X[t] = sum_n x[n] exp(DIR * 2*pi*i * n*t / N)      (DIR = -1 forward)
+// One stage of radix R on the current length n_s = N/s (s = product of the
+// radices already applied, m = n_s/R):
+//     a_r = x[q + s(p + r m)],   y[q + s(R p + t)] = W_N^{p t s} * DFT_R(a)_t
+// Each stage loads its butterfly inputs into registers, synchronises, then
+// stores its outputs in place (so one buffer suffices), and synchronises.
+// Radix-2/3/4/5/8/16 butterflies run in registers; twiddles W_N^k come from a
+// table computed on the host in extended precision.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace spk {
+
+template <typename T> struct cx;
+template <> struct cx<float>  { using t = float2; };
+template <> struct cx<double> { using t = double2; };
+template <typename T> using C2 = typename cx<T>::t;
+
+template <typename T> __device__ __forceinline__ C2<T> mk(T x, T y) { C2<T> r; r.x = x; r.y = y; return r; }
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { a.x += b.x; a.y += b.y; return a; }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+    V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename V> __device__ __forceinline__ V cconj(V a) { a.y = -a.y; return a; }
+template <typename V, typename S> __device__ __forceinline__ V cscale(S s, V a) { a.x *= s; a.y *= s; return a; }
+// multiply by DIR*i  (DIR=-1: -i, DIR=+1: +i)
+template <int DIR, typename V> __device__ __forceinline__ V rot90(V a) {
+    V r;
+    if (DIR < 0) { r.x = a.y; r.y = -a.x; } else { r.x = -a.y; r.y = a.x; }
+    return r;
+}
+// a * (c + DIR*i*s)
+template <int DIR, typename V, typename T> __device__ __forceinline__ V rotc(V a, T c, T s) {
+    V r;
+    if (DIR < 0) { r.x = a.x * c + a.y * s; r.y = a.y * c - a.x * s; }
+    else         { r.x = a.x * c - a.y * s; r.y = a.y * c + a.x * s; }
+    return r;
+}
+
+// ---- in-register DFTs (natural-order input and output) -------------------
+template <typename T, int DIR> __device__ __forceinline__ void dft2(C2<T>* a) {
+    C2<T> t = a[0]; a[0] = cadd(t, a[1]); a[1] = csub(t, a[1]);
+}
+template <typename T, int DIR> __device__ __forceinline__ void dft4(C2<T>* a) {
+    C2<T> s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
+    C2<T> s13 = cadd(a[1], a[3]), d13 = rot90<DIR>(csub(a[1], a[3]));
+    a[0] = cadd(s02, s13); a[2] = csub(s02, s13);
+    a[1] = cadd(d02, d13); a[3] = csub(d02, d13);
+}
+template <typename T, int DIR> __device__ __forceinline__ void dft8(C2<T>* a) {
+    const T h = (T)0.70710678118654752440;   // cos(pi/4)
+    C2<T> e[4] = {a[0], a[2], a[4], a[6]};
+    C2<T> o[4] = {a[1], a[3], a[5], a[7]};
+    dft4<T, DIR>(e); dft4<T, DIR>(o);
+    o[1] = rotc<DIR>(o[1], h, h);
+    o[2] = rot90<DIR>(o[2]);
+    o[3] = rotc<DIR>(o[3], -h, h);
+#pragma unroll
+    for (int k = 0; k < 4; k++) { a[k] = cadd(e[k], o[k]); a[k + 4] = csub(e[k], o[k]); }
+}
+template <typename T, int DIR> __device__ __forceinline__ void dft16(C2<T>* a) {
+    const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;   // cos, sin(pi/8)
+    const T h = (T)0.70710678118654752440;
+    C2<T> e[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) { e[k] = a[2 * k]; o[k] = a[2 * k + 1]; }
+    dft8<T, DIR>(e); dft8<T, DIR>(o);
+    o[1] = rotc<DIR>(o[1], c1, s1);
+    o[2] = rotc<DIR>(o[2], h, h);
+    o[3] = rotc<DIR>(o[3], s1, c1);
+    o[4] = rot90<DIR>(o[4]);
+    o[5] = rotc<DIR>(o[5], -s1, c1);
+    o[6] = rotc<DIR>(o[6], -h, h);
+    o[7] = rotc<DIR>(o[7], -c1, s1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) { a[k] = cadd(e[k], o[k]); a[k + 8] = csub(e[k], o[k]); }
+}
+template <typename T, int DIR> __device__ __forceinline__ void dft3(C2<T>* a) {
+    const T half = (T)0.5, s3 = (T)0.86602540378443864676;   // sin(2pi/3)
+    C2<T> t1 = cadd(a[1], a[2]);
+    C2<T> t2 = csub(a[0], cscale(half, t1));
+    C2<T> t3 = rot90<DIR>(cscale(s3, csub(a[1], a[2])));
+    a[0] = cadd(a[0], t1);
+    a[1] = cadd(t2, t3);
+    a[2] = csub(t2, t3);
+}
+template <typename T, int DIR> __device__ __forceinline__ void dft5(C2<T>* a) {
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;   // cos(2pi/5), cos(4pi/5)
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;    // sin(2pi/5), sin(4pi/5)
+    C2<T> b1 = cadd(a[1], a[4]), b2 = cadd(a[2], a[3]);
+    C2<T> d1 = csub(a[1], a[4]), d2 = csub(a[2], a[3]);
+    C2<T> r1 = cadd(a[0], cadd(cscale(c1, b1), cscale(c2, b2)));
+    C2<T> r2 = cadd(a[0], cadd(cscale(c2, b1), cscale(c1, b2)));
+    C2<T> i1 = rot90<DIR>(cadd(cscale(s1, d1), cscale(s2, d2)));
+    C2<T> i2 = rot90<DIR>(csub(cscale(s2, d1), cscale(s1, d2)));
+    a[0] = cadd(a[0], cadd(b1, b2));
+    a[1] = cadd(r1, i1); a[4] = csub(r1, i1);
+    a[2] = cadd(r2, i2); a[3] = csub(r2, i2);
+}
+template <typename T, int R, int DIR> __device__ __forceinline__ void dftR(C2<T>* a) {
+    if (R == 2) dft2<T, DIR>(a);
+    else if (R == 3) dft3<T, DIR>(a);
+    else if (R == 4) dft4<T, DIR>(a);
+    else if (R == 5) dft5<T, DIR>(a);
+    else if (R == 8) dft8<T, DIR>(a);
+    else if (R == 16) dft16<T, DIR>(a);
+}
+
+// Plan of one axis length: radices applied in order, twiddle table W_N^k.
+struct FftPlan {
+    int n;
+    int nst;
+    int radix[12];
+    const void* tw;   // C2<T>[n]: exp(-2 pi i k/n), in the pass precision
+};
+
+// One Stockham stage over all columns.  EPT = elements per thread (compile
+// time); a thread owns ceil(EPT/R) butterflies of this stage.  colfast: map
+// consecutive threads to consecutive columns (tiles whose columns are
+// adjacent in memory) instead of consecutive butterflies.
+template <typename T, int R, int DIR, int EPT>
+__device__ __forceinline__ void fft_stage(C2<T>* buf, int es, int cs, int N, int ncol, int s,
+                                          const C2<T>* __restrict__ tw, bool colfast) {
+    constexpr int BPT = (EPT + R - 1) / R;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int nbf = N / R;                 // butterflies per column
+    const int nb = nbf * ncol;
+    const int m = nbf / s;
+    C2<T> a[BPT][R];
+#pragma unroll
+    for (int u = 0; u < BPT; u++) {
+        const int b = tid + u * nthr;
+        if (b < nb) {
+            int col, beta;
+            if (colfast) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
+            const int p = beta / s, q = beta - p * s;
+            C2<T>* base = buf + (size_t)col * cs;
+#pragma unroll
+            for (int r = 0; r < R; r++) a[u][r] = base[(size_t)(q + s * (p + r * m)) * es];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < BPT; u++) {
+        const int b = tid + u * nthr;
+        if (b < nb) {
+            int col, beta;
+            if (colfast) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
+            const int p = beta / s, q = beta - p * s;
+            dftR<T, R, DIR>(a[u]);
+            C2<T>* base = buf + (size_t)col * cs;
+            base[(size_t)(q + s * (R * p)) * es] = a[u][0];
+#pragma unroll
+            for (int t = 1; t < R; t++) {
+                C2<T> w = tw[p * t * s];
+                if (DIR > 0) w.y = -w.y;
+                base[(size_t)(q + s * (R * p + t)) * es] = (p == 0) ? a[u][t] : cmul(a[u][t], w);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Full-radix stages (RF = 16 in FP32, 8 in FP64: the FP64 radix-16
+// butterfly does not fit the register budget) in a loop with one code copy,
+// then at most one stage each of radix 8, 4, 2, 3, 3, 5 for the remainder.
+// Supported lengths: RF^k * {1,2,4,8} * {1,3,9} * {1,5} (see fft_supported).
+template <typename T> struct FullRadix { static constexpr int R = 16; };
+template <> struct FullRadix<double> { static constexpr int R = 8; };
+
+template <typename T, int DIR, int EPT>
+__device__ __forceinline__ void fft_run(C2<T>* buf, int es, int cs, int ncol, const FftPlan& pl, bool cf) {
+    constexpr int RF = FullRadix<T>::R;
+    const C2<T>* tw = (const C2<T>*)pl.tw;
+    asm volatile("" : "+l"(tw));   // keep twiddle loads inside the caller's channel loop
+    const int n = pl.n;
+    int s = 1, rest = n;
+#pragma unroll 1
+    while (rest % RF == 0) { fft_stage<T, RF, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= RF; rest /= RF; }
+    if (RF > 8 && rest % 8 == 0) { fft_stage<T, 8, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 8; rest /= 8; }
+    if (rest % 4 == 0) { fft_stage<T, 4, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 4; rest /= 4; }
+    if (rest % 2 == 0) { fft_stage<T, 2, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 2; rest /= 2; }
+    if (rest % 3 == 0) { fft_stage<T, 3, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 3; rest /= 3; }
+    if (rest % 3 == 0) { fft_stage<T, 3, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 3; rest /= 3; }
+    if (rest % 5 == 0) { fft_stage<T, 5, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 5; rest /= 5; }
+}
+
+// Host check mirroring fft_run's decomposition.
+inline bool fft_supported(int n, int RF) {
+    if (n < 2) return false;
+    int rest = n;
+    while (rest % RF == 0) rest /= RF;
+    if (RF > 8 && rest % 8 == 0) rest /= 8;
+    if (rest % 4 == 0) rest /= 4;
+    if (rest % 2 == 0) rest /= 2;
+    if (rest % 3 == 0) rest /= 3;
+    if (rest % 3 == 0) rest /= 3;
+    if (rest % 5 == 0) rest /= 5;
+    return rest == 1;
+}
+
+}  // namespace spk

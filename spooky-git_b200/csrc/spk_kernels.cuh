@@ -1,0 +1,132 @@
+// spk_kernels.cuh -- argument blocks of the SPOOKY B200 passes.
+//
+// One RK3 stage is five passes over HBM (x = slowest axis, z = contiguous):
+//   X-inverse  (k_axis, axis 0): FP64 state -> x-inverse-transformed channels
+//              (+ divergence cleaning, + i*kx derivative channels, + 1/N^3)
+//   Y-inverse  (k_axis, axis 1): -> (x, y, kz) channels (+ i*ky derivative)
+//   Z          (k_zpass): z C2R of every channel line, real-space products
+//              (Basdevant stress, u x B, u theta, anisotropic heat flux),
+//              |u|,|B| maxima for dt, z R2C of the products (kz < kz_keep)
+//   Y-forward  (k_axis, axis 1): products -> (x, ky, kz), kept ky rows only
+//   X-forward  (k_xfwd): products -> (kx, ky, kz); the RHS (curls,
+//              divergences, 2/3 mask, Boussinesq, diffusion, Leray) and the
+//              low-storage RK3 / Euler update of the FP64 state.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include "spk_fft.cuh"
+
+namespace spk {
+
+struct DevGrid {
+    int nx, ny, nz, nzh;
+    int kz_keep;                    // kz index k is inside the 2/3 mask iff k < kz_keep
+    size_t nc;                      // nx*ny*nzh
+    const double *kx, *ky, *kz;     // wavevector tables (exact reference expressions)
+    const double *mx, *my, *mz;     // separable mask factors, 0.0 or 1.0
+};
+
+#define SPK_RKL_MAX 128
+
+// Device-resident step scalars (written by k_dt, read by every update pass).
+struct DevScalars {
+    double t, dt, dt_hyp, dt_par, dt_sts, t_lastsnap;
+    unsigned long long maxbits[8];  // bit patterns of max |ux| |uy| |uz| |bx| |by| |bz|
+    int step, s_rkl, err, nonfinite;
+    double rkl[SPK_RKL_MAX][5];     // stage j: mu, nu, dt*mu~, dt*gamma, 1-mu-nu
+};
+
+#define SPK_MAXJOBS 16
+
+struct AxisJob {
+    const void* in;
+    void* out;
+    int nch;        // channels handled by this job (1, or 3 when cleaning)
+    int in_state;   // input is the FP64 state (double2) instead of the pass type
+    int deriv;      // multiply the input by i*k_axis(n) before the transform
+    int clean;      // divergence-clean the 3-vector at load (state input, x pass)
+};
+
+struct AxisArgs {
+    DevGrid g;
+    FftPlan plan;
+    int axis;       // 0: x (tile = fixed j), 1: y (tile = fixed i)
+    int kt;         // tile width (k columns)
+    int kcols;      // process columns [0, kcols)
+    int row_filter; // store only rows whose mask factor along the axis is 1
+    size_t cs_in, cs_out;   // channel strides, complex elements
+    double scale;   // input scale factor
+    const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
+    int gate_stage;
+    int njobs;
+    AxisJob job[SPK_MAXJOBS];
+};
+
+enum ZMode { ZM_PRODUCTS = 0, ZM_INVERSE_ONLY = 1, ZM_RKL_FLUX = 2, ZM_TO_REAL = 3 };
+
+struct ZArgs {
+    DevGrid g;
+    FftPlan plan;           // length nz
+    int lines;              // lines per CTA
+    int mode;
+    const void* in; size_t cs_in; int nin;   // input channels (x, y, kz)
+    void* out; size_t cs_out; int nout;      // output channels (x, y, kz) or real lines
+    // input channel roles (-1 = absent); gz is derived from th in the pass
+    int ch_u, ch_b, ch_th, ch_gx, ch_gy, derive_gz;
+    // products
+    int hydro, mhd, bous, aniso, sd;
+    double chi, omegaT2;
+    int do_max;
+    unsigned long long* maxbits;
+    int* nonfinite;
+    void* breal;            // real B lines [3][nx*ny*nz], pass precision
+    int store_breal, load_breal;
+    double* real_out;       // ZM_TO_REAL: [nin][nx*ny*nz] FP64
+    const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
+    int gate_stage;
+};
+
+enum XMode { XM_RK0 = 0, XM_RK1 = 1, XM_RK2 = 2, XM_EULER = 3, XM_DFIELD = 4 };
+
+struct XfArgs {
+    DevGrid g;
+    FftPlan plan;           // length nx
+    int kt;
+    const void* nl; size_t cs_nl;           // nonlinear channels after the y-forward pass
+    int nl_T, nl_E, nl_F, nl_Q;             // first channel of each product group (-1 absent)
+    double2* U; double2* S; double2* out;   // FP64 state, RK scratch, dfield output
+    int F, VEL, MAG, TH;
+    int incompressible, mhd, bous, heat, strat, sd, aniso_rhs;
+    unsigned sts_mask;
+    double nu, nu_m, nu_th, N2;
+    int mode, clean;
+    const DevScalars* sc;
+};
+
+struct RklArgs {
+    DevGrid g;
+    FftPlan plan;           // length nx (for the flux pass)
+    int kt;
+    const void* nl; size_t cs_nl;           // q channels after the y-forward pass
+    double2* th;            // the STS variable(s) in the state
+    double2 *Uc0, *Uc1, *dU0;
+    int stage;              // 1..s
+    int nsts; int fields[8]; int kind[8];   // kind: 0 velocity(nu) 1 B(nu_m) 2 th iso(nu_th) 3 th aniso
+    double nu, nu_m, nu_th;
+    const DevScalars* sc;
+};
+
+struct DtArgs {
+    int incompressible, heat, mhd, bous, aniso, sts, with_fixed;
+    double kxmax, kymax, kzmax;
+    double nu, nu_m, nu_th, reynolds_ani, N2, OmegaT2;
+    double cfl, cfl_par, cfl_sts, safety_source, safety_sts;
+    double t_final, toutput_flow, fixed_dt;
+    unsigned sts_pos_mask;   // bit f set: field f in STS
+    int VX, VY, VZ, BX, BY, BZ, TH;
+    int advance;             // 1: t += dt, step += 1
+    int rkl_smax;
+};
+
+}  // namespace spk

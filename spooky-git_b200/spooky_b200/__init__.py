@@ -1,0 +1,301 @@
+"""Python binding of libspooky_b200.so (the C ABI in include/spooky_b200.h).
+
+The objects mirror the reference's host interface for the hot path
+(LorenzoLMP/spooky-git): ``Supervisor`` owns ``Parameters``, ``Fields``,
+``TimeStepping`` and ``RKLegendre``; ``TimeStepping.compute_dt``,
+``compute_dfield``, ``HydroMHDAdvance`` and ``RKLegendre.compute_cycle``
+keep the reference's names and meaning.  Device memory is owned by the
+context; torch tensors (CUDA) or numpy arrays (host) may be passed where a
+state array is expected.
+
+The library is required: importing works without it, but creating a context
+raises ``RuntimeError`` if ``lib/libspooky_b200.so`` is missing -- there is no
+CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .params import (SPK_FORM_FP32, SPK_FORM_PLAIN, SPK_INT_EULER, SPK_INT_RK3, SPK_STS_RKL2, Params,
+                     check_parameters, default_params, num_fields, var_list)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libspooky_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "spooky_b200.h")
+
+SPK_OK = 0
+ERRORS = {1: "SPK_ERR_ARG", 2: "SPK_ERR_UNSUPPORTED", 3: "SPK_ERR_CUDA", 4: "SPK_ERR_ALLOC",
+          5: "SPK_ERR_NONFINITE", 6: "SPK_ERR_CONFIG"}
+
+EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_sizes", "spk_set_state",
+            "spk_get_state", "spk_set_time", "spk_get_time", "spk_clean_divergence", "spk_compute_dt",
+            "spk_compute_dfield", "spk_advance", "spk_rkl_cycle", "spk_to_real", "spk_synchronize",
+            "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error"]
+
+
+class Budgets(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double * 8), ("dissipation", ctypes.c_double * 8)]
+
+
+class PassStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 24), ("ms", ctypes.c_double), ("bytes", ctypes.c_double),
+                ("launches_per_step", ctypes.c_int)]
+
+
+class SpookyError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def lib():
+    """Load the CUDA library (raises if it is not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libspooky_b200.so not built at {LIB_PATH} (run `make -C spooky-git_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, dp, ip, sp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_size_t
+        L.spk_params_default.argtypes = [ctypes.POINTER(Params)]
+        L.spk_params_default.restype = None
+        L.spk_ctx_create.argtypes = [ctypes.POINTER(Params), vp, ctypes.POINTER(vp)]
+        L.spk_ctx_destroy.argtypes = [vp]
+        L.spk_sizes.argtypes = [vp, ip, ctypes.POINTER(sp)]
+        L.spk_set_state.argtypes = [vp, vp, ctypes.c_int]
+        L.spk_get_state.argtypes = [vp, vp, ctypes.c_int]
+        L.spk_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        L.spk_get_time.argtypes = [vp, dp, dp, ip]
+        L.spk_clean_divergence.argtypes = [vp]
+        L.spk_compute_dt.argtypes = [vp, dp, dp, dp, dp]
+        L.spk_compute_dfield.argtypes = [vp, vp, vp]
+        L.spk_advance.argtypes = [vp, ctypes.c_int]
+        L.spk_rkl_cycle.argtypes = [vp, ip]
+        L.spk_to_real.argtypes = [vp, vp]
+        L.spk_synchronize.argtypes = [vp]
+        L.spk_budgets.argtypes = [vp, ctypes.POINTER(Budgets)]
+        L.spk_step_info.argtypes = [vp, ip, dp]
+        L.spk_profile_passes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PassStat), ctypes.c_int, ip]
+        L.spk_last_error.argtypes = [vp]
+        L.spk_last_error.restype = ctypes.c_char_p
+        for name in EXPORTED:
+            if name not in ("spk_params_default", "spk_last_error"):
+                getattr(L, name).restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def c_defaults():
+    """spk_params_default from the library."""
+    p = Params()
+    lib().spk_params_default(ctypes.byref(p))
+    return p
+
+
+def _ptr(a):
+    """(address, where) for a torch CUDA tensor (0) or numpy array (1)."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda:
+            return a.data_ptr(), 0
+        return a.data_ptr(), 1
+    return a.ctypes.data, 1
+
+
+class Context:
+    """One spk_ctx: the device state and the recorded step pipelines."""
+
+    def __init__(self, params, stream=None):
+        self.params = params.copy()
+        h = ctypes.c_void_p()
+        rc = lib().spk_ctx_create(ctypes.byref(self.params), stream, ctypes.byref(h))
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(None).decode())
+        self._h = h
+        nf, ncx = ctypes.c_int(), ctypes.c_size_t()
+        lib().spk_sizes(self._h, ctypes.byref(nf), ctypes.byref(ncx))
+        self.F, self.nc = nf.value, ncx.value
+        p = self.params
+        self.shape_c = (self.F, p.nx, p.ny, p.nz // 2 + 1)
+        self.shape_r = (self.F, p.nx, p.ny, p.nz)
+        self.var_list = var_list(p)
+
+    def _check(self, rc):
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().spk_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ---------------------------------------------------------------
+    def set_state(self, U):
+        if not hasattr(U, "data_ptr"):
+            U = np.ascontiguousarray(U, dtype=np.complex128)
+            assert U.size == self.F * self.nc
+        ptr, where = _ptr(U)
+        self._check(lib().spk_set_state(self._h, ptr, where))
+        if where:
+            self.synchronize()
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty(self.shape_c, dtype=np.complex128)
+        ptr, where = _ptr(out)
+        self._check(lib().spk_get_state(self._h, ptr, where))
+        return out
+
+    def set_time(self, t, step=0, t_lastsnap=0.0):
+        self._check(lib().spk_set_time(self._h, t, step, t_lastsnap))
+
+    def get_time(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(lib().spk_get_time(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
+        return t.value, dt.value, st.value
+
+    # -- reference operations ------------------------------------------------
+    def clean_divergence(self):
+        self._check(lib().spk_clean_divergence(self._h))
+
+    def compute_dt(self):
+        o = [ctypes.c_double() for _ in range(4)]
+        self._check(lib().spk_compute_dt(self._h, *[ctypes.byref(x) for x in o]))
+        return np.array([x.value for x in o])
+
+    def compute_dfield(self, U, dU):
+        """U, dU: torch CUDA complex128 tensors of shape_c."""
+        self._check(lib().spk_compute_dfield(self._h, U.data_ptr(), dU.data_ptr()))
+
+    def advance(self, nsteps=1):
+        self._check(lib().spk_advance(self._h, int(nsteps)))
+
+    def rkl_cycle(self):
+        s = ctypes.c_int()
+        self._check(lib().spk_rkl_cycle(self._h, ctypes.byref(s)))
+        return s.value
+
+    def to_real(self, R):
+        """R: torch CUDA float64 tensor of shape_r."""
+        self._check(lib().spk_to_real(self._h, R.data_ptr()))
+
+    def synchronize(self):
+        self._check(lib().spk_synchronize(self._h))
+
+    def step_info(self):
+        """(kernels launched per step, algorithmic HBM bytes per RK3 step)."""
+        k, b = ctypes.c_int(), ctypes.c_double()
+        self._check(lib().spk_step_info(self._h, ctypes.byref(k), ctypes.byref(b)))
+        return k.value, b.value
+
+    def profile_passes(self, reps=10):
+        out = (PassStat * 8)()
+        n = ctypes.c_int()
+        self._check(lib().spk_profile_passes(self._h, int(reps), out, 8, ctypes.byref(n)))
+        return [dict(name=out[i].name.decode(), ms=out[i].ms, bytes=out[i].bytes,
+                     launches_per_step=out[i].launches_per_step) for i in range(n.value)]
+
+    def budgets(self):
+        b = Budgets()
+        self._check(lib().spk_budgets(self._h, ctypes.byref(b)))
+        return np.array(b.energy[: self.F]), np.array(b.dissipation[: self.F])
+
+
+# ---------------------------------------------------------------------------
+# Reference-named objects (src/supervisor, src/fields, src/timestepping, src/rkl)
+# ---------------------------------------------------------------------------
+class Parameters:
+    """Parameters (src/parameters/parameters.hpp): the cfg subset the path reads."""
+
+    def __init__(self, params=None, **kw):
+        self.p = params.copy() if params is not None else default_params(**kw)
+        errs = check_parameters(self.p)
+        if errs:
+            raise SpookyError(6, "; ".join(errs))
+
+    def __getattr__(self, k):
+        return getattr(self.__dict__["p"], k)
+
+
+class Fields:
+    """Fields (src/fields/fields.hpp): the state lives in the context."""
+
+    def __init__(self, ctx):
+        self._ctx = ctx
+
+    def CleanFieldDivergence(self):
+        self._ctx.clean_divergence()
+
+    def set(self, U):
+        self._ctx.set_state(U)
+
+    def get(self):
+        return self._ctx.get_state()
+
+
+class RKLegendre:
+    """RKLegendre (src/rkl/rkl.hpp:42): compute_cycle on the STS variables."""
+
+    def __init__(self, ctx):
+        self._ctx = ctx
+
+    def compute_cycle(self):
+        return self._ctx.rkl_cycle()
+
+
+class TimeStepping:
+    """TimeStepping (src/timestepping/timestepping.hpp:39-43)."""
+
+    def __init__(self, ctx):
+        self._ctx = ctx
+        self.rkl = RKLegendre(ctx)
+
+    def compute_dt(self):
+        dt_hyp, dt_par, dt_sts, dt = self._ctx.compute_dt()
+        self.dt_hyp, self.dt_par, self.dt_sts, self.current_dt = dt_hyp, dt_par, dt_sts, dt
+        return dt
+
+    def compute_dfield(self, U, dU):
+        self._ctx.compute_dfield(U, dU)
+
+    def HydroMHDAdvance(self, nsteps=1):
+        """CleanFieldDivergence + HydroMHDAdvance, nsteps times (asynchronous)."""
+        self._ctx.advance(nsteps)
+
+    @property
+    def current_time(self):
+        return self._ctx.get_time()[0]
+
+    @property
+    def current_step(self):
+        return self._ctx.get_time()[2]
+
+
+class Supervisor:
+    """Supervisor (src/supervisor/supervisor.hpp:24-84) for the hot path."""
+
+    def __init__(self, params, stream=None):
+        self.param = Parameters(params)
+        self.ctx = Context(self.param.p, stream)
+        self.fields = Fields(self.ctx)
+        self.timestep = TimeStepping(self.ctx)
+
+    def executeMainLoop(self, max_steps=None):
+        """Advance until t_final (src/supervisor/supervisor.cu:169-213); the
+        host reads the device time once per step."""
+        n = 0
+        while self.timestep.current_time < self.param.t_final:
+            self.timestep.HydroMHDAdvance(1)
+            n += 1
+            if max_steps is not None and n >= max_steps:
+                break
+        self.ctx.synchronize()
+        return n
