@@ -69,6 +69,7 @@ struct spk_ctx {
     long launches;                 // kernels issued (counted by the launch helpers)
     bool bad_job;                  // a pass was built with an out-of-range channel
     const void* user_U;            // caller's state array during spk_compute_dfield
+    bool dirty;                    // state set from outside: clean u, B before the next step
     int kernels_per_step[2];
 };
 
@@ -162,7 +163,7 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N) {
     const int ept = c->fp32 ? EPT_AXIS_F : EPT_AXIS_D;
     int kt = c->fp32 ? 16 : 8;
     while (kt > 1 && (long)N * kt > (long)MAXT * ept) kt /= 2;
-    kt = std::min(kt, c->nzh);
+    while (kt > 1 && kt > c->nzh) kt /= 2;    // power of two (the pass masks and shifts by it)
     a.kt = kt;
     a.nthr = std::max(32, std::min(MAXT, rup32(((long)N * kt + ept - 1) / ept)));
     a.smem = (size_t)N * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
@@ -174,7 +175,7 @@ static AxisCfg xfwd_cfg(const spk_ctx* c) {
     const int ept = c->fp32 ? 8 : 4;
     int kt = c->fp32 ? 16 : 8;
     while (kt > 1 && (long)c->nx * kt > (long)MAXT * ept) kt /= 2;
-    kt = std::min(kt, c->nzh);
+    while (kt > 1 && kt > c->nzh) kt /= 2;
     a.kt = kt;
     a.nthr = std::max(32, std::min(MAXT, rup32(((long)c->nx * kt + ept - 1) / ept)));
     a.smem = (size_t)c->nx * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
@@ -188,7 +189,8 @@ static ZCfg z_cfg(const spk_ctx* c, int nin_all, int nout) {
     const int npin = (nin_all + 1) / 2, npout = (nout + 1) / 2;
     const int maxp = std::max(npin, std::max(npout, 1));
     const size_t csz = c->fp32 ? sizeof(float2) : sizeof(double2);
-    const size_t per_line = (size_t)(npin + npout) * c->nz * csz;
+    const int nzp = padded_len(c->nz);
+    const size_t per_line = (size_t)(npin + npout) * nzp * csz;
     int L = (int)std::max<size_t>(1, 65536 / std::max<size_t>(per_line, 1));
     L = std::min(L, 64);
     const int ept = c->fp32 ? EPT_Z_F : EPT_Z_D;
@@ -197,7 +199,7 @@ static ZCfg z_cfg(const spk_ctx* c, int nin_all, int nout) {
     z.lines = L;
     z.nthr = std::max(32, std::min(MAXT, rup32(((long)L * maxp * c->nz + ept - 1) / ept)));
     // input pairs, output pairs, then 6 x 32 values of block-max scratch
-    z.smem = (size_t)L * (npin + npout) * c->nz * csz + 6 * 32 * (c->fp32 ? sizeof(float) : sizeof(double));
+    z.smem = (size_t)L * (npin + npout) * nzp * csz + 6 * 32 * (c->fp32 ? sizeof(float) : sizeof(double));
     return z;
 }
 
@@ -260,11 +262,11 @@ static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch,
 }
 
 // first inverse pass over the state: fields in order, cleaning u and B when asked
-static void pass_x_inverse(spk_ctx* c, const double2* U, bool clean, bool with_gx) {
+static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx) {
     AxisArgs a = axis_args(c, 0);
     a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);   // scaleKernel factor
-    if (c->p.incompressible) add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_u), 3, 1, 0, clean ? 1 : 0);
-    if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, clean ? 1 : 0);
+    if (c->p.incompressible) add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_u), 3, 1, 0, 0);
+    if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, 0);
     if (c->p.boussinesq) {
         add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_th), 1, 1, 0, 0);
         if (with_gx && c->aniso_rhs) add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_gx), 1, 1, 1, 0);
@@ -295,6 +297,7 @@ static ZArgs z_args(spk_ctx* c) {
     z.sd = c->p.strat_direction;
     z.chi = 1.0 / c->p.reynolds_ani;
     z.omegaT2 = c->p.OmegaT2;
+    z.fd_nz = FastDiv::make((unsigned)c->nz);
     return z;
 }
 
@@ -480,7 +483,7 @@ static void record_step(spk_ctx* c, int parity) {
     c->launches++;
     for (int s = 0; s < nst; s++) {
         const bool first = s == 0;
-        pass_x_inverse(c, c->U, first, true);
+        pass_x_inverse(c, c->U, true);
         pass_y_inverse(c, true);
         if (first) {
             if (sts_before) {
@@ -500,7 +503,8 @@ static void record_step(spk_ctx* c, int parity) {
             pass_z_products(c, false);
         }
         pass_y_forward(c, c->nout, c->bufA, c->bufB);
-        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, first);
+        // the last stage cleans the new u and B: CleanFieldDivergence of the next step
+        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, s == nst - 1);
         xfwd(c, x);
     }
     if (sts_after) {
@@ -773,7 +777,7 @@ extern "C" int spk_ctx_create(const spk_params_t* p, void* stream, spk_ctx** out
     c->d_tab = nullptr; c->d_tw = nullptr; c->U = c->S = nullptr; c->bufA = c->bufB = nullptr;
     c->rA = c->rB = c->breal = nullptr; c->Uc0 = c->Uc1 = c->dU0 = nullptr; c->sc = nullptr;
     c->h_sc = nullptr; c->d_sums = nullptr; c->h_sums = nullptr; c->h_step = 0; c->sticky = 0;
-    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->user_U = nullptr;
+    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->user_U = nullptr; c->dirty = true;
     rc = ctx_init(c, p, stream);
     if (rc != SPK_OK) { delete c; return rc; }
     rc = ctx_alloc(c);
@@ -805,6 +809,7 @@ extern "C" int spk_sizes(const spk_ctx* c, int* nf, size_t* ncx) {
 extern "C" int spk_set_state(spk_ctx* c, const double* U, int where) {
     if (!c || !U) return SPK_ERR_ARG;
     CK(cudaMemcpyAsync(c->U, U, sizeof(double2) * c->nc * c->F, where ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
+    c->dirty = true;
     return SPK_OK;
 }
 
@@ -841,8 +846,15 @@ extern "C" int spk_get_time(spk_ctx* c, double* t, double* dt, int* step) {
     return SPK_OK;
 }
 
+static void launch_clean(spk_ctx* c) {
+    if (c->p.incompressible) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc);
+    if (c->p.mhd) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc);
+    c->dirty = false;
+}
+
 extern "C" int spk_clean_divergence(spk_ctx* c) {
     if (!c) return SPK_ERR_ARG;
+    c->dirty = false;
     if (c->p.incompressible) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc);
     if (c->p.mhd) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc);
     return launch_status(c);
@@ -852,7 +864,7 @@ extern "C" int spk_compute_dt(spk_ctx* c, double* dt_hyp, double* dt_par, double
     if (!c) return SPK_ERR_ARG;
     if (c->p.incompressible) {
         k_reset_max<<<1, 32, 0, c->stream>>>(c->sc);
-        pass_x_inverse(c, c->U, false, false);
+        pass_x_inverse(c, c->U, false);
         pass_y_inverse(c, false);
         pass_z_inverse_only(c, true, c->sts_aniso);
     }
@@ -880,7 +892,7 @@ extern "C" int spk_compute_dfield(spk_ctx* c, const double* Uin, double* dUout) 
         return launch_status(c);
     }
     c->user_U = U;
-    pass_x_inverse(c, U, false, true);
+    pass_x_inverse(c, U, true);
     c->user_U = nullptr;
     pass_y_inverse(c, true);
     pass_z_products(c, false);
@@ -894,6 +906,13 @@ extern "C" int spk_compute_dfield(spk_ctx* c, const double* Uin, double* dUout) 
 extern "C" int spk_advance(spk_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SPK_ERR_ARG;
     const bool alternate = c->p.supertimestepping && c->nsts > 0 && !c->p.sts_every_step;
+    // Each step ends with the divergence cleaning of the next step fused into
+    // its last update; a state set from outside is cleaned here once.
+    if (nsteps > 0 && c->dirty) {
+        launch_clean(c);
+        int rc = launch_status(c);
+        if (rc) return rc;
+    }
     for (int it = 0; it < nsteps; it++) {
         const int par = alternate ? (c->h_step & 1) : 0;
         if (!c->have_graph[par]) {
@@ -938,7 +957,7 @@ extern "C" int spk_to_real(spk_ctx* c, double* R) {
         // heat equation: transform the single field through a temporary pipeline
         return fail(c, SPK_ERR_UNSUPPORTED, "spk_to_real needs the incompressible module");
     }
-    pass_x_inverse(c, c->U, false, false);
+    pass_x_inverse(c, c->U, false);
     pass_y_inverse(c, false);
     ZArgs z = z_args(c);
     z.mode = ZM_TO_REAL;
@@ -1041,7 +1060,7 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
     const double bytes[5] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd[2]};
     int n = 0;
     // one warm pipeline so every buffer holds stage data
-    pass_x_inverse(c, c->U, false, true);
+    pass_x_inverse(c, c->U, true);
     pass_y_inverse(c, true);
     pass_z_products(c, false);
     pass_y_forward(c, c->nout, c->bufA, c->bufB);
@@ -1049,7 +1068,7 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
         CK(cudaEventRecord(e0, c->stream));
         for (int r = 0; r < reps; r++) {
             switch (k) {
-                case 0: pass_x_inverse(c, c->U, false, true); break;
+                case 0: pass_x_inverse(c, c->U, true); break;
                 case 1: pass_y_inverse(c, true); break;
                 case 2: pass_z_products(c, false); break;
                 case 3: pass_y_forward(c, c->nout, c->bufA, c->bufB); break;

@@ -121,16 +121,71 @@ struct FftPlan {
     const void* tw;   // C2<T>[n]: exp(-2 pi i k/n), in the pass precision
 };
 
-// One Stockham stage over all columns.  EPT = elements per thread (compile
-// time); a thread owns ceil(EPT/R) butterflies of this stage.  colfast: map
-// consecutive threads to consecutive columns (tiles whose columns are
-// adjacent in memory) instead of consecutive butterflies.
-template <typename T, int R, int DIR, int EPT>
-__device__ __forceinline__ void fft_stage(C2<T>* buf, int es, int cs, int N, int ncol, int s,
-                                          const C2<T>* __restrict__ tw, bool colfast) {
+// Element n of a column at n (PAD = 0) or n + n/16 (PAD = 1: one pad slot
+// per 16 elements breaks the stride-R bank conflicts of contiguous columns).
+template <int PAD> __device__ __forceinline__ int padi(int n) { return PAD ? n + (n >> 4) : n; }
+__host__ __device__ inline int padded_len(int n) { return n + (n >> 4); }
+
+// One Stockham stage over all columns, power-of-two geometry: every index is
+// a shift or a mask.  ln = log2 N, lncol = log2 ncol, ls = log2 s.
+// EPT = elements per thread (compile time); a thread owns ceil(EPT/R)
+// butterflies.  COLFAST: consecutive threads take consecutive columns
+// (columns adjacent in memory), else consecutive butterflies of a column.
+template <typename T, int R, int LR, int DIR, int EPT, bool COLFAST, int PAD>
+__device__ __forceinline__ void stage_p2(C2<T>* buf, int es, int cs, int ln, int ncol, int lncol, int ls,
+                                         const C2<T>* __restrict__ tw) {
     constexpr int BPT = (EPT + R - 1) / R;
     const int nthr = blockDim.x, tid = threadIdx.x;
-    const int nbf = N / R;                 // butterflies per column
+    const int lnbf = ln - LR;          // log2(N/R)
+    const int lm = lnbf - ls;          // log2(m)
+    const int nb = ncol << lnbf;
+    const int smask = (1 << ls) - 1;
+    C2<T> a[BPT][R];
+#pragma unroll
+    for (int u = 0; u < BPT; u++) {
+        const int b = tid + u * nthr;
+        if (b < nb) {
+            int col, beta;
+            if (COLFAST) { col = b & ((1 << lncol) - 1); beta = b >> lncol; }
+            else         { beta = b & ((1 << lnbf) - 1); col = b >> lnbf; }
+            const int p = beta >> ls, q = beta & smask;
+            const C2<T>* base = buf + (size_t)col * cs;
+            const int i0 = q + (p << ls);
+#pragma unroll
+            for (int r = 0; r < R; r++) a[u][r] = base[padi<PAD>(i0 + (r << (ls + lm))) * es];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < BPT; u++) {
+        const int b = tid + u * nthr;
+        if (b < nb) {
+            int col, beta;
+            if (COLFAST) { col = b & ((1 << lncol) - 1); beta = b >> lncol; }
+            else         { beta = b & ((1 << lnbf) - 1); col = b >> lnbf; }
+            const int p = beta >> ls, q = beta & smask;
+            dftR<T, R, DIR>(a[u]);
+            C2<T>* base = buf + (size_t)col * cs;
+            const int o0 = q + ((R * p) << ls);
+            base[padi<PAD>(o0) * es] = a[u][0];
+#pragma unroll
+            for (int t = 1; t < R; t++) {
+                C2<T> w = tw[(p * t) << ls];
+                if (DIR > 0) w.y = -w.y;
+                base[padi<PAD>(o0 + (t << ls)) * es] = (p == 0) ? a[u][t] : cmul(a[u][t], w);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Same stage for any length (integer division; lengths with factors 3, 5).
+template <typename T, int R, int DIR, int EPT, bool COLFAST, int PAD>
+__device__ __forceinline__ void stage_gen(C2<T>* buf, int es, int cs, int N, int ncol, int s,
+                                          const C2<T>* __restrict__ tw) {
+    constexpr int BPT = (EPT + R - 1) / R;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int nbf = N / R;
     const int nb = nbf * ncol;
     const int m = nbf / s;
     C2<T> a[BPT][R];
@@ -139,11 +194,11 @@ __device__ __forceinline__ void fft_stage(C2<T>* buf, int es, int cs, int N, int
         const int b = tid + u * nthr;
         if (b < nb) {
             int col, beta;
-            if (colfast) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
+            if (COLFAST) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
             const int p = beta / s, q = beta - p * s;
-            C2<T>* base = buf + (size_t)col * cs;
+            const C2<T>* base = buf + (size_t)col * cs;
 #pragma unroll
-            for (int r = 0; r < R; r++) a[u][r] = base[(size_t)(q + s * (p + r * m)) * es];
+            for (int r = 0; r < R; r++) a[u][r] = base[padi<PAD>(q + s * (p + r * m)) * es];
         }
     }
     __syncthreads();
@@ -152,16 +207,16 @@ __device__ __forceinline__ void fft_stage(C2<T>* buf, int es, int cs, int N, int
         const int b = tid + u * nthr;
         if (b < nb) {
             int col, beta;
-            if (colfast) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
+            if (COLFAST) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
             const int p = beta / s, q = beta - p * s;
             dftR<T, R, DIR>(a[u]);
             C2<T>* base = buf + (size_t)col * cs;
-            base[(size_t)(q + s * (R * p)) * es] = a[u][0];
+            base[padi<PAD>(q + s * (R * p)) * es] = a[u][0];
 #pragma unroll
             for (int t = 1; t < R; t++) {
                 C2<T> w = tw[p * t * s];
                 if (DIR > 0) w.y = -w.y;
-                base[(size_t)(q + s * (R * p + t)) * es] = (p == 0) ? a[u][t] : cmul(a[u][t], w);
+                base[padi<PAD>(q + s * (R * p + t)) * es] = (p == 0) ? a[u][t] : cmul(a[u][t], w);
             }
         }
     }
@@ -170,26 +225,39 @@ __device__ __forceinline__ void fft_stage(C2<T>* buf, int es, int cs, int N, int
 
 // Full-radix stages (RF = 16 in FP32, 8 in FP64: the FP64 radix-16
 // butterfly does not fit the register budget) in a loop with one code copy,
-// then at most one stage each of radix 8, 4, 2, 3, 3, 5 for the remainder.
+// then at most one stage each of radix 8, 4, 2 (power-of-two lengths), or
+// 8, 4, 2, 3, 3, 5 for the general path.
 // Supported lengths: RF^k * {1,2,4,8} * {1,3,9} * {1,5} (see fft_supported).
-template <typename T> struct FullRadix { static constexpr int R = 16; };
-template <> struct FullRadix<double> { static constexpr int R = 8; };
+template <typename T> struct FullRadix { static constexpr int R = 16; static constexpr int LR = 4; };
+template <> struct FullRadix<double> { static constexpr int R = 8; static constexpr int LR = 3; };
 
-template <typename T, int DIR, int EPT>
-__device__ __forceinline__ void fft_run(C2<T>* buf, int es, int cs, int ncol, const FftPlan& pl, bool cf) {
-    constexpr int RF = FullRadix<T>::R;
+__host__ __device__ inline int ilog2(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
+
+template <typename T, int DIR, int EPT, bool COLFAST, int PAD>
+__device__ __forceinline__ void fft_run(C2<T>* buf, int es, int cs, int ncol, const FftPlan& pl) {
+    constexpr int RF = FullRadix<T>::R, LRF = FullRadix<T>::LR;
     const C2<T>* tw = (const C2<T>*)pl.tw;
     asm volatile("" : "+l"(tw));   // keep twiddle loads inside the caller's channel loop
     const int n = pl.n;
+    if ((n & (n - 1)) == 0 && (!COLFAST || (ncol & (ncol - 1)) == 0)) {
+        const int ln = ilog2(n), lncol = ilog2(ncol);
+        int ls = 0, rest = ln;
+#pragma unroll 1
+        while (rest >= LRF) { stage_p2<T, RF, LRF, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); ls += LRF; rest -= LRF; }
+        if (RF > 8 && rest >= 3) { stage_p2<T, 8, 3, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); ls += 3; rest -= 3; }
+        if (rest >= 2) { stage_p2<T, 4, 2, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); ls += 2; rest -= 2; }
+        if (rest >= 1) { stage_p2<T, 2, 1, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); }
+        return;
+    }
     int s = 1, rest = n;
 #pragma unroll 1
-    while (rest % RF == 0) { fft_stage<T, RF, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= RF; rest /= RF; }
-    if (RF > 8 && rest % 8 == 0) { fft_stage<T, 8, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 8; rest /= 8; }
-    if (rest % 4 == 0) { fft_stage<T, 4, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 4; rest /= 4; }
-    if (rest % 2 == 0) { fft_stage<T, 2, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 2; rest /= 2; }
-    if (rest % 3 == 0) { fft_stage<T, 3, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 3; rest /= 3; }
-    if (rest % 3 == 0) { fft_stage<T, 3, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 3; rest /= 3; }
-    if (rest % 5 == 0) { fft_stage<T, 5, DIR, EPT>(buf, es, cs, n, ncol, s, tw, cf); s *= 5; rest /= 5; }
+    while (rest % RF == 0) { stage_gen<T, RF, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= RF; rest /= RF; }
+    if (RF > 8 && rest % 8 == 0) { stage_gen<T, 8, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 8; rest /= 8; }
+    if (rest % 4 == 0) { stage_gen<T, 4, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 4; rest /= 4; }
+    if (rest % 2 == 0) { stage_gen<T, 2, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 2; rest /= 2; }
+    if (rest % 3 == 0) { stage_gen<T, 3, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 3; rest /= 3; }
+    if (rest % 3 == 0) { stage_gen<T, 3, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 3; rest /= 3; }
+    if (rest % 5 == 0) { stage_gen<T, 5, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); }
 }
 
 // Host check mirroring fft_run's decomposition.

@@ -17,68 +17,83 @@ template <typename T> __device__ __forceinline__ C2<T> from_d2(double2 v) { retu
 template <typename V> __device__ __forceinline__ double2 to_d2(V v) { return d2((double)v.x, (double)v.y); }
 
 // ---------------------------------------------------------------------------
-// Strided-axis pass (x or y).  Tile = one outer index, kt consecutive k
-// columns, all N positions along the axis; coalesced kt-wide row segments.
-// Fuses: ComplexVecAssign + scaleKernel (cufft_routines.cu:23-39), the
-// divergence cleaning (CleanDivergence, cuda_kernels_generic.cu:288-313) and
-// the i*k derivative of Gradient (cuda_kernels_generic.cu:249-260) into the
-// load of the first inverse pass.
+// Strided-axis pass (x or y).  Tile = one outer index, KT consecutive k
+// columns (KT a power of two), all N positions along the axis; coalesced
+// KT-wide row segments.  Fuses ComplexVecAssign + scaleKernel
+// (cufft_routines.cu:23-39) and the i*k derivative of Gradient
+// (cuda_kernels_generic.cu:249-260) into the load of the inverse passes.
+// Each thread issues its EPT loads before the first shared-memory store.
 // ---------------------------------------------------------------------------
 template <typename T, int DIR, int EPT>
-__global__ void __launch_bounds__(256) k_axis(const __grid_constant__ AxisArgs a) {
+__global__ void __launch_bounds__(256, 2) k_axis(const __grid_constant__ AxisArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
     const AxisJob& job = a.job[blockIdx.z];
-    const int N = a.plan.n, KT = a.kt, nzh = a.g.nzh;
+    const int N = a.plan.n, KT = a.kt, lkt = ilog2(KT), nzh = a.g.nzh;
     const int k0 = blockIdx.x * KT;
     const int o = blockIdx.y;
     const int kt = min(KT, a.kcols - k0);
     size_t stride, base;
     if (a.axis == 0) { stride = (size_t)a.g.ny * nzh; base = (size_t)o * nzh; }
     else             { stride = (size_t)nzh;          base = (size_t)o * a.g.ny * nzh; }
+    base += k0;
     const double* kax = a.axis == 0 ? a.g.kx : a.g.ky;
     const double* max_ = a.axis == 0 ? a.g.mx : a.g.my;
     const int nel = N * KT;
+    const int nthr = blockDim.x, tid = threadIdx.x;
 
     for (int c = 0; c < job.nch; c++) {
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            const int n = e / KT, col = e - n * KT;
-            C2<T> v = mk<T>((T)0, (T)0);
-            if (col < kt) {
-                const size_t idx = base + (size_t)n * stride + k0 + col;
-                if (job.in_state) {
-                    const double2* in = (const double2*)job.in;
-                    double2 x = in[(size_t)c * a.cs_in + idx];
-                    if (job.clean) {
-                        // x pass: mode (i=n, j=o, k=k0+col)
-                        const double kx = a.g.kx[n], ky = a.g.ky[o], kz = a.g.kz[k0 + col];
-                        const double2 x0 = in[idx], x1 = in[a.cs_in + idx], x2 = in[2 * a.cs_in + idx];
-                        const double sx = kx * x0.x + ky * x1.x + kz * x2.x;
-                        const double sy = kx * x0.y + ky * x1.y + kz * x2.y;
-                        const double k2 = kx * kx + ky * ky + kz * kz;
-                        const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
-                        const double kc = (c == 0 ? kx : (c == 1 ? ky : kz)) * ik2;
-                        x = d2(x.x - kc * sx, x.y - kc * sy);
-                    }
-                    if (job.deriv) x = ik_mul(kax[n], x);
-                    v = mk<T>((T)(x.x * a.scale), (T)(x.y * a.scale));
-                } else {
-                    const C2<T>* in = (const C2<T>*)job.in;
-                    v = in[(size_t)c * a.cs_in + idx];
-                    if (job.deriv) { const T k = (T)kax[n]; v = mk<T>(-k * v.y, k * v.x); }
-                    if (a.scale != 1.0) v = cscale((T)a.scale, v);
+        C2<T> v[EPT];
+        if (job.in_state) {
+            const double2* in = (const double2*)job.in + (size_t)c * a.cs_in + base;
+            double2 x[EPT];
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * nthr;
+                const int n = e >> lkt, col = e & (KT - 1);
+                x[u] = (e < nel && col < kt) ? __ldg(in + (size_t)n * stride + col) : d2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * nthr;
+                const int n = min(e >> lkt, N - 1);
+                double2 y = x[u];
+                if (job.deriv) y = ik_mul(kax[n], y);
+                v[u] = mk<T>((T)(y.x * a.scale), (T)(y.y * a.scale));
+            }
+        } else {
+            const C2<T>* in = (const C2<T>*)job.in + (size_t)c * a.cs_in + base;
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * nthr;
+                const int n = e >> lkt, col = e & (KT - 1);
+                v[u] = (e < nel && col < kt) ? in[(size_t)n * stride + col] : mk<T>((T)0, (T)0);
+            }
+            if (job.deriv || a.scale != 1.0) {
+#pragma unroll
+                for (int u = 0; u < EPT; u++) {
+                    const int e = tid + u * nthr;
+                    const int n = min(e >> lkt, N - 1);
+                    if (job.deriv) { const T k = (T)kax[n]; v[u] = mk<T>(-k * v[u].y, k * v[u].x); }
+                    if (a.scale != 1.0) v[u] = cscale((T)a.scale, v[u]);
                 }
             }
-            buf[e] = v;
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = tid + u * nthr;
+            if (e < nel) buf[e] = v[u];
         }
         __syncthreads();
-        fft_run<T, DIR, EPT>(buf, KT, 1, KT, a.plan, true);
-        C2<T>* out = (C2<T>*)job.out + (size_t)c * a.cs_out;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            const int n = e / KT, col = e - n * KT;
-            if (col < kt && (!a.row_filter || max_[n] != 0.0))
-                out[base + (size_t)n * stride + k0 + col] = buf[e];
+        fft_run<T, DIR, EPT, true, 0>(buf, KT, 1, KT, a.plan);
+        C2<T>* out = (C2<T>*)job.out + (size_t)c * a.cs_out + base;
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = tid + u * nthr;
+            const int n = e >> lkt, col = e & (KT - 1);
+            if (e < nel && col < kt && (!a.row_filter || max_[n] != 0.0))
+                out[(size_t)n * stride + col] = buf[e];
         }
         __syncthreads();
     }
@@ -116,10 +131,10 @@ __device__ __forceinline__ void warp_block_max(T* v, int n, T* red) {
 }
 
 template <typename T, int EPT>
-__global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) {
+__global__ void __launch_bounds__(256, 2) k_zpass(const __grid_constant__ ZArgs a) {
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NZ = a.g.nz, nzh = a.g.nzh, L = a.lines;
+    const int NZ = a.g.nz, nzh = a.g.nzh, L = a.lines, NZp = padded_len(NZ);
     const int nlines = a.g.nx * a.g.ny;
     const int line0 = blockIdx.x * L;
     const int nl = min(L, nlines - line0);
@@ -127,55 +142,59 @@ __global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) 
     const int npin = (nin_all + 1) / 2;
     const int npout = (a.nout + 1) / 2;
     C2<T>* inb = reinterpret_cast<C2<T>*>(smem_raw);
-    C2<T>* outb = inb + (size_t)L * npin * NZ;
+    C2<T>* outb = inb + (size_t)L * npin * NZp;
     const C2<T>* in = (const C2<T>*)a.in;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
-    // 1. load the half spectra and build the paired full sequences
-    const int nload = L * npin * nzh;
-    for (int e = threadIdx.x; e < nload; e += blockDim.x) {
-        const int k = e % nzh;
-        const int lp = e / nzh;
-        const int p = lp % npin, l = lp / npin;
-        C2<T> A = mk<T>((T)0, (T)0), B = mk<T>((T)0, (T)0);
-        if (l < nl) {
-            const size_t off = (size_t)(line0 + l) * nzh + k;
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int ch = 2 * p + h;
-                C2<T> v = mk<T>((T)0, (T)0);
-                if (ch < a.nin) {
-                    v = in[(size_t)ch * a.cs_in + off];
-                    if (a.derive_gz == 2 && ch == a.ch_th) {   // the theta channel carries i*kz*theta
-                        const T kz = (T)a.g.kz[k];
-                        v = mk<T>(-kz * v.y, kz * v.x);
-                    }
-                } else if (ch == a.nin && a.derive_gz == 1) {
-                    const C2<T> th = in[(size_t)a.ch_th * a.cs_in + off];
-                    const T kz = (T)a.g.kz[k];
-                    v = mk<T>(-kz * th.y, kz * th.x);
-                }
-                if (h == 0) A = v; else B = v;
+    // 1. a warp per (line, input pair): load both half spectra, build the
+    //    Hermitian-extended paired sequence Z = A + iB
+    auto chan_val = [&](int ch, size_t off, int k) -> C2<T> {
+        if (ch < a.nin) {
+            C2<T> v = in[(size_t)ch * a.cs_in + off];
+            if (a.derive_gz == 2 && ch == a.ch_th) {   // this channel carries i*kz*theta
+                const T kz = (T)a.g.kz[k];
+                v = mk<T>(-kz * v.y, kz * v.x);
             }
+            return v;
         }
-        C2<T>* Z = inb + (size_t)(l * npin + p) * NZ;
-        if (k == 0 || 2 * k == NZ) {
-            Z[k] = mk<T>(A.x, B.x);
-        } else {
-            Z[k] = mk<T>(A.x - B.y, A.y + B.x);
-            Z[NZ - k] = mk<T>(A.x + B.y, B.x - A.y);
+        if (ch == a.nin && a.derive_gz == 1) {
+            const C2<T> th = in[(size_t)a.ch_th * a.cs_in + off];
+            const T kz = (T)a.g.kz[k];
+            return mk<T>(-kz * th.y, kz * th.x);
+        }
+        return mk<T>((T)0, (T)0);
+    };
+    for (int lp = warp; lp < L * npin; lp += nwarp) {
+        const int l = lp / npin, p = lp - l * npin;
+        C2<T>* Z = inb + (size_t)lp * NZp;
+        for (int k = lane; k < nzh; k += 32) {
+            C2<T> A = mk<T>((T)0, (T)0), B = mk<T>((T)0, (T)0);
+            if (l < nl) {
+                const size_t off = (size_t)(line0 + l) * nzh + k;
+                A = chan_val(2 * p, off, k);
+                B = chan_val(2 * p + 1, off, k);
+            }
+            if (k == 0 || 2 * k == NZ) {
+                Z[padi<1>(k)] = mk<T>(A.x, B.x);
+            } else {
+                Z[padi<1>(k)] = mk<T>(A.x - B.y, A.y + B.x);
+                Z[padi<1>(NZ - k)] = mk<T>(A.x + B.y, B.x - A.y);
+            }
         }
     }
     __syncthreads();
-    fft_run<T, +1, EPT>(inb, 1, NZ, L * npin, a.plan, false);
+    fft_run<T, +1, EPT, false, 1>(inb, 1, NZp, L * npin, a.plan);
 
     auto val = [&](int l, int ch, int z) -> T {
-        const C2<T> v = inb[(size_t)(l * npin + (ch >> 1)) * NZ + z];
+        const C2<T> v = inb[(size_t)(l * npin + (ch >> 1)) * NZp + padi<1>(z)];
         return (ch & 1) ? v.y : v.x;
     };
+    const int npts = L * NZ;
+    const FastDiv fz = a.fd_nz;
 
     if (a.mode == ZM_TO_REAL) {
-        for (int e = threadIdx.x; e < L * NZ; e += blockDim.x) {
-            const int z = e % NZ, l = e / NZ;
+        for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+            const int l = (int)fz.div((unsigned)e), z = e - l * NZ;
             if (l >= nl) continue;
             const size_t line = (size_t)(line0 + l);
             for (int c = 0; c < a.nin; c++)
@@ -187,10 +206,9 @@ __global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) 
     // 2. real-space products
     T mu[6] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
     int bad = 0;
-    const int npts = L * NZ;
     T* breal = (T*)a.breal;
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-        const int z = e % NZ, l = e / NZ;
+        const int l = (int)fz.div((unsigned)e), z = e - l * NZ;
         T o[14];
 #pragma unroll
         for (int q = 0; q < 14; q++) o[q] = (T)0;
@@ -264,16 +282,18 @@ __global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) 
             }
         }
         if (a.nout > 0) {
-            for (int p = 0; p < npout; p++) {
-                const T hi = (2 * p + 1 < a.nout) ? o[2 * p + 1] : (T)0;
-                outb[(size_t)(l * npout + p) * NZ + z] = mk<T>(o[2 * p], hi);
+#pragma unroll
+            for (int pp = 0; pp < 7; pp++) {
+                if (pp < npout) {
+                    const T hi = (2 * pp + 1 < a.nout) ? o[2 * pp + 1] : (T)0;
+                    outb[(size_t)(l * npout + pp) * NZp + padi<1>(z)] = mk<T>(o[2 * pp], hi);
+                }
             }
         }
     }
     if (a.do_max) {
         __syncthreads();
-        // dedicated 6 x 32 scratch after the output pairs
-        T* red = reinterpret_cast<T*>(outb + (size_t)L * npout * NZ);
+        T* red = reinterpret_cast<T*>(outb + (size_t)L * npout * NZp);   // 6 x 32 scratch
         warp_block_max<T>(mu, 6, red);
         if (threadIdx.x < 6) {
             const double m = (double)red[threadIdx.x * 32];
@@ -285,23 +305,24 @@ __global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) 
     }
     if (a.nout == 0) return;
     __syncthreads();
-    fft_run<T, -1, EPT>(outb, 1, NZ, L * npout, a.plan, false);
+    fft_run<T, -1, EPT, false, 1>(outb, 1, NZp, L * npout, a.plan);
 
-    // 3. unpack the paired spectra, store kz < kz_keep
+    // 3. a warp per (line, output pair): unpack the paired spectra (D2Z of
+    //    each product), store kz < kz_keep
     const int kk = a.g.kz_keep;
     C2<T>* out = (C2<T>*)a.out;
     const T half = (T)0.5;
-    for (int e = threadIdx.x; e < L * npout * kk; e += blockDim.x) {
-        const int k = e % kk;
-        const int lp = e / kk;
-        const int p = lp % npout, l = lp / npout;
+    for (int lp = warp; lp < L * npout; lp += nwarp) {
+        const int l = lp / npout, p = lp - l * npout;
         if (l >= nl) continue;
-        const C2<T>* Z = outb + (size_t)(l * npout + p) * NZ;
-        const C2<T> zk = Z[k], zm = Z[k ? NZ - k : 0];
-        const size_t off = (size_t)(line0 + l) * nzh + k;
-        out[(size_t)(2 * p) * a.cs_out + off] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
-        if (2 * p + 1 < a.nout)
-            out[(size_t)(2 * p + 1) * a.cs_out + off] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
+        const C2<T>* Z = outb + (size_t)lp * NZp;
+        const size_t off0 = (size_t)(line0 + l) * nzh;
+        for (int k = lane; k < kk; k += 32) {
+            const C2<T> zk = Z[padi<1>(k)], zm = Z[padi<1>(k ? NZ - k : 0)];
+            out[(size_t)(2 * p) * a.cs_out + off0 + k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+            if (2 * p + 1 < a.nout)
+                out[(size_t)(2 * p + 1) * a.cs_out + off0 + k] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
+        }
     }
 }
 
@@ -315,9 +336,9 @@ __global__ void __launch_bounds__(256) k_zpass(const __grid_constant__ ZArgs a) 
 // GradPseudoPressure (:128-159) and axpyComplex (generic.cu:137-144) of
 // RungeKutta3 / ForwardEuler (hydro_mhd_advance.cu:79-248).
 // ---------------------------------------------------------------------------
-struct RKc { double a_u, b_u, a_s, b_s; };
-
-__device__ __forceinline__ void update_mode(const XfArgs& a, size_t gi, double2 X, double2 R, double dt) {
+// New state value of one mode (writes the RK scratch where the scheme needs
+// it).  In XM_DFIELD mode R goes to the output array and X is returned.
+__device__ __forceinline__ double2 step_value(const XfArgs& a, size_t gi, double2 X, double2 R, double dt) {
     const double g0 = 8.0 / 15.0, g1 = 5.0 / 12.0, g2 = 3.0 / 4.0, x0 = -17.0 / 60.0, x1 = -5.0 / 12.0;
     switch (a.mode) {
         case XM_RK0: {
@@ -325,32 +346,42 @@ __device__ __forceinline__ void update_mode(const XfArgs& a, size_t gi, double2 
             // reads the already-updated fields, hydro_mhd_advance.cu:119-122)
             const double bu = g0 * dt, bs = x0 * dt;
             const double2 Un = d2(1.0 * X.x + bu * R.x, 1.0 * X.y + bu * R.y);
-            a.U[gi] = Un;
             a.S[gi] = d2(1.0 * Un.x + bs * R.x, 1.0 * Un.y + bs * R.y);
-        } break;
+            return Un;
+        }
         case XM_RK1: {
             const double bu = g1 * dt, bs = x1 * dt;
             const double2 S = a.S[gi];
             const double2 Un = d2(1.0 * S.x + bu * R.x, 1.0 * S.y + bu * R.y);
-            a.U[gi] = Un;
             a.S[gi] = d2(1.0 * Un.x + bs * R.x, 1.0 * Un.y + bs * R.y);
-        } break;
+            return Un;
+        }
         case XM_RK2: {
             const double bu = g2 * dt;
             const double2 S = a.S[gi];
-            a.U[gi] = d2(1.0 * S.x + bu * R.x, 1.0 * S.y + bu * R.y);
-        } break;
+            return d2(1.0 * S.x + bu * R.x, 1.0 * S.y + bu * R.y);
+        }
         case XM_EULER:
-            a.U[gi] = d2(1.0 * X.x + dt * R.x, 1.0 * X.y + dt * R.y);
-            break;
+            return d2(1.0 * X.x + dt * R.x, 1.0 * X.y + dt * R.y);
         default:
             a.out[gi] = R;
-            break;
+            return X;
     }
 }
 
+// CleanDivergence (cuda_kernels_generic.cu:288-313) of a 3-vector at one mode.
+__device__ __forceinline__ void clean3(double2* V, double kx, double ky, double kz) {
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
+    const double sx = kx * V[0].x + ky * V[1].x + kz * V[2].x;
+    const double sy = kx * V[0].y + ky * V[1].y + kz * V[2].y;
+    V[0] = d2(V[0].x - kx * ik2 * sx, V[0].y - kx * ik2 * sy);
+    V[1] = d2(V[1].x - ky * ik2 * sx, V[1].y - ky * ik2 * sy);
+    V[2] = d2(V[2].x - kz * ik2 * sx, V[2].y - kz * ik2 * sy);
+}
+
 template <typename T, int EPT>
-__global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) {
+__global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
     const int N = a.g.nx, KT = a.kt, nzh = a.g.nzh;
@@ -372,10 +403,10 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
             buf[e] = (col < kt) ? src[base + (size_t)n * stride + k0 + col] : mk<T>((T)0, (T)0);
         }
         __syncthreads();
-        fft_run<T, -1, EPT>(buf, KT, 1, KT, a.plan, true);
+        fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);
     };
 
-    double2 usd[EPT];   // (cleaned) u_strat of each owned mode, for the theta group
+    double2 usd[EPT];   // u_strat of each owned mode, for the theta group
 #pragma unroll
     for (int u = 0; u < EPT; u++) usd[u] = d2(0.0, 0.0);
 
@@ -420,13 +451,6 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
             double2 X[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.VEL + c) * nc + gi];
-            if (a.clean) {
-                const double sx = kx * X[0].x + ky * X[1].x + kz * X[2].x;
-                const double sy = kx * X[0].y + ky * X[1].y + kz * X[2].y;
-                const double kk[3] = {kx, ky, kz};
-#pragma unroll
-                for (int c = 0; c < 3; c++) X[c] = d2(X[c].x - kk[c] * ik2 * sx, X[c].y - kk[c] * ik2 * sy);
-            }
             const bool m = nl_on && a.g.mx[n] != 0.0 && a.g.mz[k] != 0.0;
             double2 R[3];
 #pragma unroll
@@ -452,8 +476,15 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
             const double kk[3] = {kx, ky, kz};
 #pragma unroll
             for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
+            double2 Un[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) update_mode(a, (size_t)(a.VEL + c) * nc + gi, X[c], R[c], dt);
+            for (int c = 0; c < 3; c++) Un[c] = step_value(a, (size_t)(a.VEL + c) * nc + gi, X[c], R[c], dt);
+            if (a.mode != XM_DFIELD) {
+                // CleanFieldDivergence of the next step, applied to the new state
+                if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.U[(size_t)(a.VEL + c) * nc + gi] = Un[c];
+            }
         }
     }
 
@@ -495,15 +526,8 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
             double2 X[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.MAG + c) * nc + gi];
-            if (a.clean) {
-                const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
-                const double sx = kx * X[0].x + ky * X[1].x + kz * X[2].x;
-                const double sy = kx * X[0].y + ky * X[1].y + kz * X[2].y;
-                const double kk[3] = {kx, ky, kz};
-#pragma unroll
-                for (int c = 0; c < 3; c++) X[c] = d2(X[c].x - kk[c] * ik2 * sx, X[c].y - kk[c] * ik2 * sy);
-            }
             const bool m = nl_on && a.g.mx[n] != 0.0 && a.g.mz[k] != 0.0;
+            double2 Un[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const double2 s = to_d2(acc[u][c]);
@@ -512,7 +536,12 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
                     const double f = -a.nu_m * k2;
                     R = d2(R.x + f * X[c].x, R.y + f * X[c].y);
                 }
-                update_mode(a, (size_t)(a.MAG + c) * nc + gi, X[c], R, dt);
+                Un[c] = step_value(a, (size_t)(a.MAG + c) * nc + gi, X[c], R, dt);
+            }
+            if (a.mode != XM_DFIELD) {
+                if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.U[(size_t)(a.MAG + c) * nc + gi] = Un[c];
             }
         }
     }
@@ -567,7 +596,8 @@ __global__ void __launch_bounds__(256) k_xfwd(const __grid_constant__ XfArgs a) 
                     R = d2(R.x + f * X.x, R.y + f * X.y);
                 }
             }
-            update_mode(a, (size_t)a.TH * nc + gi, X, R, dt);
+            const double2 Un = step_value(a, (size_t)a.TH * nc + gi, X, R, dt);
+            if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
         }
     }
 }
@@ -591,7 +621,8 @@ __global__ void k_heat(const __grid_constant__ XfArgs a) {
             const double f = -a.nu_th * (kx * kx + ky * ky + kz * kz);
             R = d2(f * X.x, f * X.y);
         }
-        update_mode(a, (size_t)a.TH * nc + gi, X, R, dt);
+        const double2 Un = step_value(a, (size_t)a.TH * nc + gi, X, R, dt);
+        if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
     }
 }
 
@@ -773,7 +804,7 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
 // Anisotropic conduction STS stage: x-forward of the heat-flux channels,
 // DivergenceMask (generic.cu:315-334) into dtheta, then the stage update.
 template <typename T, int EPT>
-__global__ void __launch_bounds__(256) k_xfwd_rkl(const __grid_constant__ RklArgs a, double2* U, int vslot) {
+__global__ void __launch_bounds__(256, 2) k_xfwd_rkl(const __grid_constant__ RklArgs a, double2* U, int vslot) {
     if (a.stage > a.sc->s_rkl) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
@@ -798,7 +829,7 @@ __global__ void __launch_bounds__(256) k_xfwd_rkl(const __grid_constant__ RklArg
                 buf[e] = (col < kt) ? src[base + (size_t)n * stride + k0 + col] : mk<T>((T)0, (T)0);
             }
             __syncthreads();
-            fft_run<T, -1, EPT>(buf, KT, 1, KT, a.plan, true);
+            fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);
 #pragma unroll
             for (int u = 0; u < EPT; u++) {
                 const int e = tid + u * nthr;

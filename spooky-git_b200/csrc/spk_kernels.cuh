@@ -19,6 +19,28 @@
 
 namespace spk {
 
+// Division by a runtime constant d >= 1 for x < 2^31: q = (umulhi(x, m) + x) >> l
+// with l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1 (Granlund and
+// Montgomery, PLDI 1994, round-up method).
+struct FastDiv {
+    unsigned m, l;
+    __host__ __device__ inline unsigned div(unsigned x) const {
+#ifdef __CUDA_ARCH__
+        return (__umulhi(x, m) + x) >> l;
+#else
+        return (unsigned)(((unsigned long long)x * m >> 32) + x) >> l;
+#endif
+    }
+    static FastDiv make(unsigned d) {
+        FastDiv f;
+        unsigned l = 0;
+        while ((1ull << l) < d) l++;
+        f.l = l;
+        f.m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+        return f;
+    }
+};
+
 struct DevGrid {
     int nx, ny, nz, nzh;
     int kz_keep;                    // kz index k is inside the 2/3 mask iff k < kz_keep
@@ -85,6 +107,7 @@ struct ZArgs {
     double* real_out;       // ZM_TO_REAL: [nin][nx*ny*nz] FP64
     const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
     int gate_stage;
+    FastDiv fd_nz;          // division by NZ
 };
 
 enum XMode { XM_RK0 = 0, XM_RK1 = 1, XM_RK2 = 2, XM_EULER = 3, XM_DFIELD = 4 };

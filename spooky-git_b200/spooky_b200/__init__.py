@@ -95,6 +95,14 @@ def c_defaults():
     return p
 
 
+def _torch_sync():
+    """Finish torch's queued work (tensors passed in may still be in flight)."""
+    import sys
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.synchronize()
+
+
 def _ptr(a):
     """(address, where) for a torch CUDA tensor (0) or numpy array (1)."""
     if hasattr(a, "data_ptr"):
@@ -139,6 +147,8 @@ class Context:
 
     # -- state ---------------------------------------------------------------
     def set_state(self, U):
+        if hasattr(U, "is_cuda") and U.is_cuda:
+            _torch_sync()
         if not hasattr(U, "data_ptr"):
             U = np.ascontiguousarray(U, dtype=np.complex128)
             assert U.size == self.F * self.nc
@@ -172,8 +182,12 @@ class Context:
         return np.array([x.value for x in o])
 
     def compute_dfield(self, U, dU):
-        """U, dU: torch CUDA complex128 tensors of shape_c."""
+        """U, dU: torch CUDA complex128 tensors of shape_c.  Waits for torch's
+        current stream before and for the context stream after, so the
+        tensors can be used on either side without further synchronisation."""
+        _torch_sync()
         self._check(lib().spk_compute_dfield(self._h, U.data_ptr(), dU.data_ptr()))
+        self.synchronize()
 
     def advance(self, nsteps=1):
         self._check(lib().spk_advance(self._h, int(nsteps)))
@@ -184,8 +198,10 @@ class Context:
         return s.value
 
     def to_real(self, R):
-        """R: torch CUDA float64 tensor of shape_r."""
+        """R: torch CUDA float64 tensor of shape_r (complete on return)."""
+        _torch_sync()
         self._check(lib().spk_to_real(self._h, R.data_ptr()))
+        self.synchronize()
 
     def synchronize(self):
         self._check(lib().spk_synchronize(self._h))
