@@ -4,6 +4,8 @@
 // Supervisor/Fields/TimeStepping/RKLegendre; every step is recorded once
 // into a CUDA graph (two graphs when RKL2 alternates before/after RK3) and
 // replayed without host synchronisation.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -67,9 +69,11 @@ struct spk_ctx {
     std::string err;
     int sticky;
     long launches;                 // kernels issued (counted by the launch helpers)
-    bool bad_job;                  // a pass was built with an out-of-range channel
+    bool bad_job;                  // a pass could not be built (channel range, tensor map)
+    const char* bad_why;
     const void* user_U;            // caller's state array during spk_compute_dfield
     bool dirty;                    // state set from outside: clean u, B before the next step
+    int num_sms;
     int kernels_per_step[2];
 };
 
@@ -89,31 +93,22 @@ static int fail(spk_ctx* c, int code, const std::string& msg) {
 // buffer addressing
 // ---------------------------------------------------------------------------
 static size_t csize(const spk_ctx* c) { return c->fp32 ? sizeof(float2) : sizeof(double2); }
-// Channel ch of a pass buffer; channels outside the buffer abort the launch
+static size_t chan_bytes(const spk_ctx* c) { return c->g.ncs * csize(c); }
+static int buf_channels(const spk_ctx* c, const void* base) {
+    return (base == c->rA || base == c->rB) ? 3 : c->nbuf_ch;
+}
+// Channel ch of a pass buffer; channels outside the buffer give nullptr
 // (add_job / zpass refuse null pointers) instead of addressing other memory.
 static void* chan(const spk_ctx* c, void* base, int ch) {
-    const int nch = (base == c->rA || base == c->rB) ? 3 : c->nbuf_ch;
-    if (!base || ch < 0 || ch >= nch) return nullptr;
-    return (char*)base + (size_t)ch * c->nc * csize(c);
-}
-
-static AxisArgs axis_args(spk_ctx* c, int ax) {
-    AxisArgs a;
-    memset(&a, 0, sizeof(a));
-    a.g = c->g;
-    a.plan = ax == 0 ? c->plan_x : c->plan_y;
-    a.axis = ax;
-    a.kcols = c->nzh;
-    a.cs_in = a.cs_out = c->nc;
-    a.scale = 1.0;
-    return a;
+    if (!base || ch < 0 || ch >= buf_channels(c, base)) return nullptr;
+    return (char*)base + (size_t)ch * chan_bytes(c);
 }
 
 // True when [p, p + nch channels) lies inside one of the context's arrays.
 static bool span_ok(const spk_ctx* c, const void* p, int nch, bool state) {
     if (!p || nch < 1) return false;
     const char* q = (const char*)p;
-    const size_t cb = state ? c->nc * sizeof(double2) : c->nc * csize(c);
+    const size_t cb = state ? c->nc * sizeof(double2) : chan_bytes(c);
     const size_t need = (size_t)nch * cb;
     auto inside = [&](const void* base, size_t bytes) {
         const char* b = (const char*)base;
@@ -125,6 +120,71 @@ static bool span_ok(const spk_ctx* c, const void* p, int nch, bool state) {
            inside(c->rA, 3 * cb) || inside(c->rB, 3 * cb);
 }
 
+// The array a channel pointer belongs to: (base, channels, channel index).
+static bool locate(const spk_ctx* c, const void* p, bool state, const void** base, int* nchan, int* ch) {
+    const char* q = (const char*)p;
+    if (state) {
+        const void* cands[2] = {c->U, c->user_U};
+        for (const void* b : cands) {
+            if (!b) continue;
+            const size_t cb = c->nc * sizeof(double2);
+            if (q >= (const char*)b && q < (const char*)b + (size_t)c->F * cb && (size_t)(q - (const char*)b) % cb == 0) {
+                *base = b; *nchan = c->F; *ch = (int)((q - (const char*)b) / cb);
+                return true;
+            }
+        }
+        return false;
+    }
+    const void* cands[4] = {c->bufA, c->bufB, c->rA, c->rB};
+    for (const void* b : cands) {
+        if (!b) continue;
+        const size_t cb = chan_bytes(c);
+        if (cb == 0) return false;
+        const int n = buf_channels(c, b);
+        if (q >= (const char*)b && q < (const char*)b + (size_t)n * cb && (size_t)(q - (const char*)b) % cb == 0) {
+            *base = b; *nchan = n; *ch = (int)((q - (const char*)b) / cb);
+            return true;
+        }
+    }
+    return false;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+// 4-D tensor map [channel][x][y][k scalars] of a state array (FP64, rows of
+// nzh complex) or a pass buffer (pass type, rows of nzs complex, logical
+// extent nzh so that k >= nzh reads as zero), box = KT columns x box_rows
+// positions along the axis.
+static bool make_tmap(const spk_ctx* c, const void* base, int nchan, bool state, int axis, int kt, int box_rows,
+                      CUtensorMap* tm) {
+    if (!g_encode) return false;
+    const bool f64 = state || !c->fp32;
+    const size_t esz = f64 ? 8 : 4;
+    const size_t row = state ? (size_t)c->nzh : (size_t)c->g.nzs;
+    cuuint64_t dims[4] = {(cuuint64_t)(2 * c->nzh), (cuuint64_t)c->ny, (cuuint64_t)c->nx, (cuuint64_t)nchan};
+    cuuint64_t strides[3] = {(cuuint64_t)(2 * row * esz), (cuuint64_t)(2 * row * esz * c->ny),
+                             (cuuint64_t)(2 * row * esz * c->ny * c->nx)};
+    cuuint32_t box[4];
+    if (axis == 0) { box[0] = 2 * kt; box[1] = 1; box[2] = box_rows; box[3] = 1; }
+    else           { box[0] = 2 * kt; box[1] = box_rows; box[2] = 1; box[3] = 1; }
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = g_encode(tm, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                          const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+static AxisArgs axis_args(spk_ctx* c, int ax) {
+    AxisArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->g;
+    a.plan = ax == 0 ? c->plan_x : c->plan_y;
+    a.axis = ax;
+    a.kcols = c->nzh;
+    a.scale = 1.0;
+    return a;
+}
 
 // ---------------------------------------------------------------------------
 // FFT plans: radices from {16 (FP32 only), 8, 4, 2, 3, 5}; twiddles in long double.
@@ -158,15 +218,15 @@ static inline int rup32(long x) { return (int)(((x + 31) / 32) * 32); }
 
 struct AxisCfg { int kt; int nthr; size_t smem; };
 
-static AxisCfg axis_cfg(const spk_ctx* c, int N) {
+static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     AxisCfg a;
     const int ept = c->fp32 ? EPT_AXIS_F : EPT_AXIS_D;
-    int kt = c->fp32 ? 16 : 8;
-    while (kt > 1 && (long)N * kt > (long)MAXT * ept) kt /= 2;
-    while (kt > 1 && kt > c->nzh) kt /= 2;    // power of two (the pass masks and shifts by it)
+    int kt = (c->fp32 && !state_in) ? 16 : 8;    // 128-byte row segments of the input
+    while (kt > 2 && (long)N * kt > (long)MAXT * ept) kt /= 2;
+    while (kt > 2 && kt > c->nzh) kt /= 2;       // power of two, >= 2 (16-byte TMA rows in FP32)
     a.kt = kt;
     a.nthr = std::max(32, std::min(MAXT, rup32(((long)N * kt + ept - 1) / ept)));
-    a.smem = (size_t)N * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
+    a.smem = 0;
     return a;
 }
 
@@ -204,22 +264,40 @@ static ZCfg z_cfg(const spk_ctx* c, int nin_all, int nout) {
 }
 
 template <typename T>
-static void launch_axis(spk_ctx* c, AxisArgs& a, int dir, int outer) {
-    const AxisCfg cf = axis_cfg(c, a.plan.n);
-    a.kt = cf.kt;
-    dim3 grid((a.kcols + cf.kt - 1) / cf.kt, outer, a.njobs);
+static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
     constexpr int ept = sizeof(T) == 4 ? EPT_AXIS_F : EPT_AXIS_D;
+    const int N = a.plan.n;
+    const int nthr = std::max(32, std::min(MAXT, rup32(((long)N * a.kt + ept - 1) / ept)));
+    const size_t in_elem = a.convert ? sizeof(double2) : sizeof(C2<T>);
+    const size_t stage = (((size_t)N * a.kt * in_elem) + 127) & ~(size_t)127;
+    a.nst = (int)std::max<size_t>(2, std::min<size_t>(4, 98304 / stage));
+    size_t smem = 256 + a.nst * stage + (a.convert ? (size_t)N * a.kt * sizeof(C2<T>) : 0);
+    while (a.nst > 2 && smem > 200 * 1024) { a.nst--; smem -= stage; }
+    const int nouter = a.axis == 0 ? c->ny : c->nx;
+    const long total = (long)a.njobs * nouter * ((a.kcols + a.kt - 1) / a.kt);
+    if (total <= 0) return;
+    a.err = &c->sc->err;
+    int per_sm = 1;
+    if (dir > 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis<T, +1, ept>, nthr, smem);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis<T, -1, ept>, nthr, smem);
+    const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
     c->launches++;
-    if (dir > 0) k_axis<T, +1, ept><<<grid, cf.nthr, cf.smem, c->stream>>>(a);
-    else k_axis<T, -1, ept><<<grid, cf.nthr, cf.smem, c->stream>>>(a);
+    if (dir > 0) k_axis<T, +1, ept><<<grid, nthr, smem, c->stream>>>(a);
+    else k_axis<T, -1, ept><<<grid, nthr, smem, c->stream>>>(a);
 }
 
 static void axis(spk_ctx* c, AxisArgs& a, int dir) {
-    if (c->bad_job) { c->err = "internal: a pass job addressed a channel outside its buffer"; c->sticky = SPK_ERR_ARG; return; }
+    if (c->bad_job) {
+        char buf[256];
+        snprintf(buf, sizeof(buf), " (axis %d, jobs %d, nbuf_ch %d, ncs %zu, nc %zu)", a.axis, a.njobs, c->nbuf_ch,
+                 (size_t)c->g.ncs, (size_t)c->nc);
+        c->err = std::string("internal: ") + c->bad_why + buf;
+        c->sticky = SPK_ERR_ARG;
+        return;
+    }
     if (a.njobs == 0) return;
-    const int outer = a.axis == 0 ? c->ny : c->nx;
-    if (c->fp32) launch_axis<float>(c, a, dir, outer);
-    else launch_axis<double>(c, a, dir, outer);
+    if (c->fp32) launch_axis<float>(c, a, dir);
+    else launch_axis<double>(c, a, dir);
 }
 
 static void zpass(spk_ctx* c, ZArgs& z) {
@@ -252,13 +330,45 @@ static int ew_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 1
 // ---------------------------------------------------------------------------
 // argument builders
 // ---------------------------------------------------------------------------
+// nch consecutive channels from `in` (state array or pass buffer) to `out`,
+// one job (and one tensor map) per channel.
 static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch, int in_state, int deriv, int clean) {
-    if (!span_ok(c, in, nch, in_state != 0) || !span_ok(c, out, nch, false) || a.njobs >= SPK_MAXJOBS) {
+    (void)clean;
+    const void* base;
+    int nchan, ch0;
+    const char* why = nullptr;
+    if (!span_ok(c, in, nch, in_state != 0)) why = "pass job input outside its array";
+    else if (!span_ok(c, out, nch, false)) why = "pass job output outside its buffer";
+    else if (a.njobs + nch > SPK_MAXJOBS) why = "too many pass jobs";
+    else if (!locate(c, in, in_state != 0, &base, &nchan, &ch0)) why = "pass job input not at a channel boundary";
+    if (why) {
         c->bad_job = true;
+        c->bad_why = why;
         return;
     }
-    AxisJob& j = a.job[a.njobs++];
-    j.in = in; j.out = out; j.nch = nch; j.in_state = in_state; j.deriv = deriv; j.clean = clean;
+    const int N = a.plan.n;
+    const AxisCfg cf = axis_cfg(c, N, in_state != 0);
+    if (a.njobs > 0 && a.kt != cf.kt) { c->bad_job = true; c->bad_why = "jobs of one pass need one tile width"; return; }
+    a.kt = cf.kt;
+    a.box_rows = N;                               // rows per TMA box: a divisor of N, <= 256
+    while (a.box_rows > 256) {
+        int d = 256;
+        while (N % d) d--;
+        a.box_rows = d;
+    }
+    if (in_state && c->fp32) a.convert = 1;
+    for (int q = 0; q < nch; q++) {
+        AxisJob& j = a.job[a.njobs++];
+        if (!make_tmap(c, base, nchan, in_state != 0, a.axis, a.kt, a.box_rows, &j.tm)) {
+            c->bad_job = true;
+            c->bad_why = "cuTensorMapEncodeTiled rejected a pass tensor map";
+            return;
+        }
+        j.out = (char*)out + (size_t)q * chan_bytes(c);
+        j.ch = ch0 + q;
+        j.in_state = in_state;
+        j.deriv = deriv;
+    }
 }
 
 // first inverse pass over the state: fields in order, cleaning u and B when asked
@@ -288,8 +398,8 @@ static ZArgs z_args(spk_ctx* c) {
     memset(&z, 0, sizeof(z));
     z.g = c->g;
     z.plan = c->plan_z;
-    z.in = c->bufB; z.cs_in = c->nc;
-    z.out = c->bufA; z.cs_out = c->nc;
+    z.in = c->bufB; z.cs_in = c->g.ncs;
+    z.out = c->bufA; z.cs_out = c->g.ncs;
     z.ch_u = z.ch_b = z.ch_th = z.ch_gx = z.ch_gy = -1;
     z.maxbits = c->sc->maxbits;
     z.nonfinite = &c->sc->nonfinite;
@@ -341,7 +451,7 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     memset(&x, 0, sizeof(x));
     x.g = c->g;
     x.plan = c->plan_x;
-    x.nl = c->bufB; x.cs_nl = c->nc;
+    x.nl = c->bufB; x.cs_nl = c->g.ncs;
     x.nl_T = c->out_T; x.nl_E = c->out_E; x.nl_F = c->out_F; x.nl_Q = c->out_Q;
     x.U = U; x.S = c->S; x.out = nullptr;
     x.F = c->F; x.VEL = c->VEL; x.MAG = c->MAG; x.TH = c->TH;
@@ -381,7 +491,7 @@ static RklArgs rkl_args(spk_ctx* c, int stage) {
     memset(&r, 0, sizeof(r));
     r.g = c->g;
     r.plan = c->plan_x;
-    r.nl = c->rB; r.cs_nl = c->nc;
+    r.nl = c->rB; r.cs_nl = c->g.ncs;
     r.Uc0 = c->Uc0; r.Uc1 = c->Uc1; r.dU0 = c->dU0;
     r.stage = stage;
     r.nsts = c->nsts;
@@ -665,6 +775,20 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
 static int ctx_alloc(spk_ctx* c) {
     const size_t nc = c->nc;
     const size_t cs = csize(c);
+    // device properties and the tensor-map encoder (driver entry point,
+    // resolved through the runtime: no link-time dependency on libcuda)
+    {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+        if (!g_encode) {
+            cudaDriverEntryPointQueryResult q;
+            void* fn = nullptr;
+            CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+            if (q != cudaDriverEntryPointSuccess || !fn) return fail(c, SPK_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+            g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+        }
+    }
     // tables
     CK(cudaMalloc(&c->d_tab, sizeof(double) * (2 * ((size_t)c->nx + c->ny + c->nzh))));
     double* t = c->d_tab;
@@ -676,6 +800,8 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMemcpy(m + c->nx, c->my.data(), sizeof(double) * c->ny, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(m + c->nx + c->ny, c->mz.data(), sizeof(double) * c->nzh, cudaMemcpyHostToDevice));
     c->g.nx = c->nx; c->g.ny = c->ny; c->g.nz = c->nz; c->g.nzh = c->nzh;
+    c->g.nzs = c->nzh + (c->nzh & 1);            // even rows: 16-byte TMA strides in FP32
+    c->g.ncs = (size_t)c->nx * c->ny * c->g.nzs;
     c->g.kz_keep = c->kz_keep; c->g.nc = nc;
     c->g.kx = t; c->g.ky = t + c->nx; c->g.kz = t + c->nx + c->ny;
     c->g.mx = m; c->g.my = m + c->nx; c->g.mz = m + c->nx + c->ny;
@@ -704,10 +830,10 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMemset(c->U, 0, sizeof(double2) * nc * c->F));
     CK(cudaMemset(c->S, 0, sizeof(double2) * nc * c->F));
     if (c->p.incompressible) {
-        CK(cudaMalloc(&c->bufA, cs * nc * c->nbuf_ch));
-        CK(cudaMalloc(&c->bufB, cs * nc * c->nbuf_ch));
-        CK(cudaMemset(c->bufA, 0, cs * nc * c->nbuf_ch));
-        CK(cudaMemset(c->bufB, 0, cs * nc * c->nbuf_ch));
+        CK(cudaMalloc(&c->bufA, cs * c->g.ncs * c->nbuf_ch));
+        CK(cudaMalloc(&c->bufB, cs * c->g.ncs * c->nbuf_ch));
+        CK(cudaMemset(c->bufA, 0, cs * c->g.ncs * c->nbuf_ch));
+        CK(cudaMemset(c->bufB, 0, cs * c->g.ncs * c->nbuf_ch));
     }
     if (c->nsts > 0) {
         CK(cudaMalloc(&c->Uc0, sizeof(double2) * nc * c->nsts));
@@ -718,10 +844,10 @@ static int ctx_alloc(spk_ctx* c) {
         CK(cudaMemset(c->dU0, 0, sizeof(double2) * nc * c->nsts));
     }
     if (c->sts_aniso) {
-        CK(cudaMalloc(&c->rA, cs * nc * 3));
-        CK(cudaMalloc(&c->rB, cs * nc * 3));
-        CK(cudaMemset(c->rA, 0, cs * nc * 3));
-        CK(cudaMemset(c->rB, 0, cs * nc * 3));
+        CK(cudaMalloc(&c->rA, cs * c->g.ncs * 3));
+        CK(cudaMalloc(&c->rB, cs * c->g.ncs * 3));
+        CK(cudaMemset(c->rA, 0, cs * c->g.ncs * 3));
+        CK(cudaMemset(c->rB, 0, cs * c->g.ncs * 3));
         CK(cudaMalloc(&c->breal, (c->fp32 ? sizeof(float) : sizeof(double)) * c->nr * 3));
     }
     CK(cudaMalloc(&c->sc, sizeof(DevScalars)));
@@ -777,7 +903,7 @@ extern "C" int spk_ctx_create(const spk_params_t* p, void* stream, spk_ctx** out
     c->d_tab = nullptr; c->d_tw = nullptr; c->U = c->S = nullptr; c->bufA = c->bufB = nullptr;
     c->rA = c->rB = c->breal = nullptr; c->Uc0 = c->Uc1 = c->dU0 = nullptr; c->sc = nullptr;
     c->h_sc = nullptr; c->d_sums = nullptr; c->h_sums = nullptr; c->h_step = 0; c->sticky = 0;
-    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->user_U = nullptr; c->dirty = true;
+    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->bad_why = ""; c->user_U = nullptr; c->dirty = true;
     rc = ctx_init(c, p, stream);
     if (rc != SPK_OK) { delete c; return rc; }
     rc = ctx_alloc(c);

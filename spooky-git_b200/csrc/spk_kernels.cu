@@ -17,83 +17,131 @@ template <typename T> __device__ __forceinline__ C2<T> from_d2(double2 v) { retu
 template <typename V> __device__ __forceinline__ double2 to_d2(V v) { return d2((double)v.x, (double)v.y); }
 
 // ---------------------------------------------------------------------------
-// Strided-axis pass (x or y).  Tile = one outer index, KT consecutive k
-// columns (KT a power of two), all N positions along the axis; coalesced
-// KT-wide row segments.  Fuses ComplexVecAssign + scaleKernel
-// (cufft_routines.cu:23-39) and the i*k derivative of Gradient
-// (cuda_kernels_generic.cu:249-260) into the load of the inverse passes.
-// Each thread issues its EPT loads before the first shared-memory store.
+// Strided-axis pass (x or y), persistent and pipelined.  Tile = one channel,
+// one outer index, KT consecutive k columns, all N positions along the axis
+// ([N][KT] in shared memory, the TMA box layout).  Thread 0 keeps nst tiles
+// in flight with cp.async.bulk.tensor loads completing on per-stage
+// mbarriers; the CTA transforms the oldest tile and stores it.  Fuses
+// ComplexVecAssign + scaleKernel (cufft_routines.cu:23-39) and the i*k
+// derivative of Gradient (cuda_kernels_generic.cu:249-260) into the
+// pre-transform pass over shared memory.
 // ---------------------------------------------------------------------------
+#define SPK_WAIT_ITERS (1u << 24)
+
 template <typename T, int DIR, int EPT>
 __global__ void __launch_bounds__(256, 2) k_axis(const __grid_constant__ AxisArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
-    const AxisJob& job = a.job[blockIdx.z];
-    const int N = a.plan.n, KT = a.kt, lkt = ilog2(KT), nzh = a.g.nzh;
-    const int k0 = blockIdx.x * KT;
-    const int o = blockIdx.y;
-    const int kt = min(KT, a.kcols - k0);
-    size_t stride, base;
-    if (a.axis == 0) { stride = (size_t)a.g.ny * nzh; base = (size_t)o * nzh; }
-    else             { stride = (size_t)nzh;          base = (size_t)o * a.g.ny * nzh; }
-    base += k0;
-    const double* kax = a.axis == 0 ? a.g.kx : a.g.ky;
-    const double* max_ = a.axis == 0 ? a.g.mx : a.g.my;
+    const int N = a.plan.n, KT = a.kt, lkt = ilog2(KT), NST = a.nst;
     const int nel = N * KT;
     const int nthr = blockDim.x, tid = threadIdx.x;
+    const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
+    const int nkb = (a.kcols + KT - 1) / KT;
+    const int total = a.njobs * nouter * nkb;
+    const size_t in_elem = a.convert ? sizeof(double2) : sizeof(C2<T>);
+    const size_t stage_bytes = ((size_t)nel * in_elem + 127) & ~(size_t)127;
+    // 128-byte aligned base: NST barriers, then the stage buffers
+    unsigned char* sbase = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sbase);
+    unsigned char* stages = sbase + 128;
+    C2<T>* wbuf = reinterpret_cast<C2<T>*>(stages + (size_t)NST * stage_bytes);   // when converting
+    const double* kax = a.axis == 0 ? a.g.kx : a.g.ky;
+    const double* max_ = a.axis == 0 ? a.g.mx : a.g.my;
+    const size_t stride = a.axis == 0 ? (size_t)a.g.ny * a.g.nzs : (size_t)a.g.nzs;
+    const uint32_t tile_bytes = (uint32_t)((size_t)nel * in_elem);
+    const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
-    for (int c = 0; c < job.nch; c++) {
-        C2<T> v[EPT];
-        if (job.in_state) {
-            const double2* in = (const double2*)job.in + (size_t)c * a.cs_in + base;
-            double2 x[EPT];
+    auto issue = [&](int t, int s) {
+        const int jb = t / (nouter * nkb);
+        const int rem = t - jb * nouter * nkb;
+        const int o = rem / nkb, kb = rem - o * nkb;
+        const AxisJob& jo = a.job[jb];
+        unsigned char* dst = stages + (size_t)s * stage_bytes;
+        mbar_expect_tx(&bar[s], tile_bytes);
+        for (int b = 0; b < N / a.box_rows; b++) {
+            if (a.axis == 0) tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, o, b * a.box_rows, jo.ch);
+            else             tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, b * a.box_rows, o, jo.ch);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int s = 0; s < NST; s++) {
+            const int t = blockIdx.x + s * gridDim.x;
+            if (t < total) issue(t, s);
+        }
+
+    int i = 0;
+    bool aborted = false;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, i++) {
+        const int s = i % NST;
+        const uint32_t par = (uint32_t)((i / NST) & 1);
+        const bool ok = mbar_wait(&bar[s], par, SPK_WAIT_ITERS);
+        if (__syncthreads_or(!ok)) { aborted = true; break; }
+        const int jb = t / (nouter * nkb);
+        const int rem = t - jb * nouter * nkb;
+        const int o = rem / nkb, kb = rem - o * nkb;
+        const AxisJob& jo = a.job[jb];
+        const int k0 = kb * KT;
+        const int kt = min(KT, a.kcols - k0);
+        unsigned char* stg = stages + (size_t)s * stage_bytes;
+        C2<T>* work;
+        const int tn = t + NST * gridDim.x;
+        if (a.convert) {
+            // FP64 state -> pass type, with the scale and the derivative
+            const double2* src = reinterpret_cast<const double2*>(stg);
 #pragma unroll
             for (int u = 0; u < EPT; u++) {
                 const int e = tid + u * nthr;
-                const int n = e >> lkt, col = e & (KT - 1);
-                x[u] = (e < nel && col < kt) ? __ldg(in + (size_t)n * stride + col) : d2(0.0, 0.0);
+                if (e < nel) {
+                    double2 x = src[e];
+                    if (jo.deriv) x = ik_mul(kax[e >> lkt], x);
+                    wbuf[e] = mk<T>((T)(x.x * a.scale), (T)(x.y * a.scale));
+                }
             }
-#pragma unroll
-            for (int u = 0; u < EPT; u++) {
-                const int e = tid + u * nthr;
-                const int n = min(e >> lkt, N - 1);
-                double2 y = x[u];
-                if (job.deriv) y = ik_mul(kax[n], y);
-                v[u] = mk<T>((T)(y.x * a.scale), (T)(y.y * a.scale));
-            }
+            __syncthreads();
+            if (tid == 0 && tn < total) issue(tn, s);   // the stage was only read
+            work = wbuf;
         } else {
-            const C2<T>* in = (const C2<T>*)job.in + (size_t)c * a.cs_in + base;
-#pragma unroll
-            for (int u = 0; u < EPT; u++) {
-                const int e = tid + u * nthr;
-                const int n = e >> lkt, col = e & (KT - 1);
-                v[u] = (e < nel && col < kt) ? in[(size_t)n * stride + col] : mk<T>((T)0, (T)0);
-            }
-            if (job.deriv || a.scale != 1.0) {
+            work = reinterpret_cast<C2<T>*>(stg);
+            if (jo.deriv || a.scale != 1.0) {
+                const T sc = (T)a.scale;
 #pragma unroll
                 for (int u = 0; u < EPT; u++) {
                     const int e = tid + u * nthr;
-                    const int n = min(e >> lkt, N - 1);
-                    if (job.deriv) { const T k = (T)kax[n]; v[u] = mk<T>(-k * v[u].y, k * v[u].x); }
-                    if (a.scale != 1.0) v[u] = cscale((T)a.scale, v[u]);
+                    if (e < nel) {
+                        C2<T> v = work[e];
+                        if (jo.deriv) { const T kk = (T)kax[e >> lkt]; v = mk<T>(-kk * v.y, kk * v.x); }
+                        work[e] = mk<T>(v.x * sc, v.y * sc);
+                    }
                 }
+                __syncthreads();
             }
         }
-#pragma unroll
-        for (int u = 0; u < EPT; u++) {
-            const int e = tid + u * nthr;
-            if (e < nel) buf[e] = v[u];
-        }
-        __syncthreads();
-        fft_run<T, DIR, EPT, true, 0>(buf, KT, 1, KT, a.plan);
-        C2<T>* out = (C2<T>*)job.out + (size_t)c * a.cs_out + base;
+        fft_run<T, DIR, EPT, true, 0>(work, KT, 1, KT, a.plan);
+        size_t base = a.axis == 0 ? (size_t)o * a.g.nzs : (size_t)o * a.g.ny * a.g.nzs;
+        C2<T>* out = (C2<T>*)jo.out + base + k0;
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
             const int e = tid + u * nthr;
             const int n = e >> lkt, col = e & (KT - 1);
             if (e < nel && col < kt && (!a.row_filter || max_[n] != 0.0))
-                out[(size_t)n * stride + col] = buf[e];
+                out[(size_t)n * stride + col] = work[e];
+        }
+        fence_proxy_async_smem();   // this thread's writes to the stage precede the next TMA fill
+        __syncthreads();
+        if (!a.convert && tid == 0 && tn < total) issue(tn, s);
+    }
+    if (aborted) {
+        // a load never completed: report it, then give every stage a bounded
+        // chance to drain before the shared memory is released
+        if (tid == 0) {
+            atomicExch(a.err, 2);
+            for (int s = 0; s < NST; s++) mbar_wait(&bar[s], (uint32_t)(((i + s) / NST) & 1), SPK_WAIT_ITERS);
         }
         __syncthreads();
     }
@@ -133,7 +181,7 @@ __device__ __forceinline__ void warp_block_max(T* v, int n, T* red) {
 template <typename T, int EPT>
 __global__ void __launch_bounds__(256, 2) k_zpass(const __grid_constant__ ZArgs a) {
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int NZ = a.g.nz, nzh = a.g.nzh, L = a.lines, NZp = padded_len(NZ);
     const int nlines = a.g.nx * a.g.ny;
     const int line0 = blockIdx.x * L;
@@ -170,7 +218,7 @@ __global__ void __launch_bounds__(256, 2) k_zpass(const __grid_constant__ ZArgs 
         for (int k = lane; k < nzh; k += 32) {
             C2<T> A = mk<T>((T)0, (T)0), B = mk<T>((T)0, (T)0);
             if (l < nl) {
-                const size_t off = (size_t)(line0 + l) * nzh + k;
+                const size_t off = (size_t)(line0 + l) * a.g.nzs + k;
                 A = chan_val(2 * p, off, k);
                 B = chan_val(2 * p + 1, off, k);
             }
@@ -316,7 +364,7 @@ __global__ void __launch_bounds__(256, 2) k_zpass(const __grid_constant__ ZArgs 
         const int l = lp / npout, p = lp - l * npout;
         if (l >= nl) continue;
         const C2<T>* Z = outb + (size_t)lp * NZp;
-        const size_t off0 = (size_t)(line0 + l) * nzh;
+        const size_t off0 = (size_t)(line0 + l) * a.g.nzs;
         for (int k = lane; k < kk; k += 32) {
             const C2<T> zk = Z[padi<1>(k)], zm = Z[padi<1>(k ? NZ - k : 0)];
             out[(size_t)(2 * p) * a.cs_out + off0 + k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
@@ -382,7 +430,7 @@ __device__ __forceinline__ void clean3(double2* V, double kx, double ky, double 
 
 template <typename T, int EPT>
 __global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
     const int N = a.g.nx, KT = a.kt, nzh = a.g.nzh;
     const size_t nc = a.g.nc;
@@ -396,11 +444,20 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs 
     const int nel = N * KT;
     const C2<T>* nl = (const C2<T>*)a.nl;
 
+    const size_t nstride = (size_t)a.g.ny * a.g.nzs, nbase = (size_t)j * a.g.nzs + k0;   // pass buffers
     auto load_fft = [&](int ch) {
-        const C2<T>* src = nl + (size_t)ch * a.cs_nl;
-        for (int e = tid; e < nel; e += nthr) {
+        const C2<T>* src = nl + (size_t)ch * a.cs_nl + nbase;
+        C2<T> v[EPT];
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = tid + u * nthr;
             const int n = e / KT, col = e - n * KT;
-            buf[e] = (col < kt) ? src[base + (size_t)n * stride + k0 + col] : mk<T>((T)0, (T)0);
+            v[u] = (e < nel && col < kt) ? src[(size_t)n * nstride + col] : mk<T>((T)0, (T)0);
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = tid + u * nthr;
+            if (e < nel) buf[e] = v[u];
         }
         __syncthreads();
         fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);
@@ -806,7 +863,7 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
 template <typename T, int EPT>
 __global__ void __launch_bounds__(256, 2) k_xfwd_rkl(const __grid_constant__ RklArgs a, double2* U, int vslot) {
     if (a.stage > a.sc->s_rkl) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
     const double* cf = a.sc->rkl[a.stage];
     const int N = a.g.nx, KT = a.kt, nzh = a.g.nzh;
@@ -821,12 +878,13 @@ __global__ void __launch_bounds__(256, 2) k_xfwd_rkl(const __grid_constant__ Rkl
     C2<T> acc[EPT];
 #pragma unroll
     for (int u = 0; u < EPT; u++) acc[u] = mk<T>((T)0, (T)0);
+    const size_t nstride = (size_t)a.g.ny * a.g.nzs, nbase = (size_t)j * a.g.nzs + k0;   // pass buffers
     if (nl_on) {
         for (int c = 0; c < 3; c++) {
-            const C2<T>* src = nl + (size_t)c * a.cs_nl;
+            const C2<T>* src = nl + (size_t)c * a.cs_nl + nbase;
             for (int e = tid; e < nel; e += nthr) {
                 const int n = e / KT, col = e - n * KT;
-                buf[e] = (col < kt) ? src[base + (size_t)n * stride + k0 + col] : mk<T>((T)0, (T)0);
+                buf[e] = (col < kt) ? src[(size_t)n * nstride + col] : mk<T>((T)0, (T)0);
             }
             __syncthreads();
             fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);

@@ -15,7 +15,10 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <cuda.h>
+
 #include "spk_fft.cuh"
+#include "spk_tma.cuh"
 
 namespace spk {
 
@@ -43,8 +46,10 @@ struct FastDiv {
 
 struct DevGrid {
     int nx, ny, nz, nzh;
+    int nzs;                        // row length of the pass buffers (nzh rounded up to even)
     int kz_keep;                    // kz index k is inside the 2/3 mask iff k < kz_keep
-    size_t nc;                      // nx*ny*nzh
+    size_t nc;                      // nx*ny*nzh (state modes per field)
+    size_t ncs;                     // nx*ny*nzs (pass-buffer elements per channel)
     const double *kx, *ky, *kz;     // wavevector tables (exact reference expressions)
     const double *mx, *my, *mz;     // separable mask factors, 0.0 or 1.0
 };
@@ -61,26 +66,31 @@ struct DevScalars {
 
 #define SPK_MAXJOBS 16
 
+// One channel of a strided-axis pass: a 4-D tensor map of the input array
+// ([channel][x][y][k], k in scalars) and the output channel base.
 struct AxisJob {
-    const void* in;
+    alignas(64) CUtensorMap tm;
     void* out;
-    int nch;        // channels handled by this job (1, or 3 when cleaning)
+    int ch;         // channel coordinate of the input in its tensor map
     int in_state;   // input is the FP64 state (double2) instead of the pass type
     int deriv;      // multiply the input by i*k_axis(n) before the transform
-    int clean;      // divergence-clean the 3-vector at load (state input, x pass)
+    int pad_;
 };
 
 struct AxisArgs {
     DevGrid g;
     FftPlan plan;
     int axis;       // 0: x (tile = fixed j), 1: y (tile = fixed i)
-    int kt;         // tile width (k columns)
+    int kt;         // tile width (k columns, a power of two)
     int kcols;      // process columns [0, kcols)
     int row_filter; // store only rows whose mask factor along the axis is 1
-    size_t cs_in, cs_out;   // channel strides, complex elements
+    int box_rows;   // rows per TMA box (<= 256); N / box_rows boxes per tile
+    int nst;        // pipeline stages
+    int convert;    // input type differs from the pass type (FP64 state in the FP32 form)
     double scale;   // input scale factor
     const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
     int gate_stage;
+    int* err;       // error word (set when a TMA wait runs out)
     int njobs;
     AxisJob job[SPK_MAXJOBS];
 };
