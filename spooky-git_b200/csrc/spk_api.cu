@@ -317,8 +317,9 @@ static void zpass(spk_ctx* c, ZArgs& z) {
 }
 
 static void xfwd(spk_ctx* c, XfArgs& x) {
-    const AxisCfg cf = xfwd_cfg(c);
+    AxisCfg cf = xfwd_cfg(c);
     x.kt = cf.kt;
+    if (x.strat) cf.smem = ((cf.smem + 15) & ~(size_t)15) + (size_t)c->nx * cf.kt * sizeof(double2);
     dim3 grid((c->nzh + cf.kt - 1) / cf.kt, c->ny);
     c->launches++;
     if (c->fp32) k_xfwd<float, 8><<<grid, cf.nthr, cf.smem, c->stream>>>(x);
@@ -765,7 +766,7 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     // FFT plans (lengths the device decomposition covers)
     const int rf = c->fp32 ? 16 : 8;
     if (!fft_supported(c->nx, rf) || !fft_supported(c->ny, rf) || !fft_supported(c->nz, rf))
-        return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be (16 or 8)^k times {1,2,4,8} x {1,3,9} x {1,5}");
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be powers of two between 2 and 1024");
     make_plan(c->nx, 16, &c->plan_x);
     make_plan(c->ny, 16, &c->plan_y);
     make_plan(c->nz, 16, &c->plan_z);

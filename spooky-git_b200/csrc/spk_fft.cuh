@@ -179,55 +179,11 @@ __device__ __forceinline__ void stage_p2(C2<T>* buf, int es, int cs, int ln, int
     __syncthreads();
 }
 
-// Same stage for any length (integer division; lengths with factors 3, 5).
-template <typename T, int R, int DIR, int EPT, bool COLFAST, int PAD>
-__device__ __forceinline__ void stage_gen(C2<T>* buf, int es, int cs, int N, int ncol, int s,
-                                          const C2<T>* __restrict__ tw) {
-    constexpr int BPT = (EPT + R - 1) / R;
-    const int nthr = blockDim.x, tid = threadIdx.x;
-    const int nbf = N / R;
-    const int nb = nbf * ncol;
-    const int m = nbf / s;
-    C2<T> a[BPT][R];
-#pragma unroll
-    for (int u = 0; u < BPT; u++) {
-        const int b = tid + u * nthr;
-        if (b < nb) {
-            int col, beta;
-            if (COLFAST) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
-            const int p = beta / s, q = beta - p * s;
-            const C2<T>* base = buf + (size_t)col * cs;
-#pragma unroll
-            for (int r = 0; r < R; r++) a[u][r] = base[padi<PAD>(q + s * (p + r * m)) * es];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < BPT; u++) {
-        const int b = tid + u * nthr;
-        if (b < nb) {
-            int col, beta;
-            if (COLFAST) { col = b % ncol; beta = b / ncol; } else { beta = b % nbf; col = b / nbf; }
-            const int p = beta / s, q = beta - p * s;
-            dftR<T, R, DIR>(a[u]);
-            C2<T>* base = buf + (size_t)col * cs;
-            base[padi<PAD>(q + s * (R * p)) * es] = a[u][0];
-#pragma unroll
-            for (int t = 1; t < R; t++) {
-                C2<T> w = tw[p * t * s];
-                if (DIR > 0) w.y = -w.y;
-                base[padi<PAD>(q + s * (R * p + t)) * es] = (p == 0) ? a[u][t] : cmul(a[u][t], w);
-            }
-        }
-    }
-    __syncthreads();
-}
-
 // Full-radix stages (RF = 16 in FP32, 8 in FP64: the FP64 radix-16
 // butterfly does not fit the register budget) in a loop with one code copy,
-// then at most one stage each of radix 8, 4, 2 (power-of-two lengths), or
-// 8, 4, 2, 3, 3, 5 for the general path.
-// Supported lengths: RF^k * {1,2,4,8} * {1,3,9} * {1,5} (see fft_supported).
+// then at most one stage each of radix 8, 4, 2.  Power-of-two lengths only:
+// a general-length path in the same kernel costs registers (and spills) even
+// when it never runs.
 template <typename T> struct FullRadix { static constexpr int R = 16; static constexpr int LR = 4; };
 template <> struct FullRadix<double> { static constexpr int R = 8; static constexpr int LR = 3; };
 
@@ -239,8 +195,8 @@ __device__ __forceinline__ void fft_run(C2<T>* buf, int es, int cs, int ncol, co
     const C2<T>* tw = (const C2<T>*)pl.tw;
     asm volatile("" : "+l"(tw));   // keep twiddle loads inside the caller's channel loop
     const int n = pl.n;
-    if ((n & (n - 1)) == 0 && (!COLFAST || (ncol & (ncol - 1)) == 0)) {
-        const int ln = ilog2(n), lncol = ilog2(ncol);
+    {
+        const int ln = ilog2(n), lncol = ilog2(ncol);   // COLFAST requires a power-of-two ncol
         int ls = 0, rest = ln;
 #pragma unroll 1
         while (rest >= LRF) { stage_p2<T, RF, LRF, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); ls += LRF; rest -= LRF; }
@@ -249,29 +205,12 @@ __device__ __forceinline__ void fft_run(C2<T>* buf, int es, int cs, int ncol, co
         if (rest >= 1) { stage_p2<T, 2, 1, DIR, EPT, COLFAST, PAD>(buf, es, cs, ln, ncol, lncol, ls, tw); }
         return;
     }
-    int s = 1, rest = n;
-#pragma unroll 1
-    while (rest % RF == 0) { stage_gen<T, RF, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= RF; rest /= RF; }
-    if (RF > 8 && rest % 8 == 0) { stage_gen<T, 8, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 8; rest /= 8; }
-    if (rest % 4 == 0) { stage_gen<T, 4, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 4; rest /= 4; }
-    if (rest % 2 == 0) { stage_gen<T, 2, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 2; rest /= 2; }
-    if (rest % 3 == 0) { stage_gen<T, 3, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 3; rest /= 3; }
-    if (rest % 3 == 0) { stage_gen<T, 3, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); s *= 3; rest /= 3; }
-    if (rest % 5 == 0) { stage_gen<T, 5, DIR, EPT, COLFAST, PAD>(buf, es, cs, n, ncol, s, tw); }
 }
 
-// Host check mirroring fft_run's decomposition.
+// Host check mirroring fft_run: power-of-two lengths, 2 <= n <= 1024.
 inline bool fft_supported(int n, int RF) {
-    if (n < 2) return false;
-    int rest = n;
-    while (rest % RF == 0) rest /= RF;
-    if (RF > 8 && rest % 8 == 0) rest /= 8;
-    if (rest % 4 == 0) rest /= 4;
-    if (rest % 2 == 0) rest /= 2;
-    if (rest % 3 == 0) rest /= 3;
-    if (rest % 3 == 0) rest /= 3;
-    if (rest % 5 == 0) rest /= 5;
-    return rest == 1;
+    (void)RF;
+    return n >= 2 && n <= 1024 && (n & (n - 1)) == 0;
 }
 
 }  // namespace spk

@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(256, 2) k_axis(const __grid_constant__ AxisArg
         if (a.convert) {
             // FP64 state -> pass type, with the scale and the derivative
             const double2* src = reinterpret_cast<const double2*>(stg);
-#pragma unroll
+#pragma unroll 4
             for (int u = 0; u < EPT; u++) {
                 const int e = tid + u * nthr;
                 if (e < nel) {
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(256, 2) k_axis(const __grid_constant__ AxisArg
             work = reinterpret_cast<C2<T>*>(stg);
             if (jo.deriv || a.scale != 1.0) {
                 const T sc = (T)a.scale;
-#pragma unroll
+#pragma unroll 4
                 for (int u = 0; u < EPT; u++) {
                     const int e = tid + u * nthr;
                     if (e < nel) {
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256, 2) k_axis(const __grid_constant__ AxisArg
         fft_run<T, DIR, EPT, true, 0>(work, KT, 1, KT, a.plan);
         size_t base = a.axis == 0 ? (size_t)o * a.g.nzs : (size_t)o * a.g.ny * a.g.nzs;
         C2<T>* out = (C2<T>*)jo.out + base + k0;
-#pragma unroll
+#pragma unroll 4
         for (int u = 0; u < EPT; u++) {
             const int e = tid + u * nthr;
             const int n = e >> lkt, col = e & (KT - 1);
@@ -257,87 +257,81 @@ __global__ void __launch_bounds__(256, 2) k_zpass(const __grid_constant__ ZArgs 
     T* breal = (T*)a.breal;
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
         const int l = (int)fz.div((unsigned)e), z = e - l * NZ;
-        T o[14];
+        // output channel ch of this point -> half of the paired complex slot
+        T* orow = reinterpret_cast<T*>(outb + (size_t)l * npout * NZp + padi<1>(z));
+        auto put = [&](int ch, T v) { orow[(size_t)(ch >> 1) * NZp * 2 + (ch & 1)] = v; };
+        if (l >= nl) {
+            for (int ch = 0; ch < 2 * npout; ch++) put(ch, (T)0);
+            continue;
+        }
+        const size_t line = (size_t)(line0 + l);
+        T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
+        if (a.ch_u >= 0) { ux = val(l, a.ch_u, z); uy = val(l, a.ch_u + 1, z); uz = val(l, a.ch_u + 2, z); }
+        if (a.load_breal) {
+            bx = breal[(0 * (size_t)nlines + line) * NZ + z];
+            by = breal[(1 * (size_t)nlines + line) * NZ + z];
+            bz = breal[(2 * (size_t)nlines + line) * NZ + z];
+        } else if (a.ch_b >= 0) {
+            bx = val(l, a.ch_b, z); by = val(l, a.ch_b + 1, z); bz = val(l, a.ch_b + 2, z);
+        }
+        if (a.ch_th >= 0 && a.derive_gz != 2) th = val(l, a.ch_th, z);
+        if (a.ch_gx >= 0) gx = val(l, a.ch_gx, z);
+        if (a.ch_gy >= 0) gy = val(l, a.ch_gy, z);
+        if (a.derive_gz == 1) gz = val(l, a.nin, z);
+        else if (a.derive_gz == 2) gz = val(l, a.ch_th, z);
+        if (a.store_breal) {
+            breal[(0 * (size_t)nlines + line) * NZ + z] = bx;
+            breal[(1 * (size_t)nlines + line) * NZ + z] = by;
+            breal[(2 * (size_t)nlines + line) * NZ + z] = bz;
+        }
+        if (a.do_max) {
+            const T av[6] = {fabs(ux), fabs(uy), fabs(uz), fabs(bx), fabs(by), fabs(bz)};
 #pragma unroll
-        for (int q = 0; q < 14; q++) o[q] = (T)0;
-        if (l < nl) {
-            const size_t line = (size_t)(line0 + l);
-            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
-            if (a.ch_u >= 0) { ux = val(l, a.ch_u, z); uy = val(l, a.ch_u + 1, z); uz = val(l, a.ch_u + 2, z); }
-            if (a.load_breal) {
-                bx = breal[(0 * (size_t)nlines + line) * NZ + z];
-                by = breal[(1 * (size_t)nlines + line) * NZ + z];
-                bz = breal[(2 * (size_t)nlines + line) * NZ + z];
-            } else if (a.ch_b >= 0) {
-                bx = val(l, a.ch_b, z); by = val(l, a.ch_b + 1, z); bz = val(l, a.ch_b + 2, z);
-            }
-            if (a.ch_th >= 0 && a.derive_gz != 2) th = val(l, a.ch_th, z);
-            if (a.ch_gx >= 0) gx = val(l, a.ch_gx, z);
-            if (a.ch_gy >= 0) gy = val(l, a.ch_gy, z);
-            if (a.derive_gz == 1) gz = val(l, a.nin, z);
-            else if (a.derive_gz == 2) gz = val(l, a.ch_th, z);
-            if (a.store_breal) {
-                breal[(0 * (size_t)nlines + line) * NZ + z] = bx;
-                breal[(1 * (size_t)nlines + line) * NZ + z] = by;
-                breal[(2 * (size_t)nlines + line) * NZ + z] = bz;
-            }
-            if (a.do_max) {
-                const T v6[6] = {ux, uy, uz, bx, by, bz};
-#pragma unroll
-                for (int q = 0; q < 6; q++) {
-                    const T av = fabs(v6[q]);
-                    if (!isfinite(av)) bad = 1;
-                    mu[q] = fmax(mu[q], av);
-                }
-            }
-            int q = 0;
-            if (a.mode == ZM_PRODUCTS) {
-                if (a.hydro) {
-                    if (!a.mhd) {
-                        o[0] = ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0;
-                        o[1] = ux * uy;
-                        o[2] = ux * uz;
-                        o[3] = (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0;
-                        o[4] = uy * uz;
-                    } else {
-                        o[0] = ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0;
-                        o[1] = ux * uy - bx * by;
-                        o[2] = ux * uz - bx * bz;
-                        o[3] = (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0;
-                        o[4] = uy * uz - by * bz;
-                    }
-                    q = 5;
-                }
-                if (a.mhd) {
-                    o[q] = -by * uz + bz * uy;
-                    o[q + 1] = bx * uz - bz * ux;
-                    o[q + 2] = -bx * uy + by * ux;
-                    q += 3;
-                }
-                if (a.bous) {
-                    o[q] = ux * th; o[q + 1] = uy * th; o[q + 2] = uz * th;
-                    q += 3;
-                }
-            }
-            if (a.aniso) {
-                const T bgt = bx * gx + by * gy + bz * gz;
-                const T b2 = bx * bx + by * by + bz * bz;
-                const T bs = a.sd == 0 ? bx : (a.sd == 1 ? by : bz);
-                const T chi = (T)a.chi, W = (T)a.omegaT2;
-                o[q] = chi * bx * (bgt + W * bs) / b2;
-                o[q + 1] = chi * by * (bgt + W * bs) / b2;
-                o[q + 2] = chi * bz * (bgt + W * bs) / b2;
+            for (int q = 0; q < 6; q++) {
+                if (!isfinite(av[q])) bad = 1;
+                mu[q] = fmax(mu[q], av[q]);
             }
         }
-        if (a.nout > 0) {
-#pragma unroll
-            for (int pp = 0; pp < 7; pp++) {
-                if (pp < npout) {
-                    const T hi = (2 * pp + 1 < a.nout) ? o[2 * pp + 1] : (T)0;
-                    outb[(size_t)(l * npout + pp) * NZp + padi<1>(z)] = mk<T>(o[2 * pp], hi);
+        int q = 0;
+        if (a.mode == ZM_PRODUCTS) {
+            if (a.hydro) {
+                if (!a.mhd) {
+                    put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0);
+                    put(1, ux * uy);
+                    put(2, ux * uz);
+                    put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0);
+                    put(4, uy * uz);
+                } else {
+                    put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0);
+                    put(1, ux * uy - bx * by);
+                    put(2, ux * uz - bx * bz);
+                    put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0);
+                    put(4, uy * uz - by * bz);
                 }
+                q = 5;
+            }
+            if (a.mhd) {
+                put(q, -by * uz + bz * uy);
+                put(q + 1, bx * uz - bz * ux);
+                put(q + 2, -bx * uy + by * ux);
+                q += 3;
+            }
+            if (a.bous) {
+                put(q, ux * th); put(q + 1, uy * th); put(q + 2, uz * th);
+                q += 3;
             }
         }
+        if (a.aniso) {
+            const T bgt = bx * gx + by * gy + bz * gz;
+            const T b2 = bx * bx + by * by + bz * bz;
+            const T bs = a.sd == 0 ? bx : (a.sd == 1 ? by : bz);
+            const T chi = (T)a.chi, W = (T)a.omegaT2;
+            put(q, chi * bx * (bgt + W * bs) / b2);
+            put(q + 1, chi * by * (bgt + W * bs) / b2);
+            put(q + 2, chi * bz * (bgt + W * bs) / b2);
+            q += 3;
+        }
+        if (a.nout > 0 && (a.nout & 1)) put(a.nout, (T)0);
     }
     if (a.do_max) {
         __syncthreads();
@@ -463,9 +457,9 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs 
         fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);
     };
 
-    double2 usd[EPT];   // u_strat of each owned mode, for the theta group
-#pragma unroll
-    for (int u = 0; u < EPT; u++) usd[u] = d2(0.0, 0.0);
+    // u_strat of each mode of the tile (read before the velocity update),
+    // for the theta group; only allocated with stratification
+    double2* usd = reinterpret_cast<double2*>(smem_raw + (((size_t)nel * sizeof(C2<T>) + 15) & ~(size_t)15));
 
     // ---------------- velocity ----------------
     if (a.incompressible) {
@@ -517,8 +511,9 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs 
             }
             if (a.strat) {
                 const double2 th = a.U[(size_t)a.TH * nc + gi];
-                R[a.sd] = d2(R[a.sd].x - th.x, R[a.sd].y - th.y);
-                usd[u] = X[a.sd];
+                if (a.sd == 0)      { R[0] = d2(R[0].x - th.x, R[0].y - th.y); usd[e] = X[0]; }
+                else if (a.sd == 1) { R[1] = d2(R[1].x - th.x, R[1].y - th.y); usd[e] = X[1]; }
+                else                { R[2] = d2(R[2].x - th.x, R[2].y - th.y); usd[e] = X[2]; }
             }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -643,7 +638,7 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const __grid_constant__ XfArgs 
             const bool m = nl_on && a.g.mx[n] != 0.0 && a.g.mz[k] != 0.0;
             const double2 s0 = to_d2(acc[u][0]);
             double2 R = m ? d2(s0.y, -s0.x) : d2(0.0, 0.0);   // -i * mask * k.(u theta)
-            if (a.strat) R = d2(R.x + a.N2 * usd[u].x, R.y + a.N2 * usd[u].y);
+            if (a.strat) { const double2 us = usd[e]; R = d2(R.x + a.N2 * us.x, R.y + a.N2 * us.y); }
             if (!th_sts) {
                 if (a.aniso_rhs) {
                     const double2 s1 = to_d2(acc[u][1]);
