@@ -168,6 +168,38 @@ typedef struct spk_pass_stat {
 } spk_pass_stat_t;
 int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out, int* n_out);
 
+/* TimeStepping::compute_dfield for callers that cannot allocate device
+ * memory.  No counterpart in the reference.
+ *
+ * Some callers cannot call cudaMalloc: their device memory belongs to another
+ * allocator (a fixed pool, an embedding framework), they run in a real-time
+ * loop that must not take cudaMalloc's implicit device synchronisation, or
+ * they must not fail for lack of memory once started.  This entry point
+ * computes dU = RHS(U) like spk_compute_dfield, with no context and no
+ * allocation: every scratch array it needs (pass buffers, wavevector tables,
+ * FFT twiddles, device scalars) lives in one file-scope device array of
+ * SPK_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits.  The caller passes the input U and the output dU
+ * (device pointers, [F][Nc] complex FP64) and a stream (NULL: the legacy
+ * default stream); the work is queued on that stream.
+ *
+ * - The scratch needed is about 2 * C * nx * ny * nzs * (8 bytes in the FP32
+ *   form, 16 in the plain form), nzs = nz/2+1 rounded up to even, C = 5 (HD),
+ *   8 (MHD or Boussinesq), 14 (MHD + Boussinesq + anisotropic conduction);
+ *   the heat equation needs only tables.  So every configuration fits at
+ *   32^3, and at 64^3 the FP32 form of HD, MHD and Boussinesq does.  Larger
+ *   grids are rejected with SPK_ERR_UNSUPPORTED and a message
+ *   (spk_last_error(NULL)) giving the size needed.
+ * - The first call on a device looks up the array's device address and sets
+ *   the kernels' shared-memory limits; make that first call before any
+ *   stream capture.
+ * - Every call shares the one array and clears what must start at zero;
+ *   calls whose GPU work overlaps (other streams, other threads) race on it.
+ * - Calls no cudaMalloc/cudaFree and no allocating library routine; errors
+ *   are reported through spk_last_error(NULL). */
+#define SPK_NOALLOC_SCRATCH_BYTES (24u << 20)
+int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U, double* dU, void* cuda_stream);
+
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */
 const char* spk_last_error(const spk_ctx* ctx);

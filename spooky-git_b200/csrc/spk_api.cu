@@ -1218,3 +1218,137 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
     if (n_out) *n_out = n;
     return launch_status(c);
 }
+
+// ---------------------------------------------------------------------------
+// RHS without any allocation (spk_compute_dfield_noalloc)
+//
+// Some callers cannot call cudaMalloc: code that runs while another
+// component owns the device memory (a fixed pool, an embedding framework's
+// allocator), real-time loops that must not take cudaMalloc's implicit
+// device synchronisation, and code paths that must not fail for lack of
+// memory after start-up.  For them the RHS is computed with every scratch
+// array of the pipeline (pass buffers, wavevector tables, FFT twiddles,
+// device scalars) carved out of one file-scope device array.  The array is
+// part of the loaded library: every GPU that loads it holds these bytes
+// until the process exits.
+// ---------------------------------------------------------------------------
+#define SPK_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SPK_NOALLOC_SCRATCH_BYTES];
+// Device addresses of g_noalloc_scratch, one per device.  In host code the
+// array's name is only a stand-in: a kernel must receive this address.
+static void* g_noalloc_ptr[SPK_NOALLOC_MAX_DEVICES];
+
+// Once per device, with that device current: the scratch address, the
+// shared-memory limits of the pass kernels and the tensor-map encoder.
+static int noalloc_setup(int dev) {
+    if (g_noalloc_ptr[dev]) return SPK_OK;
+    spk_ctx* c = nullptr;   // errors go to spk_last_error(NULL)
+    void* ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    const int big = 200 * 1024;
+    CK(cudaFuncSetAttribute(k_zpass<float, EPT_Z_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_zpass<double, EPT_Z_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<float, 1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<float, -1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<double, 1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_axis<double, -1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    if (!g_encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(nullptr, SPK_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    g_noalloc_ptr[dev] = ptr;
+    return SPK_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* Uin, double* dUout, void* cuda_stream) {
+    if (!p || !Uin || !dUout) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    std::string why;
+    int rc = check_params(p, why);
+    if (rc != SPK_OK) return fail(nullptr, rc, why);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SPK_NOALLOC_MAX_DEVICES)
+        return fail(nullptr, SPK_ERR_CUDA, "no usable current device");
+
+    // a context on the host stack, bound to the scratch array (no device
+    // or pinned allocation; the caller's stream, or the legacy stream)
+    spk_ctx ctx{};
+    spk_ctx* c = &ctx;
+    c->sticky = 0; c->bad_job = false; c->bad_why = ""; c->user_U = nullptr; c->dirty = false;
+    rc = ctx_init(c, p, cuda_stream ? cuda_stream : (void*)cudaStreamLegacy);
+    if (rc != SPK_OK) return rc;
+    c->num_sms = 148;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+
+    const size_t cs = csize(c);
+    c->g.nx = c->nx; c->g.ny = c->ny; c->g.nz = c->nz; c->g.nzh = c->nzh;
+    c->g.nzs = c->nzh + (c->nzh & 1);
+    c->g.ncs = (size_t)c->nx * c->ny * c->g.nzs;
+    c->g.kz_keep = c->kz_keep; c->g.nc = c->nc;
+    const size_t ntab = 2 * ((size_t)c->nx + c->ny + c->nzh);
+    const size_t ntw = (size_t)c->nx + c->ny + c->nz;
+    const size_t o_tab = 0;
+    const size_t o_tw = align256(o_tab + sizeof(double) * ntab);
+    const size_t o_sc = align256(o_tw + cs * ntw);
+    const size_t bufbytes = c->p.incompressible ? align256(cs * c->g.ncs * c->nbuf_ch) : 0;
+    const size_t o_bufA = align256(o_sc + sizeof(DevScalars));
+    const size_t o_bufB = o_bufA + bufbytes;
+    const size_t need = o_bufB + bufbytes;
+    if (need > (size_t)SPK_NOALLOC_SCRATCH_BYTES) {
+        char msg[200];
+        snprintf(msg, sizeof(msg), "grid %dx%dx%d needs %.1f MiB of scratch; spk_compute_dfield_noalloc holds %u MiB",
+                 c->nx, c->ny, c->nz, need / 1048576.0, (unsigned)(SPK_NOALLOC_SCRATCH_BYTES >> 20));
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, msg);
+    }
+    rc = noalloc_setup(dev);
+    if (rc != SPK_OK) return rc;
+    char* base = (char*)g_noalloc_ptr[dev];
+    double* t = (double*)(base + o_tab);
+    double* m = t + c->nx + c->ny + c->nzh;
+    c->d_tab = t;
+    c->g.kx = t; c->g.ky = t + c->nx; c->g.kz = t + c->nx + c->ny;
+    c->g.mx = m; c->g.my = m + c->nx; c->g.mz = m + c->nx + c->ny;
+    c->d_tw = base + o_tw;
+    c->sc = (DevScalars*)(base + o_sc);
+    c->bufA = c->p.incompressible ? base + o_bufA : nullptr;
+    c->bufB = c->p.incompressible ? base + o_bufB : nullptr;
+
+    // tables and twiddles (the array keeps the previous call's contents)
+    std::vector<double> tab(ntab);
+    std::copy(c->kx.begin(), c->kx.end(), tab.begin());
+    std::copy(c->ky.begin(), c->ky.end(), tab.begin() + c->nx);
+    std::copy(c->kz.begin(), c->kz.end(), tab.begin() + c->nx + c->ny);
+    std::copy(c->mx.begin(), c->mx.end(), tab.begin() + ntab / 2);
+    std::copy(c->my.begin(), c->my.end(), tab.begin() + ntab / 2 + c->nx);
+    std::copy(c->mz.begin(), c->mz.end(), tab.begin() + ntab / 2 + c->nx + c->ny);
+    CK(cudaMemcpyAsync(t, tab.data(), sizeof(double) * ntab, cudaMemcpyHostToDevice, c->stream));
+    std::vector<double> tw, all;
+    FftPlan* pls[3] = {&c->plan_x, &c->plan_y, &c->plan_z};
+    size_t off = 0;
+    for (int a = 0; a < 3; a++) {
+        twiddles(pls[a]->n, tw);
+        all.insert(all.end(), tw.begin(), tw.end());
+        pls[a]->tw = (char*)c->d_tw + off * cs;
+        off += pls[a]->n;
+    }
+    if (c->fp32) {
+        std::vector<float> tf(all.begin(), all.end());
+        CK(cudaMemcpyAsync(c->d_tw, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice, c->stream));
+    } else {
+        CK(cudaMemcpyAsync(c->d_tw, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, c->stream));
+    }
+    // what must start at zero: the device scalars and the pass buffers
+    CK(cudaMemsetAsync(c->sc, 0, sizeof(DevScalars), c->stream));
+    if (bufbytes) CK(cudaMemsetAsync(base + o_bufA, 0, 2 * bufbytes, c->stream));
+
+    rc = spk_compute_dfield(c, Uin, dUout);
+    if (rc != SPK_OK) g_create_error = c->err;
+    return rc;
+}

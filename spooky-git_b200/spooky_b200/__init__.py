@@ -31,7 +31,8 @@ ERRORS = {1: "SPK_ERR_ARG", 2: "SPK_ERR_UNSUPPORTED", 3: "SPK_ERR_CUDA", 4: "SPK
 EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_sizes", "spk_set_state",
             "spk_get_state", "spk_set_time", "spk_get_time", "spk_clean_divergence", "spk_compute_dt",
             "spk_compute_dfield", "spk_advance", "spk_rkl_cycle", "spk_to_real", "spk_synchronize",
-            "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error"]
+            "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error",
+            "spk_compute_dfield_noalloc"]
 
 
 class Budgets(ctypes.Structure):
@@ -80,6 +81,7 @@ def lib():
         L.spk_step_info.argtypes = [vp, ip, dp]
         L.spk_profile_passes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PassStat), ctypes.c_int, ip]
         L.spk_last_error.argtypes = [vp]
+        L.spk_compute_dfield_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -110,6 +112,27 @@ def _ptr(a):
             return a.data_ptr(), 0
         return a.data_ptr(), 1
     return a.ctypes.data, 1
+
+
+NOALLOC_SCRATCH_BYTES = 24 << 20
+
+
+def compute_dfield_noalloc(params, U, dU, stream=None):
+    """dU = RHS(U) through spk_compute_dfield_noalloc: no context and no
+    device allocation, for callers whose device memory belongs to another
+    allocator or that must not allocate once running.  All scratch lives in
+    one NOALLOC_SCRATCH_BYTES array inside the library; larger grids raise
+    SpookyError(SPK_ERR_UNSUPPORTED).  U, dU: torch CUDA complex128 tensors of
+    shape (F, nx, ny, nz//2+1).  stream: a CUDA stream handle (int) or None
+    for the legacy default stream.  Waits for torch's queued work before the
+    call and for the device after it.  Calls that overlap on the GPU race on
+    the shared scratch array."""
+    p = params.copy()
+    _torch_sync()
+    rc = lib().spk_compute_dfield_noalloc(ctypes.byref(p), U.data_ptr(), dU.data_ptr(), stream)
+    if rc != SPK_OK:
+        raise SpookyError(rc, lib().spk_last_error(None).decode())
+    _torch_sync()
 
 
 class Context:
