@@ -167,6 +167,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
+                         "(the small case for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -220,6 +223,19 @@ def main():
         ctx.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         return ctx, max_over_ranks(ms), clocks
+
+    if args.profile_run:
+        ctxp, msp, _ = timed_run(SPK_FORM_FP32)
+        kps, bytes_step = ctxp.step_info()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "n": n, "ms_per_step": msp, "steps": args.steps,
+                              "warmup": args.warmup, "kernels_per_step": kps, "step_bytes": bytes_step}),
+                  flush=True)
+        del ctxp
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
     clk_path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_rank{rank}.csv")
