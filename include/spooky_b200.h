@@ -190,9 +190,8 @@ int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out
  *   32^3, and at 64^3 the FP32 form of HD, MHD and Boussinesq does.  Larger
  *   grids are rejected with SPK_ERR_UNSUPPORTED and a message
  *   (spk_last_error(NULL)) giving the size needed.
- * - The first call on a device looks up the array's device address and sets
- *   the kernels' shared-memory limits; make that first call before any
- *   stream capture.
+ * - The first call on a device looks up the array's device address; make
+ *   that first call before any stream capture.
  * - Every call shares the one array and clears what must start at zero;
  *   calls whose GPU work overlaps (other streams, other threads) race on it.
  * - Calls no cudaMalloc/cudaFree and no allocating library routine; errors

@@ -19,15 +19,12 @@
 #include "spk_kernels.cuh"
 
 #include "spk_kernels.cu"
+#include "spk_pass2.cu"
 
 using namespace spk;
 
 static std::string g_create_error;
 
-#define EPT_AXIS_F 16
-#define EPT_AXIS_D 8
-#define EPT_Z_F 16
-#define EPT_Z_D 8
 #define MAXT 256
 
 struct spk_ctx {
@@ -218,14 +215,17 @@ static inline int rup32(long x) { return (int)(((x + 31) / 32) * 32); }
 
 struct AxisCfg { int kt; int nthr; size_t smem; };
 
+// Tile width of a strided-axis pass: the host mirror of axis_kt<T, LN, CONV>
+// (KT columns x TPC threads = 256 threads, KT <= 64; an FP64 input tile in
+// the FP32 form is half as wide).
 static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     AxisCfg a;
-    const int ept = c->fp32 ? EPT_AXIS_F : EPT_AXIS_D;
-    int kt = (c->fp32 && !state_in) ? 16 : 8;    // 128-byte row segments of the input
-    while (kt > 2 && (long)N * kt > (long)MAXT * ept) kt /= 2;
-    while (kt > 2 && kt > c->nzh) kt /= 2;       // power of two, >= 2 (16-byte TMA rows in FP32)
+    const RegFftGeom g = regfft_geom(N, c->fp32);
+    int kt = std::min(64, 256 / g.TPC);
+    if (c->fp32 && state_in && kt > 2) kt /= 2;
+    kt = std::max(kt, 2);
     a.kt = kt;
-    a.nthr = std::max(32, std::min(MAXT, rup32(((long)N * kt + ept - 1) / ept)));
+    a.nthr = kt * g.TPC;
     a.smem = 0;
     return a;
 }
@@ -242,48 +242,61 @@ static AxisCfg xfwd_cfg(const spk_ctx* c) {
     return a;
 }
 
-struct ZCfg { int lines; int nthr; size_t smem; };
+template <typename T, int LN, int DIR, bool CONV>
+static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
+    constexpr int N = 1 << LN;
+    constexpr int KT = axis_kt<T, LN, CONV>();
+    const int nthr = KT * RegFft<T, LN>::TPC;
+    if (a.kt != KT) { c->err = "internal: axis tile width mismatch"; c->sticky = SPK_ERR_ARG; return; }
+    const size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
+    const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
+    // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
+    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)N * sizeof(C2<T>) + (size_t)N * sizeof(T) + N + 16;
+    // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
+    long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
+    a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
+    const size_t smem = fixed + (size_t)a.nst * stage;
+    cudaFuncSetAttribute(k_axis2<T, LN, DIR, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, LN, DIR, CONV>, nthr, smem);
+    const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
+    c->launches++;
+    k_axis2<T, LN, DIR, CONV><<<grid, nthr, smem, c->stream>>>(a);
+}
 
-static ZCfg z_cfg(const spk_ctx* c, int nin_all, int nout) {
-    ZCfg z;
-    const int npin = (nin_all + 1) / 2, npout = (nout + 1) / 2;
-    const int maxp = std::max(npin, std::max(npout, 1));
-    const size_t csz = c->fp32 ? sizeof(float2) : sizeof(double2);
-    const int nzp = padded_len(c->nz);
-    const size_t per_line = (size_t)(npin + npout) * nzp * csz;
-    int L = (int)std::max<size_t>(1, 65536 / std::max<size_t>(per_line, 1));
-    L = std::min(L, 64);
-    const int ept = c->fp32 ? EPT_Z_F : EPT_Z_D;
-    L = std::min(L, std::max(1, MAXT * ept / (maxp * c->nz)));
-    L = std::min<long>(L, (long)c->nx * c->ny);
-    z.lines = L;
-    z.nthr = std::max(32, std::min(MAXT, rup32(((long)L * maxp * c->nz + ept - 1) / ept)));
-    // input pairs, output pairs, then 6 x 32 values of block-max scratch
-    z.smem = (size_t)L * (npin + npout) * nzp * csz + 6 * 32 * (c->fp32 ? sizeof(float) : sizeof(double));
-    return z;
+template <typename T, int LN, int DIR>
+static void launch_axis_conv(spk_ctx* c, AxisArgs& a, long total) {
+    if constexpr (sizeof(T) == 4 && DIR > 0) {
+        if (a.convert) { launch_axis_ln<T, LN, DIR, true>(c, a, total); return; }
+    }
+    launch_axis_ln<T, LN, DIR, false>(c, a, total);
+}
+
+template <typename T, int DIR>
+static void launch_axis_dir(spk_ctx* c, AxisArgs& a, long total) {
+    switch (ilog2(a.plan.n)) {
+        case 1: launch_axis_conv<T, 1, DIR>(c, a, total); break;
+        case 2: launch_axis_conv<T, 2, DIR>(c, a, total); break;
+        case 3: launch_axis_conv<T, 3, DIR>(c, a, total); break;
+        case 4: launch_axis_conv<T, 4, DIR>(c, a, total); break;
+        case 5: launch_axis_conv<T, 5, DIR>(c, a, total); break;
+        case 6: launch_axis_conv<T, 6, DIR>(c, a, total); break;
+        case 7: launch_axis_conv<T, 7, DIR>(c, a, total); break;
+        case 8: launch_axis_conv<T, 8, DIR>(c, a, total); break;
+        case 9: launch_axis_conv<T, 9, DIR>(c, a, total); break;
+        case 10: launch_axis_conv<T, 10, DIR>(c, a, total); break;
+        default: c->err = "internal: axis length outside 2..1024"; c->sticky = SPK_ERR_UNSUPPORTED; break;
+    }
 }
 
 template <typename T>
 static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
-    constexpr int ept = sizeof(T) == 4 ? EPT_AXIS_F : EPT_AXIS_D;
-    const int N = a.plan.n;
-    const int nthr = std::max(32, std::min(MAXT, rup32(((long)N * a.kt + ept - 1) / ept)));
-    const size_t in_elem = a.convert ? sizeof(double2) : sizeof(C2<T>);
-    const size_t stage = (((size_t)N * a.kt * in_elem) + 127) & ~(size_t)127;
-    a.nst = (int)std::max<size_t>(2, std::min<size_t>(4, 98304 / stage));
-    size_t smem = 256 + a.nst * stage + (a.convert ? (size_t)N * a.kt * sizeof(C2<T>) : 0);
-    while (a.nst > 2 && smem > 200 * 1024) { a.nst--; smem -= stage; }
     const int nouter = a.axis == 0 ? c->ny : c->nx;
     const long total = (long)a.njobs * nouter * ((a.kcols + a.kt - 1) / a.kt);
     if (total <= 0) return;
     a.err = &c->sc->err;
-    int per_sm = 1;
-    if (dir > 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis<T, +1, ept>, nthr, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis<T, -1, ept>, nthr, smem);
-    const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
-    c->launches++;
-    if (dir > 0) k_axis<T, +1, ept><<<grid, nthr, smem, c->stream>>>(a);
-    else k_axis<T, -1, ept><<<grid, nthr, smem, c->stream>>>(a);
+    if (dir > 0) launch_axis_dir<T, +1>(c, a, total);
+    else launch_axis_dir<T, -1>(c, a, total);
 }
 
 static void axis(spk_ctx* c, AxisArgs& a, int dir) {
@@ -300,6 +313,48 @@ static void axis(spk_ctx* c, AxisArgs& a, int dir) {
     else launch_axis<double>(c, a, dir);
 }
 
+template <typename T, int LN>
+static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
+    const int nthr = 256;
+    const int slots = nthr / regfft_geom(1 << LN, sizeof(T) == 4).TPC;
+    const long nlines = (long)c->nx * c->ny;
+    auto need = [&](int lines) {
+        return zsmem_layout(1 << LN, (int)sizeof(C2<T>), z.nin, nin_all, lines, c->g.nzs, slots).total;
+    };
+    // lines per CTA: the most (<= 64) that keep two CTAs per SM
+    int L = 64;
+    while (L > 1 && need(L) > (size_t)110 * 1024) L >>= 1;
+    L = (int)std::min<long>(L, nlines);
+    const size_t smem = need(L);
+    if (smem > (size_t)227 * 1024) {
+        c->err = "internal: z pass tile exceeds shared memory";
+        c->sticky = SPK_ERR_UNSUPPORTED;
+        return;
+    }
+    z.lines = L;
+    cudaFuncSetAttribute(k_zpass2<T, LN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nblk = (int)((nlines + L - 1) / L);
+    c->launches++;
+    k_zpass2<T, LN><<<nblk, nthr, smem, c->stream>>>(z);
+}
+
+template <typename T>
+static void launch_zpass(spk_ctx* c, ZArgs& z, int nin_all) {
+    switch (ilog2(c->nz)) {
+        case 1: launch_zpass_ln<T, 1>(c, z, nin_all); break;
+        case 2: launch_zpass_ln<T, 2>(c, z, nin_all); break;
+        case 3: launch_zpass_ln<T, 3>(c, z, nin_all); break;
+        case 4: launch_zpass_ln<T, 4>(c, z, nin_all); break;
+        case 5: launch_zpass_ln<T, 5>(c, z, nin_all); break;
+        case 6: launch_zpass_ln<T, 6>(c, z, nin_all); break;
+        case 7: launch_zpass_ln<T, 7>(c, z, nin_all); break;
+        case 8: launch_zpass_ln<T, 8>(c, z, nin_all); break;
+        case 9: launch_zpass_ln<T, 9>(c, z, nin_all); break;
+        case 10: launch_zpass_ln<T, 10>(c, z, nin_all); break;
+        default: c->err = "internal: z length outside 2..1024"; c->sticky = SPK_ERR_UNSUPPORTED; break;
+    }
+}
+
 static void zpass(spk_ctx* c, ZArgs& z) {
     if (!span_ok(c, z.in, std::max(z.nin, 1), false) || (z.nout > 0 && !span_ok(c, z.out, z.nout, false)) ||
         ((z.store_breal || z.load_breal) && !c->breal)) {
@@ -308,25 +363,12 @@ static void zpass(spk_ctx* c, ZArgs& z) {
         return;
     }
     const int nin_all = z.nin + (z.derive_gz == 1 ? 1 : 0);
-    const ZCfg cf = z_cfg(c, nin_all, z.nout);
-    z.lines = cf.lines;
-    const int nblk = (int)(((size_t)c->nx * c->ny + cf.lines - 1) / cf.lines);
-    c->launches++;
-    if (c->fp32) k_zpass<float, EPT_Z_F><<<nblk, cf.nthr, cf.smem, c->stream>>>(z);
-    else k_zpass<double, EPT_Z_D><<<nblk, cf.nthr, cf.smem, c->stream>>>(z);
+    if (c->fp32) launch_zpass<float>(c, z, nin_all);
+    else launch_zpass<double>(c, z, nin_all);
 }
 
-static void xfwd(spk_ctx* c, XfArgs& x) {
-    AxisCfg cf = xfwd_cfg(c);
-    x.kt = cf.kt;
-    if (x.strat) cf.smem = ((cf.smem + 15) & ~(size_t)15) + (size_t)c->nx * cf.kt * sizeof(double2);
-    dim3 grid((c->nzh + cf.kt - 1) / cf.kt, c->ny);
-    c->launches++;
-    if (c->fp32) k_xfwd<float, 8><<<grid, cf.nthr, cf.smem, c->stream>>>(x);
-    else k_xfwd<double, 4><<<grid, cf.nthr, cf.smem, c->stream>>>(x);
-}
-
-static int ew_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+static int ew_blocks(size_t n) {
+    return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 // ---------------------------------------------------------------------------
 // argument builders
@@ -404,6 +446,7 @@ static ZArgs z_args(spk_ctx* c) {
     z.ch_u = z.ch_b = z.ch_th = z.ch_gx = z.ch_gy = -1;
     z.maxbits = c->sc->maxbits;
     z.nonfinite = &c->sc->nonfinite;
+    z.err = &c->sc->err;
     z.breal = c->breal;
     z.sd = c->p.strat_direction;
     z.chi = 1.0 / c->p.reynolds_ani;
@@ -447,12 +490,37 @@ static void pass_y_forward(spk_ctx* c, int nch, void* in, void* out) {
     if (a.kcols > 0) axis(c, a, -1);
 }
 
+// x-forward pass of the products (bufB -> bufA): kept ky rows in, kept kx
+// rows out, kz < kz_keep.
+static void pass_x_forward(spk_ctx* c) {
+    AxisArgs a = axis_args(c, 0);
+    a.kcols = c->kz_keep;
+    a.row_filter = 1;
+    a.outer_filter = 1;
+    add_job(c, a, c->bufB, c->bufA, c->nout, 0, 0, 0);
+    if (a.kcols > 0) axis(c, a, -1);
+}
+
+// elementwise RHS + Leray + time update of every mode
+static void rhs(spk_ctx* c, XfArgs& x) {
+    const FastDiv fz = FastDiv::make((unsigned)c->nzh);
+    c->launches++;
+    if (c->fp32) k_rhs<float><<<ew_blocks(c->nc), 256, 0, c->stream>>>(x, fz);
+    else k_rhs<double><<<ew_blocks(c->nc), 256, 0, c->stream>>>(x, fz);
+}
+
+static void xfwd(spk_ctx* c, XfArgs& x) {
+    pass_x_forward(c);
+    rhs(c, x);
+}
+
 static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     XfArgs x;
     memset(&x, 0, sizeof(x));
     x.g = c->g;
     x.plan = c->plan_x;
-    x.nl = c->bufB; x.cs_nl = c->g.ncs;
+    x.nl = c->bufA; x.cs_nl = c->g.ncs;   // products after the x-forward pass
+    x.lny = ilog2(c->ny);
     x.nl_T = c->out_T; x.nl_E = c->out_E; x.nl_F = c->out_F; x.nl_Q = c->out_Q;
     x.U = U; x.S = c->S; x.out = nullptr;
     x.F = c->F; x.VEL = c->VEL; x.MAG = c->MAG; x.TH = c->TH;
@@ -860,14 +928,6 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
     // shared-memory limits of the instantiations used
     const int big = 200 * 1024;
-    CK(cudaFuncSetAttribute(k_zpass<float, EPT_Z_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_zpass<double, EPT_Z_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<float, 1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<float, -1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<double, 1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<double, -1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     CK(cudaFuncSetAttribute(k_xfwd_rkl<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     CK(cudaFuncSetAttribute(k_xfwd_rkl<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     return SPK_OK;
@@ -1126,27 +1186,29 @@ extern "C" const char* spk_last_error(const spk_ctx* c) {
 // ---------------------------------------------------------------------------
 // accounting and per-pass timing
 // ---------------------------------------------------------------------------
-struct PassBytes { double x_inv, y_inv, z, y_fwd, x_fwd[3]; };
+struct PassBytes { double x_inv, y_inv, z, y_fwd, x_fwd, rhs[3]; };
 
 // Algorithmic HBM bytes of each pass: every array the pass must read or
 // write, once; products only where the 2/3 mask keeps them.
 static PassBytes pass_bytes(const spk_ctx* c) {
     PassBytes b;
     const double nc = (double)c->nc, b_t = (double)csize(c), s16 = 16.0;
-    int ny_keep = 0;
+    int nx_keep = 0, ny_keep = 0;
+    for (int i = 0; i < c->nx; i++) nx_keep += c->mx[i] != 0.0;
     for (int j = 0; j < c->ny; j++) ny_keep += c->my[j] != 0.0;
     const double nkz = (double)c->nx * c->ny * c->kz_keep;          // after the z R2C
     const double nkyz = (double)c->nx * ny_keep * c->kz_keep;       // after the y forward
+    const double nkxyz = (double)nx_keep * ny_keep * c->kz_keep;    // after the x forward
     const int nx_in = c->F + (c->aniso_rhs ? 1 : 0);                // x inverse outputs (gx extra)
     b.x_inv = c->F * nc * s16 + nx_in * nc * b_t;
     b.y_inv = nx_in * nc * b_t + c->nin * nc * b_t;
     b.z = c->nin * nc * b_t + c->nout * nkz * b_t;
     b.y_fwd = c->nout * nkz * b_t + c->nout * nkyz * b_t;
-    const double nl = c->nout * nkyz * b_t;
-    const double strat = c->p.stratification ? 2.0 * nc * s16 : 0.0;   // theta and u_strat re-read
-    b.x_fwd[0] = nl + 3.0 * c->F * nc * s16 + strat;    // U r, U w, S w
-    b.x_fwd[1] = nl + 4.0 * c->F * nc * s16 + strat;    // U r, S r, U w, S w
-    b.x_fwd[2] = nl + 3.0 * c->F * nc * s16 + strat;    // U r, S r, U w
+    b.x_fwd = c->nout * nkyz * b_t + c->nout * nkxyz * b_t;
+    const double nl = c->nout * nkxyz * b_t;
+    b.rhs[0] = nl + 3.0 * c->F * nc * s16;    // U r, U w, S w
+    b.rhs[1] = nl + 4.0 * c->F * nc * s16;    // U r, S r, U w, S w
+    b.rhs[2] = nl + 3.0 * c->F * nc * s16;    // U r, S r, U w
     return b;
 }
 
@@ -1170,7 +1232,7 @@ extern "C" int spk_step_info(spk_ctx* c, int* kps, double* bytes) {
             *bytes = 3.0 * 3.0 * c->F * (double)c->nc * 16.0;
         } else {
             const PassBytes b = pass_bytes(c);
-            *bytes = 3.0 * (b.x_inv + b.y_inv + b.z + b.y_fwd) + b.x_fwd[0] + b.x_fwd[1] + b.x_fwd[2];
+            *bytes = 3.0 * (b.x_inv + b.y_inv + b.z + b.y_fwd + b.x_fwd) + b.rhs[0] + b.rhs[1] + b.rhs[2];
         }
     }
     return SPK_OK;
@@ -1183,15 +1245,16 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     const PassBytes pb = pass_bytes(c);
-    const char* names[5] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward_rhs_rk"};
-    const double bytes[5] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd[2]};
+    const char* names[6] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward", "rhs_rk"};
+    const double bytes[6] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd, pb.rhs[2]};
     int n = 0;
     // one warm pipeline so every buffer holds stage data
     pass_x_inverse(c, c->U, true);
     pass_y_inverse(c, true);
     pass_z_products(c, false);
     pass_y_forward(c, c->nout, c->bufA, c->bufB);
-    for (int k = 0; k < 5 && n < max_out; k++) {
+    pass_x_forward(c);
+    for (int k = 0; k < 6 && n < max_out; k++) {
         CK(cudaEventRecord(e0, c->stream));
         for (int r = 0; r < reps; r++) {
             switch (k) {
@@ -1199,7 +1262,8 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
                 case 1: pass_y_inverse(c, true); break;
                 case 2: pass_z_products(c, false); break;
                 case 3: pass_y_forward(c, c->nout, c->bufA, c->bufB); break;
-                default: { XfArgs x = xf_args(c, c->U, XM_RK2, false); xfwd(c, x); } break;
+                case 4: pass_x_forward(c); break;
+                default: { XfArgs x = xf_args(c, c->U, XM_RK2, false); rhs(c, x); } break;
             }
         }
         CK(cudaEventRecord(e1, c->stream));
@@ -1239,22 +1303,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SPK_NOALLOC_SCR
 // array's name is only a stand-in: a kernel must receive this address.
 static void* g_noalloc_ptr[SPK_NOALLOC_MAX_DEVICES];
 
-// Once per device, with that device current: the scratch address, the
-// shared-memory limits of the pass kernels and the tensor-map encoder.
+// Once per device, with that device current: the scratch address (and,
+// once per process, the tensor-map encoder).
 static int noalloc_setup(int dev) {
     if (g_noalloc_ptr[dev]) return SPK_OK;
     spk_ctx* c = nullptr;   // errors go to spk_last_error(NULL)
     void* ptr = nullptr;
     CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    const int big = 200 * 1024;
-    CK(cudaFuncSetAttribute(k_zpass<float, EPT_Z_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_zpass<double, EPT_Z_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<float, 1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<float, -1, EPT_AXIS_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<double, 1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_axis<double, -1, EPT_AXIS_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     if (!g_encode) {
         cudaDriverEntryPointQueryResult q;
         void* fn = nullptr;

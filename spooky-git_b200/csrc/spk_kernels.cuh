@@ -84,6 +84,7 @@ struct AxisArgs {
     int kt;         // tile width (k columns, a power of two)
     int kcols;      // process columns [0, kcols)
     int row_filter; // store only rows whose mask factor along the axis is 1
+    int outer_filter; // skip tiles whose outer index has mask factor 0 (no load, no store)
     int box_rows;   // rows per TMA box (<= 256); N / box_rows boxes per tile
     int nst;        // pipeline stages
     int convert;    // input type differs from the pass type (FP64 state in the FP32 form)
@@ -112,6 +113,7 @@ struct ZArgs {
     int do_max;
     unsigned long long* maxbits;
     int* nonfinite;
+    int* err;               // set to 2 when a bulk copy never completed
     void* breal;            // real B lines [3][nx*ny*nz], pass precision
     int store_breal, load_breal;
     double* real_out;       // ZM_TO_REAL: [nin][nx*ny*nz] FP64
@@ -135,6 +137,7 @@ struct XfArgs {
     double nu, nu_m, nu_th, N2;
     int mode, clean;
     const DevScalars* sc;
+    int lny;                // log2 ny (elementwise RHS kernel)
 };
 
 struct RklArgs {

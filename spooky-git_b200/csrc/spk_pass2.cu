@@ -1,0 +1,565 @@
+// spk_pass2.cu -- strided-axis FFT pass on the register-resident FFT.
+//
+// Tile = one channel, one outer index, KT consecutive k columns, all N
+// positions along the axis ([N][KT] in shared memory, the TMA box layout).
+// A persistent CTA keeps nst tiles in flight with cp.async.bulk.tensor loads
+// completing on per-stage mbarriers (bounded waits).  For each tile, thread
+// (column c, sub-index q) reads its first-stage legs straight from the
+// stage buffer -- converting the FP64 state, applying the 1/N^3 scale of
+// scaleKernel (cufft_routines.cu:23-39) and the i*k derivative of Gradient
+// (cuda_kernels_generic.cu:249-260) on the way -- releases the stage to the
+// next load, runs the transform in registers with one shared-memory
+// exchange per further stage, and stores X[k] from registers to the pass
+// buffer (kept ky rows only in the y-forward pass).
+#include "spk_regfft.cuh"
+
+namespace spk {
+
+// Tile width of the strided-axis pass: KT columns x TPC threads = 256
+// threads (KT <= 64); an FP64 input tile in the FP32 form (CONV) is half as
+// wide so that one pipeline stage stays at 32 KB.
+template <typename T, int LN, bool CONV>
+__host__ __device__ constexpr int axis_kt() {
+    constexpr int tpc = RegFft<T, LN>::TPC;
+    constexpr int kt = (256 / tpc) > 64 ? 64 : (256 / tpc);
+    return (CONV && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
+}
+
+template <typename T, int LN, int DIR, bool CONV>
+__global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
+    using F = RegFft<T, LN>;
+    constexpr int N = F::N;
+    constexpr int KT = axis_kt<T, LN, CONV>(), LKT = ilog2c(KT);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (a.gate && a.gate_stage > a.gate->s_rkl) return;
+    const int NST = a.nst;
+    const int tid = threadIdx.x;
+    const int c = tid & (KT - 1), q = tid >> LKT;
+    const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
+    const int nkb = (a.kcols + KT - 1) / KT;
+    const int total = a.njobs * nouter * nkb;
+    constexpr size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
+    constexpr size_t stage_bytes = ((size_t)N * KT * in_elem + 127) & ~(size_t)127;
+    unsigned char* sbase = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sbase);
+    unsigned char* stages = sbase + 128;
+    C2<T>* xbuf = reinterpret_cast<C2<T>*>(stages + (size_t)NST * stage_bytes);
+    C2<T>* tw = xbuf + (size_t)N * KT;
+    T* kax = reinterpret_cast<T*>(tw + N);                           // wavenumbers along the axis
+    unsigned char* keep = reinterpret_cast<unsigned char*>(kax + N);  // row mask factor != 0
+    const int stride = a.axis == 0 ? a.g.ny * a.g.nzs : a.g.nzs;
+    constexpr uint32_t tile_bytes = (uint32_t)((size_t)N * KT * in_elem);
+    const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
+
+    const double* omask = a.axis == 0 ? a.g.my : a.g.mx;   // mask factor of the outer index
+    auto issue = [&](int t, int s) {
+        const int jb = t / (nouter * nkb);
+        const int rem = t - jb * nouter * nkb;
+        const int o = rem / nkb, kb = rem - o * nkb;
+        const AxisJob& jo = a.job[jb];
+        unsigned char* dst = stages + (size_t)s * stage_bytes;
+        if (a.outer_filter && omask[o] == 0.0) {   // skipped tile: complete the phase with no bytes
+            mbar_expect_tx(&bar[s], 0);
+            return;
+        }
+        mbar_expect_tx(&bar[s], tile_bytes);
+        for (int b = 0; b < N / a.box_rows; b++) {
+            if (a.axis == 0) tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, o, b * a.box_rows, jo.ch);
+            else             tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, b * a.box_rows, o, jo.ch);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    {
+        const C2<T>* twg = (const C2<T>*)a.plan.tw;
+        const double* kg = a.axis == 0 ? a.g.kx : a.g.ky;
+        const double* mg = a.axis == 0 ? a.g.mx : a.g.my;
+        for (int i = tid; i < N; i += blockDim.x) {
+            tw[i] = twg[i];
+            kax[i] = (T)kg[i];
+            keep[i] = mg[i] != 0.0;
+        }
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int s = 0; s < NST; s++) {
+            const int t = blockIdx.x + s * gridDim.x;
+            if (t < total) issue(t, s);
+        }
+
+    int i = 0;
+    bool aborted = false;
+    C2<T> r[F::E];
+    for (int t = blockIdx.x; t < total; t += gridDim.x, i++) {
+        const int s = i % NST;
+        const uint32_t par = (uint32_t)((i / NST) & 1);
+        const bool ok = mbar_wait(&bar[s], par, SPK_WAIT_ITERS);
+        if (__syncthreads_or(!ok)) { aborted = true; break; }
+        const int jb = t / (nouter * nkb);
+        const int rem = t - jb * nouter * nkb;
+        const int o = rem / nkb, kb = rem - o * nkb;
+        const AxisJob& jo = a.job[jb];
+        const int k0 = kb * KT;
+        const int kt = min(KT, a.kcols - k0);
+        const unsigned char* stg = stages + (size_t)s * stage_bytes;
+        const bool deriv = jo.deriv != 0;
+        const double scale = a.scale;
+        const bool skip = a.outer_filter && omask[o] == 0.0;   // uniform over the CTA
+        if (skip) {
+        } else if constexpr (CONV) {
+            const double2* src = reinterpret_cast<const double2*>(stg);
+            const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
+            regfft_load<T, LN, DIR>(r, q, [&](int n) -> C2<T> {
+                double2 x = src[n * KT + c];
+                if (deriv) x = ik_mul(kd[n], x);
+                return mk<T>((T)(x.x * scale), (T)(x.y * scale));
+            });
+        } else {
+            const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
+            const T sc = (T)scale;
+            regfft_load<T, LN, DIR>(r, q, [&](int n) -> C2<T> {
+                C2<T> v = src[n * KT + c];
+                if (deriv) { const T kk = kax[n]; v = mk<T>(-kk * v.y, kk * v.x); }
+                return mk<T>(v.x * sc, v.y * sc);
+            });
+        }
+        __syncthreads();   // every thread has read the stage
+        const int tn = t + NST * gridDim.x;
+        if (tid == 0 && tn < total) {
+            fence_proxy_async_smem();
+            issue(tn, s);
+        }
+        const size_t base = a.axis == 0 ? (size_t)o * a.g.nzs : (size_t)o * a.g.ny * a.g.nzs;
+        C2<T>* out = (C2<T>*)jo.out + base + k0;
+        const bool col_ok = c < kt;
+        const bool filt = a.row_filter != 0;
+        if (skip) continue;
+        regfft_run<T, LN, DIR>(
+            r, q, tw, [&](int L) { return xbuf + (size_t)L * KT + c; },
+            [&](int k, C2<T> v) {
+                if (col_ok && (!filt || keep[k])) out[k * stride + c] = v;
+            });
+    }
+    if (aborted) {
+        if (tid == 0) {
+            atomicExch(a.err, 2);
+            for (int s = 0; s < NST; s++) mbar_wait(&bar[s], (uint32_t)(((i + s) / NST) & 1), SPK_WAIT_ITERS);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z pass on the register FFT.  A CTA owns L consecutive (i,j) lines:
+//  1. one bulk copy per input channel brings the L half spectra (rows of
+//     nzs complex) into shared memory;
+//  2. the input channels, paired into complex sequences Z = A + iB
+//     (Hermitian-extended, DC/Nyquist imaginary parts dropped), are
+//     inverse-transformed; the real fields go to shared memory;
+//  3. maxima of |u|, |B| for compute_dt (compute_dt.cu:82-101,196-210) and
+//     the real B lines for the anisotropic STS flux, when asked;
+//  4. the products, formed point by point inside the forward transform's
+//     load -- TracelessShearMatrix[MHD] (cuda_kernels.cu:39-55, 216-234),
+//     MagneticEmf (:240-252), EnergyFluxVector (:277-289),
+//     ComputeBGradTheta + ComputeAnisotropicHeatFlux (:360-383) -- are
+//     paired again and forward-transformed; the paired spectra are unpacked
+//     into the half spectra of each product (their D2Z), kz < kz_keep.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T z_product(const ZArgs& a, int ch, T ux, T uy, T uz, T bx, T by, T bz, T th, T gx, T gy,
+                                       T gz) {
+    int q = 0;
+    if (a.mode == ZM_PRODUCTS) {
+        if (a.hydro) {
+            if (ch < 5) {
+                if (!a.mhd) {
+                    switch (ch) {
+                        case 0: return ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0;
+                        case 1: return ux * uy;
+                        case 2: return ux * uz;
+                        case 3: return (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0;
+                        default: return uy * uz;
+                    }
+                }
+                switch (ch) {
+                    case 0: return ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0;
+                    case 1: return ux * uy - bx * by;
+                    case 2: return ux * uz - bx * bz;
+                    case 3: return (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0;
+                    default: return uy * uz - by * bz;
+                }
+            }
+            q = 5;
+        }
+        if (a.mhd) {
+            if (ch < q + 3) {
+                const int c = ch - q;
+                return c == 0 ? -by * uz + bz * uy : (c == 1 ? bx * uz - bz * ux : -bx * uy + by * ux);
+            }
+            q += 3;
+        }
+        if (a.bous) {
+            if (ch < q + 3) {
+                const int c = ch - q;
+                return c == 0 ? ux * th : (c == 1 ? uy * th : uz * th);
+            }
+            q += 3;
+        }
+    }
+    if (a.aniso && ch < q + 3) {
+        const int c = ch - q;
+        const T bgt = bx * gx + by * gy + bz * gz;
+        const T b2 = bx * bx + by * by + bz * bz;
+        const T bs = a.sd == 0 ? bx : (a.sd == 1 ? by : bz);
+        const T chi = (T)a.chi, W = (T)a.omegaT2;
+        const T bc = c == 0 ? bx : (c == 1 ? by : bz);
+        return chi * bc * (bgt + W * bs) / b2;
+    }
+    return (T)0;
+}
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared-memory carve of k_zpass2 (host and device agree through this).
+struct ZSmem { size_t tw, raw, real, xb, total; };
+__host__ __device__ inline ZSmem zsmem_layout(int n, int csz, int nin, int nin_all, int lines, int nzs, int slots) {
+    ZSmem z;
+    const int rs = n + 16, xs = n + (n >> 4);
+    z.tw = 128;
+    z.raw = align16(z.tw + (size_t)n * csz);
+    z.real = align16(z.raw + (size_t)nin * lines * nzs * csz);
+    z.xb = align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
+    z.total = align16(z.xb + (size_t)slots * xs * csz);
+    return z;
+}
+
+template <typename T, int LN>
+__global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs a) {
+    using F = RegFft<T, LN>;
+    constexpr int N = F::N, LTPC = F::LTPC, TPC = F::TPC;
+    constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
+    constexpr int XS = N + (N >> 4);      // exchange slot (one pad element per 16)
+    if (a.gate && a.gate_stage > a.gate->s_rkl) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int L = a.lines, nzs = a.g.nzs;
+    const int nlines = a.g.nx * a.g.ny;
+    const int line0 = blockIdx.x * L;
+    const int nl = min(L, nlines - line0);
+    const int nin = a.nin;
+    const int nin_all = nin + (a.derive_gz == 1 ? 1 : 0);
+    const int npin = (nin_all + 1) / 2, npout = (a.nout + 1) / 2;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int slots = nthr >> LTPC;
+    const int sigma = tid >> LTPC, q = tid & (TPC - 1);
+    const ZSmem lay = zsmem_layout(N, (int)sizeof(C2<T>), nin, nin_all, L, nzs, slots);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+    C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
+    C2<T>* raw = reinterpret_cast<C2<T>*>(smem_raw + lay.raw);
+    T* real = reinterpret_cast<T*>(smem_raw + lay.real);
+    C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
+    const C2<T>* in = (const C2<T>*)a.in;
+
+    // 1. bulk copies of the input half spectra
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)((size_t)nl * nzs * sizeof(C2<T>));
+        mbar_expect_tx(bar, bytes * (uint32_t)nin);
+        for (int ch = 0; ch < nin; ch++)
+            bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
+    }
+    {
+        const C2<T>* twg = (const C2<T>*)a.plan.tw;
+        for (int i = tid; i < N; i += nthr) tw[i] = twg[i];
+    }
+    const bool ok = mbar_wait(bar, 0, SPK_WAIT_ITERS);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+            atomicExch(a.err, 2);
+            mbar_wait(bar, 0, SPK_WAIT_ITERS);   // bounded drain of the copies in flight
+        }
+        __syncthreads();
+        return;
+    }
+
+    auto xaddr = [&](int Lx) { return xb + (size_t)sigma * XS + padi<1>(Lx); };
+    C2<T> r[F::E];
+
+    // 2. inverse transforms of the input pairs
+    const int ninv = npin * L;
+    for (int base = 0; base < ninv; base += slots) {
+        const int tau = base + sigma;
+        const bool valid = tau < ninv;
+        const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
+        auto chv = [&](int ch, int k) -> C2<T> {
+            if (ch < nin) {
+                C2<T> v = raw[((size_t)ch * L + l) * nzs + k];
+                if (a.derive_gz == 2 && ch == a.ch_th) {
+                    const T kz = (T)a.g.kz[k];
+                    v = mk<T>(-kz * v.y, kz * v.x);
+                }
+                return v;
+            }
+            if (ch == nin && a.derive_gz == 1) {
+                const C2<T> th = raw[((size_t)a.ch_th * L + l) * nzs + k];
+                const T kz = (T)a.g.kz[k];
+                return mk<T>(-kz * th.y, kz * th.x);
+            }
+            return mk<T>((T)0, (T)0);
+        };
+        regfft_load<T, LN, +1>(r, q, [&](int n) -> C2<T> {
+            constexpr int NH = N >> 1;
+            const int k = n <= NH ? n : N - n;
+            const C2<T> A = chv(2 * p, k), B = chv(2 * p + 1, k);
+            if (n == 0 || n == NH) return mk<T>(A.x, B.x);
+            if (n < NH) return mk<T>(A.x - B.y, A.y + B.x);
+            return mk<T>(A.x + B.y, B.x - A.y);
+        });
+        const bool to_real = a.mode == ZM_TO_REAL && valid && l < nl;
+        regfft_run<T, LN, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
+            if (!valid) return;
+            real[((size_t)(2 * p) * L + l) * RS + z] = v.x;
+            if (2 * p + 1 < nin_all) real[((size_t)(2 * p + 1) * L + l) * RS + z] = v.y;
+            if (to_real) {
+                const size_t line = (size_t)(line0 + l);
+                if (2 * p < nin) a.real_out[((size_t)(2 * p) * nlines + line) * N + z] = (double)v.x;
+                if (2 * p + 1 < nin) a.real_out[((size_t)(2 * p + 1) * nlines + line) * N + z] = (double)v.y;
+            }
+        });
+    }
+    __syncthreads();
+    if (a.mode == ZM_TO_REAL) return;
+
+    auto R = [&](int ch, int l, int z) -> T { return real[((size_t)ch * L + l) * RS + z]; };
+    T* breal = (T*)a.breal;
+
+    // 3. maxima for the CFL condition, real B for the STS flux
+    if (a.do_max || a.store_breal) {
+        T mu[6] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
+        int bad = 0;
+        for (int e = tid; e < nl * N; e += nthr) {
+            const int l = e >> LN, z = e & (N - 1);
+            const size_t line = (size_t)(line0 + l);
+            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0;
+            if (a.ch_u >= 0) { ux = R(a.ch_u, l, z); uy = R(a.ch_u + 1, l, z); uz = R(a.ch_u + 2, l, z); }
+            if (a.ch_b >= 0) { bx = R(a.ch_b, l, z); by = R(a.ch_b + 1, l, z); bz = R(a.ch_b + 2, l, z); }
+            if (a.store_breal) {
+                breal[(0 * (size_t)nlines + line) * N + z] = bx;
+                breal[(1 * (size_t)nlines + line) * N + z] = by;
+                breal[(2 * (size_t)nlines + line) * N + z] = bz;
+            }
+            if (a.do_max) {
+                const T av[6] = {fabs(ux), fabs(uy), fabs(uz), fabs(bx), fabs(by), fabs(bz)};
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    if (!isfinite(av[c])) bad = 1;
+                    mu[c] = fmax(mu[c], av[c]);
+                }
+            }
+        }
+        if (a.do_max) {
+            // the xb area is free here: 6 x 32 block-max scratch
+            T* red = reinterpret_cast<T*>(xb);
+            warp_block_max<T>(mu, 6, red);
+            if (tid < 6) {
+                const double m = (double)red[tid * 32];
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+                unsigned long long* dst = a.maxbits + tid;
+                if (bits > *((volatile unsigned long long*)dst)) atomicMax(dst, bits);
+            }
+            if (bad) atomicOr(a.nonfinite, 1);
+            __syncthreads();
+        }
+    }
+    if (a.nout == 0) return;
+
+    // 4. products, forward transforms, unpacked half spectra
+    const int kk = a.g.kz_keep;
+    C2<T>* out = (C2<T>*)a.out;
+    const T half = (T)0.5;
+    const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+    const int nfw = npout * L;
+    for (int base = 0; base < nfw; base += slots) {
+        __syncthreads();   // the previous round's unpack has read the exchange slots
+        const int tau = base + sigma;
+        const bool valid = tau < nfw;
+        const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
+        const size_t line = (size_t)(line0 + l);
+        regfft_load<T, LN, -1>(r, q, [&](int z) -> C2<T> {
+            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
+            if (a.ch_u >= 0) { ux = R(a.ch_u, l, z); uy = R(a.ch_u + 1, l, z); uz = R(a.ch_u + 2, l, z); }
+            if (a.load_breal) {
+                if (l < nl) {
+                    bx = breal[(0 * (size_t)nlines + line) * N + z];
+                    by = breal[(1 * (size_t)nlines + line) * N + z];
+                    bz = breal[(2 * (size_t)nlines + line) * N + z];
+                }
+            } else if (a.ch_b >= 0) {
+                bx = R(a.ch_b, l, z); by = R(a.ch_b + 1, l, z); bz = R(a.ch_b + 2, l, z);
+            }
+            if (a.ch_th >= 0 && a.derive_gz != 2) th = R(a.ch_th, l, z);
+            if (a.ch_gx >= 0) gx = R(a.ch_gx, l, z);
+            if (a.ch_gy >= 0) gy = R(a.ch_gy, l, z);
+            if (a.derive_gz == 1) gz = R(nin, l, z);
+            else if (a.derive_gz == 2) gz = R(a.ch_th, l, z);
+            const T v0 = z_product<T>(a, 2 * p, ux, uy, uz, bx, by, bz, th, gx, gy, gz);
+            const T v1 = 2 * p + 1 < a.nout ? z_product<T>(a, 2 * p + 1, ux, uy, uz, bx, by, bz, th, gx, gy, gz) : (T)0;
+            return mk<T>(v0, v1);
+        });
+        regfft_run<T, LN, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; });
+        __syncthreads();
+        for (int s2 = warp; s2 < slots; s2 += nwarp) {
+            const int tau2 = base + s2;
+            if (tau2 >= nfw) break;
+            const int p2 = tau2 / L, l2 = tau2 - p2 * L;
+            if (l2 >= nl) continue;
+            const C2<T>* Z = xb + (size_t)s2 * XS;
+            const size_t off0 = (size_t)(line0 + l2) * nzs;
+            for (int k = lane; k < kk; k += 32) {
+                const C2<T> zk = Z[padi<1>(k)], zm = Z[padi<1>(k ? N - k : 0)];
+                out[(size_t)(2 * p2) * a.cs_out + off0 + k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+                if (2 * p2 + 1 < a.nout)
+                    out[(size_t)(2 * p2 + 1) * a.cs_out + off0 + k] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RHS, Leray projection and time update, one mode per thread, after the
+// x-forward pass has transformed the products:
+//   NonLinHydroAdv (cuda_kernels.cu:82-98), MagneticShear (:257-272),
+//   NonLinBoussinesqAdv (:293-304) with the 2/3 mask (DivergenceMask,
+//   cuda_kernels_generic.cu:315-334), BoussinesqStrat (:310-325), the
+//   parabolic terms (physics.cu:145-230: nablaOpVector/Scalar, or the
+//   anisotropic flux divergence of AnisotropicHeatFlux), GradPseudoPressure
+//   (:128-159), and axpyComplex of RungeKutta3 / ForwardEuler
+//   (hydro_mhd_advance.cu:79-248), with CleanDivergence of the next step
+//   (cuda_kernels_generic.cu:288-313) on the last stage.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
+    const size_t nc = a.g.nc;
+    const int nzh = a.g.nzh, lny = a.lny, nzs = a.g.nzs;
+    const double dt = a.sc->dt;
+    const C2<T>* nl = (const C2<T>*)a.nl;
+    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+        const unsigned line = fzh.div((unsigned)gi);
+        const int k = (int)(gi - (size_t)line * nzh);
+        const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
+        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const bool m = a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0;
+        const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
+        auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
+        double2 th_old = d2(0.0, 0.0), usd = d2(0.0, 0.0);
+        if (a.bous) th_old = a.U[(size_t)a.TH * nc + gi];
+
+        if (a.incompressible) {
+            double2 X[3], R[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.VEL + c) * nc + gi];
+            double2 s0 = d2(0.0, 0.0), s1 = d2(0.0, 0.0), s2 = d2(0.0, 0.0);
+            if (m && a.nl_T >= 0) {
+                const double2 t0 = P(a.nl_T), t1 = P(a.nl_T + 1), t2 = P(a.nl_T + 2), t3 = P(a.nl_T + 3), t4 = P(a.nl_T + 4);
+                // k_j T_ij with T = [[t0 t1 t2] [t1 t3 t4] [t2 t4 -t0-t3]]
+                s0 = d2(kx * t0.x + ky * t1.x + kz * t2.x, kx * t0.y + ky * t1.y + kz * t2.y);
+                s1 = d2(kx * t1.x + ky * t3.x + kz * t4.x, kx * t1.y + ky * t3.y + kz * t4.y);
+                s2 = d2(kx * t2.x + ky * t4.x - kz * (t0.x + t3.x), kx * t2.y + ky * t4.y - kz * (t0.y + t3.y));
+            }
+            R[0] = d2(s0.y, -s0.x);   // -i * mask * k_j T_ij
+            R[1] = d2(s1.y, -s1.x);
+            R[2] = d2(s2.y, -s2.x);
+            if (a.strat) {
+                if (a.sd == 0)      { R[0] = d2(R[0].x - th_old.x, R[0].y - th_old.y); usd = X[0]; }
+                else if (a.sd == 1) { R[1] = d2(R[1].x - th_old.x, R[1].y - th_old.y); usd = X[1]; }
+                else                { R[2] = d2(R[2].x - th_old.x, R[2].y - th_old.y); usd = X[2]; }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if (!((a.sts_mask >> (a.VEL + c)) & 1u)) {
+                    const double f = -a.nu * k2;
+                    R[c] = d2(R[c].x + f * X[c].x, R[c].y + f * X[c].y);
+                }
+            }
+            // Leray: dU += i k (i k.dU)/k^2
+            const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
+            const double sx = kx * R[0].x + ky * R[1].x + kz * R[2].x;
+            const double sy = kx * R[0].y + ky * R[1].y + kz * R[2].y;
+            const double kk[3] = {kx, ky, kz};
+#pragma unroll
+            for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
+            double2 Un[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) Un[c] = step_value(a, (size_t)(a.VEL + c) * nc + gi, X[c], R[c], dt);
+            if (a.mode != XM_DFIELD) {
+                if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.U[(size_t)(a.VEL + c) * nc + gi] = Un[c];
+            }
+        }
+
+        if (a.mhd) {
+            double2 X[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.MAG + c) * nc + gi];
+            double2 s0 = d2(0.0, 0.0), s1 = d2(0.0, 0.0), s2 = d2(0.0, 0.0);
+            if (m && a.nl_E >= 0) {
+                const double2 e0 = P(a.nl_E), e1 = P(a.nl_E + 1), e2 = P(a.nl_E + 2);
+                // k x E
+                s0 = d2(ky * e2.x - kz * e1.x, ky * e2.y - kz * e1.y);
+                s1 = d2(kz * e0.x - kx * e2.x, kz * e0.y - kx * e2.y);
+                s2 = d2(kx * e1.x - ky * e0.x, kx * e1.y - ky * e0.y);
+            }
+            const double2 S3[3] = {s0, s1, s2};
+            double2 Un[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double2 R = d2(-S3[c].y, S3[c].x);   // i * mask * (k x E)
+                if (!((a.sts_mask >> (a.MAG + c)) & 1u)) {
+                    const double f = -a.nu_m * k2;
+                    R = d2(R.x + f * X[c].x, R.y + f * X[c].y);
+                }
+                Un[c] = step_value(a, (size_t)(a.MAG + c) * nc + gi, X[c], R, dt);
+            }
+            if (a.mode != XM_DFIELD) {
+                if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.U[(size_t)(a.MAG + c) * nc + gi] = Un[c];
+            }
+        }
+
+        if (a.bous) {
+            const double2 X = th_old;
+            double2 R = d2(0.0, 0.0);
+            if (m && a.nl_F >= 0) {
+                const double2 f0 = P(a.nl_F), f1 = P(a.nl_F + 1), f2 = P(a.nl_F + 2);
+                const double2 s = d2(kx * f0.x + ky * f1.x + kz * f2.x, kx * f0.y + ky * f1.y + kz * f2.y);
+                R = d2(s.y, -s.x);   // -i * mask * k.(u theta)
+            }
+            if (a.strat) R = d2(R.x + a.N2 * usd.x, R.y + a.N2 * usd.y);
+            if (!((a.sts_mask >> a.TH) & 1u)) {
+                if (a.aniso_rhs) {
+                    if (m && a.nl_Q >= 0) {
+                        const double2 q0 = P(a.nl_Q), q1 = P(a.nl_Q + 1), q2 = P(a.nl_Q + 2);
+                        const double2 s = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
+                        R = d2(R.x - s.y, R.y + s.x);   // += i * mask * k.q
+                    }
+                } else {
+                    const double f = -a.nu_th * k2;
+                    R = d2(R.x + f * X.x, R.y + f * X.y);
+                }
+            }
+            const double2 Un = step_value(a, (size_t)a.TH * nc + gi, X, R, dt);
+            if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
+        }
+    }
+}
+
+}  // namespace spk

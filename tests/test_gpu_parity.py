@@ -76,6 +76,28 @@ def test_compute_dfield_matches_oracle(case, shape, form):
     assert rel_l2(dUd.cpu().numpy(), ref) < TOL_RHS[form]
 
 
+# Long axes: every transform length from 2 to 1024 and every stage layout of
+# the register FFT (one stage, full stages, full stages + a radix-2/4/8 tail)
+# along x, y and z, in both precisions.
+LONG_SHAPES = [(256, 32, 16), (32, 256, 8), (1024, 8, 4), (8, 512, 16), (128, 64, 2), (16, 8, 512),
+               (64, 16, 1024), (4, 2, 256)]
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+@pytest.mark.parametrize("shape", LONG_SHAPES)
+def test_compute_dfield_long_axes_matches_oracle(shape, form):
+    case = "bous_mhd_aniso" if shape[0] * shape[1] * shape[2] <= 65536 else "mhd"
+    p = default_params(gridsize=shape, boxsize=(1.0, 1.5, 2.0), form=form, **CASES[case])
+    U = make_state(p, seed=17)
+    ref = O.Oracle(p).compute_dfield(U)
+    ctx = Context(p)
+    Ud = torch_dev(U)
+    dUd = torch_dev(np.zeros_like(U))
+    ctx.compute_dfield(Ud, dUd)
+    ctx.synchronize()
+    assert rel_l2(dUd.cpu().numpy(), ref) < TOL_RHS[form]
+
+
 @pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
 @pytest.mark.parametrize("shape", [(16, 16, 16), (32, 8, 16), (8, 8, 2)])
 def test_to_real_matches_oracle(shape, form):
