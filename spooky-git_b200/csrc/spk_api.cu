@@ -251,7 +251,8 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     const size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
-    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)N * sizeof(C2<T>) + (size_t)N * sizeof(T) + N + 16;
+    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, LN>::TWN * sizeof(C2<T>) +
+                         (size_t)N * sizeof(T) + N + 16;
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
@@ -315,16 +316,28 @@ static void axis(spk_ctx* c, AxisArgs& a, int dir) {
 
 template <typename T, int LN>
 static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
-    const int nthr = 256;
-    const int slots = nthr / regfft_geom(1 << LN, sizeof(T) == 4).TPC;
+    const int nthr = 128;
+    const int slots = std::max(1, nthr / RegFft<T, LN>::TPC);
     const long nlines = (long)c->nx * c->ny;
+    const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
     auto need = [&](int lines) {
-        return zsmem_layout(1 << LN, (int)sizeof(C2<T>), z.nin, nin_all, lines, c->g.nzs, slots).total;
+        return zsmem_layout(1 << LN, RegFft<T, LN>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
+                            slots).total;
     };
-    // lines per CTA: the most (<= 64) that keep two CTAs per SM
-    int L = 64;
-    while (L > 1 && need(L) > (size_t)110 * 1024) L >>= 1;
-    L = (int)std::min<long>(L, nlines);
+    // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
+    auto rounds = [&](long n) { return (n + slots - 1) / slots; };
+    int L = 1;
+    double best = -1.0;
+    for (int cand = 1; cand <= 64 && cand <= nlines; cand *= 2) {
+        const size_t sm = need(cand);
+        if (sm > (size_t)227 * 1024) break;
+        const long work = (long)(npin + npout) * cand;
+        const long cap = (rounds((long)npin * cand) + rounds((long)npout * cand)) * slots;
+        const double util = (double)work / (double)std::max<long>(cap, 1);
+        const int ctas = (int)std::min<size_t>(4, (size_t)(233472 / (sm + 1024)));
+        const double score = util * ctas;
+        if (score >= best) { best = score; L = cand; }
+    }
     const size_t smem = need(L);
     if (smem > (size_t)227 * 1024) {
         c->err = "internal: z pass tile exceeds shared memory";

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     unsigned char* stages = sbase + 128;
     C2<T>* xbuf = reinterpret_cast<C2<T>*>(stages + (size_t)NST * stage_bytes);
     C2<T>* tw = xbuf + (size_t)N * KT;
-    T* kax = reinterpret_cast<T*>(tw + N);                           // wavenumbers along the axis
+    T* kax = reinterpret_cast<T*>(tw + F::TWN);                      // wavenumbers along the axis
     unsigned char* keep = reinterpret_cast<unsigned char*>(kax + N);  // row mask factor != 0
     const int stride = a.axis == 0 ? a.g.ny * a.g.nzs : a.g.nzs;
     constexpr uint32_t tile_bytes = (uint32_t)((size_t)N * KT * in_elem);
@@ -77,8 +77,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const C2<T>* twg = (const C2<T>*)a.plan.tw;
         const double* kg = a.axis == 0 ? a.g.kx : a.g.ky;
         const double* mg = a.axis == 0 ? a.g.mx : a.g.my;
+        regfft_fill_twiddles<T, LN>(tw, twg, tid, blockDim.x);
         for (int i = tid; i < N; i += blockDim.x) {
-            tw[i] = twg[i];
             kax[i] = (T)kg[i];
             keep[i] = mg[i] != 0.0;
         }
@@ -159,85 +159,37 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
 //  2. the input channels, paired into complex sequences Z = A + iB
 //     (Hermitian-extended, DC/Nyquist imaginary parts dropped), are
 //     inverse-transformed; the real fields go to shared memory;
-//  3. maxima of |u|, |B| for compute_dt (compute_dt.cu:82-101,196-210) and
-//     the real B lines for the anisotropic STS flux, when asked;
-//  4. the products, formed point by point inside the forward transform's
-//     load -- TracelessShearMatrix[MHD] (cuda_kernels.cu:39-55, 216-234),
-//     MagneticEmf (:240-252), EnergyFluxVector (:277-289),
-//     ComputeBGradTheta + ComputeAnisotropicHeatFlux (:360-383) -- are
-//     paired again and forward-transformed; the paired spectra are unpacked
-//     into the half spectra of each product (their D2Z), kz < kz_keep.
+//  3. one pass over the points forms the maxima of |u|, |B| for compute_dt
+//     (compute_dt.cu:82-101,196-210), the real B lines for the anisotropic
+//     STS flux, and the products -- TracelessShearMatrix[MHD]
+//     (cuda_kernels.cu:39-55, 216-234), MagneticEmf (:240-252),
+//     EnergyFluxVector (:277-289), ComputeBGradTheta +
+//     ComputeAnisotropicHeatFlux (:360-383) -- as complex pairs in the input
+//     area, which is free by then;
+//  4. the product pairs are forward-transformed and unpacked into the half
+//     spectra of each product (their D2Z), kz < kz_keep.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T z_product(const ZArgs& a, int ch, T ux, T uy, T uz, T bx, T by, T bz, T th, T gx, T gy,
-                                       T gz) {
-    int q = 0;
-    if (a.mode == ZM_PRODUCTS) {
-        if (a.hydro) {
-            if (ch < 5) {
-                if (!a.mhd) {
-                    switch (ch) {
-                        case 0: return ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0;
-                        case 1: return ux * uy;
-                        case 2: return ux * uz;
-                        case 3: return (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0;
-                        default: return uy * uz;
-                    }
-                }
-                switch (ch) {
-                    case 0: return ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0;
-                    case 1: return ux * uy - bx * by;
-                    case 2: return ux * uz - bx * bz;
-                    case 3: return (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0;
-                    default: return uy * uz - by * bz;
-                }
-            }
-            q = 5;
-        }
-        if (a.mhd) {
-            if (ch < q + 3) {
-                const int c = ch - q;
-                return c == 0 ? -by * uz + bz * uy : (c == 1 ? bx * uz - bz * ux : -bx * uy + by * ux);
-            }
-            q += 3;
-        }
-        if (a.bous) {
-            if (ch < q + 3) {
-                const int c = ch - q;
-                return c == 0 ? ux * th : (c == 1 ? uy * th : uz * th);
-            }
-            q += 3;
-        }
-    }
-    if (a.aniso && ch < q + 3) {
-        const int c = ch - q;
-        const T bgt = bx * gx + by * gy + bz * gz;
-        const T b2 = bx * bx + by * by + bz * bz;
-        const T bs = a.sd == 0 ? bx : (a.sd == 1 ? by : bz);
-        const T chi = (T)a.chi, W = (T)a.omegaT2;
-        const T bc = c == 0 ? bx : (c == 1 ? by : bz);
-        return chi * bc * (bgt + W * bs) / b2;
-    }
-    return (T)0;
-}
-
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Shared-memory carve of k_zpass2 (host and device agree through this).
-struct ZSmem { size_t tw, raw, real, xb, total; };
-__host__ __device__ inline ZSmem zsmem_layout(int n, int csz, int nin, int nin_all, int lines, int nzs, int slots) {
+// Shared-memory carve of k_zpass2 (host and device agree through this):
+// barrier, twiddle tables, input half spectra (later: the product pairs),
+// real fields, exchange slots.
+struct ZSmem { size_t tw, area, real, xb, total; };
+__host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
+                                              int nzs, int slots) {
     ZSmem z;
     const int rs = n + 16, xs = n + (n >> 4);
     z.tw = 128;
-    z.raw = align16(z.tw + (size_t)n * csz);
-    z.real = align16(z.raw + (size_t)nin * lines * nzs * csz);
+    z.area = align16(z.tw + (size_t)twn * csz);
+    const size_t raw = (size_t)nin * lines * nzs * csz, prod = (size_t)npout * lines * n * csz;
+    z.real = align16(z.area + (raw > prod ? raw : prod));
     z.xb = align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
     z.total = align16(z.xb + (size_t)slots * xs * csz);
     return z;
 }
 
 template <typename T, int LN>
-__global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs a) {
+__global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, LN>;
     constexpr int N = F::N, LTPC = F::LTPC, TPC = F::TPC;
     constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
@@ -254,13 +206,15 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
-    const ZSmem lay = zsmem_layout(N, (int)sizeof(C2<T>), nin, nin_all, L, nzs, slots);
+    const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
-    C2<T>* raw = reinterpret_cast<C2<T>*>(smem_raw + lay.raw);
+    C2<T>* raw = reinterpret_cast<C2<T>*>(smem_raw + lay.area);
+    C2<T>* prod = raw;                    // the product pairs reuse the input area
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
     const C2<T>* in = (const C2<T>*)a.in;
+    const int LRS = L * RS;
 
     // 1. bulk copies of the input half spectra
     if (tid == 0) {
@@ -274,10 +228,7 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
         for (int ch = 0; ch < nin; ch++)
             bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
     }
-    {
-        const C2<T>* twg = (const C2<T>*)a.plan.tw;
-        for (int i = tid; i < N; i += nthr) tw[i] = twg[i];
-    }
+    regfft_fill_twiddles<T, LN>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
     const bool ok = mbar_wait(bar, 0, SPK_WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
@@ -292,11 +243,15 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
     C2<T> r[F::E];
 
     // 2. inverse transforms of the input pairs
+    const bool simple = a.derive_gz == 0;
     const int ninv = npin * L;
     for (int base = 0; base < ninv; base += slots) {
         const int tau = base + sigma;
         const bool valid = tau < ninv;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
+        const C2<T>* pa = raw + (size_t)(2 * p * L + l) * nzs;
+        const C2<T>* pb = pa + (size_t)L * nzs;
+        const bool hasA = 2 * p < nin, hasB = 2 * p + 1 < nin;
         auto chv = [&](int ch, int k) -> C2<T> {
             if (ch < nin) {
                 C2<T> v = raw[((size_t)ch * L + l) * nzs + k];
@@ -316,16 +271,25 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
         regfft_load<T, LN, +1>(r, q, [&](int n) -> C2<T> {
             constexpr int NH = N >> 1;
             const int k = n <= NH ? n : N - n;
-            const C2<T> A = chv(2 * p, k), B = chv(2 * p + 1, k);
+            C2<T> A, B;
+            if (simple) {
+                A = hasA ? pa[k] : mk<T>((T)0, (T)0);
+                B = hasB ? pb[k] : mk<T>((T)0, (T)0);
+            } else {
+                A = chv(2 * p, k);
+                B = chv(2 * p + 1, k);
+            }
             if (n == 0 || n == NH) return mk<T>(A.x, B.x);
             if (n < NH) return mk<T>(A.x - B.y, A.y + B.x);
             return mk<T>(A.x + B.y, B.x - A.y);
         });
+        T* pr = real + (size_t)(2 * p * L + l) * RS;
+        const bool has1 = 2 * p + 1 < nin_all;
         const bool to_real = a.mode == ZM_TO_REAL && valid && l < nl;
         regfft_run<T, LN, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
             if (!valid) return;
-            real[((size_t)(2 * p) * L + l) * RS + z] = v.x;
-            if (2 * p + 1 < nin_all) real[((size_t)(2 * p + 1) * L + l) * RS + z] = v.y;
+            pr[z] = v.x;
+            if (has1) pr[LRS + z] = v.y;
             if (to_real) {
                 const size_t line = (size_t)(line0 + l);
                 if (2 * p < nin) a.real_out[((size_t)(2 * p) * nlines + line) * N + z] = (double)v.x;
@@ -336,25 +300,37 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
     __syncthreads();
     if (a.mode == ZM_TO_REAL) return;
 
-    auto R = [&](int ch, int l, int z) -> T { return real[((size_t)ch * L + l) * RS + z]; };
+    // 3. one pass over the points: CFL maxima, real B for the STS flux, and
+    //    the products, stored as complex pairs (channel 2p, 2p+1)
     T* breal = (T*)a.breal;
-
-    // 3. maxima for the CFL condition, real B for the STS flux
-    if (a.do_max || a.store_breal) {
+    const bool want_prod = a.nout > 0;
+    {
         T mu[6] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
         int bad = 0;
-        for (int e = tid; e < nl * N; e += nthr) {
+        T* prodT = reinterpret_cast<T*>(prod);
+        const size_t pstride = (size_t)L * N * 2;   // scalars between product pairs
+        for (int e = tid; e < L * N; e += nthr) {
             const int l = e >> LN, z = e & (N - 1);
+            const bool live = l < nl;
             const size_t line = (size_t)(line0 + l);
-            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0;
-            if (a.ch_u >= 0) { ux = R(a.ch_u, l, z); uy = R(a.ch_u + 1, l, z); uz = R(a.ch_u + 2, l, z); }
-            if (a.ch_b >= 0) { bx = R(a.ch_b, l, z); by = R(a.ch_b + 1, l, z); bz = R(a.ch_b + 2, l, z); }
-            if (a.store_breal) {
+            const T* fr = real + (size_t)l * RS + z;
+            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
+            if (a.ch_u >= 0) { ux = fr[a.ch_u * LRS]; uy = fr[(a.ch_u + 1) * LRS]; uz = fr[(a.ch_u + 2) * LRS]; }
+            if (a.load_breal) {
+                if (live) {
+                    bx = breal[(0 * (size_t)nlines + line) * N + z];
+                    by = breal[(1 * (size_t)nlines + line) * N + z];
+                    bz = breal[(2 * (size_t)nlines + line) * N + z];
+                }
+            } else if (a.ch_b >= 0) {
+                bx = fr[a.ch_b * LRS]; by = fr[(a.ch_b + 1) * LRS]; bz = fr[(a.ch_b + 2) * LRS];
+            }
+            if (live && a.store_breal) {
                 breal[(0 * (size_t)nlines + line) * N + z] = bx;
                 breal[(1 * (size_t)nlines + line) * N + z] = by;
                 breal[(2 * (size_t)nlines + line) * N + z] = bz;
             }
-            if (a.do_max) {
+            if (live && a.do_max) {
                 const T av[6] = {fabs(ux), fabs(uy), fabs(uz), fabs(bx), fabs(by), fabs(bz)};
 #pragma unroll
                 for (int c = 0; c < 6; c++) {
@@ -362,9 +338,57 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
                     mu[c] = fmax(mu[c], av[c]);
                 }
             }
+            if (!want_prod) continue;
+            if (a.ch_th >= 0 && a.derive_gz != 2) th = fr[a.ch_th * LRS];
+            if (a.ch_gx >= 0) gx = fr[a.ch_gx * LRS];
+            if (a.ch_gy >= 0) gy = fr[a.ch_gy * LRS];
+            if (a.derive_gz == 1) gz = fr[nin * LRS];
+            else if (a.derive_gz == 2) gz = fr[a.ch_th * LRS];
+            T* pp = prodT + ((size_t)l * N + z) * 2;
+            auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1)] = v; };
+            int qc = 0;
+            if (a.mode == ZM_PRODUCTS) {
+                if (a.hydro) {
+                    if (!a.mhd) {
+                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0);
+                        put(1, ux * uy);
+                        put(2, ux * uz);
+                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0);
+                        put(4, uy * uz);
+                    } else {
+                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0);
+                        put(1, ux * uy - bx * by);
+                        put(2, ux * uz - bx * bz);
+                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0);
+                        put(4, uy * uz - by * bz);
+                    }
+                    qc = 5;
+                }
+                if (a.mhd) {
+                    put(qc, -by * uz + bz * uy);
+                    put(qc + 1, bx * uz - bz * ux);
+                    put(qc + 2, -bx * uy + by * ux);
+                    qc += 3;
+                }
+                if (a.bous) {
+                    put(qc, ux * th); put(qc + 1, uy * th); put(qc + 2, uz * th);
+                    qc += 3;
+                }
+            }
+            if (a.aniso) {
+                const T bgt = bx * gx + by * gy + bz * gz;
+                const T b2 = bx * bx + by * by + bz * bz;
+                const T bs = a.sd == 0 ? bx : (a.sd == 1 ? by : bz);
+                const T chi = (T)a.chi, W = (T)a.omegaT2;
+                put(qc, chi * bx * (bgt + W * bs) / b2);
+                put(qc + 1, chi * by * (bgt + W * bs) / b2);
+                put(qc + 2, chi * bz * (bgt + W * bs) / b2);
+                qc += 3;
+            }
+            if (a.nout & 1) put(a.nout, (T)0);
         }
         if (a.do_max) {
-            // the xb area is free here: 6 x 32 block-max scratch
+            // the exchange slots are free here: 6 x 32 block-max scratch
             T* red = reinterpret_cast<T*>(xb);
             warp_block_max<T>(mu, 6, red);
             if (tid < 6) {
@@ -374,44 +398,24 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
                 if (bits > *((volatile unsigned long long*)dst)) atomicMax(dst, bits);
             }
             if (bad) atomicOr(a.nonfinite, 1);
-            __syncthreads();
         }
     }
-    if (a.nout == 0) return;
+    if (!want_prod) return;
+    __syncthreads();   // products written; the block-max scratch read
 
-    // 4. products, forward transforms, unpacked half spectra
+    // 4. forward transforms of the product pairs, unpacked half spectra
     const int kk = a.g.kz_keep;
     C2<T>* out = (C2<T>*)a.out;
     const T half = (T)0.5;
     const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
     const int nfw = npout * L;
     for (int base = 0; base < nfw; base += slots) {
-        __syncthreads();   // the previous round's unpack has read the exchange slots
+        if (base > 0) __syncthreads();   // the previous round's unpack has read the exchange slots
         const int tau = base + sigma;
         const bool valid = tau < nfw;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
-        const size_t line = (size_t)(line0 + l);
-        regfft_load<T, LN, -1>(r, q, [&](int z) -> C2<T> {
-            T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
-            if (a.ch_u >= 0) { ux = R(a.ch_u, l, z); uy = R(a.ch_u + 1, l, z); uz = R(a.ch_u + 2, l, z); }
-            if (a.load_breal) {
-                if (l < nl) {
-                    bx = breal[(0 * (size_t)nlines + line) * N + z];
-                    by = breal[(1 * (size_t)nlines + line) * N + z];
-                    bz = breal[(2 * (size_t)nlines + line) * N + z];
-                }
-            } else if (a.ch_b >= 0) {
-                bx = R(a.ch_b, l, z); by = R(a.ch_b + 1, l, z); bz = R(a.ch_b + 2, l, z);
-            }
-            if (a.ch_th >= 0 && a.derive_gz != 2) th = R(a.ch_th, l, z);
-            if (a.ch_gx >= 0) gx = R(a.ch_gx, l, z);
-            if (a.ch_gy >= 0) gy = R(a.ch_gy, l, z);
-            if (a.derive_gz == 1) gz = R(nin, l, z);
-            else if (a.derive_gz == 2) gz = R(a.ch_th, l, z);
-            const T v0 = z_product<T>(a, 2 * p, ux, uy, uz, bx, by, bz, th, gx, gy, gz);
-            const T v1 = 2 * p + 1 < a.nout ? z_product<T>(a, 2 * p + 1, ux, uy, uz, bx, by, bz, th, gx, gy, gz) : (T)0;
-            return mk<T>(v0, v1);
-        });
+        const C2<T>* pp = prod + (size_t)(p * L + l) * N;
+        regfft_load<T, LN, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
         regfft_run<T, LN, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; });
         __syncthreads();
         for (int s2 = warp; s2 < slots; s2 += nwarp) {
@@ -421,11 +425,13 @@ __global__ void __launch_bounds__(256, 2) k_zpass2(const __grid_constant__ ZArgs
             if (l2 >= nl) continue;
             const C2<T>* Z = xb + (size_t)s2 * XS;
             const size_t off0 = (size_t)(line0 + l2) * nzs;
+            C2<T>* o0 = out + (size_t)(2 * p2) * a.cs_out + off0;
+            C2<T>* o1 = out + (size_t)(2 * p2 + 1) * a.cs_out + off0;
+            const bool two = 2 * p2 + 1 < a.nout;
             for (int k = lane; k < kk; k += 32) {
                 const C2<T> zk = Z[padi<1>(k)], zm = Z[padi<1>(k ? N - k : 0)];
-                out[(size_t)(2 * p2) * a.cs_out + off0 + k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
-                if (2 * p2 + 1 < a.nout)
-                    out[(size_t)(2 * p2 + 1) * a.cs_out + off0 + k] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
+                o0[k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+                if (two) o1[k] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
             }
         }
     }

@@ -16,7 +16,8 @@
 // shared-memory exchange each (so a 256-point FP32 transform makes exactly
 // one), and the last stage hands X[k] to the caller's `store(k, v)` from
 // registers (a global store, a shared-memory store, a product).  Twiddles
-// W_N^j come from a shared-memory table of the pass precision.
+// come from per-stage shared-memory tables of the pass precision, laid out
+// so that the threads of one transform read consecutive words.
 #pragma once
 #include "spk_fft.cuh"
 
@@ -36,7 +37,25 @@ struct RegFft {
     static constexpr int NS = (LN + LRF - 1) / LRF;          // stages
     static constexpr int lr(int s) { return s < NFULL ? LRF : LN - NFULL * LRF; }
     static constexpr int ls(int s) { return s == 0 ? 0 : ls(s - 1) + lr(s - 1); }   // log2 P_s
+    // Twiddle tables: stage s (H_s > 1) keeps W_N^{(m t) P_s} at tbase(s) + t*H_s + m,
+    // M_s entries, so that consecutive m (consecutive threads) read consecutive words.
+    static constexpr int tbase(int s) { return s == 0 ? 0 : tbase(s - 1) + (N >> ls(s - 1)); }
+    static constexpr int TWN = NS > 1 ? tbase(NS - 1) : 1;   // entries over all stages
 };
+
+// Fill the per-stage twiddle tables from the table W_N^j (all threads call).
+template <typename T, int LN>
+__device__ __forceinline__ void regfft_fill_twiddles(C2<T>* tws, const C2<T>* twg, int tid, int nthr) {
+    using F = RegFft<T, LN>;
+    for (int i = tid; i < F::TWN; i += nthr) {
+        int s = 0;
+        while (s + 1 < F::NS && i >= F::tbase(s + 1)) s++;
+        const int lh = LN - F::ls(s) - F::lr(s);
+        const int e = i - F::tbase(s);
+        const int t = e >> lh, m = e & ((1 << lh) - 1);
+        tws[i] = twg[(m * t) << F::ls(s)];
+    }
+}
 
 template <typename T, int R, int DIR> __device__ __forceinline__ void dft_pow2(C2<T>* a) {
     if constexpr (R == 2) dft2<T, DIR>(a);
@@ -45,7 +64,7 @@ template <typename T, int R, int DIR> __device__ __forceinline__ void dft_pow2(C
     else if constexpr (R == 16) dft16<T, DIR>(a);
 }
 
-// W_N^j (DIR = -1) or its conjugate (DIR = +1) from the table exp(-2 pi i j/N).
+// Table entry j (W_N^k for some k, DIR = -1) or its conjugate (DIR = +1).
 template <typename T, int DIR> __device__ __forceinline__ C2<T> twd(const C2<T>* tw, int j) {
     C2<T> w = tw[j];
     if (DIR > 0) w.y = -w.y;
@@ -54,7 +73,8 @@ template <typename T, int DIR> __device__ __forceinline__ C2<T> twd(const C2<T>*
 
 // Run stage S (butterflies of this thread, q = sub-index within the
 // transform) on registers a[E] whose legs are already loaded; apply the
-// twiddles.  Leg t of butterfly u ends in a[u*R + t].
+// twiddles from the per-stage tables (regfft_fill_twiddles).  Leg t of
+// butterfly u ends in a[u*R + t].
 template <typename T, int LN, int DIR, int S>
 __device__ __forceinline__ void regfft_stage_math(C2<T>* a, int q, const C2<T>* tw) {
     using F = RegFft<T, LN>;
@@ -68,11 +88,9 @@ __device__ __forceinline__ void regfft_stage_math(C2<T>* a, int q, const C2<T>* 
         if constexpr (LH > 0) {
             const int beta = q + (u << F::LTPC);
             const int m = beta & ((1 << LH) - 1);
+            const C2<T>* tws = tw + F::tbase(S) + m;
 #pragma unroll
-            for (int t = 1; t < R; t++) {
-                a[u * R + t] = cmul(a[u * R + t], twd<T, DIR>(tw, (m * t) << LP));
-                asm volatile("" ::: "memory");   // one twiddle live at a time
-            }
+            for (int t = 1; t < R; t++) a[u * R + t] = cmul(a[u * R + t], twd<T, DIR>(tws, t << LH));
         }
     }
 }
@@ -102,7 +120,8 @@ __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
 
 // Full transform.  load(n) gives input n; xaddr(L) is the shared-memory slot
 // of exchange element L (the caller picks layout and padding); store(k, v)
-// receives X[k].  Every thread of the CTA must call it: each exchange
+// receives X[k]; tw holds the per-stage twiddle tables.  Every thread of
+// the CTA must call it: each exchange
 // starts with a barrier (earlier reads of the buffer, including a previous
 // tile's, are complete) and ends with one (the writes are visible).
 template <typename T, int LN, int DIR, int S, typename XA>
