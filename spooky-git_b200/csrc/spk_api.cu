@@ -517,9 +517,11 @@ static void pass_x_forward(spk_ctx* c) {
 // elementwise RHS + Leray + time update of every mode
 static void rhs(spk_ctx* c, XfArgs& x) {
     const FastDiv fz = FastDiv::make((unsigned)c->nzh);
+    // 128-thread CTAs, three per SM: every load of a mode is issued up front
+    const int grid = (int)std::min<size_t>((c->nc + 127) / 128, (size_t)c->num_sms * 3 * 8);
     c->launches++;
-    if (c->fp32) k_rhs<float><<<ew_blocks(c->nc), 256, 0, c->stream>>>(x, fz);
-    else k_rhs<double><<<ew_blocks(c->nc), 256, 0, c->stream>>>(x, fz);
+    if (c->fp32) k_rhs<float><<<grid, 128, 0, c->stream>>>(x, fz);
+    else k_rhs<double><<<grid, 128, 0, c->stream>>>(x, fz);
 }
 
 static void xfwd(spk_ctx* c, XfArgs& x) {

@@ -449,49 +449,105 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
 //   (hydro_mhd_advance.cu:79-248), with CleanDivergence of the next step
 //   (cuda_kernels_generic.cu:288-313) on the last stage.
 // ---------------------------------------------------------------------------
+// New state value of one mode given its RK scratch value S (read up front).
+__device__ __forceinline__ double2 rk_value(const XfArgs& a, size_t gi, double2 X, double2 S, double2 R, double dt) {
+    const double g0 = 8.0 / 15.0, g1 = 5.0 / 12.0, g2 = 3.0 / 4.0, x0 = -17.0 / 60.0, x1 = -5.0 / 12.0;
+    switch (a.mode) {
+        case XM_RK0: {
+            // U1 = U + g0 dt R, then S = U1 + x0 dt R (the second axpyComplex
+            // reads the already-updated fields, hydro_mhd_advance.cu:119-122)
+            const double bu = g0 * dt, bs = x0 * dt;
+            const double2 Un = d2(1.0 * X.x + bu * R.x, 1.0 * X.y + bu * R.y);
+            a.S[gi] = d2(1.0 * Un.x + bs * R.x, 1.0 * Un.y + bs * R.y);
+            return Un;
+        }
+        case XM_RK1: {
+            const double bu = g1 * dt, bs = x1 * dt;
+            const double2 Un = d2(1.0 * S.x + bu * R.x, 1.0 * S.y + bu * R.y);
+            a.S[gi] = d2(1.0 * Un.x + bs * R.x, 1.0 * Un.y + bs * R.y);
+            return Un;
+        }
+        case XM_RK2: {
+            const double bu = g2 * dt;
+            return d2(1.0 * S.x + bu * R.x, 1.0 * S.y + bu * R.y);
+        }
+        case XM_EULER:
+            return d2(1.0 * X.x + dt * R.x, 1.0 * X.y + dt * R.y);
+        default:
+            a.out[gi] = R;
+            return X;
+    }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
+__global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
     const size_t nc = a.g.nc;
     const int nzh = a.g.nzh, lny = a.lny, nzs = a.g.nzs;
     const double dt = a.sc->dt;
     const C2<T>* nl = (const C2<T>*)a.nl;
+    const bool needS = a.mode == XM_RK1 || a.mode == XM_RK2;
+    const double2 z0 = d2(0.0, 0.0);
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const unsigned line = fzh.div((unsigned)gi);
         const int k = (int)(gi - (size_t)line * nzh);
         const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
-        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
-        const double k2 = kx * kx + ky * ky + kz * kz;
         const bool m = a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0;
         const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
         auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
-        double2 th_old = d2(0.0, 0.0), usd = d2(0.0, 0.0);
-        if (a.bous) th_old = a.U[(size_t)a.TH * nc + gi];
+
+        // every load of the mode first (state, RK scratch, products), so that
+        // they are all in flight together
+        double2 Xu[3] = {z0, z0, z0}, Xb[3] = {z0, z0, z0}, Xt = z0;
+        double2 Su[3] = {z0, z0, z0}, Sb[3] = {z0, z0, z0}, St = z0;
+        double2 t0 = z0, t1 = z0, t2 = z0, t3 = z0, t4 = z0, e0 = z0, e1 = z0, e2 = z0;
+        double2 f0 = z0, f1 = z0, f2 = z0, q0 = z0, q1 = z0, q2 = z0;
+        if (a.incompressible) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                Xu[c] = a.U[(size_t)(a.VEL + c) * nc + gi];
+                if (needS) Su[c] = a.S[(size_t)(a.VEL + c) * nc + gi];
+            }
+        }
+        if (a.mhd) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                Xb[c] = a.U[(size_t)(a.MAG + c) * nc + gi];
+                if (needS) Sb[c] = a.S[(size_t)(a.MAG + c) * nc + gi];
+            }
+        }
+        if (a.bous) {
+            Xt = a.U[(size_t)a.TH * nc + gi];
+            if (needS) St = a.S[(size_t)a.TH * nc + gi];
+        }
+        if (m) {
+            if (a.incompressible && a.nl_T >= 0) { t0 = P(a.nl_T); t1 = P(a.nl_T + 1); t2 = P(a.nl_T + 2); t3 = P(a.nl_T + 3); t4 = P(a.nl_T + 4); }
+            if (a.mhd && a.nl_E >= 0) { e0 = P(a.nl_E); e1 = P(a.nl_E + 1); e2 = P(a.nl_E + 2); }
+            if (a.bous && a.nl_F >= 0) { f0 = P(a.nl_F); f1 = P(a.nl_F + 1); f2 = P(a.nl_F + 2); }
+            if (a.bous && a.aniso_rhs && a.nl_Q >= 0) { q0 = P(a.nl_Q); q1 = P(a.nl_Q + 1); q2 = P(a.nl_Q + 2); }
+        }
+        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        double2 usd = z0;
 
         if (a.incompressible) {
-            double2 X[3], R[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.VEL + c) * nc + gi];
-            double2 s0 = d2(0.0, 0.0), s1 = d2(0.0, 0.0), s2 = d2(0.0, 0.0);
-            if (m && a.nl_T >= 0) {
-                const double2 t0 = P(a.nl_T), t1 = P(a.nl_T + 1), t2 = P(a.nl_T + 2), t3 = P(a.nl_T + 3), t4 = P(a.nl_T + 4);
-                // k_j T_ij with T = [[t0 t1 t2] [t1 t3 t4] [t2 t4 -t0-t3]]
-                s0 = d2(kx * t0.x + ky * t1.x + kz * t2.x, kx * t0.y + ky * t1.y + kz * t2.y);
-                s1 = d2(kx * t1.x + ky * t3.x + kz * t4.x, kx * t1.y + ky * t3.y + kz * t4.y);
-                s2 = d2(kx * t2.x + ky * t4.x - kz * (t0.x + t3.x), kx * t2.y + ky * t4.y - kz * (t0.y + t3.y));
-            }
-            R[0] = d2(s0.y, -s0.x);   // -i * mask * k_j T_ij
+            double2 R[3];
+            // -i * mask * k_j T_ij with T = [[t0 t1 t2] [t1 t3 t4] [t2 t4 -t0-t3]]
+            const double2 s0 = d2(kx * t0.x + ky * t1.x + kz * t2.x, kx * t0.y + ky * t1.y + kz * t2.y);
+            const double2 s1 = d2(kx * t1.x + ky * t3.x + kz * t4.x, kx * t1.y + ky * t3.y + kz * t4.y);
+            const double2 s2 = d2(kx * t2.x + ky * t4.x - kz * (t0.x + t3.x), kx * t2.y + ky * t4.y - kz * (t0.y + t3.y));
+            R[0] = d2(s0.y, -s0.x);
             R[1] = d2(s1.y, -s1.x);
             R[2] = d2(s2.y, -s2.x);
             if (a.strat) {
-                if (a.sd == 0)      { R[0] = d2(R[0].x - th_old.x, R[0].y - th_old.y); usd = X[0]; }
-                else if (a.sd == 1) { R[1] = d2(R[1].x - th_old.x, R[1].y - th_old.y); usd = X[1]; }
-                else                { R[2] = d2(R[2].x - th_old.x, R[2].y - th_old.y); usd = X[2]; }
+                if (a.sd == 0)      { R[0] = d2(R[0].x - Xt.x, R[0].y - Xt.y); usd = Xu[0]; }
+                else if (a.sd == 1) { R[1] = d2(R[1].x - Xt.x, R[1].y - Xt.y); usd = Xu[1]; }
+                else                { R[2] = d2(R[2].x - Xt.x, R[2].y - Xt.y); usd = Xu[2]; }
             }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 if (!((a.sts_mask >> (a.VEL + c)) & 1u)) {
                     const double f = -a.nu * k2;
-                    R[c] = d2(R[c].x + f * X[c].x, R[c].y + f * X[c].y);
+                    R[c] = d2(R[c].x + f * Xu[c].x, R[c].y + f * Xu[c].y);
                 }
             }
             // Leray: dU += i k (i k.dU)/k^2
@@ -503,7 +559,7 @@ __global__ void __launch_bounds__(256) k_rhs(const __grid_constant__ XfArgs a, F
             for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
             double2 Un[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) Un[c] = step_value(a, (size_t)(a.VEL + c) * nc + gi, X[c], R[c], dt);
+            for (int c = 0; c < 3; c++) Un[c] = rk_value(a, (size_t)(a.VEL + c) * nc + gi, Xu[c], Su[c], R[c], dt);
             if (a.mode != XM_DFIELD) {
                 if (a.clean) clean3(Un, kx, ky, kz);
 #pragma unroll
@@ -512,27 +568,19 @@ __global__ void __launch_bounds__(256) k_rhs(const __grid_constant__ XfArgs a, F
         }
 
         if (a.mhd) {
-            double2 X[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) X[c] = a.U[(size_t)(a.MAG + c) * nc + gi];
-            double2 s0 = d2(0.0, 0.0), s1 = d2(0.0, 0.0), s2 = d2(0.0, 0.0);
-            if (m && a.nl_E >= 0) {
-                const double2 e0 = P(a.nl_E), e1 = P(a.nl_E + 1), e2 = P(a.nl_E + 2);
-                // k x E
-                s0 = d2(ky * e2.x - kz * e1.x, ky * e2.y - kz * e1.y);
-                s1 = d2(kz * e0.x - kx * e2.x, kz * e0.y - kx * e2.y);
-                s2 = d2(kx * e1.x - ky * e0.x, kx * e1.y - ky * e0.y);
-            }
-            const double2 S3[3] = {s0, s1, s2};
+            // i * mask * (k x E)
+            const double2 S3[3] = {d2(ky * e2.x - kz * e1.x, ky * e2.y - kz * e1.y),
+                                   d2(kz * e0.x - kx * e2.x, kz * e0.y - kx * e2.y),
+                                   d2(kx * e1.x - ky * e0.x, kx * e1.y - ky * e0.y)};
             double2 Un[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                double2 R = d2(-S3[c].y, S3[c].x);   // i * mask * (k x E)
+                double2 R = d2(-S3[c].y, S3[c].x);
                 if (!((a.sts_mask >> (a.MAG + c)) & 1u)) {
                     const double f = -a.nu_m * k2;
-                    R = d2(R.x + f * X[c].x, R.y + f * X[c].y);
+                    R = d2(R.x + f * Xb[c].x, R.y + f * Xb[c].y);
                 }
-                Un[c] = step_value(a, (size_t)(a.MAG + c) * nc + gi, X[c], R, dt);
+                Un[c] = rk_value(a, (size_t)(a.MAG + c) * nc + gi, Xb[c], Sb[c], R, dt);
             }
             if (a.mode != XM_DFIELD) {
                 if (a.clean) clean3(Un, kx, ky, kz);
@@ -542,27 +590,19 @@ __global__ void __launch_bounds__(256) k_rhs(const __grid_constant__ XfArgs a, F
         }
 
         if (a.bous) {
-            const double2 X = th_old;
-            double2 R = d2(0.0, 0.0);
-            if (m && a.nl_F >= 0) {
-                const double2 f0 = P(a.nl_F), f1 = P(a.nl_F + 1), f2 = P(a.nl_F + 2);
-                const double2 s = d2(kx * f0.x + ky * f1.x + kz * f2.x, kx * f0.y + ky * f1.y + kz * f2.y);
-                R = d2(s.y, -s.x);   // -i * mask * k.(u theta)
-            }
+            const double2 s = d2(kx * f0.x + ky * f1.x + kz * f2.x, kx * f0.y + ky * f1.y + kz * f2.y);
+            double2 R = d2(s.y, -s.x);   // -i * mask * k.(u theta)
             if (a.strat) R = d2(R.x + a.N2 * usd.x, R.y + a.N2 * usd.y);
             if (!((a.sts_mask >> a.TH) & 1u)) {
                 if (a.aniso_rhs) {
-                    if (m && a.nl_Q >= 0) {
-                        const double2 q0 = P(a.nl_Q), q1 = P(a.nl_Q + 1), q2 = P(a.nl_Q + 2);
-                        const double2 s = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
-                        R = d2(R.x - s.y, R.y + s.x);   // += i * mask * k.q
-                    }
+                    const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
+                    R = d2(R.x - sq.y, R.y + sq.x);   // += i * mask * k.q
                 } else {
                     const double f = -a.nu_th * k2;
-                    R = d2(R.x + f * X.x, R.y + f * X.y);
+                    R = d2(R.x + f * Xt.x, R.y + f * Xt.y);
                 }
             }
-            const double2 Un = step_value(a, (size_t)a.TH * nc + gi, X, R, dt);
+            const double2 Un = rk_value(a, (size_t)a.TH * nc + gi, Xt, St, R, dt);
             if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
         }
     }
