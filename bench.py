@@ -249,6 +249,7 @@ def main():
     U64 = ctx64.get_state()
     rel = float(np.linalg.norm((U32 - U64).ravel()) / np.linalg.norm(U64.ravel()))
     t32 = ctx32.get_time()
+    prof64 = ctx64.profile_passes(reps=5)   # after the comparison: profiling rewrites the state
     del ctx64
     torch.cuda.empty_cache()
 
@@ -283,6 +284,10 @@ def main():
         pz["gbs"] = pz["bytes"] / (pz["ms"] * 1e-3) / 1e9
         pz["frac_of_peak"] = pz["gbs"] / peak
         pz["share_of_step"] = pz["ms"] * pz["launches_per_step"] / ms32
+    for pz in prof64:
+        pz["gbs"] = pz["bytes"] / (pz["ms"] * 1e-3) / 1e9
+        pz["frac_of_peak"] = pz["gbs"] / peak
+        pz["share_of_step"] = pz["ms"] * pz["launches_per_step"] / ms64
     dom = max(prof, key=lambda d: d["ms"] * d["launches_per_step"])
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -305,7 +310,9 @@ def main():
             "config": config_dict(n, world),
             "plain_fp64": {"value": world * 1000.0 / ms64, "unit": "steps/s", "ms_per_step": ms64,
                            "bytes_per_step": bytes_step64,
-                           "step_hbm_frac": bytes_step64 / (ms64 * 1e-3) / 1e9 / peak},
+                           "step_hbm_frac": bytes_step64 / (ms64 * 1e-3) / 1e9 / peak,
+                           "passes": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in pz.items()}
+                                      for pz in prof64]},
             "fp32_vs_fp64_rel_l2": rel, "fp32_vs_fp64_after_steps": args.warmup + args.steps,
             "sim_time": t32[0], "last_dt": t32[1],
             "mmode_steps_per_s": value * n ** 3 / 1e6,

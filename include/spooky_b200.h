@@ -56,6 +56,8 @@ extern "C" {
 #define SPK_FORM_FP32   1   /* FFT passes and products in FP32, FP64 state and RK/RKL  */
 
 /* ---- super-time-stepping algorithms (Parameters::sts_algorithm) ---------- */
+#define SPK_STS_STS     1   /* parsed but not implemented here (SPK_ERR_UNSUPPORTED) */
+#define SPK_STS_RKL1    2   /* parsed but not implemented here (SPK_ERR_UNSUPPORTED) */
 #define SPK_STS_RKL2    3
 
 /* ---- integrators --------------------------------------------------------- */
@@ -93,6 +95,19 @@ typedef struct spk_params {
 
 /* Fill *p with the reference's defaults (parameters.cu:77-505). */
 void spk_params_default(spk_params_t* p);
+
+/* Parameters::Parameters(Supervisor&, char* configfile)
+ * (src/parameters/parameters.cu:59-505) for the keys this path reads, then
+ * Parameters::checkParameters (:511-566).  The text is libconfig format (the
+ * reference's spooky.cfg); *p starts from spk_params_default and each key
+ * keeps its default when absent or of another type (an integer written for a
+ * float key is ignored, as libconfig's typed lookups do).  form, fixed_dt,
+ * integrator and sts_every_step are not configuration keys and keep their
+ * defaults.  Returns SPK_OK, SPK_ERR_ARG (unreadable or malformed: the
+ * message from spk_last_error(NULL) names the line) or SPK_ERR_CONFIG
+ * (inconsistent modules: *p is filled, the message says why). */
+int spk_params_from_file(const char* path, spk_params_t* p);
+int spk_params_from_string(const char* text, spk_params_t* p);
 
 typedef struct spk_ctx spk_ctx;
 

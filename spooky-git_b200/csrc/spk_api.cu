@@ -20,6 +20,7 @@
 
 #include "spk_kernels.cu"
 #include "spk_pass2.cu"
+#include "spk_config.hpp"
 
 using namespace spk;
 
@@ -345,10 +346,15 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
         return;
     }
     z.lines = L;
-    cudaFuncSetAttribute(k_zpass2<T, LN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int nblk = (int)((nlines + L - 1) / L);
     c->launches++;
-    k_zpass2<T, LN><<<nblk, nthr, smem, c->stream>>>(z);
+    if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
+        cudaFuncSetAttribute(k_zpass2<T, LN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, LN, true><<<nblk, nthr, smem, c->stream>>>(z);
+    } else {
+        cudaFuncSetAttribute(k_zpass2<T, LN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, LN, false><<<nblk, nthr, smem, c->stream>>>(z);
+    }
 }
 
 template <typename T>
@@ -741,6 +747,104 @@ static int check_params(const spk_params_t* p, std::string& why) {
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
     return SPK_OK;
+}
+
+// Parameters::Parameters (src/parameters/parameters.cu:59-505) for the keys
+// of this path, from a parsed libconfig-format file: every lookup that
+// fails (absent, or of another type) keeps the default, as in the reference.
+static int params_from_config(const spkcfg::Setting& root, spk_params_t* p) {
+    using namespace spkcfg;
+    spk_params_default(p);
+    get_bool(root, "modules.with2d", &p->with2d);
+    get_bool(root, "modules.incompressible", &p->incompressible);
+    get_bool(root, "modules.heat_equation", &p->heat_equation);
+    get_bool(root, "modules.boussinesq", &p->boussinesq);
+    get_bool(root, "modules.stratification", &p->stratification);
+    get_int(root, "modules.strat_direction", &p->strat_direction);
+    get_bool(root, "modules.mhd", &p->mhd);
+    get_bool(root, "modules.anisotropic_diffusion", &p->anisotropic_diffusion);
+    get_bool(root, "modules.supertimestepping", &p->supertimestepping);
+    // sts_algorithm / sts_variables (:111-156): read only with supertimestepping;
+    // no (or an empty) variable list switches it off
+    std::vector<std::string> sts_vars;
+    if (p->supertimestepping) {
+        std::string alg;
+        if (get_string(root, "modules.sts_algorithm", &alg)) {
+            p->sts_algorithm = alg == "rkl2" ? SPK_STS_RKL2 : (alg == "rkl1" ? SPK_STS_RKL1 : (alg == "sts" ? SPK_STS_STS : 0));
+            const Setting* sv = lookup(root, "modules.sts_variables");
+            if (sv && (sv->type == T_LIST || sv->type == T_ARRAY) && !sv->items.empty()) {
+                for (const Setting& e : sv->items)
+                    if (e.type == T_STRING) sts_vars.push_back(e.sval);
+            } else {
+                p->supertimestepping = 0;
+            }
+        }
+    }
+    get_float(root, "physics.boxsize.[0]", &p->lx);
+    get_float(root, "physics.boxsize.[1]", &p->ly);
+    get_float(root, "physics.boxsize.[2]", &p->lz);
+    get_int(root, "physics.gridsize.[0]", &p->nx);
+    get_int(root, "physics.gridsize.[1]", &p->ny);
+    get_int(root, "physics.gridsize.[2]", &p->nz);
+    double re = 1.0, rem = 1.0, reth = 1.0;
+    get_float(root, "physics.reynolds", &re);
+    get_float(root, "physics.reynolds_magnetic", &rem);
+    get_float(root, "physics.reynolds_thermic", &reth);
+    p->nu = 1. / re;
+    p->nu_m = 1. / rem;
+    p->nu_th = 1. / reth;
+    get_float(root, "physics.reynolds_anisotropic", &p->reynolds_ani);
+    get_float(root, "physics.brunt_vaissala_squared", &p->N2);
+    get_float(root, "physics.mti_frequency_squared", &p->OmegaT2);
+    get_float(root, "code.cfl", &p->cfl);
+    get_float(root, "code.cfl_par", &p->cfl_par);
+    get_float(root, "code.cfl_sts", &p->cfl_sts);
+    get_int(root, "code.safety_sts", &p->safety_sts);
+    get_float(root, "code.safety_source", &p->safety_source);
+    get_float(root, "code.t_initial", &p->t_initial);
+    get_float(root, "code.t_final", &p->t_final);
+    get_bool(root, "code.antialiasing", &p->antialiasing);
+    get_float(root, "output.snapshot_step", &p->toutput_flow);
+    // STS variables -> bits of the field order of Parameters::popVariablesGrid (:617-638)
+    std::vector<std::string> names;
+    if (p->heat_equation) names = {"th"};
+    else if (p->incompressible) {
+        names = {"vx", "vy", "vz"};
+        if (p->mhd) { names.push_back("bx"); names.push_back("by"); names.push_back("bz"); }
+        if (p->boussinesq) names.push_back("th");
+    }
+    p->sts_vars_mask = 0;
+    for (const std::string& v : sts_vars)
+        for (size_t f = 0; f < names.size(); f++)
+            if (names[f] == v) p->sts_vars_mask |= 1u << f;
+    std::string why;
+    const int rc = check_params(p, why);
+    if (rc == SPK_ERR_CONFIG) return fail(nullptr, rc, why);
+    return SPK_OK;
+}
+
+extern "C" int spk_params_from_string(const char* text, spk_params_t* p) {
+    if (!text || !p) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    const std::string t(text);
+    spkcfg::Setting root;
+    std::string err;
+    if (!spkcfg::Parser(t).parse(root, err)) return fail(nullptr, SPK_ERR_ARG, "configuration: " + err);
+    return params_from_config(root, p);
+}
+
+extern "C" int spk_params_from_file(const char* path, spk_params_t* p) {
+    if (!path || !p) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return fail(nullptr, SPK_ERR_ARG, std::string("cannot open configuration file ") + path);
+    std::string t;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), fp)) > 0) t.append(buf, n);
+    fclose(fp);
+    spkcfg::Setting root;
+    std::string err;
+    if (!spkcfg::Parser(t).parse(root, err)) return fail(nullptr, SPK_ERR_ARG, std::string(path) + ": " + err);
+    return params_from_config(root, p);
 }
 
 static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {

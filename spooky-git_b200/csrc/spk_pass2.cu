@@ -174,13 +174,15 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
 // Shared-memory carve of k_zpass2 (host and device agree through this):
 // barrier, twiddle tables, input half spectra (later: the product pairs),
 // real fields, exchange slots.
-struct ZSmem { size_t tw, area, real, xb, total; };
+struct ZSmem { size_t tw, zero, junk, area, real, xb, total; };
 __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
                                               int nzs, int slots) {
     ZSmem z;
     const int rs = n + 16, xs = n + (n >> 4);
     z.tw = 128;
-    z.area = align16(z.tw + (size_t)twn * csz);
+    z.zero = align16(z.tw + (size_t)twn * csz);              // a zero half spectrum (missing pair partner)
+    z.junk = align16(z.zero + (size_t)nzs * csz);            // a real row that idle transforms write
+    z.area = align16(z.junk + (size_t)rs * (csz / 2));
     const size_t raw = (size_t)nin * lines * nzs * csz, prod = (size_t)npout * lines * n * csz;
     z.real = align16(z.area + (raw > prod ? raw : prod));
     z.xb = align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
@@ -188,7 +190,9 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     return z;
 }
 
-template <typename T, int LN>
+// GEN: derived gradient channels or the to-real output (the general path);
+// otherwise every input channel is a plain half spectrum.
+template <typename T, int LN, bool GEN>
 __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, LN>;
     constexpr int N = F::N, LTPC = F::LTPC, TPC = F::TPC;
@@ -209,6 +213,8 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
+    C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
+    T* junk = reinterpret_cast<T*>(smem_raw + lay.junk);
     C2<T>* raw = reinterpret_cast<C2<T>*>(smem_raw + lay.area);
     C2<T>* prod = raw;                    // the product pairs reuse the input area
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
@@ -229,6 +235,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
     }
     regfft_fill_twiddles<T, LN>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
+    for (int i = tid; i < nzs; i += nthr) zrow[i] = mk<T>((T)0, (T)0);
     const bool ok = mbar_wait(bar, 0, SPK_WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
@@ -243,15 +250,13 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     C2<T> r[F::E];
 
     // 2. inverse transforms of the input pairs
-    const bool simple = a.derive_gz == 0;
     const int ninv = npin * L;
     for (int base = 0; base < ninv; base += slots) {
         const int tau = base + sigma;
         const bool valid = tau < ninv;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
         const C2<T>* pa = raw + (size_t)(2 * p * L + l) * nzs;
-        const C2<T>* pb = pa + (size_t)L * nzs;
-        const bool hasA = 2 * p < nin, hasB = 2 * p + 1 < nin;
+        const C2<T>* pb = 2 * p + 1 < nin ? pa + (size_t)L * nzs : zrow;
         auto chv = [&](int ch, int k) -> C2<T> {
             if (ch < nin) {
                 C2<T> v = raw[((size_t)ch * L + l) * nzs + k];
@@ -272,9 +277,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             constexpr int NH = N >> 1;
             const int k = n <= NH ? n : N - n;
             C2<T> A, B;
-            if (simple) {
-                A = hasA ? pa[k] : mk<T>((T)0, (T)0);
-                B = hasB ? pb[k] : mk<T>((T)0, (T)0);
+            if constexpr (!GEN) {
+                A = pa[k];
+                B = pb[k];
             } else {
                 A = chv(2 * p, k);
                 B = chv(2 * p + 1, k);
@@ -283,14 +288,14 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             if (n < NH) return mk<T>(A.x - B.y, A.y + B.x);
             return mk<T>(A.x + B.y, B.x - A.y);
         });
-        T* pr = real + (size_t)(2 * p * L + l) * RS;
-        const bool has1 = 2 * p + 1 < nin_all;
-        const bool to_real = a.mode == ZM_TO_REAL && valid && l < nl;
+        // an idle transform (and the missing partner of an odd last pair) writes the junk row
+        T* pr0 = valid ? real + (size_t)(2 * p * L + l) * RS : junk;
+        T* pr1 = (valid && 2 * p + 1 < nin_all) ? pr0 + LRS : junk;
+        const bool to_real = GEN && a.mode == ZM_TO_REAL && valid && l < nl;
         regfft_run<T, LN, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
-            if (!valid) return;
-            pr[z] = v.x;
-            if (has1) pr[LRS + z] = v.y;
-            if (to_real) {
+            pr0[z] = v.x;
+            pr1[z] = v.y;
+            if (GEN && to_real) {
                 const size_t line = (size_t)(line0 + l);
                 if (2 * p < nin) a.real_out[((size_t)(2 * p) * nlines + line) * N + z] = (double)v.x;
                 if (2 * p + 1 < nin) a.real_out[((size_t)(2 * p + 1) * nlines + line) * N + z] = (double)v.y;
@@ -308,6 +313,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         T mu[6] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
         int bad = 0;
         T* prodT = reinterpret_cast<T*>(prod);
+        const T third = (T)(1.0 / 3.0);
         const size_t pstride = (size_t)L * N * 2;   // scalars between product pairs
         for (int e = tid; e < L * N; e += nthr) {
             const int l = e >> LN, z = e & (N - 1);
@@ -350,16 +356,16 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             if (a.mode == ZM_PRODUCTS) {
                 if (a.hydro) {
                     if (!a.mhd) {
-                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz) / (T)3.0);
+                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz) * third);
                         put(1, ux * uy);
                         put(2, ux * uz);
-                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz) / (T)3.0);
+                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz) * third);
                         put(4, uy * uz);
                     } else {
-                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) / (T)3.0);
+                        put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) * third);
                         put(1, ux * uy - bx * by);
                         put(2, ux * uz - bx * bz);
-                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) / (T)3.0);
+                        put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) * third);
                         put(4, uy * uz - by * bz);
                     }
                     qc = 5;

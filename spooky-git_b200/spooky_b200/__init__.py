@@ -32,7 +32,7 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_get_state", "spk_set_time", "spk_get_time", "spk_clean_divergence", "spk_compute_dt",
             "spk_compute_dfield", "spk_advance", "spk_rkl_cycle", "spk_to_real", "spk_synchronize",
             "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error",
-            "spk_compute_dfield_noalloc"]
+            "spk_compute_dfield_noalloc", "spk_params_from_file", "spk_params_from_string"]
 
 
 class Budgets(ctypes.Structure):
@@ -82,6 +82,8 @@ def lib():
         L.spk_profile_passes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PassStat), ctypes.c_int, ip]
         L.spk_last_error.argtypes = [vp]
         L.spk_compute_dfield_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp]
+        L.spk_params_from_file.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
+        L.spk_params_from_string.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -112,6 +114,27 @@ def _ptr(a):
             return a.data_ptr(), 0
         return a.data_ptr(), 1
     return a.ctypes.data, 1
+
+
+def params_from_file(path):
+    """Parameters of a libconfig-format spooky.cfg (spk_params_from_file):
+    the reference's keys and defaults, then its module checks.  Raises
+    SpookyError (SPK_ERR_ARG for unreadable or malformed files, SPK_ERR_CONFIG
+    for inconsistent modules)."""
+    p = Params()
+    rc = lib().spk_params_from_file(os.fsencode(path), ctypes.byref(p))
+    if rc != SPK_OK:
+        raise SpookyError(rc, lib().spk_last_error(None).decode())
+    return p
+
+
+def params_from_string(text):
+    """As params_from_file, for configuration text."""
+    p = Params()
+    rc = lib().spk_params_from_string(text.encode(), ctypes.byref(p))
+    if rc != SPK_OK:
+        raise SpookyError(rc, lib().spk_last_error(None).decode())
+    return p
 
 
 NOALLOC_SCRATCH_BYTES = 24 << 20

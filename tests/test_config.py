@@ -1,0 +1,163 @@
+"""CPU tests of the libconfig-format reader behind spk_params_from_file /
+spk_params_from_string: the reference's keys and defaults
+(Parameters::Parameters, src/parameters/parameters.cu:59-505), libconfig's
+typed lookups (no automatic int -> float conversion), the STS variable list
+and Parameters::checkParameters (:511-566).  No GPU call is made."""
+import os
+
+import pytest
+
+import spooky_b200 as S
+from spooky_b200.params import Params, default_params, SPK_STS_RKL2
+
+FULL = """
+# a configuration in the reference's layout
+configname = "MTI-like" "test";   // adjacent strings concatenate
+
+modules:
+{
+    debug = 0;
+    incompressible = true;
+    heat_equation = false;
+    boussinesq = TRUE;
+    stratification = true;
+    strat_direction = 0x2;
+    mhd = true;
+    anisotropic_diffusion = true;
+    supertimestepping = true;
+    sts_algorithm = "rkl2";
+    sts_variables = ("th");
+};
+
+physics:
+{
+    boxsize = (1.0, 2.0, 3.5);
+    gridsize = (64, 32, 16);
+    reynolds = 100000.0;
+    reynolds_thermic = 1e6;
+    reynolds_magnetic = 2.5e4;
+    reynolds_anisotropic = 100.0;
+    brunt_vaissala_squared = 0.1;
+    mti_frequency_squared = 1.0;
+};
+
+/* code parameters
+   over several lines */
+code:
+{
+    cfl = 1.2;
+    cfl_par = 0.9;
+    safety_sts = 100;
+    safety_source = 0.25;
+    t_initial = 0.5;
+    t_final = 2.0;
+    antialiasing = false;
+    restart = false;
+};
+
+output: { timevar_step = 0.1; snapshot_step = 0.5; timevar_vars = ["ev", "em"]; };
+"""
+
+
+def test_full_configuration_matches_the_reference_defaults_and_keys():
+    p = S.params_from_string(FULL)
+    want = default_params(incompressible=1, boussinesq=1, stratification=1, strat_direction=2, mhd=1,
+                          anisotropic_diffusion=1, supertimestepping=1, sts_variables=["th"],
+                          boxsize=(1.0, 2.0, 3.5), gridsize=(64, 32, 16), reynolds=1e5, reynolds_thermic=1e6,
+                          reynolds_magnetic=2.5e4, reynolds_ani=100.0, N2=0.1, OmegaT2=1.0, cfl=1.2, cfl_par=0.9,
+                          safety_sts=100, safety_source=0.25, t_initial=0.5, t_final=2.0, antialiasing=0,
+                          toutput_flow=0.5)
+    for name, _ in Params._fields_:
+        assert getattr(p, name) == getattr(want, name), name
+    assert p.sts_algorithm == SPK_STS_RKL2
+    assert p.sts_vars_mask == 1 << 6   # th is the seventh field of vx vy vz bx by bz th
+
+
+def test_empty_configuration_gives_the_reference_defaults_and_fails_the_module_check():
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string("")
+    assert e.value.code == 6   # neither incompressible nor heat_equation
+
+
+def test_integer_written_for_a_float_key_keeps_the_default():
+    # libconfig's lookup_float does not accept an integer setting (no automatic
+    # conversion), so the reference keeps reynolds = 1.0
+    p = S.params_from_string("modules: { incompressible = true; }; physics: { reynolds = 100; };")
+    assert p.nu == 1.0
+    p = S.params_from_string("modules: { incompressible = true; }; physics: { reynolds = 100.0; };")
+    assert p.nu == 1.0 / 100.0
+    # and a float written for an integer key, or a number for a bool key, keeps the default
+    p = S.params_from_string("modules: { incompressible = true; mhd = 1; }; physics: { gridsize = (16.0, 8, 8); };")
+    assert p.mhd == 0 and (p.nx, p.ny, p.nz) == (32, 8, 8)
+
+
+def test_sts_variable_list():
+    base = "modules: { incompressible = true; mhd = true; supertimestepping = true; sts_algorithm = \"rkl2\"; %s };"
+    p = S.params_from_string(base % 'sts_variables = ("bx", "vz", "nope");')
+    assert p.supertimestepping == 1 and p.sts_vars_mask == (1 << 3) | (1 << 2)
+    p = S.params_from_string(base % 'sts_variables = ["by"];')
+    assert p.sts_vars_mask == 1 << 4
+    # an empty or missing list switches super-time-stepping off (parameters.cu:123-147)
+    assert S.params_from_string(base % "sts_variables = ();").supertimestepping == 0
+    assert S.params_from_string(base % "").supertimestepping == 0
+    # without supertimestepping the list is not read
+    p = S.params_from_string('modules: { incompressible = true; sts_variables = ("vx"); };')
+    assert p.supertimestepping == 0 and p.sts_vars_mask == 0
+
+
+def test_heat_equation_sts_variable_and_unknown_algorithm():
+    p = S.params_from_string('modules: { heat_equation = true; supertimestepping = true; sts_algorithm = "rkl1";'
+                             ' sts_variables = ("th"); };')
+    assert p.sts_vars_mask == 1 and p.sts_algorithm == 2
+
+
+@pytest.mark.parametrize("text", [
+    "a : 1; b = 2, c = 3",                          # ':' assignment, ',' terminator, last terminator optional
+    "g = { h = { i = [1, 2, 0x10]; }; };",
+    "l = (1, \"two\", 3.0, (4, 5), { x = 1; });",   # lists mix types and nest
+    "s = \"esc \\\" \\\\ \\t \\x41\";",
+    "f = (1e3, -2.5E-2, .5, 7.);",
+    "big = 5000000000; lng = 12L;",
+])
+def test_syntax_accepted(text):
+    # parse errors raise; module errors (no module chosen) give code 6
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string(text)
+    assert e.value.code == 6
+
+
+@pytest.mark.parametrize("text,line", [
+    ("modules:\n{\n  incompressible true;\n};", 3),
+    ("a = [1, 2.0];", 1),
+    ("a = (1, 2,);", 1),
+    ("\n\na = \"unterminated;\n", 3),
+    ("x = {\n y = 1;\n", 3),
+    ("a = 1; a = 2;", 1),
+    ("@include \"other.cfg\"", 1),
+])
+def test_syntax_errors_name_the_line(text, line):
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string(text)
+    assert e.value.code == 1
+    assert f"line {line}:" in str(e.value)
+
+
+def test_module_consistency_checks():
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string("modules: { incompressible = true; heat_equation = true; };")
+    assert e.value.code == 6 and "mutually exclusive" in str(e.value)
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string("modules: { incompressible = true; anisotropic_diffusion = true; boussinesq = true; };")
+    assert e.value.code == 6
+
+
+def test_read_from_file(tmp_path):
+    path = tmp_path / "spooky.cfg"
+    path.write_text(FULL)
+    p = S.params_from_file(str(path))
+    q = S.params_from_string(FULL)
+    for name, _ in Params._fields_:
+        assert getattr(p, name) == getattr(q, name), name
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_file(os.path.join(str(tmp_path), "missing.cfg"))
+    assert e.value.code == 1 and "cannot open" in str(e.value)

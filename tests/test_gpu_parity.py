@@ -170,6 +170,36 @@ def test_config1_taylor_green_32_fixed_dt_100_steps():
     assert np.allclose(e_gpu, e_orc, rtol=1e-10)
 
 
+def test_config2_mhd128_fp32_form_within_1e5_of_fp64_after_1000_steps():
+    """128^3 MHD, box 2pi, nu=eta=1e-3, B0=0.1z, CFL 1.5, random solenoidal u, B
+    with E(k) ~ k^4 exp(-2(k/4)^2), rms 1 (seeds 1, 2).  The plain form follows
+    the FP64 oracle (3 steps, rel L2 <= 1e-10); after 1000 steps the FP32 form is
+    within rel L2 1e-5 of the plain form and its total energy within 1e-6."""
+    from spooky_b200.initial import mhd_random_state
+    L = 2 * np.pi
+    kw = dict(incompressible=1, mhd=1, gridsize=(128, 128, 128), boxsize=(L, L, L), reynolds=1e3,
+              reynolds_magnetic=1e3, cfl=1.5, t_final=1e30, toutput_flow=1e30)
+    p64 = default_params(form=SPK_FORM_PLAIN, **kw)
+    p32 = default_params(form=SPK_FORM_FP32, **kw)
+    U0 = mhd_random_state(p64)
+    o = O.Oracle(p64)
+    o.set_state(U0)
+    o.step(3)
+    c64, c32 = Context(p64), Context(p32)
+    c64.set_state(U0)
+    c32.set_state(U0)
+    c64.advance(3)
+    assert rel_l2(c64.get_state(), o.get_state()) < 1e-10
+    c64.advance(997)
+    c32.advance(1000)
+    c64.synchronize()
+    c32.synchronize()
+    assert rel_l2(c32.get_state(), c64.get_state()) < 1e-5
+    e32, _ = c32.budgets()
+    e64, _ = c64.budgets()
+    assert abs(np.sum(e32) - np.sum(e64)) / np.sum(e64) < 1e-6
+
+
 def test_taylor_green_reference_check():
     """tests/taylor-green-vortex/check-taylor-green.py:129-155 at 32^3 (L1 < 1e-7)."""
     n = 32
