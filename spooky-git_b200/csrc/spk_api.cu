@@ -185,20 +185,8 @@ static AxisArgs axis_args(spk_ctx* c, int ax) {
 }
 
 // ---------------------------------------------------------------------------
-// FFT plans: radices from {16 (FP32 only), 8, 4, 2, 3, 5}; twiddles in long double.
+// FFT twiddles W_N^k in long double (rounded once to the pass precision).
 // ---------------------------------------------------------------------------
-static bool make_plan(int n, int maxr, FftPlan* pl) {
-    pl->n = n;
-    pl->nst = 0;
-    int r = n;
-    const int cands[] = {16, 8, 4, 2, 3, 5};
-    for (int cnd : cands) {
-        if (cnd > maxr) continue;
-        while (r % cnd == 0 && pl->nst < 12) { pl->radix[pl->nst++] = cnd; r /= cnd; }
-    }
-    return r == 1;
-}
-
 static void twiddles(int n, std::vector<double>& out) {
     const long double PI = 3.141592653589793238462643383279502884L;
     out.resize(2 * (size_t)n);
@@ -212,7 +200,6 @@ static void twiddles(int n, std::vector<double>& out) {
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
-static inline int rup32(long x) { return (int)(((x + 31) / 32) * 32); }
 
 struct AxisCfg { int kt; int nthr; size_t smem; };
 
@@ -231,17 +218,6 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     return a;
 }
 
-static AxisCfg xfwd_cfg(const spk_ctx* c) {
-    AxisCfg a;
-    const int ept = c->fp32 ? 8 : 4;
-    int kt = c->fp32 ? 16 : 8;
-    while (kt > 1 && (long)c->nx * kt > (long)MAXT * ept) kt /= 2;
-    while (kt > 1 && kt > c->nzh) kt /= 2;
-    a.kt = kt;
-    a.nthr = std::max(32, std::min(MAXT, rup32(((long)c->nx * kt + ept - 1) / ept)));
-    a.smem = (size_t)c->nx * kt * (c->fp32 ? sizeof(float2) : sizeof(double2));
-    return a;
-}
 
 template <typename T, int LN, int DIR, bool CONV>
 static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
@@ -253,7 +229,7 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
     const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, LN>::TWN * sizeof(C2<T>) +
-                         (size_t)N * sizeof(T) + N + 16;
+                         (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
@@ -626,15 +602,20 @@ static void record_rkl_cycle(spk_ctx* c) {
             f.kcols = c->kz_keep; f.row_filter = 1;
             add_job(c, f, c->rA, c->rB, 3, 0, 0, 0);
             if (f.kcols > 0) axis(c, f, -1);
+            // x forward of the flux (kept ky rows in, kept kx rows out)
+            AxisArgs x = axis_args(c, 0);
+            x.gate = c->sc; x.gate_stage = st;
+            x.kcols = c->kz_keep; x.row_filter = 1; x.outer_filter = 1;
+            add_job(c, x, c->rB, c->rA, 3, 0, 0, 0);
+            if (x.kcols > 0) axis(c, x, -1);
             RklArgs r = rkl_args(c, st);
-            const AxisCfg cf = xfwd_cfg(c);
-            r.kt = cf.kt;
-            dim3 grid((c->nzh + cf.kt - 1) / cf.kt, c->ny);
+            r.nl = c->rA;
             int vslot = 0;
             for (int v = 0; v < c->nsts; v++) if (c->sts_kind[v] == 3) vslot = v;
+            const FastDiv fz = FastDiv::make((unsigned)c->nzh);
             c->launches++;
-            if (c->fp32) k_xfwd_rkl<float, 8><<<grid, cf.nthr, cf.smem, c->stream>>>(r, c->U, vslot);
-            else k_xfwd_rkl<double, 4><<<grid, cf.nthr, cf.smem, c->stream>>>(r, c->U, vslot);
+            if (c->fp32) k_rkl_flux<float><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, ilog2(c->ny));
+            else k_rkl_flux<double><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, ilog2(c->ny));
         }
     }
 }
@@ -950,13 +931,12 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     c->nout = oc;
     c->nbuf_ch = std::max(std::max(c->nin + 1, c->nout), 3);
 
-    // FFT plans (lengths the device decomposition covers)
-    const int rf = c->fp32 ? 16 : 8;
-    if (!fft_supported(c->nx, rf) || !fft_supported(c->ny, rf) || !fft_supported(c->nz, rf))
+    // transform lengths the register-resident FFT covers
+    if (!fft_supported(c->nx) || !fft_supported(c->ny) || !fft_supported(c->nz))
         return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be powers of two between 2 and 1024");
-    make_plan(c->nx, 16, &c->plan_x);
-    make_plan(c->ny, 16, &c->plan_y);
-    make_plan(c->nz, 16, &c->plan_z);
+    c->plan_x.n = c->nx;
+    c->plan_y.n = c->ny;
+    c->plan_z.n = c->nz;
     return SPK_OK;
 }
 
@@ -1045,10 +1025,6 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
-    // shared-memory limits of the instantiations used
-    const int big = 200 * 1024;
-    CK(cudaFuncSetAttribute(k_xfwd_rkl<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd_rkl<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     return SPK_OK;
 }
 

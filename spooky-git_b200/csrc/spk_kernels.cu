@@ -290,61 +290,6 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
 
 // Anisotropic conduction STS stage: x-forward of the heat-flux channels,
 // DivergenceMask (generic.cu:315-334) into dtheta, then the stage update.
-template <typename T, int EPT>
-__global__ void __launch_bounds__(256, 2) k_xfwd_rkl(const __grid_constant__ RklArgs a, double2* U, int vslot) {
-    if (a.stage > a.sc->s_rkl) return;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    C2<T>* buf = reinterpret_cast<C2<T>*>(smem_raw);
-    const double* cf = a.sc->rkl[a.stage];
-    const int N = a.g.nx, KT = a.kt, nzh = a.g.nzh;
-    const size_t nc = a.g.nc;
-    const int k0 = blockIdx.x * KT, j = blockIdx.y;
-    const int kt = min(KT, nzh - k0);
-    const size_t stride = (size_t)a.g.ny * nzh, base = (size_t)j * nzh;
-    const double ky = a.g.ky[j], my = a.g.my[j];
-    const bool nl_on = (my != 0.0) && (k0 < a.g.kz_keep);
-    const int nthr = blockDim.x, tid = threadIdx.x, nel = N * KT;
-    const C2<T>* nl = (const C2<T>*)a.nl;
-    C2<T> acc[EPT];
-#pragma unroll
-    for (int u = 0; u < EPT; u++) acc[u] = mk<T>((T)0, (T)0);
-    const size_t nstride = (size_t)a.g.ny * a.g.nzs, nbase = (size_t)j * a.g.nzs + k0;   // pass buffers
-    if (nl_on) {
-        for (int c = 0; c < 3; c++) {
-            const C2<T>* src = nl + (size_t)c * a.cs_nl + nbase;
-            for (int e = tid; e < nel; e += nthr) {
-                const int n = e / KT, col = e - n * KT;
-                buf[e] = (col < kt) ? src[(size_t)n * nstride + col] : mk<T>((T)0, (T)0);
-            }
-            __syncthreads();
-            fft_run<T, -1, EPT, true, 0>(buf, KT, 1, KT, a.plan);
-#pragma unroll
-            for (int u = 0; u < EPT; u++) {
-                const int e = tid + u * nthr;
-                if (e < nel) {
-                    const int n = e / KT, col = e - n * KT;
-                    const T kc = c == 0 ? (T)a.g.kx[n] : (c == 1 ? (T)ky : (T)a.g.kz[min(k0 + col, nzh - 1)]);
-                    acc[u] = cadd(acc[u], cscale(kc, buf[e]));
-                }
-            }
-            __syncthreads();
-        }
-    }
-    double2* Uc = U + (size_t)a.fields[vslot] * nc;
-#pragma unroll
-    for (int u = 0; u < EPT; u++) {
-        const int e = tid + u * nthr;
-        if (e >= nel) continue;
-        const int n = e / KT, col = e - n * KT;
-        if (col >= kt) continue;
-        const int k = k0 + col;
-        const size_t gi = base + (size_t)n * stride + k;
-        const bool m = nl_on && a.g.mx[n] != 0.0 && a.g.mz[k] != 0.0;
-        const double2 s = to_d2(acc[u]);
-        const double2 dU = m ? d2(-s.y, s.x) : d2(0.0, 0.0);   // i * mask * k.q
-        rkl_update(a, cf, (size_t)vslot * nc, gi, Uc, dU);
-    }
-}
 
 // FP64 energy / dissipation sums with the half-spectrum weights
 // (computeEnergy, spooky_output_functions.cu:23-55).

@@ -47,18 +47,18 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     C2<T>* tw = xbuf + (size_t)N * KT;
     T* kax = reinterpret_cast<T*>(tw + F::TWN);                      // wavenumbers along the axis
     unsigned char* keep = reinterpret_cast<unsigned char*>(kax + N);  // row mask factor != 0
+    unsigned char* okeep = keep + N;                                  // outer-index mask factor != 0
     const int stride = a.axis == 0 ? a.g.ny * a.g.nzs : a.g.nzs;
     constexpr uint32_t tile_bytes = (uint32_t)((size_t)N * KT * in_elem);
     const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
-    const double* omask = a.axis == 0 ? a.g.my : a.g.mx;   // mask factor of the outer index
     auto issue = [&](int t, int s) {
         const int jb = t / (nouter * nkb);
         const int rem = t - jb * nouter * nkb;
         const int o = rem / nkb, kb = rem - o * nkb;
         const AxisJob& jo = a.job[jb];
         unsigned char* dst = stages + (size_t)s * stage_bytes;
-        if (a.outer_filter && omask[o] == 0.0) {   // skipped tile: complete the phase with no bytes
+        if (a.outer_filter && !okeep[o]) {   // skipped tile: complete the phase with no bytes
             mbar_expect_tx(&bar[s], 0);
             return;
         }
@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             kax[i] = (T)kg[i];
             keep[i] = mg[i] != 0.0;
         }
+        const double* og = a.axis == 0 ? a.g.my : a.g.mx;   // mask factor of the outer index
+        for (int i = tid; i < nouter; i += blockDim.x) okeep[i] = og[i] != 0.0;
     }
     __syncthreads();
     if (tid == 0)
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const unsigned char* stg = stages + (size_t)s * stage_bytes;
         const bool deriv = jo.deriv != 0;
         const double scale = a.scale;
-        const bool skip = a.outer_filter && omask[o] == 0.0;   // uniform over the CTA
+        const bool skip = a.outer_filter && !okeep[o];   // uniform over the CTA
         if (skip) {
         } else if constexpr (CONV) {
             const double2* src = reinterpret_cast<const double2*>(stg);
@@ -611,6 +613,39 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
             const double2 Un = rk_value(a, (size_t)a.TH * nc + gi, Xt, St, R, dt);
             if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RKL2 stage of the anisotropic heat flux, one mode per thread, after the
+// x-forward pass has transformed the three flux components:
+// dtheta = i * mask * k.q (AnisotropicHeatFlux divergence,
+// anisotropic_conduction.cu:10-62) and the RKL2 stage update of
+// compute_cycle_RKL2 (rkl.cu:437-591).  Skipped for stages beyond the
+// cycle's stage count.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArgs a, double2* U, int vslot, FastDiv fzh,
+                                                  int lny) {
+    if (a.stage > a.sc->s_rkl) return;
+    const double* cf = a.sc->rkl[a.stage];
+    const size_t nc = a.g.nc;
+    const int nzh = a.g.nzh, nzs = a.g.nzs;
+    const C2<T>* nl = (const C2<T>*)a.nl;
+    double2* Uc = U + (size_t)a.fields[vslot] * nc;
+    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+        const unsigned line = fzh.div((unsigned)gi);
+        const int k = (int)(gi - (size_t)line * nzh);
+        const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
+        double2 dU = d2(0.0, 0.0);
+        if (a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0) {
+            const size_t li = (size_t)line * nzs + k;
+            const double2 q0 = to_d2(nl[li]), q1 = to_d2(nl[a.cs_nl + li]), q2 = to_d2(nl[2 * a.cs_nl + li]);
+            const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+            const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
+            dU = d2(-sq.y, sq.x);   // i * mask * k.q
+        }
+        rkl_update(a, cf, (size_t)vslot * nc, gi, Uc, dU);
     }
 }
 
