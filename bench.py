@@ -159,6 +159,124 @@ def cpu_baseline_sample(n):
             "sample": f"{steps} RK3 step(s) of {n}^3 MHD from the same initial state (FP64 C oracle, OpenMP)"}
 
 
+ENSEMBLE_SIZES = (16, 32, 64)
+
+
+def ensemble_boxes(nbox, seed=2024):
+    """Config 4: box sizes uniform over ENSEMBLE_SIZES, HD or MHD with equal
+    odds, nu and eta log-uniform in [1e-4, 1e-2], FP32 form; ICs drawn per box
+    like config 2 (random solenoidal u and B, E(k) ~ k^4 exp(-2(k/4)^2), rms 1,
+    B0 = 0.1 z), seeds from the box index."""
+    rng = np.random.default_rng(seed)
+    L = 2 * np.pi
+    boxes = []
+    for i in range(nbox):
+        n = int(rng.choice(ENSEMBLE_SIZES))
+        mhd = int(rng.integers(0, 2))
+        nu, eta = 10 ** rng.uniform(-4, -2), 10 ** rng.uniform(-4, -2)
+        p = default_params(incompressible=1, mhd=mhd, gridsize=(n, n, n), boxsize=(L, L, L), reynolds=1.0 / nu,
+                           reynolds_magnetic=1.0 / eta, cfl=1.5, form=SPK_FORM_FP32, t_final=1e30,
+                           toutput_flow=1e30)
+        boxes.append((i, p))
+    return boxes
+
+
+def box_state(i, p):
+    from spooky_b200.initial import random_solenoidal, to_spectral
+    u = random_solenoidal(p, 1000 + 2 * i)
+    if not p.mhd:
+        return to_spectral(u)
+    B = random_solenoidal(p, 1001 + 2 * i)
+    B[2] += 0.1
+    return to_spectral(np.concatenate([u, B]))
+
+
+def partition_boxes(costs, world):
+    """Greedy longest-processing-time assignment of boxes to ranks by cost
+    (N^3 log N per box): returns one list of box indices per rank."""
+    order = sorted(range(len(costs)), key=lambda i: -costs[i])
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: load[k])
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def run_ensemble(args, world, rank, local_rank):
+    import torch
+    import torch.distributed as dist
+    import spooky_b200 as S
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    boxes = ensemble_boxes(args.boxes)
+    costs = [p.nx * p.ny * p.nz * np.log2(p.nx * p.ny * p.nz) for _, p in boxes]
+    mine = partition_boxes(costs, world)[rank]
+    params = [boxes[i][1] for i in mine]
+    states = [box_state(*boxes[i]) for i in mine]
+    stream = torch.cuda.Stream()
+    ens = S.Ensemble(params, stream=stream.cuda_stream)
+    for b, U in zip(ens.boxes, states):
+        b.set_state(U)
+    ens.advance(args.warmup)
+    ens.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kps = ens.kernels_per_step()
+    ens.synchronize()
+    finite = all(np.isfinite(b.budgets()[0]).all() for b in ens.boxes)
+    ens.close()
+    # one box at a time: each box alone through its own graph, on a sample
+    nsample = min(len(mine), 64)
+    one_ms = 0.0
+    for k in range(nsample):
+        ctx = S.Context(params[k], stream=stream.cuda_stream)
+        ctx.set_state(states[k])
+        ctx.advance(args.warmup)
+        ctx.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        ctx.advance(args.steps)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        one_ms += a0.elapsed_time(a1)
+        ctx.close()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank == 0:
+        value = args.boxes * args.steps / (ms * 1e-3)
+        sizes = {str(n): sum(1 for _, p in boxes if p.nx == n) for n in ENSEMBLE_SIZES}
+        line = {
+            "metric": "ensemble box-steps/s (config 4: independent HD/MHD boxes, FP32 form, one graph per step)",
+            "value": value, "unit": "box-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak" if world == 1 else "strong",
+            "vs_baseline": None, "dtype": "fp32 passes, fp64 state", "data": "synthetic (seeded random fields)",
+            "config": {"workload": f"{args.boxes} boxes, sizes {list(ENSEMBLE_SIZES)}^3 uniform, HD/MHD 50/50, "
+                                   f"nu, eta log-uniform [1e-4, 1e-2], CFL 1.5", "boxes_per_size": sizes,
+                       "parallelism": f"boxes partitioned over {world} rank(s) by N^3 log N"},
+            "one_box_at_a_time": {"value": nsample * args.steps / (one_ms * 1e-3), "unit": "box-steps/s",
+                                  "sample_boxes": nsample, "rank": 0},
+            "kernels_per_ensemble_step_rank0": kps,
+            "gpu_launches": kps * args.steps,
+            "all_finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -167,6 +285,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="batched-ensemble workload instead: --boxes independent HD/MHD boxes (config 4)")
+    ap.add_argument("--boxes", type=int, default=512)
     ap.add_argument("--profile-run", action="store_true",
                     help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")
@@ -180,6 +301,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)
+        return
+    if args.ensemble:
+        run_ensemble(args, world, rank, local_rank)
         return
 
     import torch

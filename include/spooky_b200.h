@@ -214,6 +214,24 @@ int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out
 #define SPK_NOALLOC_SCRATCH_BYTES (24u << 20)
 int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U, double* dU, void* cuda_stream);
 
+/* Ensembles of independent boxes.  No counterpart in the reference, which
+ * advances one box per process.  Each box gets its own context (so every
+ * spk_* call above works on it through spk_ensemble_box), and
+ * spk_ensemble_advance launches one CUDA graph per step holding the whole
+ * step of every box as parallel branches.  Boxes may differ in size,
+ * modules and parameters; super-time-stepping that alternates between steps
+ * is not supported (SPK_ERR_UNSUPPORTED).  Per-box calls made while an
+ * ensemble step is in flight are ordered after it (their box streams wait
+ * for the ensemble stream); spk_ensemble_synchronize waits for all. */
+typedef struct spk_ensemble spk_ensemble;
+int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cuda_stream, spk_ensemble** out);
+int spk_ensemble_destroy(spk_ensemble* ens);
+int spk_ensemble_size(const spk_ensemble* ens, int* nbox);
+int spk_ensemble_box(spk_ensemble* ens, int i, spk_ctx** box);
+int spk_ensemble_advance(spk_ensemble* ens, int nsteps);
+int spk_ensemble_synchronize(spk_ensemble* ens);
+int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
+
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */
 const char* spk_last_error(const spk_ctx* ctx);

@@ -1274,6 +1274,169 @@ extern "C" int spk_budgets(spk_ctx* c, spk_budgets_t* out) {
     return SPK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Ensembles of independent boxes.  The reference runs one box per process;
+// here every box keeps its own context (state, buffers, stream) and one
+// CUDA graph holds the whole step of every box as parallel branches forked
+// from the ensemble stream and joined back to it, so an ensemble step is a
+// single graph launch and the boxes' small kernels fill the GPU together.
+// ---------------------------------------------------------------------------
+struct spk_ensemble {
+    std::vector<spk_ctx*> box;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t gexec = nullptr;
+    bool have_graph = false;
+    int kernels_per_step = 0;
+};
+
+static int ens_fail(const std::string& msg, int code) { return fail(nullptr, code, msg); }
+
+extern "C" int spk_ensemble_destroy(spk_ensemble* e) {
+    if (!e) return SPK_ERR_ARG;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->have_graph) cudaGraphExecDestroy(e->gexec);
+    for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    for (spk_ctx* c : e->box) spk_ctx_destroy(c);
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cuda_stream, spk_ensemble** out) {
+    if (!boxes || nbox <= 0 || !out) return ens_fail("null argument or empty ensemble", SPK_ERR_ARG);
+    *out = nullptr;
+    for (int i = 0; i < nbox; i++) {
+        const spk_params_t& p = boxes[i];
+        if (p.supertimestepping && !p.sts_every_step)
+            return ens_fail("ensemble box " + std::to_string(i) +
+                                ": super-time-stepping that alternates between steps is not supported in ensembles",
+                            SPK_ERR_UNSUPPORTED);
+    }
+    spk_ensemble* e = new spk_ensemble();
+    e->stream = (cudaStream_t)cuda_stream;
+    if (!e->stream) {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete e;
+            return ens_fail("cudaStreamCreateWithFlags failed", SPK_ERR_CUDA);
+        }
+        e->own_stream = true;
+    }
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+        spk_ensemble_destroy(e);
+        return ens_fail("cudaEventCreate failed", SPK_ERR_CUDA);
+    }
+    for (int i = 0; i < nbox; i++) {
+        spk_ctx* c = nullptr;
+        const int rc = spk_ctx_create(&boxes[i], nullptr, &c);   // each box on a stream of its own
+        if (rc != SPK_OK) {
+            const std::string msg = "ensemble box " + std::to_string(i) + ": " + g_create_error;
+            spk_ensemble_destroy(e);
+            return ens_fail(msg, rc);
+        }
+        e->box.push_back(c);
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            spk_ensemble_destroy(e);
+            return ens_fail("cudaEventCreate failed", SPK_ERR_CUDA);
+        }
+        e->join.push_back(ev);
+    }
+    *out = e;
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_size(const spk_ensemble* e, int* nbox) {
+    if (!e || !nbox) return SPK_ERR_ARG;
+    *nbox = (int)e->box.size();
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_box(spk_ensemble* e, int i, spk_ctx** box) {
+    if (!e || !box || i < 0 || i >= (int)e->box.size()) return ens_fail("ensemble box index out of range", SPK_ERR_ARG);
+    *box = e->box[(size_t)i];
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_advance(spk_ensemble* e, int nsteps) {
+    if (!e || nsteps < 0) return SPK_ERR_ARG;
+    if (nsteps == 0) return SPK_OK;
+    // states set from outside are cleaned once (as spk_advance does), each
+    // on its box stream, and the ensemble stream waits for them
+    for (size_t i = 0; i < e->box.size(); i++) {
+        spk_ctx* c = e->box[i];
+        if (c->dirty) {
+            launch_clean(c);
+            const int rc = launch_status(c);
+            if (rc) return ens_fail("ensemble box " + std::to_string(i) + ": " + c->err, rc);
+        }
+        // work queued on the box stream (set_state, cleaning) precedes the step
+        if (cudaEventRecord(e->join[i], c->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->stream, e->join[i], 0) != cudaSuccess)
+            return ens_fail("ensemble stream ordering failed", SPK_ERR_CUDA);
+    }
+    if (!e->have_graph) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return ens_fail("ensemble graph capture failed to start", SPK_ERR_CUDA);
+        cudaEventRecord(e->fork, e->stream);
+        int bad = SPK_OK;
+        std::string why;
+        long launches = 0;
+        for (size_t i = 0; i < e->box.size() && bad == SPK_OK; i++) {
+            spk_ctx* c = e->box[i];
+            cudaStreamWaitEvent(c->stream, e->fork, 0);      // the box stream joins the capture
+            const long l0 = c->launches;
+            record_step(c, 0);
+            launches += c->launches - l0;
+            c->kernels_per_step[0] = (int)(c->launches - l0);
+            if (c->sticky) { bad = c->sticky; why = "ensemble box " + std::to_string(i) + ": " + c->err; }
+            cudaEventRecord(e->join[i], c->stream);
+            cudaStreamWaitEvent(e->stream, e->join[i], 0);   // and joins back
+        }
+        const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (bad != SPK_OK || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return bad != SPK_OK ? ens_fail(why, bad)
+                                 : ens_fail(std::string("ensemble graph capture: ") + cudaGetErrorString(ce), SPK_ERR_CUDA);
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return ens_fail(std::string("ensemble graph instantiate: ") + cudaGetErrorString(ie), SPK_ERR_CUDA);
+        e->have_graph = true;
+        e->kernels_per_step = (int)launches;
+    }
+    for (int it = 0; it < nsteps; it++) {
+        if (cudaGraphLaunch(e->gexec, e->stream) != cudaSuccess) return ens_fail("ensemble graph launch failed", SPK_ERR_CUDA);
+        for (spk_ctx* c : e->box) c->h_step++;
+    }
+    // per-box calls after this (get_state, budgets) run on the box streams
+    cudaEventRecord(e->fork, e->stream);
+    for (spk_ctx* c : e->box) cudaStreamWaitEvent(c->stream, e->fork, 0);
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_synchronize(spk_ensemble* e) {
+    if (!e) return SPK_ERR_ARG;
+    const cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ens_fail(std::string("ensemble: ") + cudaGetErrorString(ce), SPK_ERR_CUDA);
+    for (size_t i = 0; i < e->box.size(); i++) {
+        spk_ctx* c = e->box[i];
+        const int rc = spk_synchronize(c);
+        if (rc) return ens_fail("ensemble box " + std::to_string(i) + ": " + c->err, rc);
+    }
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_kernels_per_step(const spk_ensemble* e, int* kernels) {
+    if (!e || !kernels) return SPK_ERR_ARG;
+    *kernels = e->kernels_per_step;
+    return SPK_OK;
+}
+
 extern "C" const char* spk_last_error(const spk_ctx* c) {
     return c ? c->err.c_str() : g_create_error.c_str();
 }

@@ -32,7 +32,9 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_get_state", "spk_set_time", "spk_get_time", "spk_clean_divergence", "spk_compute_dt",
             "spk_compute_dfield", "spk_advance", "spk_rkl_cycle", "spk_to_real", "spk_synchronize",
             "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error",
-            "spk_compute_dfield_noalloc", "spk_params_from_file", "spk_params_from_string"]
+            "spk_compute_dfield_noalloc", "spk_params_from_file", "spk_params_from_string",
+            "spk_ensemble_create", "spk_ensemble_destroy", "spk_ensemble_size", "spk_ensemble_box",
+            "spk_ensemble_advance", "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step"]
 
 
 class Budgets(ctypes.Structure):
@@ -84,6 +86,13 @@ def lib():
         L.spk_compute_dfield_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp]
         L.spk_params_from_file.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
         L.spk_params_from_string.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
+        L.spk_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, vp, ctypes.POINTER(vp)]
+        L.spk_ensemble_destroy.argtypes = [vp]
+        L.spk_ensemble_size.argtypes = [vp, ip]
+        L.spk_ensemble_box.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.spk_ensemble_advance.argtypes = [vp, ctypes.c_int]
+        L.spk_ensemble_synchronize.argtypes = [vp]
+        L.spk_ensemble_kernels_per_step.argtypes = [vp, ip]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -161,12 +170,17 @@ def compute_dfield_noalloc(params, U, dU, stream=None):
 class Context:
     """One spk_ctx: the device state and the recorded step pipelines."""
 
-    def __init__(self, params, stream=None):
+    def __init__(self, params, stream=None, _handle=None):
         self.params = params.copy()
-        h = ctypes.c_void_p()
-        rc = lib().spk_ctx_create(ctypes.byref(self.params), stream, ctypes.byref(h))
-        if rc != SPK_OK:
-            raise SpookyError(rc, lib().spk_last_error(None).decode())
+        if _handle is None:
+            h = ctypes.c_void_p()
+            rc = lib().spk_ctx_create(ctypes.byref(self.params), stream, ctypes.byref(h))
+            if rc != SPK_OK:
+                raise SpookyError(rc, lib().spk_last_error(None).decode())
+            self._owned = True
+        else:   # a box of an Ensemble: the ensemble owns the context
+            h = _handle
+            self._owned = False
         self._h = h
         nf, ncx = ctypes.c_int(), ctypes.c_size_t()
         lib().spk_sizes(self._h, ctypes.byref(nf), ctypes.byref(ncx))
@@ -182,7 +196,8 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().spk_ctx_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib().spk_ctx_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -274,6 +289,53 @@ class Context:
 # ---------------------------------------------------------------------------
 # Reference-named objects (src/supervisor, src/fields, src/timestepping, src/rkl)
 # ---------------------------------------------------------------------------
+class Ensemble:
+    """Independent boxes advanced together (spk_ensemble_*): one CUDA graph
+    launch per step for all boxes.  boxes[i] is a Context view of box i (state,
+    time, budgets); the ensemble owns the contexts."""
+
+    def __init__(self, params_list, stream=None):
+        arr = (Params * len(params_list))(*[p.copy() for p in params_list])
+        h = ctypes.c_void_p()
+        rc = lib().spk_ensemble_create(arr, len(params_list), stream, ctypes.byref(h))
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(None).decode())
+        self._h = h
+        self.boxes = []
+        for i, p in enumerate(params_list):
+            bh = ctypes.c_void_p()
+            self._check(lib().spk_ensemble_box(self._h, i, ctypes.byref(bh)))
+            self.boxes.append(Context(p, _handle=bh))
+
+    def _check(self, rc):
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(None).decode())
+
+    def advance(self, nsteps=1):
+        self._check(lib().spk_ensemble_advance(self._h, int(nsteps)))
+
+    def synchronize(self):
+        self._check(lib().spk_ensemble_synchronize(self._h))
+
+    def kernels_per_step(self):
+        k = ctypes.c_int()
+        self._check(lib().spk_ensemble_kernels_per_step(self._h, ctypes.byref(k)))
+        return k.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for b in self.boxes:
+                b._h = None
+            lib().spk_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Parameters:
     """Parameters (src/parameters/parameters.hpp): the cfg subset the path reads."""
 

@@ -1,0 +1,74 @@
+"""Ensembles of independent boxes (spk_ensemble_*): every box advanced inside
+the ensemble's single graph must follow the same box advanced alone."""
+import numpy as np
+import pytest
+
+import spooky_b200 as S
+from fields import random_solenoidal, to_spectral
+from spooky_b200 import Context, Ensemble
+from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, default_params
+
+L = 2 * np.pi
+
+
+def box_params():
+    out = []
+    out.append(default_params(incompressible=1, gridsize=(16, 16, 16), boxsize=(L, L, L), reynolds=100.0,
+                               form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
+    out.append(default_params(incompressible=1, mhd=1, gridsize=(32, 32, 32), boxsize=(L, L, L), reynolds=1e3,
+                               reynolds_magnetic=500.0, form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
+    out.append(default_params(incompressible=1, gridsize=(32, 16, 64), boxsize=(1.0, 0.5, 2.0), reynolds=300.0,
+                               form=SPK_FORM_PLAIN, t_final=1e30, toutput_flow=1e30))
+    out.append(default_params(incompressible=1, mhd=1, boussinesq=1, stratification=1, anisotropic_diffusion=1,
+                               gridsize=(16, 16, 32), boxsize=(1.0, 1.0, 1.0), reynolds=100.0, reynolds_magnetic=100.0,
+                               reynolds_thermic=100.0, reynolds_ani=20.0, N2=1.0, OmegaT2=1.0, form=SPK_FORM_PLAIN,
+                               t_final=1e30, toutput_flow=1e30))
+    out.append(default_params(heat_equation=1, gridsize=(16, 8, 8), reynolds_thermic=10.0, form=SPK_FORM_PLAIN,
+                               t_final=1e30, toutput_flow=1e30))
+    return out
+
+
+def initial_state(p, seed):
+    fields = []
+    if p.incompressible:
+        fields += list(random_solenoidal(p, seed, kpeak=3.0))
+    if p.mhd:
+        B = random_solenoidal(p, seed + 50, kpeak=3.0, rms=0.5)
+        B[0] += 0.2
+        fields += list(B)
+    if p.boussinesq or p.heat_equation:
+        rng = np.random.default_rng(seed + 99)
+        fields.append(0.2 * rng.standard_normal((p.nx, p.ny, p.nz)))
+    return to_spectral(np.stack(fields))
+
+
+@pytest.mark.gpu
+def test_ensemble_boxes_follow_the_same_boxes_alone():
+    params = box_params()
+    states = [initial_state(p, 10 + i) for i, p in enumerate(params)]
+    ens = Ensemble(params)
+    for b, U in zip(ens.boxes, states):
+        b.set_state(U)
+    ens.advance(4)
+    ens.advance(3)
+    ens.synchronize()
+    assert ens.kernels_per_step() > 0
+    for i, (p, U) in enumerate(zip(params, states)):
+        ctx = Context(p)
+        ctx.set_state(U)
+        ctx.advance(7)
+        ctx.synchronize()
+        got, want = ens.boxes[i].get_state(), ctx.get_state()
+        assert np.array_equal(got, want), i
+        assert ens.boxes[i].get_time() == ctx.get_time(), i
+    ens.close()
+
+
+def test_ensemble_rejects_alternating_sts_and_empty_lists():
+    p = default_params(incompressible=1, boussinesq=1, supertimestepping=1, sts_variables=["th"])
+    with pytest.raises(S.SpookyError) as e:
+        Ensemble([p])
+    assert e.value.code == 2 and "alternates" in str(e.value)
+    with pytest.raises(S.SpookyError) as e:
+        Ensemble([])
+    assert e.value.code == 1
