@@ -215,19 +215,25 @@ int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out
 int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U, double* dU, void* cuda_stream);
 
 /* Ensembles of independent boxes.  No counterpart in the reference, which
- * advances one box per process.  Each box gets its own context (so every
- * spk_* call above works on it through spk_ensemble_box), and
- * spk_ensemble_advance launches one CUDA graph per step holding the whole
- * step of every box as parallel branches.  Boxes may differ in size,
- * modules and parameters; super-time-stepping that alternates between steps
- * is not supported (SPK_ERR_UNSUPPORTED).  Per-box calls made while an
- * ensemble step is in flight are ordered after it (their box streams wait
- * for the ensemble stream); spk_ensemble_synchronize waits for all. */
+ * advances one box per process.  Boxes that share everything but their
+ * viscosity, resistivity and thermal diffusivity form a group: one set of
+ * arrays holds the group's boxes side by side and every pass kernel covers
+ * all of them in one launch, each box with its own dt.  Groups run as
+ * parallel branches of one CUDA graph: spk_ensemble_advance launches it once
+ * per step.  Super-time-stepping that alternates between steps is not
+ * supported (SPK_ERR_UNSUPPORTED), nor super-time-stepping boxes sharing a
+ * group.  Boxes are numbered in the order given; state arrays are a box's
+ * [F][Nc] complex FP64 (where: 0 device, 1 host).  Per-box calls made while
+ * a step is in flight are ordered after it; spk_ensemble_synchronize waits
+ * for the whole ensemble and reports the first error of any box. */
 typedef struct spk_ensemble spk_ensemble;
 int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cuda_stream, spk_ensemble** out);
 int spk_ensemble_destroy(spk_ensemble* ens);
-int spk_ensemble_size(const spk_ensemble* ens, int* nbox);
-int spk_ensemble_box(spk_ensemble* ens, int i, spk_ctx** box);
+int spk_ensemble_size(const spk_ensemble* ens, int* nbox, int* ngroups);
+int spk_ensemble_set_state(spk_ensemble* ens, int box, const double* U, int where);
+int spk_ensemble_get_state(spk_ensemble* ens, int box, double* U, int where);
+int spk_ensemble_get_time(spk_ensemble* ens, int box, double* t, double* dt, int* step);
+int spk_ensemble_budgets(spk_ensemble* ens, int box, spk_budgets_t* out);
 int spk_ensemble_advance(spk_ensemble* ens, int nsteps);
 int spk_ensemble_synchronize(spk_ensemble* ens);
 int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);

@@ -72,6 +72,10 @@ struct spk_ctx {
     const void* user_U;            // caller's state array during spk_compute_dfield
     bool dirty;                    // state set from outside: clean u, B before the next step
     int num_sms;
+    // boxes of one geometry side by side (ensembles): U, S [nb][F][nc], pass
+    // buffers [nb][nbuf_ch][ncs], DevScalars[nb] with each box's viscosities
+    int nb = 1;
+    std::vector<double> bnu, bnu_m, bnu_th;
     int kernels_per_step[2];
 };
 
@@ -127,7 +131,7 @@ static bool locate(const spk_ctx* c, const void* p, bool state, const void** bas
             if (!b) continue;
             const size_t cb = c->nc * sizeof(double2);
             if (q >= (const char*)b && q < (const char*)b + (size_t)c->F * cb && (size_t)(q - (const char*)b) % cb == 0) {
-                *base = b; *nchan = c->F; *ch = (int)((q - (const char*)b) / cb);
+                *base = b; *nchan = c->F * (b == c->U ? c->nb : 1); *ch = (int)((q - (const char*)b) / cb);
                 return true;
             }
         }
@@ -140,7 +144,7 @@ static bool locate(const spk_ctx* c, const void* p, bool state, const void** bas
         if (cb == 0) return false;
         const int n = buf_channels(c, b);
         if (q >= (const char*)b && q < (const char*)b + (size_t)n * cb && (size_t)(q - (const char*)b) % cb == 0) {
-            *base = b; *nchan = n; *ch = (int)((q - (const char*)b) / cb);
+            *base = b; *nchan = n * ((b == c->bufA || b == c->bufB) ? c->nb : 1); *ch = (int)((q - (const char*)b) / cb);
             return true;
         }
     }
@@ -181,6 +185,8 @@ static AxisArgs axis_args(spk_ctx* c, int ax) {
     a.axis = ax;
     a.kcols = c->nzh;
     a.scale = 1.0;
+    a.nb = c->nb;
+    a.out_box_ch = c->nbuf_ch;
     return a;
 }
 
@@ -322,7 +328,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
         return;
     }
     z.lines = L;
-    const int nblk = (int)((nlines + L - 1) / L);
+    const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
     if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
         cudaFuncSetAttribute(k_zpass2<T, LN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -395,6 +401,12 @@ static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch,
         a.box_rows = d;
     }
     if (in_state && c->fp32) a.convert = 1;
+    a.in_box_ch = in_state ? c->F : buf_channels(c, base);
+    if (c->nb > 1 && (base == c->rA || base == c->rB || base == c->user_U)) {
+        c->bad_job = true;
+        c->bad_why = "a single-box buffer in a multi-box pass";
+        return;
+    }
     for (int q = 0; q < nch; q++) {
         AxisJob& j = a.job[a.njobs++];
         if (!make_tmap(c, base, nchan, in_state != 0, a.axis, a.kt, a.box_rows, &j.tm)) {
@@ -447,6 +459,9 @@ static ZArgs z_args(spk_ctx* c) {
     z.chi = 1.0 / c->p.reynolds_ani;
     z.omegaT2 = c->p.OmegaT2;
     z.fd_nz = FastDiv::make((unsigned)c->nz);
+    z.nb = c->nb;
+    z.in_box = z.out_box = (size_t)c->nbuf_ch * c->g.ncs;
+    z.scs = c->sc;
     return z;
 }
 
@@ -500,7 +515,7 @@ static void pass_x_forward(spk_ctx* c) {
 static void rhs(spk_ctx* c, XfArgs& x) {
     const FastDiv fz = FastDiv::make((unsigned)c->nzh);
     // 128-thread CTAs, three per SM: every load of a mode is issued up front
-    const int grid = (int)std::min<size_t>((c->nc + 127) / 128, (size_t)c->num_sms * 3 * 8);
+    const int grid = (int)std::min<size_t>((c->nc * c->nb + 127) / 128, (size_t)c->num_sms * 3 * 8);
     c->launches++;
     if (c->fp32) k_rhs<float><<<grid, 128, 0, c->stream>>>(x, fz);
     else k_rhs<double><<<grid, 128, 0, c->stream>>>(x, fz);
@@ -518,6 +533,10 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     x.plan = c->plan_x;
     x.nl = c->bufA; x.cs_nl = c->g.ncs;   // products after the x-forward pass
     x.lny = ilog2(c->ny);
+    x.lnl = ilog2(c->nx) + ilog2(c->ny);
+    x.nb = c->nb;
+    x.box_state = (size_t)c->F * c->nc;
+    x.box_nl = (size_t)c->nbuf_ch * c->g.ncs;
     x.nl_T = c->out_T; x.nl_E = c->out_E; x.nl_F = c->out_F; x.nl_Q = c->out_Q;
     x.U = U; x.S = c->S; x.out = nullptr;
     x.F = c->F; x.VEL = c->VEL; x.MAG = c->MAG; x.TH = c->TH;
@@ -649,18 +668,18 @@ static void record_step(spk_ctx* c, int parity) {
     const int nst = euler ? 1 : 3;
     if (p.heat_equation) {
         DtArgs d = dt_args(c, true);
-        k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+        k_dt<<<c->nb, 32, 0, c->stream>>>(d, c->sc);
         c->launches++;
         if (sts_before) record_rkl_cycle(c);
         for (int s = 0; s < nst; s++) {
             XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, false);
-            k_heat<<<ew_blocks(c->nc), 256, 0, c->stream>>>(x);
+            k_heat<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(x);
             c->launches++;
         }
         if (sts_after) record_rkl_cycle(c);
         return;
     }
-    k_reset_max<<<1, 32, 0, c->stream>>>(c->sc);
+    k_reset_max<<<c->nb, 32, 0, c->stream>>>(c->sc);
     c->launches++;
     for (int s = 0; s < nst; s++) {
         const bool first = s == 0;
@@ -670,14 +689,14 @@ static void record_step(spk_ctx* c, int parity) {
             if (sts_before) {
                 pass_z_inverse_only(c, true, c->sts_aniso);
                 DtArgs d = dt_args(c, true);
-                k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+                k_dt<<<c->nb, 32, 0, c->stream>>>(d, c->sc);
                 c->launches++;
                 record_rkl_cycle(c);
                 pass_z_products(c, false);
             } else {
                 pass_z_products(c, true);
                 DtArgs d = dt_args(c, true);
-                k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
+                k_dt<<<c->nb, 32, 0, c->stream>>>(d, c->sc);
                 c->launches++;
             }
         } else {
@@ -993,15 +1012,16 @@ static int ctx_alloc(spk_ctx* c) {
         off += n;
     }
     // state and buffers
-    CK(cudaMalloc(&c->U, sizeof(double2) * nc * c->F));
-    CK(cudaMalloc(&c->S, sizeof(double2) * nc * c->F));
-    CK(cudaMemset(c->U, 0, sizeof(double2) * nc * c->F));
-    CK(cudaMemset(c->S, 0, sizeof(double2) * nc * c->F));
+    const size_t nb = (size_t)c->nb;
+    CK(cudaMalloc(&c->U, sizeof(double2) * nc * c->F * nb));
+    CK(cudaMalloc(&c->S, sizeof(double2) * nc * c->F * nb));
+    CK(cudaMemset(c->U, 0, sizeof(double2) * nc * c->F * nb));
+    CK(cudaMemset(c->S, 0, sizeof(double2) * nc * c->F * nb));
     if (c->p.incompressible) {
-        CK(cudaMalloc(&c->bufA, cs * c->g.ncs * c->nbuf_ch));
-        CK(cudaMalloc(&c->bufB, cs * c->g.ncs * c->nbuf_ch));
-        CK(cudaMemset(c->bufA, 0, cs * c->g.ncs * c->nbuf_ch));
-        CK(cudaMemset(c->bufB, 0, cs * c->g.ncs * c->nbuf_ch));
+        CK(cudaMalloc(&c->bufA, cs * c->g.ncs * c->nbuf_ch * nb));
+        CK(cudaMalloc(&c->bufB, cs * c->g.ncs * c->nbuf_ch * nb));
+        CK(cudaMemset(c->bufA, 0, cs * c->g.ncs * c->nbuf_ch * nb));
+        CK(cudaMemset(c->bufB, 0, cs * c->g.ncs * c->nbuf_ch * nb));
     }
     if (c->nsts > 0) {
         CK(cudaMalloc(&c->Uc0, sizeof(double2) * nc * c->nsts));
@@ -1018,11 +1038,16 @@ static int ctx_alloc(spk_ctx* c) {
         CK(cudaMemset(c->rB, 0, cs * c->g.ncs * 3));
         CK(cudaMalloc(&c->breal, (c->fp32 ? sizeof(float) : sizeof(double)) * c->nr * 3));
     }
-    CK(cudaMalloc(&c->sc, sizeof(DevScalars)));
-    CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
-    memset(c->h_sc, 0, sizeof(DevScalars));
-    c->h_sc->t = c->p.t_initial;
-    CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->sc, sizeof(DevScalars) * nb));
+    CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars) * nb));
+    memset(c->h_sc, 0, sizeof(DevScalars) * nb);
+    for (size_t b = 0; b < nb; b++) {
+        c->h_sc[b].t = c->p.t_initial;
+        c->h_sc[b].nu = c->bnu.empty() ? c->p.nu : c->bnu[b];
+        c->h_sc[b].nu_m = c->bnu_m.empty() ? c->p.nu_m : c->bnu_m[b];
+        c->h_sc[b].nu_th = c->bnu_th.empty() ? c->p.nu_th : c->bnu_th[b];
+    }
+    CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars) * nb, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
     return SPK_OK;
@@ -1113,7 +1138,7 @@ extern "C" int spk_set_time(spk_ctx* c, double t, int step, double t_lastsnap) {
 }
 
 static int pull_scalars(spk_ctx* c) {
-    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(DevScalars) * c->nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return SPK_OK;
 }
@@ -1129,16 +1154,17 @@ extern "C" int spk_get_time(spk_ctx* c, double* t, double* dt, int* step) {
 }
 
 static void launch_clean(spk_ctx* c) {
-    if (c->p.incompressible) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc);
-    if (c->p.mhd) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc);
+    const size_t bs = (size_t)c->F * c->nc;
+    if (c->p.incompressible)
+        k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc, bs, c->nb);
+    if (c->p.mhd)
+        k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc, bs, c->nb);
     c->dirty = false;
 }
 
 extern "C" int spk_clean_divergence(spk_ctx* c) {
     if (!c) return SPK_ERR_ARG;
-    c->dirty = false;
-    if (c->p.incompressible) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc);
-    if (c->p.mhd) k_clean<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc);
+    launch_clean(c);
     return launch_status(c);
 }
 
@@ -1254,15 +1280,19 @@ extern "C" int spk_synchronize(spk_ctx* c) {
     CK(cudaStreamSynchronize(c->stream));
     int rc = pull_scalars(c);
     if (rc) return rc;
-    if (c->h_sc->err) return fail(c, SPK_ERR_ARG, "RKL2 stage count exceeded the recorded bound");
-    if (c->h_sc->nonfinite) return fail(c, SPK_ERR_NONFINITE, "non-finite value in the real-space fields");
+    for (int b = 0; b < c->nb; b++) {
+        const std::string box = c->nb > 1 ? " (box " + std::to_string(b) + " of the group)" : "";
+        if (c->h_sc[b].err == 1) return fail(c, SPK_ERR_ARG, "RKL2 stage count exceeded the recorded bound" + box);
+        if (c->h_sc[b].err == 2) return fail(c, SPK_ERR_CUDA, "a bulk/TMA copy wait ran out in a pass kernel" + box);
+        if (c->h_sc[b].nonfinite) return fail(c, SPK_ERR_NONFINITE, "non-finite value in the real-space fields" + box);
+    }
     return SPK_OK;
 }
 
-extern "C" int spk_budgets(spk_ctx* c, spk_budgets_t* out) {
-    if (!c || !out) return SPK_ERR_ARG;
+// Energy budgets of box b (0 for a single-box context).
+static int box_budgets(spk_ctx* c, int b, spk_budgets_t* out) {
     CK(cudaMemsetAsync(c->d_sums, 0, sizeof(double) * 16, c->stream));
-    k_budgets<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->F, c->d_sums);
+    k_budgets<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)b * c->F * c->nc, c->F, c->d_sums);
     CK(cudaMemcpyAsync(c->h_sums, c->d_sums, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const double n2 = (double)c->nr * (double)c->nr;
@@ -1274,19 +1304,80 @@ extern "C" int spk_budgets(spk_ctx* c, spk_budgets_t* out) {
     return SPK_OK;
 }
 
+extern "C" int spk_budgets(spk_ctx* c, spk_budgets_t* out) {
+    if (!c || !out) return SPK_ERR_ARG;
+    return box_budgets(c, 0, out);
+}
+
 // ---------------------------------------------------------------------------
-// Ensembles of independent boxes.  The reference runs one box per process;
-// here every box keeps its own context (state, buffers, stream) and one
-// CUDA graph holds the whole step of every box as parallel branches forked
-// from the ensemble stream and joined back to it, so an ensemble step is a
-// single graph launch and the boxes' small kernels fill the GPU together.
+// Ensembles of independent boxes.  The reference runs one box per process.
+// Here boxes that share everything but their viscosities (nu, nu_m, nu_th)
+// form a group: one context whose arrays hold the group's boxes side by
+// side, whose pass kernels cover all of them in one launch (the box is part
+// of the tile / line / mode index) and whose DevScalars hold one dt and one
+// set of viscosities per box.  Groups run as parallel branches of one CUDA
+// graph, so an ensemble step is a single graph launch of a few launches per
+// group.
 // ---------------------------------------------------------------------------
+static bool same_group(const spk_params_t& a, const spk_params_t& b) {
+    return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.lx == b.lx && a.ly == b.ly && a.lz == b.lz &&
+           a.incompressible == b.incompressible && a.heat_equation == b.heat_equation && a.mhd == b.mhd &&
+           a.boussinesq == b.boussinesq && a.stratification == b.stratification &&
+           a.strat_direction == b.strat_direction && a.anisotropic_diffusion == b.anisotropic_diffusion &&
+           a.supertimestepping == b.supertimestepping && a.sts_algorithm == b.sts_algorithm &&
+           a.sts_vars_mask == b.sts_vars_mask && a.with2d == b.with2d && a.antialiasing == b.antialiasing &&
+           a.reynolds_ani == b.reynolds_ani && a.N2 == b.N2 && a.OmegaT2 == b.OmegaT2 && a.cfl == b.cfl &&
+           a.cfl_par == b.cfl_par && a.cfl_sts == b.cfl_sts && a.safety_source == b.safety_source &&
+           a.safety_sts == b.safety_sts && a.t_initial == b.t_initial && a.t_final == b.t_final &&
+           a.toutput_flow == b.toutput_flow && a.fixed_dt == b.fixed_dt && a.integrator == b.integrator &&
+           a.sts_every_step == b.sts_every_step && a.form == b.form;
+}
+
+// A context for nb boxes of one geometry (nu, nu_m, nu_th per box).
+static int ctx_create_group(const spk_params_t& p0, const std::vector<double>& nu, const std::vector<double>& nu_m,
+                            const std::vector<double>& nu_th, spk_ctx** out) {
+    std::string why;
+    int rc = check_params(&p0, why);
+    if (rc != SPK_OK) return fail(nullptr, rc, why);
+    spk_ctx* c = new spk_ctx();
+    memset(c->have_graph, 0, sizeof(c->have_graph));
+    c->d_tab = nullptr; c->d_tw = nullptr; c->U = c->S = nullptr; c->bufA = c->bufB = nullptr;
+    c->rA = c->rB = c->breal = nullptr; c->Uc0 = c->Uc1 = c->dU0 = nullptr; c->sc = nullptr;
+    c->h_sc = nullptr; c->d_sums = nullptr; c->h_sums = nullptr; c->h_step = 0; c->sticky = 0;
+    c->launches = 0; c->kernels_per_step[0] = c->kernels_per_step[1] = 0; c->bad_job = false; c->bad_why = "";
+    c->user_U = nullptr; c->dirty = true;
+    c->nb = (int)nu.size();
+    c->bnu = nu; c->bnu_m = nu_m; c->bnu_th = nu_th;
+    rc = ctx_init(c, &p0, nullptr);
+    if (rc != SPK_OK) { delete c; return rc; }
+    if (c->nsts > 0 && c->nb > 1) {
+        ctx_free(c);
+        delete c;
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, "super-time-stepping boxes cannot share a group");
+    }
+    if ((size_t)c->nb * c->nc >= (1ull << 31)) {
+        ctx_free(c);
+        delete c;
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, "a group of boxes above 2^31 modes");
+    }
+    rc = ctx_alloc(c);
+    if (rc != SPK_OK) {
+        g_create_error = c->err;
+        ctx_free(c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return SPK_OK;
+}
+
 struct spk_ensemble {
-    std::vector<spk_ctx*> box;
+    std::vector<spk_ctx*> group;               // one context per geometry
+    std::vector<std::pair<int, int>> where;    // box -> (group, index in the group)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
+    std::vector<cudaEvent_t> join;             // one per group
     cudaGraphExec_t gexec = nullptr;
     bool have_graph = false;
     int kernels_per_step = 0;
@@ -1300,7 +1391,7 @@ extern "C" int spk_ensemble_destroy(spk_ensemble* e) {
     if (e->have_graph) cudaGraphExecDestroy(e->gexec);
     for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
-    for (spk_ctx* c : e->box) spk_ctx_destroy(c);
+    for (spk_ctx* c : e->group) spk_ctx_destroy(c);
     if (e->own_stream) cudaStreamDestroy(e->stream);
     delete e;
     return SPK_OK;
@@ -1316,7 +1407,19 @@ extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cu
                                 ": super-time-stepping that alternates between steps is not supported in ensembles",
                             SPK_ERR_UNSUPPORTED);
     }
+    // groups in order of first appearance
+    std::vector<std::vector<int>> members;
+    std::vector<std::pair<int, int>> where((size_t)nbox);
+    for (int i = 0; i < nbox; i++) {
+        int gidx = -1;
+        for (size_t gq = 0; gq < members.size(); gq++)
+            if (same_group(boxes[members[gq][0]], boxes[i])) { gidx = (int)gq; break; }
+        if (gidx < 0) { gidx = (int)members.size(); members.emplace_back(); }
+        where[(size_t)i] = {gidx, (int)members[(size_t)gidx].size()};
+        members[(size_t)gidx].push_back(i);
+    }
     spk_ensemble* e = new spk_ensemble();
+    e->where = where;
     e->stream = (cudaStream_t)cuda_stream;
     if (!e->stream) {
         if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1329,15 +1432,21 @@ extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cu
         spk_ensemble_destroy(e);
         return ens_fail("cudaEventCreate failed", SPK_ERR_CUDA);
     }
-    for (int i = 0; i < nbox; i++) {
+    for (size_t gq = 0; gq < members.size(); gq++) {
+        std::vector<double> nu, nu_m, nu_th;
+        for (int i : members[gq]) {
+            nu.push_back(boxes[i].nu);
+            nu_m.push_back(boxes[i].nu_m);
+            nu_th.push_back(boxes[i].nu_th);
+        }
         spk_ctx* c = nullptr;
-        const int rc = spk_ctx_create(&boxes[i], nullptr, &c);   // each box on a stream of its own
+        const int rc = ctx_create_group(boxes[members[gq][0]], nu, nu_m, nu_th, &c);
         if (rc != SPK_OK) {
-            const std::string msg = "ensemble box " + std::to_string(i) + ": " + g_create_error;
+            const std::string msg = "ensemble box " + std::to_string(members[gq][0]) + ": " + g_create_error;
             spk_ensemble_destroy(e);
             return ens_fail(msg, rc);
         }
-        e->box.push_back(c);
+        e->group.push_back(c);
         cudaEvent_t ev;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
             spk_ensemble_destroy(e);
@@ -1349,33 +1458,74 @@ extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cu
     return SPK_OK;
 }
 
-extern "C" int spk_ensemble_size(const spk_ensemble* e, int* nbox) {
-    if (!e || !nbox) return SPK_ERR_ARG;
-    *nbox = (int)e->box.size();
+extern "C" int spk_ensemble_size(const spk_ensemble* e, int* nbox, int* ngroups) {
+    if (!e) return SPK_ERR_ARG;
+    if (nbox) *nbox = (int)e->where.size();
+    if (ngroups) *ngroups = (int)e->group.size();
     return SPK_OK;
 }
 
-extern "C" int spk_ensemble_box(spk_ensemble* e, int i, spk_ctx** box) {
-    if (!e || !box || i < 0 || i >= (int)e->box.size()) return ens_fail("ensemble box index out of range", SPK_ERR_ARG);
-    *box = e->box[(size_t)i];
+static spk_ctx* ens_box(spk_ensemble* e, int i, int* b) {
+    if (!e || i < 0 || i >= (int)e->where.size()) return nullptr;
+    *b = e->where[(size_t)i].second;
+    return e->group[(size_t)e->where[(size_t)i].first];
+}
+
+extern "C" int spk_ensemble_set_state(spk_ensemble* e, int i, const double* U, int where) {
+    int b;
+    spk_ctx* c = ens_box(e, i, &b);
+    if (!c || !U) return ens_fail("ensemble box index out of range or null state", SPK_ERR_ARG);
+    const size_t n = (size_t)c->F * c->nc;
+    CK(cudaMemcpyAsync(c->U + (size_t)b * n, U, sizeof(double2) * n,
+                       where ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
+    c->dirty = true;
     return SPK_OK;
+}
+
+extern "C" int spk_ensemble_get_state(spk_ensemble* e, int i, double* U, int where) {
+    int b;
+    spk_ctx* c = ens_box(e, i, &b);
+    if (!c || !U) return ens_fail("ensemble box index out of range or null state", SPK_ERR_ARG);
+    const size_t n = (size_t)c->F * c->nc;
+    CK(cudaMemcpyAsync(U, c->U + (size_t)b * n, sizeof(double2) * n,
+                       where ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c->stream));
+    if (where) CK(cudaStreamSynchronize(c->stream));
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_get_time(spk_ensemble* e, int i, double* t, double* dt, int* step) {
+    int b;
+    spk_ctx* c = ens_box(e, i, &b);
+    if (!c) return ens_fail("ensemble box index out of range", SPK_ERR_ARG);
+    const int rc = pull_scalars(c);
+    if (rc) return rc;
+    if (t) *t = c->h_sc[b].t;
+    if (dt) *dt = c->h_sc[b].dt;
+    if (step) *step = c->h_sc[b].step;
+    return SPK_OK;
+}
+
+extern "C" int spk_ensemble_budgets(spk_ensemble* e, int i, spk_budgets_t* out) {
+    int b;
+    spk_ctx* c = ens_box(e, i, &b);
+    if (!c || !out) return ens_fail("ensemble box index out of range or null output", SPK_ERR_ARG);
+    return box_budgets(c, b, out);
 }
 
 extern "C" int spk_ensemble_advance(spk_ensemble* e, int nsteps) {
     if (!e || nsteps < 0) return SPK_ERR_ARG;
     if (nsteps == 0) return SPK_OK;
     // states set from outside are cleaned once (as spk_advance does), each
-    // on its box stream, and the ensemble stream waits for them
-    for (size_t i = 0; i < e->box.size(); i++) {
-        spk_ctx* c = e->box[i];
+    // on its group stream, and the ensemble stream waits for the groups
+    for (size_t gq = 0; gq < e->group.size(); gq++) {
+        spk_ctx* c = e->group[gq];
         if (c->dirty) {
             launch_clean(c);
             const int rc = launch_status(c);
-            if (rc) return ens_fail("ensemble box " + std::to_string(i) + ": " + c->err, rc);
+            if (rc) return ens_fail("ensemble group " + std::to_string(gq) + ": " + c->err, rc);
         }
-        // work queued on the box stream (set_state, cleaning) precedes the step
-        if (cudaEventRecord(e->join[i], c->stream) != cudaSuccess ||
-            cudaStreamWaitEvent(e->stream, e->join[i], 0) != cudaSuccess)
+        if (cudaEventRecord(e->join[gq], c->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->stream, e->join[gq], 0) != cudaSuccess)
             return ens_fail("ensemble stream ordering failed", SPK_ERR_CUDA);
     }
     if (!e->have_graph) {
@@ -1386,16 +1536,16 @@ extern "C" int spk_ensemble_advance(spk_ensemble* e, int nsteps) {
         int bad = SPK_OK;
         std::string why;
         long launches = 0;
-        for (size_t i = 0; i < e->box.size() && bad == SPK_OK; i++) {
-            spk_ctx* c = e->box[i];
-            cudaStreamWaitEvent(c->stream, e->fork, 0);      // the box stream joins the capture
+        for (size_t gq = 0; gq < e->group.size() && bad == SPK_OK; gq++) {
+            spk_ctx* c = e->group[gq];
+            cudaStreamWaitEvent(c->stream, e->fork, 0);      // the group stream joins the capture
             const long l0 = c->launches;
             record_step(c, 0);
             launches += c->launches - l0;
             c->kernels_per_step[0] = (int)(c->launches - l0);
-            if (c->sticky) { bad = c->sticky; why = "ensemble box " + std::to_string(i) + ": " + c->err; }
-            cudaEventRecord(e->join[i], c->stream);
-            cudaStreamWaitEvent(e->stream, e->join[i], 0);   // and joins back
+            if (c->sticky) { bad = c->sticky; why = "ensemble group " + std::to_string(gq) + ": " + c->err; }
+            cudaEventRecord(e->join[gq], c->stream);
+            cudaStreamWaitEvent(e->stream, e->join[gq], 0);   // and joins back
         }
         const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
         if (bad != SPK_OK || ce != cudaSuccess) {
@@ -1411,11 +1561,11 @@ extern "C" int spk_ensemble_advance(spk_ensemble* e, int nsteps) {
     }
     for (int it = 0; it < nsteps; it++) {
         if (cudaGraphLaunch(e->gexec, e->stream) != cudaSuccess) return ens_fail("ensemble graph launch failed", SPK_ERR_CUDA);
-        for (spk_ctx* c : e->box) c->h_step++;
+        for (spk_ctx* c : e->group) c->h_step++;
     }
-    // per-box calls after this (get_state, budgets) run on the box streams
+    // per-box calls after this (get_state, budgets) run on the group streams
     cudaEventRecord(e->fork, e->stream);
-    for (spk_ctx* c : e->box) cudaStreamWaitEvent(c->stream, e->fork, 0);
+    for (spk_ctx* c : e->group) cudaStreamWaitEvent(c->stream, e->fork, 0);
     return SPK_OK;
 }
 
@@ -1423,10 +1573,10 @@ extern "C" int spk_ensemble_synchronize(spk_ensemble* e) {
     if (!e) return SPK_ERR_ARG;
     const cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) return ens_fail(std::string("ensemble: ") + cudaGetErrorString(ce), SPK_ERR_CUDA);
-    for (size_t i = 0; i < e->box.size(); i++) {
-        spk_ctx* c = e->box[i];
+    for (size_t gq = 0; gq < e->group.size(); gq++) {
+        spk_ctx* c = e->group[gq];
         const int rc = spk_synchronize(c);
-        if (rc) return ens_fail("ensemble box " + std::to_string(i) + ": " + c->err, rc);
+        if (rc) return ens_fail("ensemble group " + std::to_string(gq) + ": " + c->err, rc);
     }
     return SPK_OK;
 }
@@ -1658,7 +1808,13 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
         CK(cudaMemcpyAsync(c->d_tw, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, c->stream));
     }
     // what must start at zero: the device scalars and the pass buffers
-    CK(cudaMemsetAsync(c->sc, 0, sizeof(DevScalars), c->stream));
+    // the device scalars start at zero except the viscosities the RHS reads
+    // (a copy from this stack record, no allocation)
+    DevScalars sc0;
+    memset(&sc0, 0, sizeof(sc0));
+    sc0.nu = c->p.nu; sc0.nu_m = c->p.nu_m; sc0.nu_th = c->p.nu_th;
+    // (a pageable-memory copy: staged before the call returns)
+    CK(cudaMemcpyAsync(c->sc, &sc0, sizeof(DevScalars), cudaMemcpyHostToDevice, c->stream));
     if (bufbytes) CK(cudaMemsetAsync(base + o_bufA, 0, 2 * bufbytes, c->stream));
 
     rc = spk_compute_dfield(c, Uin, dUout);

@@ -95,30 +95,35 @@ __device__ __forceinline__ void clean3(double2* V, double kx, double ky, double 
 // ---------------------------------------------------------------------------
 __global__ void k_heat(const __grid_constant__ XfArgs a) {
     const size_t nc = a.g.nc;
-    const double dt = a.sc->dt;
     const bool sts = (a.sts_mask >> a.TH) & 1u;
-    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+    for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < nc * a.nb; gb += (size_t)gridDim.x * blockDim.x) {
+        const size_t box = gb / nc, gi = gb - box * nc;
+        const double dt = a.sc[box].dt, nu_th = a.sc[box].nu_th;
+        const size_t off = box * a.box_state + (size_t)a.TH * nc + gi;
         const int k = (int)(gi % a.g.nzh);
         const size_t r = gi / a.g.nzh;
         const int j = (int)(r % a.g.ny), i = (int)(r / a.g.ny);
         const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
-        const double2 X = a.U[(size_t)a.TH * nc + gi];
+        const double2 X = a.U[off];
         double2 R = d2(0.0, 0.0);
         if (!sts) {
-            const double f = -a.nu_th * (kx * kx + ky * ky + kz * kz);
+            const double f = -nu_th * (kx * kx + ky * ky + kz * kz);
             R = d2(f * X.x, f * X.y);
         }
-        const double2 Un = step_value(a, (size_t)a.TH * nc + gi, X, R, dt);
-        if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
+        const double2 Un = step_value(a, off, X, R, dt);
+        if (a.mode != XM_DFIELD) a.U[off] = Un;
     }
 }
 
 // ---------------------------------------------------------------------------
 // Fields::CleanFieldDivergence on the state (symmetries.cu:114-130).
 // ---------------------------------------------------------------------------
-__global__ void k_clean(DevGrid g, double2* V) {
+// V: the vector field of box 0; box b's copy starts box_stride elements later.
+__global__ void k_clean(DevGrid g, double2* V0, size_t box_stride, int nb) {
     const size_t nc = g.nc;
-    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+    for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < nc * nb; gb += (size_t)gridDim.x * blockDim.x) {
+        const size_t box = gb / nc, gi = gb - box * nc;
+        double2* V = V0 + box * box_stride;
         const int k = (int)(gi % g.nzh);
         const size_t r = gi / g.nzh;
         const int j = (int)(r % g.ny), i = (int)(r / g.ny);
@@ -137,15 +142,18 @@ __global__ void k_clean(DevGrid g, double2* V) {
 // compute_dt (compute_dt.cu:15-309) from the device maxima; RKL2 stage count
 // and stage coefficients (rkl.cu:467-494, 540-586).  One thread.
 // ---------------------------------------------------------------------------
-__global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* sc) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
+    // one block per box; the box's own viscosities come from its scalars
+    if (threadIdx.x != 0) return;
+    DevScalars* sc = scs + blockIdx.x;
+    const double nu = sc->nu, nu_m = sc->nu_m, nu_th = sc->nu_th;
     double gamma_v = 0.0, gamma_th = 0.0, gamma_par = 0.0, gamma_b = 0.0, gamma_tmp, gamma_sts = 0.0;
     const double kxmax = a.kxmax, kymax = a.kymax, kzmax = a.kzmax;
     double current_dt = sc->dt;
     double dt_hyp = 0.0, dt_par = 0.0, dt_sts = 0.0;
     auto in_sts = [&](int f) { return (a.sts_pos_mask >> f) & 1u; };
     if (a.heat) {
-        gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * a.nu_th;
+        gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * nu_th;
         if (!in_sts(a.TH)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         dt_par = a.cfl * a.cfl_par / gamma_par;
         dt_sts = a.cfl_par / gamma_sts;
@@ -156,11 +164,11 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* sc) {
         const double maxfy = __longlong_as_double((long long)sc->maxbits[1]);
         const double maxfz = __longlong_as_double((long long)sc->maxbits[2]);
         gamma_v = ((kxmax + 0.0 * kymax) * maxfx + kymax * maxfy + kzmax * maxfz);
-        gamma_tmp = (kxmax) * (kxmax) * a.nu;
+        gamma_tmp = (kxmax) * (kxmax) * nu;
         if (!in_sts(a.VX)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
-        gamma_tmp = kymax * kymax * a.nu;
+        gamma_tmp = kymax * kymax * nu;
         if (!in_sts(a.VY)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
-        gamma_tmp = kzmax * kzmax * a.nu;
+        gamma_tmp = kzmax * kzmax * nu;
         if (!in_sts(a.VZ)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         if (a.bous) {
             gamma_th += sqrt(fabs(a.N2)) / a.safety_source;
@@ -168,7 +176,7 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* sc) {
                 gamma_th += sqrt(fabs(a.OmegaT2)) / a.safety_source;
                 gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * (1. / a.reynolds_ani);
             } else {
-                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * a.nu_th;
+                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * nu_th;
             }
             if (!in_sts(a.TH)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         }
@@ -177,11 +185,11 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* sc) {
             const double maxby = __longlong_as_double((long long)sc->maxbits[4]);
             const double maxbz = __longlong_as_double((long long)sc->maxbits[5]);
             gamma_b = (kxmax) * maxbx + kymax * maxby + kzmax * maxbz;
-            gamma_tmp = (kxmax) * (kxmax) * a.nu_m;
+            gamma_tmp = (kxmax) * (kxmax) * nu_m;
             if (!in_sts(a.BX)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
-            gamma_tmp = kymax * kymax * a.nu_m;
+            gamma_tmp = kymax * kymax * nu_m;
             if (!in_sts(a.BY)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
-            gamma_tmp = kzmax * kzmax * a.nu_m;
+            gamma_tmp = kzmax * kzmax * nu_m;
             if (!in_sts(a.BZ)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         }
         dt_hyp = a.cfl / (gamma_v + gamma_th + gamma_b);
@@ -241,7 +249,7 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* sc) {
 
 // reset the dt maxima before the first stage of a step
 __global__ void k_reset_max(DevScalars* sc) {
-    if (threadIdx.x < 8) sc->maxbits[threadIdx.x] = 0ull;
+    if (threadIdx.x < 8) sc[blockIdx.x].maxbits[threadIdx.x] = 0ull;   // one block per box
 }
 
 // ---------------------------------------------------------------------------

@@ -62,6 +62,7 @@ struct DevScalars {
     unsigned long long maxbits[8];  // bit patterns of max |ux| |uy| |uz| |bx| |by| |bz|
     int step, s_rkl, err, nonfinite;
     double rkl[SPK_RKL_MAX][5];     // stage j: mu, nu, dt*mu~, dt*gamma, 1-mu-nu
+    double nu, nu_m, nu_th;         // this box's viscosity, resistivity, thermal diffusivity
 };
 
 #define SPK_MAXJOBS 16
@@ -85,6 +86,9 @@ struct AxisArgs {
     int kcols;      // process columns [0, kcols)
     int row_filter; // store only rows whose mask factor along the axis is 1
     int outer_filter; // skip tiles whose outer index has mask factor 0 (no load, no store)
+    int nb;           // boxes of the same geometry side by side (tile index includes the box)
+    int in_box_ch;    // channel offset between boxes in the input tensor map
+    int out_box_ch;   // channel offset between boxes in the output buffer
     int box_rows;   // rows per TMA box (<= 256); N / box_rows boxes per tile
     int nst;        // pipeline stages
     int convert;    // input type differs from the pass type (FP64 state in the FP32 form)
@@ -120,6 +124,9 @@ struct ZArgs {
     const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
     int gate_stage;
     FastDiv fd_nz;          // division by NZ
+    int nb;                 // boxes side by side: line index = box * nx*ny + line
+    size_t in_box, out_box; // element offsets between boxes in `in` and `out`
+    DevScalars* scs;        // per-box scalars (CFL maxima, non-finite flag)
 };
 
 enum XMode { XM_RK0 = 0, XM_RK1 = 1, XM_RK2 = 2, XM_EULER = 3, XM_DFIELD = 4 };
@@ -138,6 +145,10 @@ struct XfArgs {
     int mode, clean;
     const DevScalars* sc;
     int lny;                // log2 ny (elementwise RHS kernel)
+    int lnl;                // log2 (nx*ny): line index -> box
+    int nb;                 // boxes side by side; sc points at nb DevScalars
+    size_t box_state;       // F*nc: state elements per box (U, S, out)
+    size_t box_nl;          // pass-buffer elements per box (products)
 };
 
 struct RklArgs {

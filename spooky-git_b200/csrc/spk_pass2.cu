@@ -37,7 +37,9 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const int c = tid & (KT - 1), q = tid >> LKT;
     const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
     const int nkb = (a.kcols + KT - 1) / KT;
-    const int total = a.njobs * nouter * nkb;
+    const int per_box = nouter * nkb;
+    const int per_job = a.nb * per_box;
+    const int total = a.njobs * per_job;   // tile t = ((job * nb + box) * nouter + o) * nkb + kb
     constexpr size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
     constexpr size_t stage_bytes = ((size_t)N * KT * in_elem + 127) & ~(size_t)127;
     unsigned char* sbase = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -53,10 +55,13 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
     auto issue = [&](int t, int s) {
-        const int jb = t / (nouter * nkb);
-        const int rem = t - jb * nouter * nkb;
+        const int jb = t / per_job;
+        const int rb = t - jb * per_job;
+        const int box = rb / per_box;
+        const int rem = rb - box * per_box;
         const int o = rem / nkb, kb = rem - o * nkb;
         const AxisJob& jo = a.job[jb];
+        const int ch = jo.ch + box * a.in_box_ch;
         unsigned char* dst = stages + (size_t)s * stage_bytes;
         if (a.outer_filter && !okeep[o]) {   // skipped tile: complete the phase with no bytes
             mbar_expect_tx(&bar[s], 0);
@@ -64,8 +69,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         }
         mbar_expect_tx(&bar[s], tile_bytes);
         for (int b = 0; b < N / a.box_rows; b++) {
-            if (a.axis == 0) tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, o, b * a.box_rows, jo.ch);
-            else             tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, b * a.box_rows, o, jo.ch);
+            if (a.axis == 0) tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, o, b * a.box_rows, ch);
+            else             tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, b * a.box_rows, o, ch);
         }
     };
 
@@ -100,8 +105,10 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const uint32_t par = (uint32_t)((i / NST) & 1);
         const bool ok = mbar_wait(&bar[s], par, SPK_WAIT_ITERS);
         if (__syncthreads_or(!ok)) { aborted = true; break; }
-        const int jb = t / (nouter * nkb);
-        const int rem = t - jb * nouter * nkb;
+        const int jb = t / per_job;
+        const int rb = t - jb * per_job;
+        const int box = rb / per_box;
+        const int rem = rb - box * per_box;
         const int o = rem / nkb, kb = rem - o * nkb;
         const AxisJob& jo = a.job[jb];
         const int k0 = kb * KT;
@@ -135,7 +142,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             issue(tn, s);
         }
         const size_t base = a.axis == 0 ? (size_t)o * a.g.nzs : (size_t)o * a.g.ny * a.g.nzs;
-        C2<T>* out = (C2<T>*)jo.out + base + k0;
+        C2<T>* out = (C2<T>*)jo.out + (size_t)box * a.out_box_ch * a.g.ncs + base + k0;
         const bool col_ok = c < kt;
         const bool filt = a.row_filter != 0;
         if (skip) continue;
@@ -204,7 +211,10 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int L = a.lines, nzs = a.g.nzs;
     const int nlines = a.g.nx * a.g.ny;
-    const int line0 = blockIdx.x * L;
+    // CTAs of box b cover lines [b*nlines, (b+1)*nlines); L divides nlines when nb > 1
+    const int blocks_per_box = (nlines + L - 1) / L;
+    const int box = blockIdx.x / blocks_per_box;
+    const int line0 = (blockIdx.x - box * blocks_per_box) * L;
     const int nl = min(L, nlines - line0);
     const int nin = a.nin;
     const int nin_all = nin + (a.derive_gz == 1 ? 1 : 0);
@@ -221,7 +231,8 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     C2<T>* prod = raw;                    // the product pairs reuse the input area
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
-    const C2<T>* in = (const C2<T>*)a.in;
+    const C2<T>* in = (const C2<T>*)a.in + (size_t)box * a.in_box;
+    DevScalars* bsc = a.scs + box;
     const int LRS = L * RS;
 
     // 1. bulk copies of the input half spectra
@@ -241,7 +252,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     const bool ok = mbar_wait(bar, 0, SPK_WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
-            atomicExch(a.err, 2);
+            atomicExch(&bsc->err, 2);
             mbar_wait(bar, 0, SPK_WAIT_ITERS);   // bounded drain of the copies in flight
         }
         __syncthreads();
@@ -402,10 +413,10 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             if (tid < 6) {
                 const double m = (double)red[tid * 32];
                 const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
-                unsigned long long* dst = a.maxbits + tid;
+                unsigned long long* dst = bsc->maxbits + tid;
                 if (bits > *((volatile unsigned long long*)dst)) atomicMax(dst, bits);
             }
-            if (bad) atomicOr(a.nonfinite, 1);
+            if (bad) atomicOr(&bsc->nonfinite, 1);
         }
     }
     if (!want_prod) return;
@@ -413,7 +424,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
 
     // 4. forward transforms of the product pairs, unpacked half spectra
     const int kk = a.g.kz_keep;
-    C2<T>* out = (C2<T>*)a.out;
+    C2<T>* out = (C2<T>*)a.out + (size_t)box * a.out_box;
     const T half = (T)0.5;
     const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
     const int nfw = npout * L;
@@ -490,16 +501,22 @@ __device__ __forceinline__ double2 rk_value(const XfArgs& a, size_t gi, double2 
 template <typename T>
 __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
     const size_t nc = a.g.nc;
-    const int nzh = a.g.nzh, lny = a.lny, nzs = a.g.nzs;
-    const double dt = a.sc->dt;
-    const C2<T>* nl = (const C2<T>*)a.nl;
+    const int nzh = a.g.nzh, lny = a.lny, nzs = a.g.nzs, lnl = a.lnl;
     const bool needS = a.mode == XM_RK1 || a.mode == XM_RK2;
     const double2 z0 = d2(0.0, 0.0);
-    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
-        const unsigned line = fzh.div((unsigned)gi);
-        const int k = (int)(gi - (size_t)line * nzh);
+    const size_t total = nc * (size_t)a.nb;
+    for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
+        // global line over the boxes -> box, line, k (nx*ny is a power of two)
+        const unsigned gline = fzh.div((unsigned)gb);
+        const int k = (int)(gb - (size_t)gline * nzh);
+        const int box = (int)(gline >> lnl);
+        const unsigned line = gline & ((1u << lnl) - 1);
         const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
+        const size_t gi = (size_t)line * nzh + k;                // mode within the box
+        const size_t bo = (size_t)box * a.box_state;            // box offset in U, S, out
+        const double dt = a.sc[box].dt, nu = a.sc[box].nu, nu_m = a.sc[box].nu_m, nu_th = a.sc[box].nu_th;
         const bool m = a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0;
+        const C2<T>* nl = (const C2<T>*)a.nl + (size_t)box * a.box_nl;
         const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
         auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
 
@@ -512,20 +529,20 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
         if (a.incompressible) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                Xu[c] = a.U[(size_t)(a.VEL + c) * nc + gi];
-                if (needS) Su[c] = a.S[(size_t)(a.VEL + c) * nc + gi];
+                Xu[c] = a.U[bo + (size_t)(a.VEL + c) * nc + gi];
+                if (needS) Su[c] = a.S[bo + (size_t)(a.VEL + c) * nc + gi];
             }
         }
         if (a.mhd) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                Xb[c] = a.U[(size_t)(a.MAG + c) * nc + gi];
-                if (needS) Sb[c] = a.S[(size_t)(a.MAG + c) * nc + gi];
+                Xb[c] = a.U[bo + (size_t)(a.MAG + c) * nc + gi];
+                if (needS) Sb[c] = a.S[bo + (size_t)(a.MAG + c) * nc + gi];
             }
         }
         if (a.bous) {
-            Xt = a.U[(size_t)a.TH * nc + gi];
-            if (needS) St = a.S[(size_t)a.TH * nc + gi];
+            Xt = a.U[bo + (size_t)a.TH * nc + gi];
+            if (needS) St = a.S[bo + (size_t)a.TH * nc + gi];
         }
         if (m) {
             if (a.incompressible && a.nl_T >= 0) { t0 = P(a.nl_T); t1 = P(a.nl_T + 1); t2 = P(a.nl_T + 2); t3 = P(a.nl_T + 3); t4 = P(a.nl_T + 4); }
@@ -554,7 +571,7 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 if (!((a.sts_mask >> (a.VEL + c)) & 1u)) {
-                    const double f = -a.nu * k2;
+                    const double f = -nu * k2;
                     R[c] = d2(R[c].x + f * Xu[c].x, R[c].y + f * Xu[c].y);
                 }
             }
@@ -567,11 +584,11 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
             for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
             double2 Un[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) Un[c] = rk_value(a, (size_t)(a.VEL + c) * nc + gi, Xu[c], Su[c], R[c], dt);
+            for (int c = 0; c < 3; c++) Un[c] = rk_value(a, bo + (size_t)(a.VEL + c) * nc + gi, Xu[c], Su[c], R[c], dt);
             if (a.mode != XM_DFIELD) {
                 if (a.clean) clean3(Un, kx, ky, kz);
 #pragma unroll
-                for (int c = 0; c < 3; c++) a.U[(size_t)(a.VEL + c) * nc + gi] = Un[c];
+                for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.VEL + c) * nc + gi] = Un[c];
             }
         }
 
@@ -585,15 +602,15 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
             for (int c = 0; c < 3; c++) {
                 double2 R = d2(-S3[c].y, S3[c].x);
                 if (!((a.sts_mask >> (a.MAG + c)) & 1u)) {
-                    const double f = -a.nu_m * k2;
+                    const double f = -nu_m * k2;
                     R = d2(R.x + f * Xb[c].x, R.y + f * Xb[c].y);
                 }
-                Un[c] = rk_value(a, (size_t)(a.MAG + c) * nc + gi, Xb[c], Sb[c], R, dt);
+                Un[c] = rk_value(a, bo + (size_t)(a.MAG + c) * nc + gi, Xb[c], Sb[c], R, dt);
             }
             if (a.mode != XM_DFIELD) {
                 if (a.clean) clean3(Un, kx, ky, kz);
 #pragma unroll
-                for (int c = 0; c < 3; c++) a.U[(size_t)(a.MAG + c) * nc + gi] = Un[c];
+                for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.MAG + c) * nc + gi] = Un[c];
             }
         }
 
@@ -606,12 +623,12 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
                     const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
                     R = d2(R.x - sq.y, R.y + sq.x);   // += i * mask * k.q
                 } else {
-                    const double f = -a.nu_th * k2;
+                    const double f = -nu_th * k2;
                     R = d2(R.x + f * Xt.x, R.y + f * Xt.y);
                 }
             }
-            const double2 Un = rk_value(a, (size_t)a.TH * nc + gi, Xt, St, R, dt);
-            if (a.mode != XM_DFIELD) a.U[(size_t)a.TH * nc + gi] = Un;
+            const double2 Un = rk_value(a, bo + (size_t)a.TH * nc + gi, Xt, St, R, dt);
+            if (a.mode != XM_DFIELD) a.U[bo + (size_t)a.TH * nc + gi] = Un;
         }
     }
 }

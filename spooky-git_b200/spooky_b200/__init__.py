@@ -33,8 +33,9 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_compute_dfield", "spk_advance", "spk_rkl_cycle", "spk_to_real", "spk_synchronize",
             "spk_budgets", "spk_step_info", "spk_profile_passes", "spk_last_error",
             "spk_compute_dfield_noalloc", "spk_params_from_file", "spk_params_from_string",
-            "spk_ensemble_create", "spk_ensemble_destroy", "spk_ensemble_size", "spk_ensemble_box",
-            "spk_ensemble_advance", "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step"]
+            "spk_ensemble_create", "spk_ensemble_destroy", "spk_ensemble_size", "spk_ensemble_set_state",
+            "spk_ensemble_get_state", "spk_ensemble_get_time", "spk_ensemble_budgets", "spk_ensemble_advance",
+            "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step"]
 
 
 class Budgets(ctypes.Structure):
@@ -88,8 +89,11 @@ def lib():
         L.spk_params_from_string.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
         L.spk_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, vp, ctypes.POINTER(vp)]
         L.spk_ensemble_destroy.argtypes = [vp]
-        L.spk_ensemble_size.argtypes = [vp, ip]
-        L.spk_ensemble_box.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.spk_ensemble_size.argtypes = [vp, ip, ip]
+        L.spk_ensemble_set_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int]
+        L.spk_ensemble_get_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int]
+        L.spk_ensemble_get_time.argtypes = [vp, ctypes.c_int, dp, dp, ip]
+        L.spk_ensemble_budgets.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Budgets)]
         L.spk_ensemble_advance.argtypes = [vp, ctypes.c_int]
         L.spk_ensemble_synchronize.argtypes = [vp]
         L.spk_ensemble_kernels_per_step.argtypes = [vp, ip]
@@ -289,10 +293,50 @@ class Context:
 # ---------------------------------------------------------------------------
 # Reference-named objects (src/supervisor, src/fields, src/timestepping, src/rkl)
 # ---------------------------------------------------------------------------
+class EnsembleBox:
+    """Box i of an Ensemble: its state, time and budgets."""
+
+    def __init__(self, ens, i, params):
+        self._e, self.i, self.params = ens, i, params.copy()
+        F = num_fields(params)
+        self.shape_c = (F, params.nx, params.ny, params.nz // 2 + 1)
+
+    def set_state(self, U):
+        _torch_sync()
+        if hasattr(U, "data_ptr"):
+            ptr, where = _ptr(U)
+            keep = U
+        else:
+            keep = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
+            ptr, where = keep.ctypes.data, 1
+        self._e._check(lib().spk_ensemble_set_state(self._e._h, self.i, ptr, where))
+        if where == 1:
+            self._e.synchronize()   # the host array may go away after this call
+        del keep
+
+    def get_state(self):
+        out = np.empty(self.shape_c, np.complex128)
+        self._e._check(lib().spk_ensemble_get_state(self._e._h, self.i, out.ctypes.data, 1))
+        return out
+
+    def get_time(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._e._check(lib().spk_ensemble_get_time(self._e._h, self.i, ctypes.byref(t), ctypes.byref(dt),
+                                                   ctypes.byref(st)))
+        return t.value, dt.value, st.value
+
+    def budgets(self):
+        b = Budgets()
+        self._e._check(lib().spk_ensemble_budgets(self._e._h, self.i, ctypes.byref(b)))
+        F = self.shape_c[0]
+        return np.array(b.energy[:F]), np.array(b.dissipation[:F])
+
+
 class Ensemble:
-    """Independent boxes advanced together (spk_ensemble_*): one CUDA graph
-    launch per step for all boxes.  boxes[i] is a Context view of box i (state,
-    time, budgets); the ensemble owns the contexts."""
+    """Independent boxes advanced together (spk_ensemble_*): boxes that differ
+    only in nu, nu_m, nu_th share one set of pass launches; one CUDA graph
+    launch per step for the whole ensemble.  boxes[i] gives box i's state,
+    time and budgets."""
 
     def __init__(self, params_list, stream=None):
         arr = (Params * len(params_list))(*[p.copy() for p in params_list])
@@ -301,11 +345,10 @@ class Ensemble:
         if rc != SPK_OK:
             raise SpookyError(rc, lib().spk_last_error(None).decode())
         self._h = h
-        self.boxes = []
-        for i, p in enumerate(params_list):
-            bh = ctypes.c_void_p()
-            self._check(lib().spk_ensemble_box(self._h, i, ctypes.byref(bh)))
-            self.boxes.append(Context(p, _handle=bh))
+        nb, ng = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().spk_ensemble_size(self._h, ctypes.byref(nb), ctypes.byref(ng)))
+        self.ngroups = ng.value
+        self.boxes = [EnsembleBox(self, i, p) for i, p in enumerate(params_list)]
 
     def _check(self, rc):
         if rc != SPK_OK:
@@ -324,8 +367,6 @@ class Ensemble:
 
     def close(self):
         if getattr(self, "_h", None):
-            for b in self.boxes:
-                b._h = None
             lib().spk_ensemble_destroy(self._h)
             self._h = None
 

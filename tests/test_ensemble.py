@@ -13,10 +13,16 @@ L = 2 * np.pi
 
 def box_params():
     out = []
+    # three boxes of one group (same geometry, different viscosities) ...
+    for nu in (1e-2, 1e-3, 3e-4):
+        out.append(default_params(incompressible=1, gridsize=(16, 16, 16), boxsize=(L, L, L), reynolds=1.0 / nu,
+                                   form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
+    # ... two of another (different resistivities), and single-box groups
     out.append(default_params(incompressible=1, gridsize=(16, 16, 16), boxsize=(L, L, L), reynolds=100.0,
                                form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
-    out.append(default_params(incompressible=1, mhd=1, gridsize=(32, 32, 32), boxsize=(L, L, L), reynolds=1e3,
-                               reynolds_magnetic=500.0, form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
+    for eta in (2e-3, 2e-4):
+        out.append(default_params(incompressible=1, mhd=1, gridsize=(32, 32, 32), boxsize=(L, L, L), reynolds=1e3,
+                                   reynolds_magnetic=1.0 / eta, form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30))
     out.append(default_params(incompressible=1, gridsize=(32, 16, 64), boxsize=(1.0, 0.5, 2.0), reynolds=300.0,
                                form=SPK_FORM_PLAIN, t_final=1e30, toutput_flow=1e30))
     out.append(default_params(incompressible=1, mhd=1, boussinesq=1, stratification=1, anisotropic_diffusion=1,
@@ -52,7 +58,7 @@ def test_ensemble_boxes_follow_the_same_boxes_alone():
     ens.advance(4)
     ens.advance(3)
     ens.synchronize()
-    assert ens.kernels_per_step() > 0
+    assert ens.ngroups == 5 and ens.kernels_per_step() > 0
     for i, (p, U) in enumerate(zip(params, states)):
         ctx = Context(p)
         ctx.set_state(U)
@@ -61,6 +67,10 @@ def test_ensemble_boxes_follow_the_same_boxes_alone():
         got, want = ens.boxes[i].get_state(), ctx.get_state()
         assert np.array_equal(got, want), i
         assert ens.boxes[i].get_time() == ctx.get_time(), i
+        e_ens, _ = ens.boxes[i].budgets()
+        e_one, _ = ctx.budgets()
+        # the budget reductions sum with atomics: equal up to summation order
+        assert np.allclose(e_ens, e_one, rtol=1e-12, atol=0), i
     ens.close()
 
 
