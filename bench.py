@@ -159,7 +159,7 @@ def cpu_baseline_sample(n):
             "sample": f"{steps} RK3 step(s) of {n}^3 MHD from the same initial state (FP64 C oracle, OpenMP)"}
 
 
-ENSEMBLE_SIZES = (16, 32, 64)
+ENSEMBLE_SIZES = (16, 24, 32, 48, 64)
 
 
 def ensemble_boxes(nbox, seed=2024):

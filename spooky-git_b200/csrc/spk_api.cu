@@ -209,7 +209,7 @@ static void twiddles(int n, std::vector<double>& out) {
 
 struct AxisCfg { int kt; int nthr; size_t smem; };
 
-// Tile width of a strided-axis pass: the host mirror of axis_kt<T, LN, CONV>
+// Tile width of a strided-axis pass: the host mirror of axis_kt<T, N, CONV>
 // (KT columns x TPC threads = 256 threads, KT <= 64; an FP64 input tile in
 // the FP32 form is half as wide).
 static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
@@ -225,60 +225,60 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
 }
 
 
-template <typename T, int LN, int DIR, bool CONV>
+template <typename T, int N, int DIR, bool CONV>
 static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
-    constexpr int N = 1 << LN;
-    constexpr int KT = axis_kt<T, LN, CONV>();
-    const int nthr = KT * RegFft<T, LN>::TPC;
+    constexpr int KT = axis_kt<T, N, CONV>();
+    const int nthr = KT * RegFft<T, N>::TPC;
     if (a.kt != KT) { c->err = "internal: axis tile width mismatch"; c->sticky = SPK_ERR_ARG; return; }
     const size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
-    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, LN>::TWN * sizeof(C2<T>) +
+    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, N>::TWN * sizeof(C2<T>) +
                          (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
     const size_t smem = fixed + (size_t)a.nst * stage;
-    cudaFuncSetAttribute(k_axis2<T, LN, DIR, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, LN, DIR, CONV>, nthr, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV>, nthr, smem);
     const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
     c->launches++;
-    k_axis2<T, LN, DIR, CONV><<<grid, nthr, smem, c->stream>>>(a);
+    k_axis2<T, N, DIR, CONV><<<grid, nthr, smem, c->stream>>>(a);
 }
 
-template <typename T, int LN, int DIR>
+template <typename T, int N, int DIR>
 static void launch_axis_conv(spk_ctx* c, AxisArgs& a, long total) {
     if constexpr (sizeof(T) == 4 && DIR > 0) {
-        if (a.convert) { launch_axis_ln<T, LN, DIR, true>(c, a, total); return; }
+        if (a.convert) { launch_axis_ln<T, N, DIR, true>(c, a, total); return; }
     }
-    launch_axis_ln<T, LN, DIR, false>(c, a, total);
+    launch_axis_ln<T, N, DIR, false>(c, a, total);
 }
+
+// Every transform length the register FFT covers (2^k and 3*2^k).
+#define SPK_FOR_EACH_LENGTH(X) \
+    X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(6) X(12) X(24) X(48) X(96) X(192) X(384) X(768)
 
 template <typename T, int DIR>
 static void launch_axis_dir(spk_ctx* c, AxisArgs& a, long total) {
-    switch (ilog2(a.plan.n)) {
-        case 1: launch_axis_conv<T, 1, DIR>(c, a, total); break;
-        case 2: launch_axis_conv<T, 2, DIR>(c, a, total); break;
-        case 3: launch_axis_conv<T, 3, DIR>(c, a, total); break;
-        case 4: launch_axis_conv<T, 4, DIR>(c, a, total); break;
-        case 5: launch_axis_conv<T, 5, DIR>(c, a, total); break;
-        case 6: launch_axis_conv<T, 6, DIR>(c, a, total); break;
-        case 7: launch_axis_conv<T, 7, DIR>(c, a, total); break;
-        case 8: launch_axis_conv<T, 8, DIR>(c, a, total); break;
-        case 9: launch_axis_conv<T, 9, DIR>(c, a, total); break;
-        case 10: launch_axis_conv<T, 10, DIR>(c, a, total); break;
-        default: c->err = "internal: axis length outside 2..1024"; c->sticky = SPK_ERR_UNSUPPORTED; break;
+    switch (a.plan.n) {
+#define SPK_AXIS_CASE(n) case n: launch_axis_conv<T, n, DIR>(c, a, total); break;
+        SPK_FOR_EACH_LENGTH(SPK_AXIS_CASE)
+#undef SPK_AXIS_CASE
+        default: c->err = "internal: unsupported axis length"; c->sticky = SPK_ERR_UNSUPPORTED; break;
     }
 }
 
 template <typename T>
 static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
     const int nouter = a.axis == 0 ? c->ny : c->nx;
-    const long total = (long)a.njobs * nouter * ((a.kcols + a.kt - 1) / a.kt);
+    const int nkb = (a.kcols + a.kt - 1) / a.kt;
+    const long total = (long)a.njobs * a.nb * nouter * nkb;
     if (total <= 0) return;
     a.err = &c->sc->err;
+    a.fd_kb = FastDiv::make((unsigned)nkb);
+    a.fd_box = FastDiv::make((unsigned)(nouter * nkb));
+    a.fd_job = FastDiv::make((unsigned)(a.nb * nouter * nkb));
     if (dir > 0) launch_axis_dir<T, +1>(c, a, total);
     else launch_axis_dir<T, -1>(c, a, total);
 }
@@ -297,14 +297,14 @@ static void axis(spk_ctx* c, AxisArgs& a, int dir) {
     else launch_axis<double>(c, a, dir);
 }
 
-template <typename T, int LN>
+template <typename T, int N>
 static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int nthr = 128;
-    const int slots = std::max(1, nthr / RegFft<T, LN>::TPC);
+    const int slots = std::max(1, nthr / RegFft<T, N>::TPC);
     const long nlines = (long)c->nx * c->ny;
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
     auto need = [&](int lines) {
-        return zsmem_layout(1 << LN, RegFft<T, LN>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
+        return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
                             slots).total;
     };
     // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
@@ -312,6 +312,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     int L = 1;
     double best = -1.0;
     for (int cand = 1; cand <= 64 && cand <= nlines; cand *= 2) {
+        if (c->nb > 1 && nlines % cand != 0) break;   // a CTA's lines stay inside one box
         const size_t sm = need(cand);
         if (sm > (size_t)227 * 1024) break;
         const long work = (long)(npin + npout) * cand;
@@ -331,28 +332,21 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
     if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
-        cudaFuncSetAttribute(k_zpass2<T, LN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_zpass2<T, LN, true><<<nblk, nthr, smem, c->stream>>>(z);
+        cudaFuncSetAttribute(k_zpass2<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, N, true><<<nblk, nthr, smem, c->stream>>>(z);
     } else {
-        cudaFuncSetAttribute(k_zpass2<T, LN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_zpass2<T, LN, false><<<nblk, nthr, smem, c->stream>>>(z);
+        cudaFuncSetAttribute(k_zpass2<T, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, N, false><<<nblk, nthr, smem, c->stream>>>(z);
     }
 }
 
 template <typename T>
 static void launch_zpass(spk_ctx* c, ZArgs& z, int nin_all) {
-    switch (ilog2(c->nz)) {
-        case 1: launch_zpass_ln<T, 1>(c, z, nin_all); break;
-        case 2: launch_zpass_ln<T, 2>(c, z, nin_all); break;
-        case 3: launch_zpass_ln<T, 3>(c, z, nin_all); break;
-        case 4: launch_zpass_ln<T, 4>(c, z, nin_all); break;
-        case 5: launch_zpass_ln<T, 5>(c, z, nin_all); break;
-        case 6: launch_zpass_ln<T, 6>(c, z, nin_all); break;
-        case 7: launch_zpass_ln<T, 7>(c, z, nin_all); break;
-        case 8: launch_zpass_ln<T, 8>(c, z, nin_all); break;
-        case 9: launch_zpass_ln<T, 9>(c, z, nin_all); break;
-        case 10: launch_zpass_ln<T, 10>(c, z, nin_all); break;
-        default: c->err = "internal: z length outside 2..1024"; c->sticky = SPK_ERR_UNSUPPORTED; break;
+    switch (c->nz) {
+#define SPK_Z_CASE(n) case n: launch_zpass_ln<T, n>(c, z, nin_all); break;
+        SPK_FOR_EACH_LENGTH(SPK_Z_CASE)
+#undef SPK_Z_CASE
+        default: c->err = "internal: unsupported z length"; c->sticky = SPK_ERR_UNSUPPORTED; break;
     }
 }
 
@@ -532,8 +526,8 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     x.g = c->g;
     x.plan = c->plan_x;
     x.nl = c->bufA; x.cs_nl = c->g.ncs;   // products after the x-forward pass
-    x.lny = ilog2(c->ny);
-    x.lnl = ilog2(c->nx) + ilog2(c->ny);
+    x.fd_ny = FastDiv::make((unsigned)c->ny);
+    x.fd_nl = FastDiv::make((unsigned)(c->nx * c->ny));
     x.nb = c->nb;
     x.box_state = (size_t)c->F * c->nc;
     x.box_nl = (size_t)c->nbuf_ch * c->g.ncs;
@@ -633,8 +627,8 @@ static void record_rkl_cycle(spk_ctx* c) {
             for (int v = 0; v < c->nsts; v++) if (c->sts_kind[v] == 3) vslot = v;
             const FastDiv fz = FastDiv::make((unsigned)c->nzh);
             c->launches++;
-            if (c->fp32) k_rkl_flux<float><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, ilog2(c->ny));
-            else k_rkl_flux<double><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, ilog2(c->ny));
+            if (c->fp32) k_rkl_flux<float><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, FastDiv::make((unsigned)c->ny));
+            else k_rkl_flux<double><<<ew_blocks(c->nc), 256, 0, c->stream>>>(r, c->U, vslot, fz, FastDiv::make((unsigned)c->ny));
         }
     }
 }
@@ -951,8 +945,8 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     c->nbuf_ch = std::max(std::max(c->nin + 1, c->nout), 3);
 
     // transform lengths the register-resident FFT covers
-    if (!fft_supported(c->nx) || !fft_supported(c->ny) || !fft_supported(c->nz))
-        return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be powers of two between 2 and 1024");
+    if (!regfft_length_ok(c->nx) || !regfft_length_ok(c->ny) || !regfft_length_ok(c->nz))
+        return fail(nullptr, SPK_ERR_UNSUPPORTED, "axis lengths must be 2^k (2..1024) or 3*2^k (6..768)");
     c->plan_x.n = c->nx;
     c->plan_y.n = c->ny;
     c->plan_z.n = c->nz;

@@ -92,7 +92,5 @@ __host__ __device__ inline int padded_len(int n) { return n + (n >> 4); }
 
 __host__ __device__ inline int ilog2(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
 
-// Lengths the register-resident transforms cover: powers of two, 2..1024.
-inline bool fft_supported(int n) { return n >= 2 && n <= 1024 && (n & (n - 1)) == 0; }
 
 }  // namespace spk

@@ -87,6 +87,7 @@ struct AxisArgs {
     int row_filter; // store only rows whose mask factor along the axis is 1
     int outer_filter; // skip tiles whose outer index has mask factor 0 (no load, no store)
     int nb;           // boxes of the same geometry side by side (tile index includes the box)
+    FastDiv fd_job, fd_box, fd_kb;   // tile -> job, box, outer index, k block (set by the launcher)
     int in_box_ch;    // channel offset between boxes in the input tensor map
     int out_box_ch;   // channel offset between boxes in the output buffer
     int box_rows;   // rows per TMA box (<= 256); N / box_rows boxes per tile
@@ -144,8 +145,8 @@ struct XfArgs {
     double nu, nu_m, nu_th, N2;
     int mode, clean;
     const DevScalars* sc;
-    int lny;                // log2 ny (elementwise RHS kernel)
-    int lnl;                // log2 (nx*ny): line index -> box
+    FastDiv fd_ny;          // division by ny (elementwise RHS kernel)
+    FastDiv fd_nl;          // division by nx*ny: line index -> box
     int nb;                 // boxes side by side; sc points at nb DevScalars
     size_t box_state;       // F*nc: state elements per box (U, S, out)
     size_t box_nl;          // pass-buffer elements per box (products)

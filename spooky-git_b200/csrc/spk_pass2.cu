@@ -18,18 +18,17 @@ namespace spk {
 // Tile width of the strided-axis pass: KT columns x TPC threads = 256
 // threads (KT <= 64); an FP64 input tile in the FP32 form (CONV) is half as
 // wide so that one pipeline stage stays at 32 KB.
-template <typename T, int LN, bool CONV>
+template <typename T, int N, bool CONV>
 __host__ __device__ constexpr int axis_kt() {
-    constexpr int tpc = RegFft<T, LN>::TPC;
+    constexpr int tpc = RegFft<T, N>::TPC;
     constexpr int kt = (256 / tpc) > 64 ? 64 : (256 / tpc);
     return (CONV && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
 }
 
-template <typename T, int LN, int DIR, bool CONV>
+template <typename T, int N, int DIR, bool CONV>
 __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
-    using F = RegFft<T, LN>;
-    constexpr int N = F::N;
-    constexpr int KT = axis_kt<T, LN, CONV>(), LKT = ilog2c(KT);
+    using F = RegFft<T, N>;
+    constexpr int KT = axis_kt<T, N, CONV>(), LKT = ilog2c(KT);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
     const int NST = a.nst;
@@ -55,11 +54,11 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
     auto issue = [&](int t, int s) {
-        const int jb = t / per_job;
+        const int jb = (int)a.fd_job.div((unsigned)t);
         const int rb = t - jb * per_job;
-        const int box = rb / per_box;
+        const int box = (int)a.fd_box.div((unsigned)rb);
         const int rem = rb - box * per_box;
-        const int o = rem / nkb, kb = rem - o * nkb;
+        const int o = (int)a.fd_kb.div((unsigned)rem), kb = rem - o * nkb;
         const AxisJob& jo = a.job[jb];
         const int ch = jo.ch + box * a.in_box_ch;
         unsigned char* dst = stages + (size_t)s * stage_bytes;
@@ -82,7 +81,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const C2<T>* twg = (const C2<T>*)a.plan.tw;
         const double* kg = a.axis == 0 ? a.g.kx : a.g.ky;
         const double* mg = a.axis == 0 ? a.g.mx : a.g.my;
-        regfft_fill_twiddles<T, LN>(tw, twg, tid, blockDim.x);
+        regfft_fill_twiddles<T, N>(tw, twg, tid, blockDim.x);
         for (int i = tid; i < N; i += blockDim.x) {
             kax[i] = (T)kg[i];
             keep[i] = mg[i] != 0.0;
@@ -105,11 +104,11 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const uint32_t par = (uint32_t)((i / NST) & 1);
         const bool ok = mbar_wait(&bar[s], par, SPK_WAIT_ITERS);
         if (__syncthreads_or(!ok)) { aborted = true; break; }
-        const int jb = t / per_job;
+        const int jb = (int)a.fd_job.div((unsigned)t);
         const int rb = t - jb * per_job;
-        const int box = rb / per_box;
+        const int box = (int)a.fd_box.div((unsigned)rb);
         const int rem = rb - box * per_box;
-        const int o = rem / nkb, kb = rem - o * nkb;
+        const int o = (int)a.fd_kb.div((unsigned)rem), kb = rem - o * nkb;
         const AxisJob& jo = a.job[jb];
         const int k0 = kb * KT;
         const int kt = min(KT, a.kcols - k0);
@@ -121,7 +120,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         } else if constexpr (CONV) {
             const double2* src = reinterpret_cast<const double2*>(stg);
             const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
-            regfft_load<T, LN, DIR>(r, q, [&](int n) -> C2<T> {
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 double2 x = src[n * KT + c];
                 if (deriv) x = ik_mul(kd[n], x);
                 return mk<T>((T)(x.x * scale), (T)(x.y * scale));
@@ -129,7 +128,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         } else {
             const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
             const T sc = (T)scale;
-            regfft_load<T, LN, DIR>(r, q, [&](int n) -> C2<T> {
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 C2<T> v = src[n * KT + c];
                 if (deriv) { const T kk = kax[n]; v = mk<T>(-kk * v.y, kk * v.x); }
                 return mk<T>(v.x * sc, v.y * sc);
@@ -146,7 +145,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const bool col_ok = c < kt;
         const bool filt = a.row_filter != 0;
         if (skip) continue;
-        regfft_run<T, LN, DIR>(
+        regfft_run<T, N, DIR>(
             r, q, tw, [&](int L) { return xbuf + (size_t)L * KT + c; },
             [&](int k, C2<T> v) {
                 if (col_ok && (!filt || keep[k])) out[k * stride + c] = v;
@@ -201,10 +200,10 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
 
 // GEN: derived gradient channels or the to-real output (the general path);
 // otherwise every input channel is a plain half spectrum.
-template <typename T, int LN, bool GEN>
+template <typename T, int N, bool GEN>
 __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs a) {
-    using F = RegFft<T, LN>;
-    constexpr int N = F::N, LTPC = F::LTPC, TPC = F::TPC;
+    using F = RegFft<T, N>;
+    constexpr int LTPC = F::LTPC, TPC = F::TPC;
     constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
     constexpr int XS = N + (N >> 4);      // exchange slot (one pad element per 16)
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
@@ -247,7 +246,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         for (int ch = 0; ch < nin; ch++)
             bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
     }
-    regfft_fill_twiddles<T, LN>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
+    regfft_fill_twiddles<T, N>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
     for (int i = tid; i < nzs; i += nthr) zrow[i] = mk<T>((T)0, (T)0);
     const bool ok = mbar_wait(bar, 0, SPK_WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
@@ -286,7 +285,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             }
             return mk<T>((T)0, (T)0);
         };
-        regfft_load<T, LN, +1>(r, q, [&](int n) -> C2<T> {
+        regfft_load<T, N, +1>(r, q, [&](int n) -> C2<T> {
             constexpr int NH = N >> 1;
             const int k = n <= NH ? n : N - n;
             C2<T> A, B;
@@ -305,7 +304,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         T* pr0 = valid ? real + (size_t)(2 * p * L + l) * RS : junk;
         T* pr1 = (valid && 2 * p + 1 < nin_all) ? pr0 + LRS : junk;
         const bool to_real = GEN && a.mode == ZM_TO_REAL && valid && l < nl;
-        regfft_run<T, LN, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
+        regfft_run<T, N, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
             pr0[z] = v.x;
             pr1[z] = v.y;
             if (GEN && to_real) {
@@ -329,7 +328,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         const T third = (T)(1.0 / 3.0);
         const size_t pstride = (size_t)L * N * 2;   // scalars between product pairs
         for (int e = tid; e < L * N; e += nthr) {
-            const int l = e >> LN, z = e & (N - 1);
+            const int l = (int)((unsigned)e / (unsigned)N), z = e - l * N;
             const bool live = l < nl;
             const size_t line = (size_t)(line0 + l);
             const T* fr = real + (size_t)l * RS + z;
@@ -434,8 +433,8 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         const bool valid = tau < nfw;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
         const C2<T>* pp = prod + (size_t)(p * L + l) * N;
-        regfft_load<T, LN, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
-        regfft_run<T, LN, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; });
+        regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
+        regfft_run<T, N, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; });
         __syncthreads();
         for (int s2 = warp; s2 < slots; s2 += nwarp) {
             const int tau2 = base + s2;
@@ -501,7 +500,8 @@ __device__ __forceinline__ double2 rk_value(const XfArgs& a, size_t gi, double2 
 template <typename T>
 __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
     const size_t nc = a.g.nc;
-    const int nzh = a.g.nzh, lny = a.lny, nzs = a.g.nzs, lnl = a.lnl;
+    const int nzh = a.g.nzh, nzs = a.g.nzs;
+    const unsigned ny = (unsigned)a.g.ny, nlines = (unsigned)(a.g.nx * a.g.ny);
     const bool needS = a.mode == XM_RK1 || a.mode == XM_RK2;
     const double2 z0 = d2(0.0, 0.0);
     const size_t total = nc * (size_t)a.nb;
@@ -509,9 +509,11 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
         // global line over the boxes -> box, line, k (nx*ny is a power of two)
         const unsigned gline = fzh.div((unsigned)gb);
         const int k = (int)(gb - (size_t)gline * nzh);
-        const int box = (int)(gline >> lnl);
-        const unsigned line = gline & ((1u << lnl) - 1);
-        const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
+        const unsigned ubox = a.fd_nl.div(gline);
+        const int box = (int)ubox;
+        const unsigned line = gline - ubox * nlines;
+        const unsigned ui = a.fd_ny.div(line);
+        const int i = (int)ui, j = (int)(line - ui * ny);
         const size_t gi = (size_t)line * nzh + k;                // mode within the box
         const size_t bo = (size_t)box * a.box_state;            // box offset in U, S, out
         const double dt = a.sc[box].dt, nu = a.sc[box].nu, nu_m = a.sc[box].nu_m, nu_th = a.sc[box].nu_th;
@@ -643,7 +645,7 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArgs a, double2* U, int vslot, FastDiv fzh,
-                                                  int lny) {
+                                                  FastDiv fny) {
     if (a.stage > a.sc->s_rkl) return;
     const double* cf = a.sc->rkl[a.stage];
     const size_t nc = a.g.nc;
@@ -653,7 +655,8 @@ __global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArg
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const unsigned line = fzh.div((unsigned)gi);
         const int k = (int)(gi - (size_t)line * nzh);
-        const int i = (int)(line >> lny), j = (int)(line & ((1u << lny) - 1));
+        const unsigned ui = fny.div(line);
+        const int i = (int)ui, j = (int)(line - ui * (unsigned)a.g.ny);
         double2 dU = d2(0.0, 0.0);
         if (a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0) {
             const size_t li = (size_t)line * nzs + k;

@@ -31,6 +31,10 @@ def box_params():
                                t_final=1e30, toutput_flow=1e30))
     out.append(default_params(heat_equation=1, gridsize=(16, 8, 8), reynolds_thermic=10.0, form=SPK_FORM_PLAIN,
                                t_final=1e30, toutput_flow=1e30))
+    for nu in (5e-3, 5e-4):   # a 3*2^k group
+        out.append(default_params(incompressible=1, mhd=1, gridsize=(24, 24, 24), boxsize=(L, L, L),
+                                   reynolds=1.0 / nu, reynolds_magnetic=300.0, form=SPK_FORM_FP32, t_final=1e30,
+                                   toutput_flow=1e30))
     return out
 
 
@@ -58,7 +62,7 @@ def test_ensemble_boxes_follow_the_same_boxes_alone():
     ens.advance(4)
     ens.advance(3)
     ens.synchronize()
-    assert ens.ngroups == 5 and ens.kernels_per_step() > 0
+    assert ens.ngroups == 6 and ens.kernels_per_step() > 0
     for i, (p, U) in enumerate(zip(params, states)):
         ctx = Context(p)
         ctx.set_state(U)

@@ -77,10 +77,12 @@ def test_compute_dfield_matches_oracle(case, shape, form):
 
 
 # Long axes: every transform length from 2 to 1024 and every stage layout of
-# the register FFT (one stage, full stages, full stages + a radix-2/4/8 tail)
-# along x, y and z, in both precisions.
+# the register FFT (one stage, full stages, full stages + a radix-2/4/8 tail,
+# and the 3*2^k lengths) along x, y and z, in both precisions.
 LONG_SHAPES = [(256, 32, 16), (32, 256, 8), (1024, 8, 4), (8, 512, 16), (128, 64, 2), (16, 8, 512),
-               (64, 16, 1024), (4, 2, 256)]
+               (64, 16, 1024), (4, 2, 256),
+               # 3*2^k lengths: a radix-3 stage, radix-4 stages, a radix-2 tail
+               (24, 48, 12), (96, 6, 24), (12, 192, 48), (6, 12, 384), (768, 6, 6), (48, 384, 6)]
 
 
 @pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
