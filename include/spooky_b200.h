@@ -199,7 +199,8 @@ int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out
  * default stream); the work is queued on that stream.
  *
  * - The scratch needed is about 2 * C * nx * ny * nzs * (8 bytes in the FP32
- *   form, 16 in the plain form), nzs = nz/2+1 rounded up to even, C = 5 (HD),
+ *   form, 16 in the plain form), nzs = nz/2+1 rounded up to even (to a
+ *   multiple of 16 / 8 from 64 up), C = 5 (HD),
  *   8 (MHD or Boussinesq), 14 (MHD + Boussinesq + anisotropic conduction);
  *   the heat equation needs only tables.  So every configuration fits at
  *   32^3, and at 64^3 the FP32 form of HD, MHD and Boussinesq does.  Larger

@@ -94,6 +94,15 @@ static int fail(spk_ctx* c, int code, const std::string& msg) {
 // ---------------------------------------------------------------------------
 // buffer addressing
 // ---------------------------------------------------------------------------
+// Row length of the pass buffers (complex elements).  At least nzh, even
+// (16-byte TMA strides); from 64 up, a multiple of 128 bytes, so that a
+// 128-byte tile row never straddles DRAM bursts (rows of the x passes are far
+// apart and share no sectors in L2).  The tensor maps keep nzh as the logical
+// extent, so the padding is never read.
+static int pass_row(int nzh, bool fp32) {
+    if (nzh < 64) return nzh + (nzh & 1);
+    return fp32 ? (nzh + 15) & ~15 : (nzh + 7) & ~7;
+}
 static size_t csize(const spk_ctx* c) { return c->fp32 ? sizeof(float2) : sizeof(double2); }
 static size_t chan_bytes(const spk_ctx* c) { return c->g.ncs * csize(c); }
 static int buf_channels(const spk_ctx* c, const void* base) {
@@ -981,7 +990,7 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMemcpy(m + c->nx, c->my.data(), sizeof(double) * c->ny, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(m + c->nx + c->ny, c->mz.data(), sizeof(double) * c->nzh, cudaMemcpyHostToDevice));
     c->g.nx = c->nx; c->g.ny = c->ny; c->g.nz = c->nz; c->g.nzh = c->nzh;
-    c->g.nzs = c->nzh + (c->nzh & 1);            // even rows: 16-byte TMA strides in FP32
+    c->g.nzs = pass_row(c->nzh, c->fp32);
     c->g.ncs = (size_t)c->nx * c->ny * c->g.nzs;
     c->g.kz_keep = c->kz_keep; c->g.nc = nc;
     c->g.kx = t; c->g.ky = t + c->nx; c->g.kz = t + c->nx + c->ny;
@@ -1746,7 +1755,7 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
 
     const size_t cs = csize(c);
     c->g.nx = c->nx; c->g.ny = c->ny; c->g.nz = c->nz; c->g.nzh = c->nzh;
-    c->g.nzs = c->nzh + (c->nzh & 1);
+    c->g.nzs = pass_row(c->nzh, c->fp32);
     c->g.ncs = (size_t)c->nx * c->ny * c->g.nzs;
     c->g.kz_keep = c->kz_keep; c->g.nc = c->nc;
     const size_t ntab = 2 * ((size_t)c->nx + c->ny + c->nzh);

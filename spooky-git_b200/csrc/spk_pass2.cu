@@ -234,7 +234,8 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     DevScalars* bsc = a.scs + box;
     const int LRS = L * RS;
 
-    // 1. bulk copies of the input half spectra
+    // 1. one bulk copy per input channel: the CTA's lines are contiguous
+    //    (rows of nzs elements, padding included: fewer, larger copies)
     if (tid == 0) {
         mbar_init(bar, 1);
         fence_mbar_init();
