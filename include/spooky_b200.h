@@ -29,7 +29,8 @@
  *   spk_advance          Supervisor::executeMainLoop body: CleanFieldDivergence +
  *                        TimeStepping::HydroMHDAdvance (src/supervisor/supervisor.cu:179-192,
  *                        src/timestepping/hydro_mhd_advance.cu:18-189)
- *   spk_rkl_cycle        RKLegendre::compute_cycle (src/rkl/rkl.cu:187-204, 437-591)
+ *   spk_rkl_cycle        RKLegendre::compute_cycle (src/rkl/rkl.cu:185-199; STS :207-283,
+ *                        RKL1 :286-434, RKL2 :437-591)
  *   spk_to_real          Supervisor::Complex2RealFields (src/supervisor/supervisor.cu:261-272)
  *   spk_budgets          computeEnergy (src/io/spooky_output_functions.cu:23-55)
  */
@@ -56,9 +57,9 @@ extern "C" {
 #define SPK_FORM_FP32   1   /* FFT passes and products in FP32, FP64 state and RK/RKL  */
 
 /* ---- super-time-stepping algorithms (Parameters::sts_algorithm) ---------- */
-#define SPK_STS_STS     1   /* parsed but not implemented here (SPK_ERR_UNSUPPORTED) */
-#define SPK_STS_RKL1    2   /* parsed but not implemented here (SPK_ERR_UNSUPPORTED) */
-#define SPK_STS_RKL2    3
+#define SPK_STS_STS     1   /* "sts": damped Chebyshev sub-steps (Alexiades, Amiez & Gremaud 1996) */
+#define SPK_STS_RKL1    2   /* "rkl1": first-order Runge-Kutta-Legendre */
+#define SPK_STS_RKL2    3   /* "rkl2": second-order Runge-Kutta-Legendre (the default) */
 
 /* ---- integrators --------------------------------------------------------- */
 #define SPK_INT_RK3     0   /* TimeStepping::RungeKutta3 (default)                       */
@@ -144,8 +145,9 @@ int spk_compute_dfield(spk_ctx* ctx, const double* U, double* dU);
  * Asynchronous on the context stream; captured once into a CUDA graph. */
 int spk_advance(spk_ctx* ctx, int nsteps);
 
-/* One RKLegendre::compute_cycle on the context state with the last dt
- * (uses the real-space B of the last compute_dt / to_real). *s_out may be NULL. */
+/* One RKLegendre::compute_cycle of params.sts_algorithm on the context state
+ * with the last dt (uses the real-space B of the last compute_dt / to_real).
+ * *s_out (may be NULL) receives the stage or sub-step count. */
 int spk_rkl_cycle(spk_ctx* ctx, int* s_out);
 
 /* Supervisor::Complex2RealFields: real fields R[f][i][j][z] (unpadded, FP64)

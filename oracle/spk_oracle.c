@@ -727,6 +727,118 @@ static void parabolic_terms_sts(orc_ctx* c, const cpx* U, double* rb, cpx* dsts)
     }
 }
 
+/* ---- STS_FindRoot / STS_CorrectTimeStep / STS_ComputeSubSteps
+ * (src/rkl/rkl.cu:594-664): the sub-step sequence of Alexiades, Amiez &
+ * Gremaud (1996), damping STS_NU = 0.001 (src/rkl/rkl.hpp:32). */
+#define ORC_STS_NU 0.001
+#define ORC_STS_MAX_STEPS 1024   /* src/rkl/rkl.hpp:30 */
+static double sts_find_root(double dt_exp, double dT, double nu) {
+    const double sq = sqrt(nu), a = (1.0 - sq) / (1.0 + sq);
+    double N = 1.0;
+    for (int k = 0; k < 128; k++) {
+        const double b = pow(a, 2.0 * N);
+        const double cc = (1.0 - b) / (1.0 + b);
+        const double db_dN = 2.0 * log(a) * b;
+        const double scrh = cc - N * 2.0 / ((1.0 + b) * (1.0 + b)) * db_dN;
+        const double fN = dT - 0.5 * dt_exp / sq * N * cc;
+        const double dfN = -0.5 * dt_exp / sq * scrh;
+        const double dN = fN / dfN;
+        N -= dN;
+        if (fabs(dN) < 1.e-5) return N;
+    }
+    return -1.0;
+}
+static double sts_correct_dt(int n0, double dta, double nu) {
+    const double a = (1.0 - sqrt(nu)) / (1.0 + sqrt(nu));
+    const double b = pow(a, 2.0 * n0), cc = (1.0 - b) / (1.0 + b);
+    return dta * 2.0 * sqrt(nu) / (n0 * cc);
+}
+
+/* ---- RKLegendre::compute_cycle_STS (src/rkl/rkl.cu:207-283): n sub-steps
+ * U <- U + tau dU (addReset, src/cuda/cuda_kernels_generic.cu:174-181), taken
+ * in the reverse order of the sequence.  Returns n, or -1 when the root
+ * search fails or n exceeds STS_MAX_STEPS (the reference reads outside its
+ * sub-step array there). */
+static int sts_cycle(orc_ctx* c) {
+    const size_t nc = c->g.nc;
+    const int ns = c->nsts;
+    const double dt_current = c->dt, dt_sts = c->dt_sts;
+    const int n = (int)floor(sts_find_root(dt_sts, dt_current, ORC_STS_NU) + 1.0);
+    if (n < 1 || n > ORC_STS_MAX_STEPS) return -1;
+    double* ts = (double*)calloc((size_t)n, sizeof(double));
+    if (n > 1) {
+        const double dtc = sts_correct_dt(n, dt_current, ORC_STS_NU);
+        for (int i = 0; i < n; i++)
+            ts[i] = dtc / ((-1.0 + ORC_STS_NU) * cos(((2.0 * i + 1.0) * M_PI) / (2.0 * n)) + 1.0 + ORC_STS_NU);
+    } else {
+        ts[0] = dt_current;
+    }
+    for (int m = 0; m < n; m++) {
+        const double tau = ts[n - m - 1];
+        memset(c->rdU, 0, sizeof(cpx) * nc * ns);
+        parabolic_terms_sts(c, c->U, c->realbuf, c->rdU);
+        for (int nv = 0; nv < ns; nv++) {
+            cpx* Uc = c->U + (size_t)c->sts_index[nv] * nc;
+            cpx* dU = c->rdU + (size_t)nv * nc;
+            #pragma omp parallel for schedule(static)
+            for (long i = 0; i < (long)nc; i++) {
+                Uc[i] = c_add(c_scale(1.0, Uc[i]), c_scale(tau, dU[i]));
+                dU[i] = (cpx){0.0, 0.0};
+            }
+        }
+    }
+    free(ts);
+    return n;
+}
+
+/* ---- RKLegendre::compute_cycle_RKL1 (src/rkl/rkl.cu:286-434) ----------- */
+static int rkl1_cycle(orc_ctx* c) {
+    const size_t nc = c->g.nc;
+    const int ns = c->nsts;
+    const double dt_current = c->dt, dt_sts = c->dt_sts;
+    const double scrh = dt_current / dt_sts;
+    const double s_str = 4.0 * scrh / (1.0 + sqrt(1.0 + 8.0 * scrh));
+    const int s_RKL = 1 + (int)(s_str);
+    const double w1 = 2.0 / (s_RKL * s_RKL + s_RKL);
+    double mu_tilde_j = w1;
+    memset(c->rdU0, 0, sizeof(cpx) * nc * ns);
+    memset(c->rdU, 0, sizeof(cpx) * nc * ns);
+    parabolic_terms_sts(c, c->U, c->realbuf, c->rdU);
+    for (int nv = 0; nv < ns; nv++) {
+        cpx* Uc = c->U + (size_t)c->sts_index[nv] * nc;
+        cpx *Uc0 = c->rUc0 + (size_t)nv * nc, *Uc1 = c->rUc1 + (size_t)nv * nc;
+        cpx *dU = c->rdU + (size_t)nv * nc, *dU0 = c->rdU0 + (size_t)nv * nc;
+        #pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)nc; i++) {
+            Uc0[i] = Uc[i];
+            dU0[i] = dU[i];
+            Uc1[i] = Uc[i];
+            Uc[i] = c_add(c_scale(1.0, Uc1[i]), c_scale(mu_tilde_j * dt_current, dU0[i]));
+        }
+    }
+    for (int stage = 2; stage <= s_RKL; stage++) {
+        const double mu_j = (2. * stage - 1.) / stage;
+        mu_tilde_j = w1 * mu_j;
+        const double nu_j = -(stage - 1.) / stage;
+        memset(c->rdU, 0, sizeof(cpx) * nc * ns);
+        parabolic_terms_sts(c, c->U, c->realbuf, c->rdU);
+        for (int nv = 0; nv < ns; nv++) {
+            cpx* Uc = c->U + (size_t)c->sts_index[nv] * nc;
+            cpx* Uc1 = c->rUc1 + (size_t)nv * nc;
+            cpx* dU = c->rdU + (size_t)nv * nc;
+            const double a = dt_current * mu_tilde_j;
+            /* rkl1_stage (src/cuda/cuda_kernels_generic.cu:146-158) */
+            #pragma omp parallel for schedule(static)
+            for (long i = 0; i < (long)nc; i++) {
+                cpx Y = c_add(c_scale(mu_j, Uc[i]), c_scale(nu_j, Uc1[i]));
+                Uc1[i] = Uc[i];
+                Uc[i] = c_add(Y, c_scale(a, dU[i]));
+            }
+        }
+    }
+    return s_RKL;
+}
+
 /* ---- RKLegendre::compute_cycle_RKL2 (src/rkl/rkl.cu:437-591) ----------- */
 static int rkl2_cycle(orc_ctx* c) {
     const size_t nc = c->g.nc;
@@ -783,9 +895,16 @@ static int rkl2_cycle(orc_ctx* c) {
     return s_RKL;
 }
 
+/* RKLegendre::compute_cycle (src/rkl/rkl.cu:185-199) */
+static int sts_dispatch(orc_ctx* c) {
+    if (c->p.sts_algorithm == SPK_STS_STS) return sts_cycle(c);
+    if (c->p.sts_algorithm == SPK_STS_RKL1) return rkl1_cycle(c);
+    return rkl2_cycle(c);
+}
+
 int orc_rkl_cycle(orc_ctx* c) {
     if (c->nsts == 0) return 0;
-    return rkl2_cycle(c);
+    return sts_dispatch(c);
 }
 
 /* axpyComplex (src/cuda/cuda_kernels_generic.cu:137-144): Z = a X + b Y */
@@ -835,14 +954,14 @@ void orc_step(orc_ctx* c, int nsteps) {
             if (p->integrator == SPK_INT_EULER) forward_euler(c); else runge_kutta3(c);
             if (p->supertimestepping) {
                 if (p->incompressible) complex2real(c, c->U, c->realbuf, c->F);
-                rkl2_cycle(c);
+                sts_dispatch(c);
             }
         } else {
-            if (p->supertimestepping && (c->step % 2) == 1) rkl2_cycle(c);
+            if (p->supertimestepping && (c->step % 2) == 1) sts_dispatch(c);
             if (p->integrator == SPK_INT_EULER) forward_euler(c); else runge_kutta3(c);
             if (p->supertimestepping && (c->step % 2) == 0) {
                 if (p->incompressible) complex2real(c, c->U, c->realbuf, c->F);
-                rkl2_cycle(c);
+                sts_dispatch(c);
             }
         }
         c->step += 1;

@@ -567,12 +567,14 @@ static DtArgs dt_args(spk_ctx* c, bool advance) {
     d.VX = c->VX; d.VY = c->VY; d.VZ = c->VZ; d.BX = c->BX; d.BY = c->BY; d.BZ = c->BZ; d.TH = c->TH;
     d.advance = advance ? 1 : 0;
     d.rkl_smax = c->rkl_smax;
+    d.sts_alg = p.sts_algorithm;
     return d;
 }
 
 // ---------------------------------------------------------------------------
-// RKL2 cycle (RKLegendre::compute_cycle_RKL2, rkl.cu:437-591); stages beyond
-// the device-computed count exit immediately.
+// Super-time-stepping cycle (RKLegendre::compute_cycle, rkl.cu:185-199:
+// STS, RKL1 or RKL2); stages beyond the device-computed count exit
+// immediately.
 // ---------------------------------------------------------------------------
 static RklArgs rkl_args(spk_ctx* c, int stage) {
     RklArgs r;
@@ -582,6 +584,7 @@ static RklArgs rkl_args(spk_ctx* c, int stage) {
     r.nl = c->rB; r.cs_nl = c->g.ncs;
     r.Uc0 = c->Uc0; r.Uc1 = c->Uc1; r.dU0 = c->dU0;
     r.stage = stage;
+    r.sts_alg = c->p.sts_algorithm;
     r.nsts = c->nsts;
     for (int v = 0; v < c->nsts; v++) { r.fields[v] = c->sts_fields[v]; r.kind[v] = c->sts_kind[v]; }
     r.nu = c->p.nu; r.nu_m = c->p.nu_m; r.nu_th = c->p.nu_th;
@@ -746,7 +749,9 @@ static int check_params(const spk_params_t* p, std::string& why) {
     if (p->nx < 2 || p->ny < 2 || p->nz < 2) { why = "grid sizes must be >= 2"; return SPK_ERR_ARG; }
     if (p->nz % 2) { why = "NZ must be even"; return SPK_ERR_UNSUPPORTED; }
     if (p->nx > 1024 || p->ny > 1024 || p->nz > 1024) { why = "axis lengths above 1024 are not supported"; return SPK_ERR_UNSUPPORTED; }
-    if (p->supertimestepping && p->sts_algorithm != SPK_STS_RKL2) { why = "only the rkl2 super-time-stepping algorithm is implemented"; return SPK_ERR_UNSUPPORTED; }
+    if (p->supertimestepping && p->sts_algorithm != SPK_STS_STS && p->sts_algorithm != SPK_STS_RKL1 && p->sts_algorithm != SPK_STS_RKL2) {
+        why = "sts_algorithm must be sts, rkl1 or rkl2"; return SPK_ERR_CONFIG;
+    }
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
     return SPK_OK;
@@ -920,7 +925,8 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
             return fail(nullptr, SPK_ERR_UNSUPPORTED, "super-time-stepping of B together with anisotropic conduction is not supported");
     }
     c->aniso_rhs = p.anisotropic_diffusion && p.boussinesq && !((c->sts_mask >> c->TH) & 1u);
-    // RKL2 stage bound
+    // bound on the stage count of one super-time-stepping cycle (the graph
+    // records this many stages; k_dt flags a cycle that needs more)
     c->rkl_smax = 0;
     if (c->nsts > 0) {
         double r;
@@ -932,8 +938,9 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
         } else {
             r = std::max(1.0, (double)p.safety_sts);
         }
-        const double s_str = 4.0 * (1.0 + 2.0 * r) / (1.0 + sqrt(9.0 + 16.0 * r));
-        c->rkl_smax = std::min(SPK_RKL_MAX - 1, 2 + (int)s_str);
+        int s = sts_stage_count(p.sts_algorithm, r);
+        if (s < 1) s = SPK_RKL_MAX;   // no STS root: take the cap
+        c->rkl_smax = std::min(SPK_RKL_MAX - 1, 1 + s);
     }
 
     // channel layout of the main pipeline
@@ -1026,12 +1033,15 @@ static int ctx_alloc(spk_ctx* c) {
         CK(cudaMemset(c->bufA, 0, cs * c->g.ncs * c->nbuf_ch * nb));
         CK(cudaMemset(c->bufB, 0, cs * c->g.ncs * c->nbuf_ch * nb));
     }
-    if (c->nsts > 0) {
-        CK(cudaMalloc(&c->Uc0, sizeof(double2) * nc * c->nsts));
+    // stage scratch: RKL2 keeps Uc0, Uc1 and dU0, RKL1 only Uc1, STS none
+    if (c->nsts > 0 && c->p.sts_algorithm != SPK_STS_STS) {
         CK(cudaMalloc(&c->Uc1, sizeof(double2) * nc * c->nsts));
+        CK(cudaMemset(c->Uc1, 0, sizeof(double2) * nc * c->nsts));
+    }
+    if (c->nsts > 0 && c->p.sts_algorithm == SPK_STS_RKL2) {
+        CK(cudaMalloc(&c->Uc0, sizeof(double2) * nc * c->nsts));
         CK(cudaMalloc(&c->dU0, sizeof(double2) * nc * c->nsts));
         CK(cudaMemset(c->Uc0, 0, sizeof(double2) * nc * c->nsts));
-        CK(cudaMemset(c->Uc1, 0, sizeof(double2) * nc * c->nsts));
         CK(cudaMemset(c->dU0, 0, sizeof(double2) * nc * c->nsts));
     }
     if (c->sts_aniso) {
@@ -1285,7 +1295,7 @@ extern "C" int spk_synchronize(spk_ctx* c) {
     if (rc) return rc;
     for (int b = 0; b < c->nb; b++) {
         const std::string box = c->nb > 1 ? " (box " + std::to_string(b) + " of the group)" : "";
-        if (c->h_sc[b].err == 1) return fail(c, SPK_ERR_ARG, "RKL2 stage count exceeded the recorded bound" + box);
+        if (c->h_sc[b].err == 1) return fail(c, SPK_ERR_ARG, "super-time-stepping stage count exceeded the recorded bound" + box);
         if (c->h_sc[b].err == 2) return fail(c, SPK_ERR_CUDA, "a bulk/TMA copy wait ran out in a pass kernel" + box);
         if (c->h_sc[b].nonfinite) return fail(c, SPK_ERR_NONFINITE, "non-finite value in the real-space fields" + box);
     }

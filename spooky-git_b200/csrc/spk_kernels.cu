@@ -139,8 +139,9 @@ __global__ void k_clean(DevGrid g, double2* V0, size_t box_stride, int nb) {
 }
 
 // ---------------------------------------------------------------------------
-// compute_dt (compute_dt.cu:15-309) from the device maxima; RKL2 stage count
-// and stage coefficients (rkl.cu:467-494, 540-586).  One thread.
+// compute_dt (compute_dt.cu:15-309) from the device maxima; the stage count
+// and stage coefficients of the super-time-stepping cycle (rkl.cu:207-591).
+// One thread per box.
 // ---------------------------------------------------------------------------
 __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
     // one block per box; the box's own viscosities come from its scalars
@@ -212,32 +213,62 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
     sc->dt_par = dt_par;
     sc->dt_sts = dt_sts;
     if (a.sts) {
-        // RKLegendre::compute_cycle_RKL2 recurrences, FP64 (rkl.cu:467-494, 540-586)
+        const int smax = min(a.rkl_smax, SPK_RKL_MAX - 1);
         const double scrh = current_dt / dt_sts;
-        const double s_str = 4.0 * (1.0 + 2.0 * scrh) / (1.0 + sqrt(9.0 + 16.0 * scrh));
-        int s = 1 + (int)(s_str);
-        if (s > a.rkl_smax || s > SPK_RKL_MAX - 1 || s < 1) { sc->err = 1; s = min(max(s, 1), min(a.rkl_smax, SPK_RKL_MAX - 1)); }
-        const double w1 = 4.0 / (s * s + s - 2.0);
-        double b_j, b_jm1, b_jm2, a_jm1;
-        b_j = b_jm1 = b_jm2 = 1.0 / 3.0;
-        a_jm1 = 1.0 - b_jm1;
-        sc->rkl[1][0] = 0.0; sc->rkl[1][1] = 0.0;
-        sc->rkl[1][2] = current_dt * (w1 / 3.0);
-        sc->rkl[1][3] = 0.0; sc->rkl[1][4] = 0.0;
-        for (int st = 2; st <= s; st++) {
-            const double mu_j = (2. * st - 1.) / st * b_j / b_jm1;
-            const double mu_tilde_j = w1 * mu_j;
-            const double gamma_j = -a_jm1 * mu_tilde_j;
-            const double nu_j = -(st - 1.) * b_j / (st * b_jm2);
-            sc->rkl[st][0] = mu_j;
-            sc->rkl[st][1] = nu_j;
-            sc->rkl[st][2] = current_dt * mu_tilde_j;
-            sc->rkl[st][3] = gamma_j * current_dt;
-            sc->rkl[st][4] = (1.0 - mu_j - nu_j);
-            b_jm2 = b_jm1;
-            b_jm1 = b_j;
+        int s;
+        if (a.sts_alg == STS_ALG_STS) {
+            // RKLegendre::compute_cycle_STS (rkl.cu:207-283): n sub-steps
+            // applied in the reverse order of the sequence, tau = ts[n - m - 1]
+            s = (int)floor(sts_sub_steps(dt_sts, current_dt, SPK_STS_DAMPING) + 1.0);
+            if (s > smax || s < 1) { sc->err = 1; s = min(max(s, 1), smax); }
+            const double dtc = s > 1 ? sts_corrected_dt(s, current_dt, SPK_STS_DAMPING) : 0.0;
+            for (int st = 1; st <= s; st++) {
+                sc->rkl[st][0] = 1.0; sc->rkl[st][1] = 0.0;
+                sc->rkl[st][2] = s > 1 ? sts_tau(dtc, s - st, s, SPK_STS_DAMPING) : current_dt;
+                sc->rkl[st][3] = 0.0; sc->rkl[st][4] = 0.0;
+            }
+        } else if (a.sts_alg == STS_ALG_RKL1) {
+            // RKLegendre::compute_cycle_RKL1 (rkl.cu:286-434)
+            s = 1 + (int)(4.0 * scrh / (1.0 + sqrt(1.0 + 8.0 * scrh)));
+            if (s > smax || s < 1) { sc->err = 1; s = min(max(s, 1), smax); }
+            const double w1 = 2.0 / (s * s + s);
+            sc->rkl[1][0] = 0.0; sc->rkl[1][1] = 0.0;
+            sc->rkl[1][2] = w1 * current_dt;
+            sc->rkl[1][3] = 0.0; sc->rkl[1][4] = 0.0;
+            for (int st = 2; st <= s; st++) {
+                const double mu_j = (2. * st - 1.) / st;
+                sc->rkl[st][0] = mu_j;
+                sc->rkl[st][1] = -(st - 1.) / st;
+                sc->rkl[st][2] = current_dt * (w1 * mu_j);
+                sc->rkl[st][3] = 0.0; sc->rkl[st][4] = 0.0;
+            }
+        } else {
+            // RKLegendre::compute_cycle_RKL2 recurrences, FP64 (rkl.cu:467-494, 540-586)
+            const double s_str = 4.0 * (1.0 + 2.0 * scrh) / (1.0 + sqrt(9.0 + 16.0 * scrh));
+            s = 1 + (int)(s_str);
+            if (s > smax || s < 1) { sc->err = 1; s = min(max(s, 1), smax); }
+            const double w1 = 4.0 / (s * s + s - 2.0);
+            double b_j, b_jm1, b_jm2, a_jm1;
+            b_j = b_jm1 = b_jm2 = 1.0 / 3.0;
             a_jm1 = 1.0 - b_jm1;
-            b_j = 0.5 * (st * st + 3.0 * st) / (st * st + 3.0 * st + 2);
+            sc->rkl[1][0] = 0.0; sc->rkl[1][1] = 0.0;
+            sc->rkl[1][2] = current_dt * (w1 / 3.0);
+            sc->rkl[1][3] = 0.0; sc->rkl[1][4] = 0.0;
+            for (int st = 2; st <= s; st++) {
+                const double mu_j = (2. * st - 1.) / st * b_j / b_jm1;
+                const double mu_tilde_j = w1 * mu_j;
+                const double gamma_j = -a_jm1 * mu_tilde_j;
+                const double nu_j = -(st - 1.) * b_j / (st * b_jm2);
+                sc->rkl[st][0] = mu_j;
+                sc->rkl[st][1] = nu_j;
+                sc->rkl[st][2] = current_dt * mu_tilde_j;
+                sc->rkl[st][3] = gamma_j * current_dt;
+                sc->rkl[st][4] = (1.0 - mu_j - nu_j);
+                b_jm2 = b_jm1;
+                b_jm1 = b_j;
+                a_jm1 = 1.0 - b_jm1;
+                b_j = 0.5 * (st * st + 3.0 * st) / (st * st + 3.0 * st + 2);
+            }
         }
         sc->s_rkl = s;
     }
@@ -253,21 +284,32 @@ __global__ void k_reset_max(DevScalars* sc) {
 }
 
 // ---------------------------------------------------------------------------
-// RKL2 stage update shared by the spectral and the anisotropic variants
-// (rkl.cu:515-532 for stage 1, rkl2_stage generic.cu:160-172 for j >= 2).
+// Super-time-stepping stage update shared by the spectral and the
+// anisotropic variants:
+//   STS  addReset, U <- U + tau dU (cuda_kernels_generic.cu:174-181);
+//   RKL1 stage 1 (rkl.cu:360-377), then rkl1_stage (generic.cu:146-158);
+//   RKL2 stage 1 (rkl.cu:515-532), then rkl2_stage (generic.cu:160-172).
+// Stage 1 of RKL1 keeps U in Uc1 only: the reference's copies to Uc0 and
+// dU0 are never read by that scheme.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void rkl_update(const RklArgs& a, const double* c, size_t off, size_t gi, double2* Uc, double2 dU) {
     double2* Uc0 = a.Uc0 + off;
     double2* Uc1 = a.Uc1 + off;
     double2* dU0 = a.dU0 + off;
-    if (a.stage == 1) {
-        const double2 U = Uc[gi];
-        Uc0[gi] = U;
-        dU0[gi] = dU;
+    const double2 U = Uc[gi];
+    if (a.sts_alg == STS_ALG_STS) {
+        Uc[gi] = d2(1.0 * U.x + c[2] * dU.x, 1.0 * U.y + c[2] * dU.y);
+    } else if (a.stage == 1) {
+        if (a.sts_alg == STS_ALG_RKL2) { Uc0[gi] = U; dU0[gi] = dU; }
         Uc1[gi] = U;
         Uc[gi] = d2(1.0 * U.x + c[2] * dU.x, 1.0 * U.y + c[2] * dU.y);
+    } else if (a.sts_alg == STS_ALG_RKL1) {
+        const double2 U1 = Uc1[gi];
+        const double2 Y = d2(c[0] * U.x + c[1] * U1.x, c[0] * U.y + c[1] * U1.y);
+        Uc1[gi] = U;
+        Uc[gi] = d2(Y.x + c[2] * dU.x, Y.y + c[2] * dU.y);
     } else {
-        const double2 U = Uc[gi], U1 = Uc1[gi], U0 = Uc0[gi], D0 = dU0[gi];
+        const double2 U1 = Uc1[gi], U0 = Uc0[gi], D0 = dU0[gi];
         const double2 Y = d2(c[0] * U.x + c[1] * U1.x, c[0] * U.y + c[1] * U1.y);
         Uc1[gi] = U;
         Uc[gi] = d2(Y.x + c[4] * U0.x + c[2] * dU.x + c[3] * D0.x, Y.y + c[4] * U0.y + c[2] * dU.y + c[3] * D0.y);

@@ -17,6 +17,8 @@
 
 #include <cuda.h>
 
+#include <math.h>
+
 #include "spk_fft.cuh"
 #include "spk_tma.cuh"
 
@@ -56,14 +58,65 @@ struct DevGrid {
 
 #define SPK_RKL_MAX 128
 
+// Super-time-stepping algorithms (values of spk_params_t::sts_algorithm).
+enum { STS_ALG_STS = 1, STS_ALG_RKL1 = 2, STS_ALG_RKL2 = 3 };
+// STS_NU, the damping of the classic STS sub-step sequence (rkl.hpp:32)
+#define SPK_STS_DAMPING 0.001
+
 // Device-resident step scalars (written by k_dt, read by every update pass).
 struct DevScalars {
     double t, dt, dt_hyp, dt_par, dt_sts, t_lastsnap;
     unsigned long long maxbits[8];  // bit patterns of max |ux| |uy| |uz| |bx| |by| |bz|
     int step, s_rkl, err, nonfinite;
-    double rkl[SPK_RKL_MAX][5];     // stage j: mu, nu, dt*mu~, dt*gamma, 1-mu-nu
+    // stage j of the super-time-stepping cycle: U <- c0 U + c1 U1 + c2 dU + c3 dU0 + c4 U0
+    // (RKL2: mu, nu, dt*mu~, dt*gamma, 1-mu-nu; RKL1: mu, nu, dt*mu~;
+    // STS: the sub-step tau in c2)
+    double rkl[SPK_RKL_MAX][5];
     double nu, nu_m, nu_th;         // this box's viscosity, resistivity, thermal diffusivity
 };
+
+// Classic super-time-stepping of Alexiades, Amiez & Gremaud (Commun. Numer.
+// Meth. Eng. 12, 31, 1996) as the reference states it (rkl.cu:594-664).
+// With a = (1 - sqrt(nu)) / (1 + sqrt(nu)) and c(N) = (1 - a^2N) / (1 + a^2N),
+// N sub-steps of the damped Chebyshev sequence advance by
+// dt_exp N c(N) / (2 sqrt(nu)) (their Eq. 2.10): sts_sub_steps solves that
+// for N = dT by Newton's method from N = 1 (128 iterations, |dN| < 1e-5;
+// -1 when it does not converge).
+__host__ __device__ inline double sts_sub_steps(double dt_exp, double dT, double damping) {
+    const double sq = sqrt(damping);
+    const double a = (1.0 - sq) / (1.0 + sq);
+    double N = 1.0;
+    for (int it = 0; it < 128; it++) {
+        const double b = pow(a, 2.0 * N);
+        const double c = (1.0 - b) / (1.0 + b);
+        const double db = 2.0 * log(a) * b;                       // d(a^2N)/dN
+        const double dc = c - N * 2.0 / ((1.0 + b) * (1.0 + b)) * db;   // d(N c)/dN
+        const double f = dT - 0.5 * dt_exp / sq * N * c;
+        const double df = -0.5 * dt_exp / sq * dc;
+        const double dN = f / df;
+        N -= dN;
+        if (fabs(dN) < 1.e-5) return N;
+    }
+    return -1.0;
+}
+// The explicit step that makes n sub-steps span dT exactly (STS_CorrectTimeStep).
+__host__ __device__ inline double sts_corrected_dt(int n, double dT, double damping) {
+    const double sq = sqrt(damping);
+    const double a = (1.0 - sq) / (1.0 + sq);
+    const double b = pow(a, 2.0 * n);
+    const double c = (1.0 - b) / (1.0 + b);
+    return dT * 2.0 * sq / (n * c);
+}
+// Sub-step i of n (STS_ComputeSubSteps, Eq. 2.9 of AAG).
+__host__ __device__ inline double sts_tau(double dt_exp, int i, int n, double damping) {
+    return dt_exp / ((-1.0 + damping) * cos(((2.0 * i + 1.0) * M_PI) / (2.0 * n)) + 1.0 + damping);
+}
+// Stage counts of one cycle for r = dt / dt_sts (rkl.cu:233-235, 324-327, 473-477).
+__host__ __device__ inline int sts_stage_count(int alg, double r) {
+    if (alg == STS_ALG_STS) return (int)floor(sts_sub_steps(1.0, r, SPK_STS_DAMPING) + 1.0);
+    if (alg == STS_ALG_RKL1) return 1 + (int)(4.0 * r / (1.0 + sqrt(1.0 + 8.0 * r)));
+    return 1 + (int)(4.0 * (1.0 + 2.0 * r) / (1.0 + sqrt(9.0 + 16.0 * r)));
+}
 
 #define SPK_MAXJOBS 16
 
@@ -160,6 +213,7 @@ struct RklArgs {
     double2* th;            // the STS variable(s) in the state
     double2 *Uc0, *Uc1, *dU0;
     int stage;              // 1..s
+    int sts_alg;            // STS_ALG_*
     int nsts; int fields[8]; int kind[8];   // kind: 0 velocity(nu) 1 B(nu_m) 2 th iso(nu_th) 3 th aniso
     double nu, nu_m, nu_th;
     const DevScalars* sc;
@@ -175,6 +229,7 @@ struct DtArgs {
     int VX, VY, VZ, BX, BY, BZ, TH;
     int advance;             // 1: t += dt, step += 1
     int rkl_smax;
+    int sts_alg;             // STS_ALG_*
 };
 
 }  // namespace spk

@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-from .params import (SPK_FORM_FP32, SPK_FORM_PLAIN, SPK_INT_EULER, SPK_INT_RK3, SPK_STS_RKL2, Params,
+from .params import (SPK_FORM_FP32, SPK_FORM_PLAIN, SPK_INT_EULER, SPK_INT_RK3, SPK_STS_RKL1, SPK_STS_RKL2, SPK_STS_STS, Params,
                      check_parameters, default_params, num_fields, var_list)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

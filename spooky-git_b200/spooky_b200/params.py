@@ -10,7 +10,10 @@ import ctypes
 
 SPK_FORM_PLAIN = 0
 SPK_FORM_FP32 = 1
+SPK_STS_STS = 1
+SPK_STS_RKL1 = 2
 SPK_STS_RKL2 = 3
+STS_ALGORITHMS = {"sts": SPK_STS_STS, "rkl1": SPK_STS_RKL1, "rkl2": SPK_STS_RKL2}
 SPK_INT_RK3 = 0
 SPK_INT_EULER = 1
 
@@ -52,7 +55,8 @@ def default_params(**overrides):
 
     ``reynolds``/``reynolds_magnetic``/``reynolds_thermic`` may be given
     instead of ``nu``/``nu_m``/``nu_th`` and are inverted as the reference
-    does.  ``sts_variables`` (a list of field names) sets ``sts_vars_mask``.
+    does.  ``sts_variables`` (a list of field names) sets ``sts_vars_mask``;
+    ``sts_algorithm`` may be given by its cfg name ("sts", "rkl1", "rkl2").
     """
     p = Params()
     p.nx = p.ny = p.nz = 32
@@ -88,6 +92,8 @@ def default_params(**overrides):
     p.sts_every_step = 0
     p.form = SPK_FORM_PLAIN
     sts_vars = overrides.pop("sts_variables", None)
+    if isinstance(overrides.get("sts_algorithm"), str):
+        overrides["sts_algorithm"] = STS_ALGORITHMS[overrides["sts_algorithm"]]
     for key, inv in (("reynolds", "nu"), ("reynolds_magnetic", "nu_m"), ("reynolds_thermic", "nu_th")):
         if key in overrides:
             setattr(p, inv, 1.0 / overrides.pop(key))

@@ -109,6 +109,13 @@ def test_heat_equation_sts_variable_and_unknown_algorithm():
     p = S.params_from_string('modules: { heat_equation = true; supertimestepping = true; sts_algorithm = "rkl1";'
                              ' sts_variables = ("th"); };')
     assert p.sts_vars_mask == 1 and p.sts_algorithm == 2
+    # the three names of RKLegendre::compute_cycle (rkl.cu:185-199); any other is a configuration error
+    text = 'modules: { heat_equation = true; supertimestepping = true; sts_algorithm = "%s"; sts_variables = ("th"); };'
+    for name, code in (("sts", 1), ("rkl1", 2), ("rkl2", 3)):
+        assert S.params_from_string(text % name).sts_algorithm == code, name
+    with pytest.raises(S.SpookyError) as e:
+        S.params_from_string(text % "rkl3")
+    assert "sts_algorithm" in str(e.value)
 
 
 @pytest.mark.parametrize("text", [

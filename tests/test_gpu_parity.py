@@ -253,17 +253,24 @@ def test_mti_eigenmode_growth_rate():
     assert abs(np.log(amp) / t - sigma) < 1e-4
 
 
-def _heat_rkl2_params(nx, **kw):
+def _heat_sts_params(nx, alg="rkl2", **kw):
     lx = 4.0
+    kw.setdefault("fixed_dt", 0.002 * lx / nx)
     return default_params(heat_equation=1, gridsize=(nx, 2, 2), boxsize=(lx, 1.0, 1.0), reynolds_thermic=1.0,
                           cfl_par=0.5, safety_sts=1, t_final=0.5, toutput_flow=100.0, antialiasing=0,
-                          supertimestepping=1, sts_variables=["th"], integrator=1, sts_every_step=1,
-                          fixed_dt=0.002 * lx / nx, **kw)
+                          supertimestepping=1, sts_algorithm=alg, sts_variables=["th"], integrator=1,
+                          sts_every_step=1, **kw)
 
 
-def test_rkl2_heat_diffusion_matches_oracle_and_analytic():
+# analytic L1 bound at t = 0.5 (the oracle's own errors at nx = 256 are
+# 3.5e-6, 3.1e-6 and 1.1e-10: first order for sts and rkl1, second for rkl2)
+HEAT_STS_L1 = {"sts": 4e-6, "rkl1": 3.5e-6, "rkl2": 1e-7}
+
+
+@pytest.mark.parametrize("alg", ["sts", "rkl1", "rkl2"])
+def test_sts_heat_diffusion_matches_oracle_and_analytic(alg):
     nx = 256
-    p = _heat_rkl2_params(nx)
+    p = _heat_sts_params(nx, alg)
     X, _, _ = grid(p)
     T0 = 1.0 / np.sqrt(2 * np.pi * 0.01) * np.exp(-0.5 * X ** 2 / 0.01)
     U = to_spectral(T0[None])
@@ -280,18 +287,39 @@ def test_rkl2_heat_diffusion_matches_oracle_and_analytic():
     sup.fields.set(U)
     sup.executeMainLoop()
     t = sup.timestep.current_time
+    assert abs(t - 0.5) < 1e-12
     KX, _, _ = kvectors(p)
     Ta = np.fft.irfftn(np.fft.rfftn(T0) * np.exp(-KX ** 2 * t), s=T0.shape, axes=(0, 1, 2))
     Tg = np.fft.irfftn(sup.ctx.get_state()[0], s=T0.shape, axes=(0, 1, 2))
-    assert np.abs(Tg - Ta).sum() / (nx * 4) < 1e-7
+    assert np.abs(Tg - Ta).sum() / (nx * 4) < HEAT_STS_L1[alg]
 
 
+@pytest.mark.parametrize("alg", ["sts", "rkl1", "rkl2"])
+def test_sts_cycle_stage_count_matches_oracle(alg):
+    """spk_rkl_cycle reports the stage count the device computed; it equals
+    the oracle's for the same dt / dt_sts."""
+    p = _heat_sts_params(64, alg, fixed_dt=0.05)
+    U = to_spectral(np.random.default_rng(3).standard_normal((1, 64, 2, 2)))
+    o = O.Oracle(p)
+    o.set_state(U)
+    o.compute_dt()
+    s_or = o.rkl_cycle()
+    ctx = Context(p)
+    ctx.set_state(U)
+    ctx.compute_dt()
+    s_gpu = ctx.rkl_cycle()
+    ctx.synchronize()
+    assert s_gpu == s_or and s_or > 3
+    assert rel_l2(ctx.get_state(), o.get_state()) < 1e-12
+
+
+@pytest.mark.parametrize("alg", ["sts", "rkl1", "rkl2"])
 @pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
-def test_rkl2_anisotropic_sts_matches_oracle(form):
-    """Boussinesq-MHD with anisotropic conduction super-time-stepped by RKL2,
+def test_sts_anisotropic_matches_oracle(form, alg):
+    """Boussinesq-MHD with anisotropic conduction super-time-stepped,
     alternating before/after RK3 (hydro_mhd_advance.cu:43-64)."""
     p = default_params(gridsize=(16, 16, 16), form=form, t_final=100.0, toutput_flow=100.0,
-                       supertimestepping=1, sts_variables=["th"], safety_sts=10, cfl_par=1.0,
+                       supertimestepping=1, sts_algorithm=alg, sts_variables=["th"], safety_sts=10, cfl_par=1.0,
                        **CASES["bous_mhd_aniso"])
     U = make_state(p, seed=31)
     o = O.Oracle(p)
@@ -304,9 +332,10 @@ def test_rkl2_anisotropic_sts_matches_oracle(form):
     assert rel_l2(ctx.get_state(), o.get_state()) < TOL_RUN[form]
 
 
-def test_isotropic_sts_velocity_matches_oracle():
+@pytest.mark.parametrize("alg", ["sts", "rkl1", "rkl2"])
+def test_isotropic_sts_velocity_matches_oracle(alg):
     p = default_params(gridsize=(16, 16, 16), t_final=100.0, toutput_flow=100.0, supertimestepping=1,
-                       sts_variables=["vx", "vy", "vz", "th"], safety_sts=5, **CASES["bous"])
+                       sts_algorithm=alg, sts_variables=["vx", "vy", "vz", "th"], safety_sts=5, **CASES["bous"])
     U = make_state(p, seed=41)
     o = O.Oracle(p)
     o.set_state(U)

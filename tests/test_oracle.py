@@ -6,7 +6,9 @@ Every check here runs on CPU (no GPU marker).  The reference checks restated:
   heat-diffusion       tests/heat-diffusion/check-heat-diffusion.py:157-166  (L1 < 1e-15)
   alfven-wave          tests/alfven-wave/check-alfven-wave.py:152-176        (L1 < 1e-7)
   mti-eigenmode        tests/mti-eigenmode/check-mti-eigenmode.py:171-200    (L1 < 1e-7)
-  heat-diffusion-sts   tests/heat-diffusion-sts/check-heat-diffusion-sts.py (L1 < 1e-7), rkl2
+  heat-diffusion-sts   tests/heat-diffusion-sts/check-heat-diffusion-sts.py: the L1 error at
+                       t = 0.5 for sts, rkl1 and rkl2, tabulated against nx (first order in
+                       dt for sts and rkl1, second order for rkl2)
   fft-forward-inverse  src/tests/tests.cu:18-137 (round trip)
 """
 import json
@@ -219,15 +221,16 @@ def test_mti_eigenmode_growth():
     assert abs(np.log(amp) / t - sigma) < 1e-4
 
 
-def test_heat_diffusion_rkl2():
-    """heat-diffusion-sts with rkl2: forward Euler at dt = 0.002 lx/nx plus an
-    RKL2 cycle every step (the reference's test build,
-    tests/heat-diffusion-sts/hydro_mhd_advance.cu and compute_dt.cu:57-62)."""
-    lx, nx = 4.0, 256
+def _heat_sts_l1(alg, nx):
+    """heat-diffusion-sts: forward Euler at dt = 0.002 lx/nx plus one
+    super-time-stepping cycle every step (the reference's test build,
+    tests/heat-diffusion-sts/hydro_mhd_advance.cu and compute_dt.cu:57-62);
+    L1 distance to the analytic decay at t = 0.5."""
+    lx = 4.0
     p = default_params(heat_equation=1, gridsize=(nx, 2, 2), boxsize=(lx, 1.0, 1.0), reynolds_thermic=1.0,
                        cfl_par=0.5, safety_sts=1, t_final=0.5, toutput_flow=0.1, antialiasing=0,
-                       supertimestepping=1, sts_variables=["th"], integrator=1, sts_every_step=1,
-                       fixed_dt=0.002 * lx / nx)
+                       supertimestepping=1, sts_algorithm=alg, sts_variables=["th"], integrator=1,
+                       sts_every_step=1, fixed_dt=0.002 * lx / nx)
     X, _, _ = grid(p)
     T0 = 1.0 / np.sqrt(2 * np.pi * 0.01) * np.exp(-0.5 * X ** 2 / 0.01)
     o = O.Oracle(p)
@@ -235,9 +238,73 @@ def test_heat_diffusion_rkl2():
     o._lastsnap = 0.0
     _run_with_snapshots(o, p)
     t = o.get_time()[0]
+    assert abs(t - 0.5) < 1e-12
     KX, _, _ = kvectors(p)
     Ta = np.fft.irfftn(np.fft.rfftn(T0) * np.exp(-KX ** 2 * t), s=T0.shape, axes=(0, 1, 2))
-    assert np.abs(o.to_real()[0] - Ta).sum() / (nx * 4) < 1e-7
+    return np.abs(o.to_real()[0] - Ta).sum() / (nx * 4)
+
+
+# L1 bound at nx = 256 and the error ratio from nx = 128 to 256 (order 1: ~2, order 2: ~4)
+HEAT_STS = {"sts": (4e-6, (1.8, 2.2)), "rkl1": (3.5e-6, (1.8, 2.2)), "rkl2": (1.5e-10, (3.6, 4.4))}
+
+
+@pytest.mark.parametrize("alg", sorted(HEAT_STS))
+def test_heat_diffusion_sts_convergence(alg):
+    bound, (lo, hi) = HEAT_STS[alg]
+    e128, e256 = _heat_sts_l1(alg, 128), _heat_sts_l1(alg, 256)
+    assert e256 < bound, e256
+    assert lo < e128 / e256 < hi, (e128, e256)
+
+
+def _single_mode_cycle(alg, ratio, m=11, nx=64, lx=4.0):
+    """One super-time-stepping cycle of dt = ratio * dt_sts applied to the
+    single mode kx = 2 pi m / lx of the heat equation: returns the stage
+    count, dt and the amplification of the mode."""
+    kw = dict(heat_equation=1, gridsize=(nx, 2, 2), boxsize=(lx, 1.0, 1.0), reynolds_thermic=1.0, cfl_par=0.5,
+              t_final=1e9, toutput_flow=1e9, antialiasing=0, supertimestepping=1, sts_algorithm=alg,
+              sts_variables=["th"], integrator=1, sts_every_step=1)
+    dt_sts = O.Oracle(default_params(fixed_dt=1e-3, **kw)).compute_dt()[2]
+    o = O.Oracle(default_params(fixed_dt=ratio * dt_sts, **kw))
+    U = np.zeros((1, nx, 2, 2), complex)
+    U[0, m, 0, 0] = 1.0
+    o.set_state(U)
+    dt = o.compute_dt()[3]
+    s = o.rkl_cycle()
+    return s, dt, o.get_state()[0, m, 0, 0], -(2 * np.pi / lx * m) ** 2 * dt
+
+
+@pytest.mark.parametrize("ratio", [1.0, 3.7, 20.0, 100.0])
+@pytest.mark.parametrize("alg", ["sts", "rkl1", "rkl2"])
+def test_sts_cycle_matches_stability_polynomial(alg, ratio):
+    """A cycle multiplies the mode exp(i k x) by the scheme's stability
+    polynomial R(z), z = -nu k^2 dt:
+      rkl1  P_s(1 + w1 z), w1 = 2/(s^2+s)             (Meyer, Balsara & Aslam 2014, RKL1)
+      rkl2  a_s + b_s P_s(1 + w1 z), w1 = 4/(s^2+s-2),
+            b_s = (s^2+s-2)/(2s(s+1)), a_s = 1 - b_s    (the same paper, RKL2)
+      sts   prod_i (1 + tau_i z / dt) over the sub-steps tau_i of
+            Alexiades, Amiez & Gremaud 1996, whose sum is dt."""
+    from numpy.polynomial import legendre
+    s, dt, got, z = _single_mode_cycle(alg, ratio)
+    if alg == "rkl1":
+        assert s == 1 + int(4 * ratio / (1 + np.sqrt(1 + 8 * ratio)) + 1e-12)
+        want = legendre.legval(1 + 2 / (s * s + s) * z, [0] * s + [1])
+    elif alg == "rkl2":
+        assert s == 1 + int(4 * (1 + 2 * ratio) / (1 + np.sqrt(9 + 16 * ratio)) + 1e-12)
+        b = (s * s + s - 2) / (2 * s * (s + 1))
+        want = 1 - b + b * legendre.legval(1 + 4 / (s * s + s - 2) * z, [0] * s + [1])
+    else:
+        nu = 1e-3
+        a = (1 - np.sqrt(nu)) / (1 + np.sqrt(nu))
+        c = (1 - a ** (2 * s)) / (1 + a ** (2 * s))
+        if s > 1:
+            tau = dt * 2 * np.sqrt(nu) / (s * c) / ((nu - 1) * np.cos((2 * np.arange(s) + 1) * np.pi / (2 * s)) + 1 + nu)
+        else:
+            tau = np.array([dt])
+        assert abs(tau.sum() / dt - 1) < 1e-13
+        # the sub-step count grows like sqrt(dt/dt_sts) at first
+        assert s >= 2 and s <= 2 + 2 * np.sqrt(ratio)
+        want = np.prod(1 + tau * z / dt)
+    assert abs(got - want) < 1e-13, (s, got, want)
 
 
 def test_energy_budget_matches_real_space():
