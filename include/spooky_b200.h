@@ -241,6 +241,86 @@ int spk_ensemble_advance(spk_ensemble* ens, int nsteps);
 int spk_ensemble_synchronize(spk_ensemble* ens);
 int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
 
+/* ---- learned subgrid closure ---------------------------------------------
+ * No counterpart in the reference.  A pointwise MLP maps eight
+ * rotation-invariant, dimensionless features of the resolved velocity
+ * gradient A = grad u (A[i][j] = du_i/dx_j) and field gradient G = grad B to
+ * an eddy viscosity and an eddy resistivity:
+ *   S = (A + A^T)/2, w = curl u, S_B = (G + G^T)/2, J = curl B,
+ *   n^2 = S:S + |w|^2/2 + S_B:S_B + |J|^2/2 (+1e-30),
+ *   features  S:S/n^2, |w|^2/(2n^2), S_B:S_B/n^2, |J|^2/(2n^2),
+ *             tr(S^3)/n^3, w.S.w/n^3, J.S.J/n^3, (w.J)^2/(4n^4);
+ *   o = W3 tanh(W2 tanh(W1 f + b1) + b2) + b3           (8 -> 32 -> 32 -> 2)
+ *   nu_t = Delta^2 n softplus(o0),  eta_t = Delta^2 n softplus(o1),
+ *   Delta^2 = (pi/kxmax * pi/kymax * pi/kzmax)^(2/3)    (dealiased cut-offs).
+ * The RHS adds -2 nu_t S to the Basdevant stress and -eta_t J to the EMF
+ * before their forward transforms, so both terms only remove energy; the dt
+ * rule adds max(nu_t) and max(eta_t) to the parabolic rates.  Parameters
+ * are floats in the order W1[32][8] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
+ *
+ * Training samples are SoA float rows (row r of every sample contiguous,
+ * rows `stride` floats apart): features[8], S[5] (xx xy xz yy yz), J[3],
+ * Delta^2 n, target stress[5] (the Basdevant channels: xx xy xz yy yz),
+ * target EMF[3].  The loss is the mean over samples of
+ *   w0 |dT - T_target|_F^2 + w1 |dE - E_target|^2
+ * (the full traceless symmetric stress in the Frobenius norm). */
+#define SPK_CLOSURE_NFEAT   8
+#define SPK_CLOSURE_HIDDEN  32
+#define SPK_CLOSURE_NPARAM  (32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2)
+#define SPK_CLOSURE_ROWS    25
+/* sample rows */
+#define SPK_CLOSURE_ROW_FEAT   0
+#define SPK_CLOSURE_ROW_S      8
+#define SPK_CLOSURE_ROW_J      13
+#define SPK_CLOSURE_ROW_SCALE  16
+#define SPK_CLOSURE_ROW_TT     17
+#define SPK_CLOSURE_ROW_TE     22
+
+/* Switch the closure on (params: SPK_CLOSURE_NPARAM host floats) or off
+ * (params NULL) for the context's RHS, steps and dt rule.  HD and MHD
+ * contexts; the next step re-records the step graph. */
+int spk_closure_set(spk_ctx* ctx, const float* params);
+
+/* The spectral products of U before their divergence / curl: the Basdevant
+ * stress (xx xy xz yy yz, traceless symmetric u u - B B) and, with MHD, the
+ * EMF u x B, forward-transformed, dealiased modes kept and the others zero
+ * (hydro.cu:19-75, mhd.cu:20-62 up to the R2C).  P: device [nprod][Nc]
+ * complex FP64, nprod = 5 (HD) or 8 (MHD).  With the closure on, the
+ * closure terms are included. */
+int spk_products(spk_ctx* ctx, const double* U, double* P, int* nprod);
+
+/* Training samples from one fine-grid state: the fine state Uf and its
+ * products are truncated to the coarse grid's dealiased modes (a sharp
+ * spectral filter at the coarse cut-off); the targets are the subgrid
+ * stress and EMF, products(filtered fine) - products(coarse of the filtered
+ * state), and the features come from the filtered state -- one sample per
+ * coarse grid point, nx*ny*nz of them, written as SoA rows (stride >=
+ * nx*ny*nz floats) into the device array samples.  Both contexts are HD or
+ * both MHD, with the same box, and the coarse grid is not finer than the
+ * fine one along any axis.  `scratch` is a device buffer of at least
+ * *scratch_bytes (from spk_closure_samples_size); the coarse context's
+ * state is overwritten with the filtered state. */
+int spk_closure_samples_size(const spk_ctx* fine, const spk_ctx* coarse, size_t* scratch_bytes, size_t* nsamples);
+int spk_closure_samples(spk_ctx* fine, const double* Uf, spk_ctx* coarse, float* samples, size_t stride,
+                        void* scratch, size_t scratch_bytes);
+
+/* Trainer: the MLP's parameters, Adam moments and gradient scratch on the
+ * device, trained on device samples by the library's own forward/backward
+ * kernels (deterministic: fixed-order reductions).  Minibatch i of a run
+ * takes samples (a * (i*batch + r) + c) mod n, r < batch, for an a coprime
+ * with n: each pass over n samples visits every sample once. */
+typedef struct spk_trainer spk_trainer;
+int spk_trainer_create(void* cuda_stream, spk_trainer** out);
+int spk_trainer_destroy(spk_trainer* tr);
+int spk_trainer_set_params(spk_trainer* tr, const float* params);        /* host floats; resets Adam */
+int spk_trainer_get_params(spk_trainer* tr, float* params);              /* host floats */
+int spk_trainer_set_samples(spk_trainer* tr, const float* samples, size_t n, size_t stride, const float w[2]);
+/* Full-batch mean loss and gradient at the current parameters (host outputs). */
+int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad);
+/* nsteps Adam steps (lr) on minibatches of `batch` samples; loss_hist
+ * (host, may be NULL) receives each step's minibatch loss. */
+int spk_trainer_train(spk_trainer* tr, int nsteps, int batch, float lr, float* loss_hist);
+
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */
 const char* spk_last_error(const spk_ctx* ctx);

@@ -105,7 +105,7 @@ private:
 class RKLegendre {
 public:
     explicit RKLegendre(spk_ctx* ctx) : ctx_(ctx) {}
-    /* RKLegendre::compute_cycle: one RKL2 cycle with the last dt; returns the stage count */
+    /* RKLegendre::compute_cycle: one cycle of the configured scheme (STS, RKL1, RKL2) with the last dt; returns the stage count */
     int compute_cycle() {
         int s = 0;
         check(spk_rkl_cycle(ctx_, &s), ctx_);

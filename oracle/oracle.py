@@ -42,6 +42,17 @@ def lib():
         L.orc_c2r.argtypes = [vp, dp, dp]
         L.orc_fft1d.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int]
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_closure_set.argtypes = [vp, dp]
+        L.orc_closure_set.restype = ctypes.c_int
+        L.orc_products.argtypes = [vp, dp, dp]
+        L.orc_products.restype = ctypes.c_int
+        L.orc_truncate.argtypes = [vp, vp, dp, ctypes.c_int, dp]
+        L.orc_closure_samples.argtypes = [vp, dp, vp, dp, ctypes.c_size_t]
+        L.orc_closure_features.argtypes = [dp, dp, dp, dp, dp]
+        L.orc_closure_features.restype = ctypes.c_double
+        L.orc_closure_mlp.argtypes = [dp, dp, dp]
+        L.orc_closure_loss_grad.argtypes = [dp, ctypes.c_size_t, ctypes.c_size_t, dp, dp, dp, dp]
+        L.orc_closure_adam.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_double]
         _LIB = L
     return _LIB
 
@@ -59,6 +70,45 @@ def fft1d(x, sign=-1):
 
 def set_threads(n):
     lib().orc_set_threads(int(n))
+
+
+# ---- learned closure (include/spooky_b200.h, SPK_CLOSURE_*) ----------------
+CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
+CLOSURE_ROWS = 25
+
+
+def closure_features(A, G):
+    """A, G: 3x3 gradients (A[i, j] = du_i/dx_j) -> (features[8], S[5], J[3], n)."""
+    A = np.ascontiguousarray(A, dtype=np.float64).reshape(9)
+    G = np.ascontiguousarray(G, dtype=np.float64).reshape(9)
+    f, S, J = np.empty(8), np.empty(5), np.empty(3)
+    n = lib().orc_closure_features(_dp(A), _dp(G), _dp(f), _dp(S), _dp(J))
+    return f, S, J, n
+
+
+def closure_mlp(params, f):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    o = np.empty(2)
+    lib().orc_closure_mlp(_dp(params), _dp(f), _dp(o))
+    return o
+
+
+def closure_loss_grad(samples, params, w):
+    """samples: [CLOSURE_ROWS, n] rows; returns (loss, grad)."""
+    X = np.ascontiguousarray(samples, dtype=np.float64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g = np.empty(CLOSURE_NPARAM)
+    loss = ctypes.c_double()
+    lib().orc_closure_loss_grad(_dp(X), X.shape[1], X.shape[1], _dp(params), _dp(w), _dp(g), ctypes.byref(loss))
+    return loss.value, g
+
+
+def closure_adam(params, grad, m, v, t, lr):
+    """In place on float64 arrays params, m, v."""
+    grad = np.ascontiguousarray(grad, dtype=np.float64)
+    lib().orc_closure_adam(_dp(params), _dp(grad), _dp(m), _dp(v), int(t), float(lr))
 
 
 class Oracle:
@@ -148,6 +198,39 @@ class Oracle:
         C = np.empty((p.nx, p.ny, p.nz // 2 + 1), dtype=np.complex128)
         lib().orc_r2c(self._h, _dp(R), _dp(C))
         return C
+
+    def closure_set(self, params):
+        if params is None:
+            return lib().orc_closure_set(self._h, None)
+        self._cparams = np.ascontiguousarray(params, dtype=np.float64)
+        rc = lib().orc_closure_set(self._h, _dp(self._cparams))
+        if rc:
+            raise ValueError("the closure needs an HD or MHD context")
+
+    def products(self, U):
+        U = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
+        p = self.params
+        P = np.zeros((8, p.nx, p.ny, p.nz // 2 + 1), dtype=np.complex128)
+        n = lib().orc_products(self._h, _dp(U), _dp(P))
+        return P[:n]
+
+    def truncate_to(self, coarse, X):
+        """Sharp spectral filter of this grid's spectra X[nch, ...] onto coarse."""
+        X = np.ascontiguousarray(X, dtype=np.complex128)
+        nch = X.shape[0]
+        q = coarse.params
+        out = np.empty((nch, q.nx, q.ny, q.nz // 2 + 1), dtype=np.complex128)
+        lib().orc_truncate(self._h, coarse._h, _dp(X), nch, _dp(out))
+        return out
+
+    def closure_samples(self, U, coarse):
+        """Samples [CLOSURE_ROWS, nx*ny*nz of coarse] from this (fine) state U."""
+        U = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
+        q = coarse.params
+        n = q.nx * q.ny * q.nz
+        X = np.empty((CLOSURE_ROWS, n))
+        lib().orc_closure_samples(self._h, _dp(U), coarse._h, _dp(X), n)
+        return X
 
     def c2r(self, C):
         p = self.params

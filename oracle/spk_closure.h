@@ -1,0 +1,35 @@
+/*
+ * spk_closure.h -- CPU FP64 restatement of the learned subgrid closure.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker of the CUDA closure kernels
+ * (features, MLP inference, loss gradient, Adam).  The closure has no
+ * counterpart in the reference; its definition is the one stated in
+ * include/spooky_b200.h (SPK_CLOSURE_*).
+ */
+#ifndef SPK_CLOSURE_ORACLE_H
+#define SPK_CLOSURE_ORACLE_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A[3*i+j] = d u_i / d x_j, G likewise for B.  Writes the 8 features, the
+ * strain S (xx xy xz yy yz), the current J and returns n. */
+double orc_closure_features(const double* A, const double* G, double* feat, double* S5, double* J3);
+
+/* MLP outputs o[2] for features f[8]; nu = scale * softplus(o0), eta = scale * softplus(o1). */
+void orc_closure_mlp(const double* params, const double* f, double* o);
+
+/* Mean loss and its gradient over samples rows (SoA, row r at samples + r*stride);
+ * w[0], w[1]: weights of the stress and EMF errors. */
+void orc_closure_loss_grad(const double* samples, size_t n, size_t stride, const double* params,
+                           const double* w, double* grad, double* loss);
+
+/* One Adam step (t >= 1) with beta1 0.9, beta2 0.999, eps 1e-8. */
+void orc_closure_adam(double* params, const double* grad, double* m, double* v, int t, double lr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

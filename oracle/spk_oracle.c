@@ -8,6 +8,7 @@
  * Reference = LorenzoLMP/spooky-git; citations are file:line in that tree.
  */
 #include "spk_oracle.h"
+#include "spk_closure.h"
 
 #include <math.h>
 #include <stdint.h>
@@ -243,6 +244,13 @@ struct orc_ctx {
     cpx *rdU, *rdU0, *rUc0, *rUc1;
     double t, dt, dt_hyp, dt_par, dt_sts, t_lastsnap;
     int step;
+    /* learned closure (spk_closure.c): parameters, Delta^2, the real-space
+     * closure terms -2 nu_t S (5) and -eta_t J (3), the gradients A, G (18) */
+    int closure_on;
+    double cparams[SPK_CLOSURE_NPARAM];
+    double delta2, nu_t_max, eta_t_max;
+    double *rclos, *rgrad;
+    cpx* ctmp;
 };
 
 int orc_num_fields(const orc_ctx* c) { return c->F; }
@@ -330,6 +338,7 @@ orc_ctx* orc_create(const spk_params_t* p) {
     c->t = p->t_initial;
     c->t_lastsnap = 0.0;
     c->step = 0;
+    c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
     return c;
 }
 
@@ -340,6 +349,7 @@ void orc_destroy(orc_ctx* c) {
     free(c->U); free(c->dU); free(c->S); free(c->tmp); free(c->work);
     free(c->realbuf); free(c->rtmp);
     free(c->rdU); free(c->rdU0); free(c->rUc0); free(c->rUc1);
+    free(c->rclos); free(c->rgrad); free(c->ctmp);
     free(c);
 }
 
@@ -384,6 +394,56 @@ static void complex2real(orc_ctx* c, const cpx* Uin, double* R, int nf) {
     for (int f = 0; f < nf; f++) c2r_3d(&c->g, Uin + (size_t)f * c->g.nc, R + (size_t)f * c->g.nr, c->work);
 }
 
+/* ---- learned closure terms (include/spooky_b200.h, SPK_CLOSURE_*): the
+ * spectral gradients of u and B to real space, then per point the features,
+ * the MLP and the terms -2 nu_t S, -eta_t J; maxima of nu_t and eta_t. */
+static void closure_fields(orc_ctx* c, const cpx* U) {
+    const size_t nr = c->g.nr, nc = c->g.nc;
+    const int mhd = c->p.mhd;
+    memset(c->rgrad, 0, sizeof(double) * 18 * nr);
+    for (int b = 0; b < (mhd ? 2 : 1); b++)
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                const cpx* X = U + (size_t)((b ? c->MAG : c->VEL) + i) * nc;
+                FOR_MODES(c) {
+                    MODE_VARS(c)
+                    const double kj = j == 0 ? kx : (j == 1 ? ky : kz);
+                    c->ctmp[id] = c_scale(kj, c_muli(X[id]));
+                }
+                c2r_3d(&c->g, c->ctmp, c->rgrad + (size_t)(9 * b + 3 * i + j) * nr, c->work);
+            }
+    double numax = 0.0, etamax = 0.0;
+    #pragma omp parallel for schedule(static) reduction(max : numax, etamax)
+    for (long q = 0; q < (long)nr; q++) {
+        double A[9], G[9], f[8], S5[5], J3[3], o[2];
+        for (int r = 0; r < 9; r++) { A[r] = c->rgrad[(size_t)r * nr + q]; G[r] = c->rgrad[(size_t)(9 + r) * nr + q]; }
+        const double n = orc_closure_features(A, G, f, S5, J3);
+        orc_closure_mlp(c->cparams, f, o);
+        const double sc = c->delta2 * n;
+        const double nu = sc * (o[0] > 30.0 ? o[0] : log1p(exp(o[0])));
+        const double eta = sc * (o[1] > 30.0 ? o[1] : log1p(exp(o[1])));
+        for (int r = 0; r < 5; r++) c->rclos[(size_t)r * nr + q] = -2.0 * nu * S5[r];
+        for (int r = 0; r < 3; r++) c->rclos[(size_t)(5 + r) * nr + q] = mhd ? -eta * J3[r] : 0.0;
+        if (nu > numax) numax = nu;
+        if (mhd && eta > etamax) etamax = eta;
+    }
+    c->nu_t_max = numax;
+    c->eta_t_max = etamax;
+}
+
+int orc_closure_set(orc_ctx* c, const double* params) {
+    if (!params) { c->closure_on = 0; return 0; }
+    if (!c->p.incompressible || c->p.boussinesq) return 1;
+    memcpy(c->cparams, params, sizeof(c->cparams));
+    if (!c->rclos) {
+        c->rclos = (double*)calloc(c->g.nr * 8, sizeof(double));
+        c->rgrad = (double*)calloc(c->g.nr * 18, sizeof(double));
+        c->ctmp = (cpx*)calloc(c->g.nc, sizeof(cpx));
+    }
+    c->closure_on = 1;
+    return 0;
+}
+
 /* ---- Physics::BasdevantHydro (src/physics/hydro.cu:19-75) -------------- */
 static void basdevant_hydro(orc_ctx* c, const double* rb, cpx* dVel) {
     const size_t nr = c->g.nr, nc = c->g.nc;
@@ -410,6 +470,8 @@ static void basdevant_hydro(orc_ctx* c, const double* rb, cpx* dVel) {
             T[4 * nr + i] = uy * uz - by * bz;
         }
     }
+    if (c->closure_on)
+        for (size_t i = 0; i < 5 * nr; i++) T[i] += c->rclos[i];
     for (int n = 0; n < 5; n++) r2c_3d(&c->g, T + (size_t)n * nr, c->tmp + (size_t)n * nc);
     const cpx* S = c->tmp;
     /* NonLinHydroAdv (src/cuda/cuda_kernels.cu:82-98): overwrites dVel */
@@ -440,6 +502,8 @@ static void curl_emf(orc_ctx* c, const double* rb, cpx* dMag) {
         E[nr + i] = bx * uz - bz * ux;
         E[2 * nr + i] = -bx * uy + by * ux;
     }
+    if (c->closure_on)
+        for (size_t i = 0; i < 3 * nr; i++) E[i] += c->rclos[5 * nr + i];
     for (int n = 0; n < 3; n++) r2c_3d(&c->g, E + (size_t)n * nr, c->tmp + (size_t)n * nc);
     const cpx* M = c->tmp;
     /* MagneticShear (src/cuda/cuda_kernels.cu:257-272): overwrites dMag */
@@ -584,6 +648,7 @@ static void compute_dfield(orc_ctx* c, const cpx* U, const double* rb, cpx* dU) 
     const size_t nc = c->g.nc;
     const spk_params_t* p = &c->p;
     if (p->incompressible) {
+        if (c->closure_on) closure_fields(c, U);
         basdevant_hydro(c, rb, dU + (size_t)c->VEL * nc);
         if (p->mhd) curl_emf(c, rb, dU + (size_t)c->MAG * nc);
         if (p->boussinesq) advect_temperature(c, rb, dU + (size_t)c->TH * nc);
@@ -677,6 +742,13 @@ static void compute_dt(orc_ctx* c) {
             if (c->sts_pos[c->BY] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
             gamma_tmp = kzmax * kzmax * p->nu_m;
             if (c->sts_pos[c->BZ] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
+        }
+        if (c->closure_on) {
+            /* the closure's eddy viscosity and resistivity as parabolic rates */
+            closure_fields(c, c->U);
+            const double k2 = kxmax * kxmax + kymax * kymax + kzmax * kzmax;
+            gamma_par += k2 * c->nu_t_max;
+            if (p->mhd) gamma_par += k2 * c->eta_t_max;
         }
         c->dt_hyp = p->cfl / (gamma_v + gamma_th + gamma_b);
         c->dt_par = p->cfl_par / gamma_par;
@@ -966,6 +1038,112 @@ void orc_step(orc_ctx* c, int nsteps) {
         }
         c->step += 1;
     }
+}
+
+/* Spectral products of U before their divergence / curl (hydro.cu:19-75,
+ * mhd.cu:20-62 up to the R2C), closure terms included when on; modes
+ * outside the 2/3 mask set to zero.  P: [nprod][Nc], nprod 5 (HD) or 8 (MHD). */
+int orc_products(orc_ctx* c, const double* Uin, double* Pout) {
+    const cpx* U = (const cpx*)Uin;
+    cpx* P = (cpx*)Pout;
+    const size_t nr = c->g.nr, nc = c->g.nc;
+    if (!c->p.incompressible) return 0;
+    complex2real(c, U, c->realbuf, c->F);
+    if (c->closure_on) closure_fields(c, U);
+    const int mhd = c->p.mhd, np = mhd ? 8 : 5;
+    double* R = (double*)calloc(nr * np, sizeof(double));
+    const double* u = c->realbuf + (size_t)c->VEL * nr;
+    const double* B = c->realbuf + (size_t)c->MAG * nr;
+    #pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nr; i++) {
+        const double ux = u[i], uy = u[nr + i], uz = u[2 * nr + i];
+        const double bx = mhd ? B[i] : 0.0, by = mhd ? B[nr + i] : 0.0, bz = mhd ? B[2 * nr + i] : 0.0;
+        R[i] = (2.0 * ux * ux - uy * uy - uz * uz - 2.0 * bx * bx + by * by + bz * bz) / 3.0;
+        R[nr + i] = ux * uy - bx * by;
+        R[2 * nr + i] = ux * uz - bx * bz;
+        R[3 * nr + i] = (-ux * ux + 2.0 * uy * uy - uz * uz + bx * bx - 2.0 * by * by + bz * bz) / 3.0;
+        R[4 * nr + i] = uy * uz - by * bz;
+        if (mhd) {
+            R[5 * nr + i] = -by * uz + bz * uy;
+            R[6 * nr + i] = bx * uz - bz * ux;
+            R[7 * nr + i] = -bx * uy + by * ux;
+        }
+    }
+    if (c->closure_on)
+        for (size_t i = 0; i < (size_t)np * nr; i++) R[i] += c->rclos[i];
+    for (int n = 0; n < np; n++) {
+        r2c_3d(&c->g, R + (size_t)n * nr, P + (size_t)n * nc);
+        cpx* X = P + (size_t)n * nc;
+        FOR_MODES(c) {
+            MODE_VARS(c)
+            if (mask == 0.0) { X[id].re = 0.0; X[id].im = 0.0; }
+        }
+    }
+    free(R);
+    return np;
+}
+
+/* Sharp spectral filter: the coarse grid's kept modes of fine-grid spectra
+ * (scaled by the point-count ratio, since the forward transform is
+ * unnormalised), zero elsewhere. */
+void orc_truncate(const orc_ctx* f, const orc_ctx* c, const double* Xf, int nch, double* Xc) {
+    const double scale = (double)c->g.nr / (double)f->g.nr;
+    for (int ch = 0; ch < nch; ch++) {
+        const cpx* A = (const cpx*)Xf + (size_t)ch * f->g.nc;
+        cpx* Bc = (cpx*)Xc + (size_t)ch * c->g.nc;
+        FOR_MODES(c) {
+            MODE_VARS(c)
+            cpx v = {0.0, 0.0};
+            if (mask != 0.0) {
+                const int ix = i_ < c->g.nx / 2 ? i_ : i_ - c->g.nx, iy = j_ < c->g.ny / 2 ? j_ : j_ - c->g.ny;
+                const int fi = ix >= 0 ? ix : ix + f->g.nx, fj = iy >= 0 ? iy : iy + f->g.ny;
+                v = c_scale(scale, A[(size_t)k_ + f->g.nzh * ((size_t)fj + (size_t)fi * f->g.ny)]);
+            }
+            Bc[id] = v;
+        }
+    }
+}
+
+/* Training samples (include/spooky_b200.h, spk_closure_samples): one per
+ * coarse point, rows of SPK_CLOSURE_ROWS doubles `stride` apart.  The coarse
+ * context's state becomes the filtered fine state. */
+void orc_closure_samples(orc_ctx* f, const double* Uf, orc_ctx* c, double* X, size_t stride) {
+    const size_t nr = c->g.nr, nc = c->g.nc;
+    const int np = c->p.mhd ? 8 : 5;
+    const int fon = f->closure_on, con = c->closure_on;
+    f->closure_on = 0;
+    c->closure_on = 0;
+    double* Pf = (double*)malloc(sizeof(cpx) * f->g.nc * np);
+    double* Pt = (double*)malloc(sizeof(cpx) * nc * np);
+    double* Pc = (double*)malloc(sizeof(cpx) * nc * np);
+    orc_products(f, Uf, Pf);
+    orc_truncate(f, c, Uf, c->F, (double*)c->U);
+    orc_truncate(f, c, Pf, np, Pt);
+    orc_products(c, (const double*)c->U, Pc);
+    for (size_t i = 0; i < 2 * nc * np; i++) Pt[i] -= Pc[i];
+    double* Rt = (double*)malloc(sizeof(double) * nr * np);
+    for (int n = 0; n < np; n++) c2r_3d(&c->g, (const cpx*)Pt + (size_t)n * nc, Rt + (size_t)n * nr, c->work);
+    if (!c->rgrad) {
+        c->rclos = (double*)calloc(nr * 8, sizeof(double));
+        c->rgrad = (double*)calloc(nr * 18, sizeof(double));
+        c->ctmp = (cpx*)calloc(nc, sizeof(cpx));
+    }
+    closure_fields(c, c->U);   /* gradients (the MLP outputs are not used) */
+    #pragma omp parallel for schedule(static)
+    for (long q = 0; q < (long)nr; q++) {
+        double A[9], G[9], fe[8], S5[5], J3[3];
+        for (int r = 0; r < 9; r++) { A[r] = c->rgrad[(size_t)r * nr + q]; G[r] = c->rgrad[(size_t)(9 + r) * nr + q]; }
+        const double n = orc_closure_features(A, G, fe, S5, J3);
+        for (int r = 0; r < 8; r++) X[(size_t)(SPK_CLOSURE_ROW_FEAT + r) * stride + q] = fe[r];
+        for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_S + r) * stride + q] = S5[r];
+        for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_J + r) * stride + q] = J3[r];
+        X[(size_t)SPK_CLOSURE_ROW_SCALE * stride + q] = c->delta2 * n;
+        for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_TT + r) * stride + q] = Rt[(size_t)r * nr + q];
+        for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_TE + r) * stride + q] = np == 8 ? Rt[(size_t)(5 + r) * nr + q] : 0.0;
+    }
+    free(Pf); free(Pt); free(Pc); free(Rt);
+    f->closure_on = fon;
+    c->closure_on = con;
 }
 
 void orc_to_real(orc_ctx* c, double* R) { complex2real(c, c->U, R, c->F); }

@@ -51,6 +51,13 @@ void orc_fft1d(int n, const double* in, double* out, int sign);
 
 void orc_set_threads(int nthreads);
 
+/* Learned closure (include/spooky_b200.h, SPK_CLOSURE_*): params NULL = off;
+ * returns nonzero for contexts other than HD / MHD. */
+int  orc_closure_set(orc_ctx* c, const double* params);
+int  orc_products(orc_ctx* c, const double* U, double* P);   /* returns nprod */
+void orc_truncate(const orc_ctx* fine, const orc_ctx* coarse, const double* Xf, int nch, double* Xc);
+void orc_closure_samples(orc_ctx* fine, const double* Uf, orc_ctx* coarse, double* X, size_t stride);
+
 #ifdef __cplusplus
 }
 #endif
