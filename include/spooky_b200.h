@@ -92,6 +92,8 @@ typedef struct spk_params {
     int    integrator;      /* SPK_INT_RK3 or SPK_INT_EULER                                        */
     int    sts_every_step;  /* 1: RKL cycle after the integrator on every step (the STS test build) */
     int    form;            /* SPK_FORM_PLAIN or SPK_FORM_FP32                                     */
+    int    closure;         /* 1: reserve the learned closure's gradient channels (HD/MHD; weights
+                               from spk_closure_set)                                               */
 } spk_params_t;
 
 /* Fill *p with the reference's defaults (parameters.cu:77-505). */

@@ -20,6 +20,7 @@
 
 #include "spk_kernels.cu"
 #include "spk_pass2.cu"
+#include "spk_closure.cu"
 #include "spk_config.hpp"
 
 using namespace spk;
@@ -59,6 +60,13 @@ struct spk_ctx {
     DevGrid g;
     // pipeline layout
     int nin, nout, ch_u, ch_b, ch_th, ch_gx, ch_gy;
+    int nin_base;                  // u, B, theta channels (no gradient channels)
+    // learned closure: d/dx and d/dy channels of u [and B] (ncl_half each),
+    // parameters on the device, Delta^2; closure_on once weights are set
+    int ch_dx = -1, ch_dy = -1, ncl_half = 0;
+    bool closure_on = false;
+    float* d_cparams = nullptr;
+    double delta2 = 0.0;
     int out_T, out_E, out_F, out_Q;
     // graphs
     cudaGraphExec_t gexec[2];
@@ -314,7 +322,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
-                            slots).total;
+                            slots, z.closure ? CL_NP : 0).total;
     };
     // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
     auto rounds = [&](long n) { return (n + slots - 1) / slots; };
@@ -340,7 +348,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     z.lines = L;
     const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
-    if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
+    if (z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.zder_n > 0) {
         cudaFuncSetAttribute(k_zpass2<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_zpass2<T, N, true><<<nblk, nthr, smem, c->stream>>>(z);
     } else {
@@ -366,7 +374,7 @@ static void zpass(spk_ctx* c, ZArgs& z) {
         c->sticky = SPK_ERR_ARG;
         return;
     }
-    const int nin_all = z.nin + (z.derive_gz == 1 ? 1 : 0);
+    const int nin_all = z.nin + (z.derive_gz == 1 ? 1 : 0) + z.zder_n;
     if (c->fp32) launch_zpass<float>(c, z, nin_all);
     else launch_zpass<double>(c, z, nin_all);
 }
@@ -434,15 +442,31 @@ static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx) {
         add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_th), 1, 1, 0, 0);
         if (with_gx && c->aniso_rhs) add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_gx), 1, 1, 1, 0);
     }
+    if (with_gx && c->closure_on) {
+        add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_dx), 3, 1, 1, 0);
+        if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_dx + 3), 3, 1, 1, 0);
+    }
     axis(c, a, +1);
 }
 
 static void pass_y_inverse(spk_ctx* c, bool with_g) {
     AxisArgs a = axis_args(c, 1);
-    const int n = with_g ? c->nin : (c->nin - (c->aniso_rhs ? 2 : 0));
-    // channels 0..n-1 one to one (gx included when present)
-    add_job(c, a, c->bufA, c->bufB, with_g ? (c->aniso_rhs ? c->ch_gx + 1 : n) : n, 0, 0, 0);
-    if (with_g && c->aniso_rhs) add_job(c, a, chan(c, c->bufA, c->ch_th), chan(c, c->bufB, c->ch_gy), 1, 0, 1, 0);
+    if (with_g && c->aniso_rhs) {
+        // u, B, theta and d/dx theta one to one; d/dy theta from theta
+        add_job(c, a, c->bufA, c->bufB, c->ch_gx + 1, 0, 0, 0);
+        add_job(c, a, chan(c, c->bufA, c->ch_th), chan(c, c->bufB, c->ch_gy), 1, 0, 1, 0);
+    } else if (with_g && c->closure_on) {
+        // u, B and their d/dx one to one; then d/dy of u, B (a second launch:
+        // the jobs of one launch are capped)
+        add_job(c, a, c->bufA, c->bufB, c->ch_dx + c->ncl_half, 0, 0, 0);
+        axis(c, a, +1);
+        AxisArgs b = axis_args(c, 1);
+        add_job(c, b, chan(c, c->bufA, c->ch_u), chan(c, c->bufB, c->ch_dy), c->ncl_half, 0, 1, 0);
+        axis(c, b, +1);
+        return;
+    } else {
+        add_job(c, a, c->bufA, c->bufB, c->nin_base, 0, 0, 0);
+    }
     axis(c, a, +1);
 }
 
@@ -469,9 +493,18 @@ static ZArgs z_args(spk_ctx* c) {
 }
 
 static void set_inputs(spk_ctx* c, ZArgs& z, bool with_g) {
-    z.nin = with_g ? c->nin : c->nin - (c->aniso_rhs ? 2 : 0);
+    z.nin = c->nin_base;
     z.ch_u = c->ch_u; z.ch_b = c->ch_b; z.ch_th = c->ch_th;
-    if (with_g && c->aniso_rhs) { z.ch_gx = c->ch_gx; z.ch_gy = c->ch_gy; z.derive_gz = 1; }
+    if (with_g && c->aniso_rhs) { z.nin += 2; z.ch_gx = c->ch_gx; z.ch_gy = c->ch_gy; z.derive_gz = 1; }
+    if (with_g && c->closure_on) {
+        z.nin += 2 * c->ncl_half;
+        z.closure = 1;
+        z.ch_dx = c->ch_dx; z.ch_dy = c->ch_dy;
+        z.zder_n = c->ncl_half;
+        for (int d = 0; d < c->ncl_half; d++) z.zder_src[d] = c->ch_u + d;
+        z.cparams = c->d_cparams;
+        z.delta2 = (float)c->delta2;
+    }
 }
 
 static void pass_z_products(spk_ctx* c, bool do_max) {
@@ -568,6 +601,7 @@ static DtArgs dt_args(spk_ctx* c, bool advance) {
     d.advance = advance ? 1 : 0;
     d.rkl_smax = c->rkl_smax;
     d.sts_alg = p.sts_algorithm;
+    d.closure = c->closure_on ? 1 : 0;
     return d;
 }
 
@@ -736,6 +770,7 @@ extern "C" void spk_params_default(spk_params_t* p) {
     p->t_initial = 0.0; p->t_final = 1.0; p->toutput_flow = 1.0;
     p->integrator = SPK_INT_RK3;
     p->form = SPK_FORM_PLAIN;
+    p->closure = 0;
 }
 
 static int check_params(const spk_params_t* p, std::string& why) {
@@ -754,6 +789,8 @@ static int check_params(const spk_params_t* p, std::string& why) {
     }
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
+    if (p->closure && (!p->incompressible || p->boussinesq)) { why = "the learned closure covers the HD and MHD modules"; return SPK_ERR_UNSUPPORTED; }
+    if (p->closure && p->supertimestepping) { why = "the learned closure with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
     return SPK_OK;
 }
 
@@ -949,7 +986,16 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     if (p.incompressible) { c->ch_u = ch; ch += 3; }
     if (p.mhd) { c->ch_b = ch; ch += 3; }
     if (p.boussinesq) { c->ch_th = ch; ch += 1; }
+    c->nin_base = ch;
     if (c->aniso_rhs) { c->ch_gx = ch; c->ch_gy = ch + 1; ch += 2; }
+    c->ch_dx = c->ch_dy = -1;
+    c->ncl_half = 0;
+    if (p.closure) {
+        c->ncl_half = p.mhd ? 6 : 3;
+        c->ch_dx = ch; ch += c->ncl_half;
+        c->ch_dy = ch; ch += c->ncl_half;
+    }
+    c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
     c->nin = ch;
     int oc = 0;
     c->out_T = c->out_E = c->out_F = c->out_Q = -1;
@@ -1063,6 +1109,10 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars) * nb, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
+    if (c->p.closure) {
+        CK(cudaMalloc(&c->d_cparams, sizeof(float) * CL_NP));
+        CK(cudaMemset(c->d_cparams, 0, sizeof(float) * CL_NP));
+    }
     return SPK_OK;
 }
 
@@ -1071,6 +1121,7 @@ static void ctx_free(spk_ctx* c) {
     cudaFree(c->d_tab); cudaFree(c->d_tw); cudaFree(c->U); cudaFree(c->S);
     cudaFree(c->bufA); cudaFree(c->bufB); cudaFree(c->rA); cudaFree(c->rB); cudaFree(c->breal);
     cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
+    cudaFree(c->d_cparams);
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->h_sums) cudaFreeHost(c->h_sums);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -1185,9 +1236,16 @@ extern "C" int spk_compute_dt(spk_ctx* c, double* dt_hyp, double* dt_par, double
     if (!c) return SPK_ERR_ARG;
     if (c->p.incompressible) {
         k_reset_max<<<1, 32, 0, c->stream>>>(c->sc);
-        pass_x_inverse(c, c->U, false);
-        pass_y_inverse(c, false);
-        pass_z_inverse_only(c, true, c->sts_aniso);
+        if (c->closure_on) {
+            // the closure's maxima come from the products pass
+            pass_x_inverse(c, c->U, true);
+            pass_y_inverse(c, true);
+            pass_z_products(c, true);
+        } else {
+            pass_x_inverse(c, c->U, false);
+            pass_y_inverse(c, false);
+            pass_z_inverse_only(c, true, c->sts_aniso);
+        }
     }
     DtArgs d = dt_args(c, false);
     k_dt<<<1, 32, 0, c->stream>>>(d, c->sc);
@@ -1343,7 +1401,7 @@ static bool same_group(const spk_params_t& a, const spk_params_t& b) {
            a.cfl_par == b.cfl_par && a.cfl_sts == b.cfl_sts && a.safety_source == b.safety_source &&
            a.safety_sts == b.safety_sts && a.t_initial == b.t_initial && a.t_final == b.t_final &&
            a.toutput_flow == b.toutput_flow && a.fixed_dt == b.fixed_dt && a.integrator == b.integrator &&
-           a.sts_every_step == b.sts_every_step && a.form == b.form;
+           a.sts_every_step == b.sts_every_step && a.form == b.form && a.closure == b.closure;
 }
 
 // A context for nb boxes of one geometry (nu, nu_m, nu_th per box).
@@ -1415,6 +1473,9 @@ extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cu
     *out = nullptr;
     for (int i = 0; i < nbox; i++) {
         const spk_params_t& p = boxes[i];
+        if (p.closure)
+            return ens_fail("ensemble box " + std::to_string(i) + ": the learned closure is not supported in ensembles",
+                            SPK_ERR_UNSUPPORTED);
         if (p.supertimestepping && !p.sts_every_step)
             return ens_fail("ensemble box " + std::to_string(i) +
                                 ": super-time-stepping that alternates between steps is not supported in ensembles",
@@ -1834,3 +1895,5 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
     if (rc != SPK_OK) g_create_error = c->err;
     return rc;
 }
+
+#include "spk_closure_api.cu"

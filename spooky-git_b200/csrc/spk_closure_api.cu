@@ -1,0 +1,298 @@
+// spk_closure_api.cu -- C ABI of the learned subgrid closure
+// (include/spooky_b200.h, SPK_CLOSURE_*): weights into a context, spectral
+// products, training samples from a fine-grid state, and the trainer.
+// Included at the end of spk_api.cu (one translation unit).
+
+extern "C" int spk_closure_set(spk_ctx* c, const float* params) {
+    if (!c) return SPK_ERR_ARG;
+    if (!c->p.closure) return fail(c, SPK_ERR_UNSUPPORTED, "the context was created without params.closure");
+    if (params) {
+        CK(cudaMemcpyAsync(c->d_cparams, params, sizeof(float) * CL_NP, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    const bool on = params != nullptr;
+    if (on != c->closure_on) {
+        // the step graphs hold the pass layout: record them again
+        for (int i = 0; i < 2; i++)
+            if (c->have_graph[i]) { cudaGraphExecDestroy(c->gexec[i]); c->have_graph[i] = false; }
+        c->closure_on = on;
+    }
+    return SPK_OK;
+}
+
+extern "C" int spk_products(spk_ctx* c, const double* U, double* P, int* nprod) {
+    if (!c || !U || !P) return SPK_ERR_ARG;
+    if (!c->p.incompressible || c->p.boussinesq || c->nb != 1)
+        return fail(c, SPK_ERR_UNSUPPORTED, "spk_products covers single HD and MHD contexts");
+    const int np = c->p.mhd ? 8 : 5;
+    c->user_U = U;
+    pass_x_inverse(c, (const double2*)U, true);
+    c->user_U = nullptr;
+    pass_y_inverse(c, true);
+    pass_z_products(c, false);
+    pass_y_forward(c, c->nout, c->bufA, c->bufB);
+    pass_x_forward(c);
+    const void* nl = chan(c, c->bufA, c->out_T);
+    const int grid = ew_blocks(c->nc * np);
+    c->launches++;
+    if (c->fp32) k_products_out<float><<<grid, 256, 0, c->stream>>>(c->g, (const C2<float>*)nl, np, (double2*)P);
+    else k_products_out<double><<<grid, 256, 0, c->stream>>>(c->g, (const C2<double>*)nl, np, (double2*)P);
+    if (nprod) *nprod = np;
+    return launch_status(c);
+}
+
+// Real fields R[nch][nr] (FP64) of nch spectral channels X[nch][Nc] in the
+// state layout: x and y inverse passes and the z to-real pass, F channels at
+// a time.  X must hold a multiple of F channels (the tensor map of each
+// chunk spans F channels; only the chunk's own are read).
+static int c2r_channels(spk_ctx* c, const double2* X, int nch, double* R) {
+    for (int c0 = 0; c0 < nch; c0 += c->F) {
+        const int m = std::min(c->F, nch - c0);
+        c->user_U = X + (size_t)c0 * c->nc;
+        AxisArgs a = axis_args(c, 0);
+        a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);
+        add_job(c, a, c->user_U, c->bufA, m, 1, 0, 0);
+        axis(c, a, +1);
+        c->user_U = nullptr;
+        AxisArgs b = axis_args(c, 1);
+        add_job(c, b, c->bufA, c->bufB, m, 0, 0, 0);
+        axis(c, b, +1);
+        ZArgs z = z_args(c);
+        z.mode = ZM_TO_REAL;
+        z.nin = m;
+        z.real_out = R + (size_t)c0 * c->nr;
+        zpass(c, z);
+        if (c->sticky) break;
+    }
+    return launch_status(c);
+}
+
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+static int pad_to(int n, int F) { return ((n + F - 1) / F) * F; }
+
+struct SampleScratch { size_t pf, pt, pc, gs, rt, rg, total; };
+static SampleScratch sample_scratch(const spk_ctx* f, const spk_ctx* c) {
+    const int np = c->p.mhd ? 8 : 5;
+    SampleScratch s;
+    s.pf = 0;
+    s.pt = s.pf + al256(sizeof(double2) * f->nc * np);
+    s.pc = s.pt + al256(sizeof(double2) * c->nc * pad_to(np, c->F));
+    s.gs = s.pc + al256(sizeof(double2) * c->nc * np);
+    s.rt = s.gs + al256(sizeof(double2) * c->nc * pad_to(18, c->F));
+    s.rg = s.rt + al256(sizeof(double) * c->nr * np);
+    s.total = s.rg + al256(sizeof(double) * c->nr * 18);
+    return s;
+}
+
+static const char* samples_mismatch(const spk_ctx* f, const spk_ctx* c) {
+    if (!f->p.incompressible || !c->p.incompressible || f->p.boussinesq || c->p.boussinesq)
+        return "closure samples need HD or MHD contexts";
+    if (f->p.mhd != c->p.mhd) return "the fine and coarse contexts differ in their modules";
+    if (f->nb != 1 || c->nb != 1) return "closure samples need single-box contexts";
+    if (f->p.lx != c->p.lx || f->p.ly != c->p.ly || f->p.lz != c->p.lz) return "the contexts have different boxes";
+    if (c->nx > f->nx || c->ny > f->ny || c->nz > f->nz) return "the coarse grid is finer than the fine grid";
+    return nullptr;
+}
+
+extern "C" int spk_closure_samples_size(const spk_ctx* f, const spk_ctx* c, size_t* bytes, size_t* ns) {
+    if (!f || !c) return fail(nullptr, SPK_ERR_ARG, "null context");
+    if (const char* why = samples_mismatch(f, c)) return fail(nullptr, SPK_ERR_UNSUPPORTED, why);
+    if (bytes) *bytes = sample_scratch(f, c).total;
+    if (ns) *ns = c->nr;
+    return SPK_OK;
+}
+
+extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, float* X, size_t stride, void* scratch,
+                                   size_t scratch_bytes) {
+    if (!f || !c || !Uf || !X || !scratch) return SPK_ERR_ARG;
+    if (const char* why = samples_mismatch(f, c)) return fail(c, SPK_ERR_UNSUPPORTED, why);
+    const SampleScratch sl = sample_scratch(f, c);
+    if (scratch_bytes < sl.total) return fail(c, SPK_ERR_ARG, "scratch smaller than spk_closure_samples_size");
+    if (stride < c->nr) return fail(c, SPK_ERR_ARG, "sample row stride below the coarse point count");
+    char* base = (char*)scratch;
+    double2* Pf = (double2*)(base + sl.pf);
+    double2* Pt = (double2*)(base + sl.pt);
+    double2* Pc = (double2*)(base + sl.pc);
+    double2* Gs = (double2*)(base + sl.gs);
+    double* Rt = (double*)(base + sl.rt);
+    double* Rg = (double*)(base + sl.rg);
+    const int np = c->p.mhd ? 8 : 5;
+    // products of the fine state (without the closure)
+    const bool fon = f->closure_on;
+    f->closure_on = false;
+    int rc = spk_products(f, Uf, (double*)Pf, nullptr);
+    f->closure_on = fon;
+    if (rc) return fail(c, rc, f->err);
+    CK(cudaStreamSynchronize(f->stream));
+    // the filtered state into the coarse context; the filtered products
+    TruncArgs t;
+    t.fnx = f->nx; t.fny = f->ny; t.fnzh = f->nzh;
+    t.cnx = c->nx; t.cny = c->ny; t.cnzh = c->nzh;
+    t.mx = c->g.mx; t.my = c->g.my; t.mz = c->g.mz;
+    t.scale = (double)c->nr / (double)f->nr;
+    t.src = (const double2*)Uf; t.dst = c->U; t.nch = c->F;
+    k_truncate<<<ew_blocks(c->nc * c->F), 256, 0, c->stream>>>(t);
+    t.src = Pf; t.dst = Pt; t.nch = np;
+    k_truncate<<<ew_blocks(c->nc * np), 256, 0, c->stream>>>(t);
+    c->launches += 2;
+    c->dirty = true;
+    // products of the filtered state on the coarse grid (without the closure)
+    const bool con = c->closure_on;
+    c->closure_on = false;
+    rc = spk_products(c, (const double*)c->U, (double*)Pc, nullptr);
+    c->closure_on = con;
+    if (rc) return rc;
+    k_sub<<<ew_blocks(c->nc * np), 256, 0, c->stream>>>(Pt, Pc, c->nc * np);
+    c->launches++;
+    rc = c2r_channels(c, Pt, np, Rt);
+    if (rc) return rc;
+    // gradients of the filtered state
+    CK(cudaMemsetAsync(Gs, 0, sizeof(double2) * c->nc * 18, c->stream));
+    k_gradients<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->VEL, c->MAG, c->p.mhd ? 2 : 1, Gs);
+    c->launches++;
+    rc = c2r_channels(c, Gs, 18, Rg);
+    if (rc) return rc;
+    k_closure_rows<<<ew_blocks(c->nr), 256, 0, c->stream>>>(Rg, Rt, np, c->nr, c->delta2, X, stride);
+    c->launches++;
+    return launch_status(c);
+}
+
+// ---------------------------------------------------------------------------
+// trainer
+// ---------------------------------------------------------------------------
+#define SPK_TRAIN_HIST 65536
+
+struct spk_trainer {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    float *params = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *partial = nullptr;
+    float *hist = nullptr, *h_hist = nullptr;
+    const float* X = nullptr;
+    size_t n = 0, stride = 0;
+    float w0 = 1.f, w1 = 1.f;
+    int t = 0;                       // Adam steps taken
+    unsigned long long cursor = 0;   // samples drawn so far
+};
+
+static size_t grad_smem() { return sizeof(float) * (((CL_NP + 3) & ~3) + (size_t)CL_ROWS * CL_LDS); }
+
+#define TCK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return fail(nullptr, SPK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int spk_trainer_create(void* stream, spk_trainer** out) {
+    if (!out) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    *out = nullptr;
+    spk_trainer* tr = new spk_trainer();
+    auto bail = [&](int rc) { spk_trainer_destroy(tr); return rc; };
+    if (stream) tr->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(nullptr, SPK_ERR_CUDA, "stream creation failed"));
+        tr->own_stream = true;
+    }
+    if (cudaMalloc(&tr->params, sizeof(float) * CL_NP) != cudaSuccess ||
+        cudaMalloc(&tr->m, sizeof(float) * CL_NP) != cudaSuccess ||
+        cudaMalloc(&tr->v, sizeof(float) * CL_NP) != cudaSuccess ||
+        cudaMalloc(&tr->grad, sizeof(float) * CL_NP) != cudaSuccess ||
+        cudaMalloc(&tr->partial, sizeof(float) * (size_t)CL_MAXBLK * (CL_NP + 1)) != cudaSuccess ||
+        cudaMalloc(&tr->hist, sizeof(float) * SPK_TRAIN_HIST) != cudaSuccess ||
+        cudaMallocHost(&tr->h_hist, sizeof(float) * SPK_TRAIN_HIST) != cudaSuccess)
+        return bail(fail(nullptr, SPK_ERR_ALLOC, "trainer allocation failed"));
+    cudaMemset(tr->params, 0, sizeof(float) * CL_NP);
+    cudaMemset(tr->m, 0, sizeof(float) * CL_NP);
+    cudaMemset(tr->v, 0, sizeof(float) * CL_NP);
+    if (cudaFuncSetAttribute(k_closure_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem()) != cudaSuccess)
+        return bail(fail(nullptr, SPK_ERR_CUDA, "shared-memory opt-in of the gradient kernel failed"));
+    *out = tr;
+    return SPK_OK;
+}
+
+extern "C" int spk_trainer_destroy(spk_trainer* tr) {
+    if (!tr) return SPK_OK;
+    cudaFree(tr->params); cudaFree(tr->m); cudaFree(tr->v); cudaFree(tr->grad); cudaFree(tr->partial);
+    cudaFree(tr->hist);
+    if (tr->h_hist) cudaFreeHost(tr->h_hist);
+    if (tr->own_stream) cudaStreamDestroy(tr->stream);
+    delete tr;
+    return SPK_OK;
+}
+
+extern "C" int spk_trainer_set_params(spk_trainer* tr, const float* params) {
+    if (!tr || !params) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    TCK(cudaMemcpyAsync(tr->params, params, sizeof(float) * CL_NP, cudaMemcpyHostToDevice, tr->stream));
+    TCK(cudaMemsetAsync(tr->m, 0, sizeof(float) * CL_NP, tr->stream));
+    TCK(cudaMemsetAsync(tr->v, 0, sizeof(float) * CL_NP, tr->stream));
+    TCK(cudaStreamSynchronize(tr->stream));
+    tr->t = 0;
+    return SPK_OK;
+}
+
+extern "C" int spk_trainer_get_params(spk_trainer* tr, float* params) {
+    if (!tr || !params) return fail(nullptr, SPK_ERR_ARG, "null argument");
+    TCK(cudaMemcpyAsync(params, tr->params, sizeof(float) * CL_NP, cudaMemcpyDeviceToHost, tr->stream));
+    TCK(cudaStreamSynchronize(tr->stream));
+    return SPK_OK;
+}
+
+extern "C" int spk_trainer_set_samples(spk_trainer* tr, const float* X, size_t n, size_t stride, const float w[2]) {
+    if (!tr || !X || n == 0 || stride < n || !w) return fail(nullptr, SPK_ERR_ARG, "bad samples");
+    tr->X = X; tr->n = n; tr->stride = stride; tr->w0 = w[0]; tr->w1 = w[1];
+    tr->cursor = 0;
+    return SPK_OK;
+}
+
+// one gradient evaluation over m samples (minibatch: drawn from the cursor)
+static void trainer_grad(spk_trainer* tr, size_t m, bool minibatch, float* loss_out) {
+    TrainArgs a;
+    a.X = tr->X; a.n = tr->n; a.stride = tr->stride; a.m = m;
+    a.minibatch = minibatch ? 1 : 0;
+    // a multiplier coprime with n: consecutive draws walk the samples in a scattered order
+    unsigned long long mult = tr->n > 2 ? ((unsigned long long)((double)tr->n * 0.6180339887498949) | 1ull) : 1ull;
+    auto gcd = [](unsigned long long x, unsigned long long y) { while (y) { unsigned long long r = x % y; x = y; y = r; } return x; };
+    while (tr->n > 2 && gcd(mult, tr->n) != 1) mult += 2;
+    a.a = mult % (tr->n > 0 ? tr->n : 1);
+    a.c = tr->n / 3;
+    a.base = tr->cursor;
+    a.params = tr->params; a.w0 = tr->w0; a.w1 = tr->w1;
+    a.partial = tr->partial;
+    const int nblk = (int)std::min<size_t>(CL_MAXBLK, (m + CL_CHUNK - 1) / CL_CHUNK);
+    k_closure_grad<<<nblk, CL_CHUNK, grad_smem(), tr->stream>>>(a);
+    k_closure_reduce<<<(CL_NP + 1 + 127) / 128, 128, 0, tr->stream>>>(tr->partial, nblk, 1.0 / (double)m, tr->grad,
+                                                                        loss_out);
+}
+
+extern "C" int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad) {
+    if (!tr || !tr->X) return fail(nullptr, SPK_ERR_ARG, "trainer without samples");
+    trainer_grad(tr, tr->n, false, tr->hist);
+    TCK(cudaGetLastError());
+    if (grad) TCK(cudaMemcpyAsync(grad, tr->grad, sizeof(float) * CL_NP, cudaMemcpyDeviceToHost, tr->stream));
+    TCK(cudaMemcpyAsync(tr->h_hist, tr->hist, sizeof(float), cudaMemcpyDeviceToHost, tr->stream));
+    TCK(cudaStreamSynchronize(tr->stream));
+    if (loss) *loss = tr->h_hist[0];
+    return SPK_OK;
+}
+
+extern "C" int spk_trainer_train(spk_trainer* tr, int nsteps, int batch, float lr, float* loss_hist) {
+    if (!tr || !tr->X || nsteps < 0 || batch < 1) return fail(nullptr, SPK_ERR_ARG, "bad training request");
+    for (int done = 0; done < nsteps;) {
+        const int k = std::min(nsteps - done, SPK_TRAIN_HIST);
+        for (int i = 0; i < k; i++) {
+            trainer_grad(tr, (size_t)batch, true, tr->hist + i);
+            tr->t++;
+            tr->cursor += (unsigned long long)batch;
+            k_closure_adam<<<(CL_NP + 255) / 256, 256, 0, tr->stream>>>(tr->params, tr->grad, tr->m, tr->v, tr->t, lr);
+        }
+        TCK(cudaGetLastError());
+        if (loss_hist) {
+            TCK(cudaMemcpyAsync(tr->h_hist, tr->hist, sizeof(float) * k, cudaMemcpyDeviceToHost, tr->stream));
+            TCK(cudaStreamSynchronize(tr->stream));
+            memcpy(loss_hist + done, tr->h_hist, sizeof(float) * k);
+        }
+        done += k;
+    }
+    TCK(cudaStreamSynchronize(tr->stream));
+    return SPK_OK;
+}

@@ -193,6 +193,12 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
             gamma_tmp = kzmax * kzmax * nu_m;
             if (!in_sts(a.BZ)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         }
+        if (a.closure) {
+            // the learned closure's eddy viscosity and resistivity as parabolic rates
+            const double k2 = kxmax * kxmax + kymax * kymax + kzmax * kzmax;
+            gamma_par += k2 * __longlong_as_double((long long)sc->maxbits[6]);
+            if (a.mhd) gamma_par += k2 * __longlong_as_double((long long)sc->maxbits[7]);
+        }
         dt_hyp = a.cfl / (gamma_v + gamma_th + gamma_b);
         dt_par = a.cfl_par / gamma_par;
         dt_sts = a.cfl_sts / gamma_sts;

@@ -66,7 +66,7 @@ enum { STS_ALG_STS = 1, STS_ALG_RKL1 = 2, STS_ALG_RKL2 = 3 };
 // Device-resident step scalars (written by k_dt, read by every update pass).
 struct DevScalars {
     double t, dt, dt_hyp, dt_par, dt_sts, t_lastsnap;
-    unsigned long long maxbits[8];  // bit patterns of max |ux| |uy| |uz| |bx| |by| |bz|
+    unsigned long long maxbits[8];  // bit patterns of max |ux| |uy| |uz| |bx| |by| |bz| nu_t eta_t
     int step, s_rkl, err, nonfinite;
     // stage j of the super-time-stepping cycle: U <- c0 U + c1 U1 + c2 dU + c3 dU0 + c4 U0
     // (RKL2: mu, nu, dt*mu~, dt*gamma, 1-mu-nu; RKL1: mu, nu, dt*mu~;
@@ -181,6 +181,13 @@ struct ZArgs {
     int nb;                 // boxes side by side: line index = box * nx*ny + line
     size_t in_box, out_box; // element offsets between boxes in `in` and `out`
     DevScalars* scs;        // per-box scalars (CFL maxima, non-finite flag)
+    // learned closure: input channels ch_dx (d/dx of u [and B]) and ch_dy
+    // (d/dy); d/dz derived in the pass from channels zder_src[] (appended
+    // after the inputs); MLP parameters (SPK_CLOSURE_NPARAM floats)
+    int closure, ch_dx, ch_dy;
+    int zder_n, zder_src[6];
+    const float* cparams;
+    float delta2;
 };
 
 enum XMode { XM_RK0 = 0, XM_RK1 = 1, XM_RK2 = 2, XM_EULER = 3, XM_DFIELD = 4 };
@@ -230,6 +237,7 @@ struct DtArgs {
     int advance;             // 1: t += dt, step += 1
     int rkl_smax;
     int sts_alg;             // STS_ALG_*
+    int closure;             // add the closure's max eddy viscosity / resistivity (maxbits[6], [7])
 };
 
 }  // namespace spk

@@ -12,6 +12,7 @@
 // exchange per further stage, and stores X[k] from registers to the pass
 // buffer (kept ky rows only in the y-forward pass).
 #include "spk_regfft.cuh"
+#include "spk_closure.cuh"
 
 namespace spk {
 
@@ -182,9 +183,9 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
 // Shared-memory carve of k_zpass2 (host and device agree through this):
 // barrier, twiddle tables, input half spectra (later: the product pairs),
 // real fields, exchange slots.
-struct ZSmem { size_t tw, zero, junk, area, real, xb, total; };
+struct ZSmem { size_t tw, zero, junk, area, real, xb, cw, total; };
 __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
-                                              int nzs, int slots) {
+                                              int nzs, int slots, int ncw) {
     ZSmem z;
     const int rs = n + 16, xs = n + (n >> 4);
     z.tw = 128;
@@ -194,7 +195,8 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     const size_t raw = (size_t)nin * lines * nzs * csz, prod = (size_t)npout * lines * n * csz;
     z.real = align16(z.area + (raw > prod ? raw : prod));
     z.xb = align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
-    z.total = align16(z.xb + (size_t)slots * xs * csz);
+    z.cw = align16(z.xb + (size_t)slots * xs * csz);         // closure MLP parameters (floats)
+    z.total = align16(z.cw + (size_t)ncw * sizeof(float));
     return z;
 }
 
@@ -216,12 +218,14 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     const int line0 = (blockIdx.x - box * blocks_per_box) * L;
     const int nl = min(L, nlines - line0);
     const int nin = a.nin;
-    const int nin_all = nin + (a.derive_gz == 1 ? 1 : 0);
+    const int nder0 = nin + (a.derive_gz == 1 ? 1 : 0);   // first closure d/dz channel
+    const int nin_all = nder0 + (GEN ? a.zder_n : 0);
     const int npin = (nin_all + 1) / 2, npout = (a.nout + 1) / 2;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
-    const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots);
+    const bool clos = GEN && a.closure;
+    const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots, clos ? CL_NP : 0);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
     C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
@@ -230,6 +234,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     C2<T>* prod = raw;                    // the product pairs reuse the input area
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
+    float* cw = reinterpret_cast<float*>(smem_raw + lay.cw);
+    if (clos)
+        for (int i = tid; i < CL_NP; i += nthr) cw[i] = a.cparams[i];   // visible after the next barrier
     const C2<T>* in = (const C2<T>*)a.in + (size_t)box * a.in_box;
     DevScalars* bsc = a.scs + box;
     const int LRS = L * RS;
@@ -284,6 +291,11 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
                 const T kz = (T)a.g.kz[k];
                 return mk<T>(-kz * th.y, kz * th.x);
             }
+            if (ch >= nder0 && ch < nin_all) {   // closure: d/dz of u [and B]
+                const C2<T> x = raw[((size_t)a.zder_src[ch - nder0] * L + l) * nzs + k];
+                const T kz = (T)a.g.kz[k];
+                return mk<T>(-kz * x.y, kz * x.x);
+            }
             return mk<T>((T)0, (T)0);
         };
         regfft_load<T, N, +1>(r, q, [&](int n) -> C2<T> {
@@ -323,7 +335,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     T* breal = (T*)a.breal;
     const bool want_prod = a.nout > 0;
     {
-        T mu[6] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
+        T mu[8] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
         int bad = 0;
         T* prodT = reinterpret_cast<T*>(prod);
         const T third = (T)(1.0 / 3.0);
@@ -366,6 +378,26 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             T* pp = prodT + ((size_t)l * N + z) * 2;
             auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1)] = v; };
             int qc = 0;
+            // learned closure: -2 nu_t S into the stress, -eta_t J into the EMF
+            float ctau[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, cemf[3] = {0.f, 0.f, 0.f};
+            if (clos) {
+                float A[9], G[9], vn, ve;
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    A[3 * i + 0] = (float)fr[(a.ch_dx + i) * LRS];
+                    A[3 * i + 1] = (float)fr[(a.ch_dy + i) * LRS];
+                    A[3 * i + 2] = (float)fr[(nder0 + i) * LRS];
+                    G[3 * i + 0] = a.mhd ? (float)fr[(a.ch_dx + 3 + i) * LRS] : 0.f;
+                    G[3 * i + 1] = a.mhd ? (float)fr[(a.ch_dy + 3 + i) * LRS] : 0.f;
+                    G[3 * i + 2] = a.mhd ? (float)fr[(nder0 + 3 + i) * LRS] : 0.f;
+                }
+                closure_point(cw, a.delta2, A, G, ctau, cemf, &vn, &ve);
+                if (live && a.do_max) {
+                    if (!isfinite(vn) || !isfinite(ve)) bad = 1;
+                    mu[6] = fmax(mu[6], (T)vn);
+                    mu[7] = fmax(mu[7], (T)(a.mhd ? ve : 0.f));
+                }
+            }
             if (a.mode == ZM_PRODUCTS) {
                 if (a.hydro) {
                     if (!a.mhd) {
@@ -381,12 +413,15 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
                         put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) * third);
                         put(4, uy * uz - by * bz);
                     }
+                    if (clos)
+#pragma unroll
+                        for (int r = 0; r < 5; r++) pp[(size_t)(r >> 1) * pstride + (r & 1)] += (T)ctau[r];
                     qc = 5;
                 }
                 if (a.mhd) {
-                    put(qc, -by * uz + bz * uy);
-                    put(qc + 1, bx * uz - bz * ux);
-                    put(qc + 2, -bx * uy + by * ux);
+                    put(qc, -by * uz + bz * uy + (T)cemf[0]);
+                    put(qc + 1, bx * uz - bz * ux + (T)cemf[1]);
+                    put(qc + 2, -bx * uy + by * ux + (T)cemf[2]);
                     qc += 3;
                 }
                 if (a.bous) {
@@ -409,8 +444,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         if (a.do_max) {
             // the exchange slots are free here: 6 x 32 block-max scratch
             T* red = reinterpret_cast<T*>(xb);
-            warp_block_max<T>(mu, 6, red);
-            if (tid < 6) {
+            const int nmax = clos ? 8 : 6;
+            warp_block_max<T>(mu, nmax, red);
+            if (tid < nmax) {
                 const double m = (double)red[tid * 32];
                 const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
                 unsigned long long* dst = bsc->maxbits + tid;

@@ -35,7 +35,14 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_compute_dfield_noalloc", "spk_params_from_file", "spk_params_from_string",
             "spk_ensemble_create", "spk_ensemble_destroy", "spk_ensemble_size", "spk_ensemble_set_state",
             "spk_ensemble_get_state", "spk_ensemble_get_time", "spk_ensemble_budgets", "spk_ensemble_advance",
-            "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step"]
+            "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step",
+            "spk_closure_set", "spk_products", "spk_closure_samples_size", "spk_closure_samples",
+            "spk_trainer_create", "spk_trainer_destroy", "spk_trainer_set_params", "spk_trainer_get_params",
+            "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train"]
+
+# learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
+CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
+CLOSURE_ROWS = 25
 
 
 class Budgets(ctypes.Structure):
@@ -97,6 +104,18 @@ def lib():
         L.spk_ensemble_advance.argtypes = [vp, ctypes.c_int]
         L.spk_ensemble_synchronize.argtypes = [vp]
         L.spk_ensemble_kernels_per_step.argtypes = [vp, ip]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.spk_closure_set.argtypes = [vp, fp]
+        L.spk_products.argtypes = [vp, vp, vp, ip]
+        L.spk_closure_samples_size.argtypes = [vp, vp, ctypes.POINTER(sp), ctypes.POINTER(sp)]
+        L.spk_closure_samples.argtypes = [vp, vp, vp, vp, sp, vp, sp]
+        L.spk_trainer_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.spk_trainer_destroy.argtypes = [vp]
+        L.spk_trainer_set_params.argtypes = [vp, fp]
+        L.spk_trainer_get_params.argtypes = [vp, fp]
+        L.spk_trainer_set_samples.argtypes = [vp, vp, sp, sp, fp]
+        L.spk_trainer_loss_grad.argtypes = [vp, fp, fp]
+        L.spk_trainer_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -288,6 +307,109 @@ class Context:
         b = Budgets()
         self._check(lib().spk_budgets(self._h, ctypes.byref(b)))
         return np.array(b.energy[: self.F]), np.array(b.dissipation[: self.F])
+
+    # -- learned closure -----------------------------------------------------
+    def closure_set(self, params):
+        """Closure weights (CLOSURE_NPARAM floats) into the RHS, or None: off."""
+        if params is None:
+            self._check(lib().spk_closure_set(self._h, None))
+            return
+        w = np.ascontiguousarray(params, dtype=np.float32)
+        assert w.size == CLOSURE_NPARAM
+        self._check(lib().spk_closure_set(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def products(self, U):
+        """Spectral products of the torch CUDA complex128 state U (shape_c):
+        a torch complex128 tensor [nprod, nx, ny, nz//2+1] (spk_products)."""
+        import torch
+        p = self.params
+        P = torch.zeros((8, p.nx, p.ny, p.nz // 2 + 1), dtype=torch.complex128, device=U.device)
+        n = ctypes.c_int()
+        _torch_sync()
+        self._check(lib().spk_products(self._h, U.data_ptr(), P.data_ptr(), ctypes.byref(n)))
+        self.synchronize()
+        return P[: n.value]
+
+
+def closure_samples(fine, Uf, coarse):
+    """Training samples of the closure from the fine context's state Uf (a
+    torch CUDA complex128 tensor): a torch float32 tensor [CLOSURE_ROWS,
+    coarse nx*ny*nz] (spk_closure_samples); coarse's state becomes the
+    filtered state."""
+    import torch
+    nbytes, ns = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = lib().spk_closure_samples_size(fine._h, coarse._h, ctypes.byref(nbytes), ctypes.byref(ns))
+    if rc != SPK_OK:
+        raise SpookyError(rc, lib().spk_last_error(None).decode())
+    scratch = torch.empty(nbytes.value, dtype=torch.uint8, device=Uf.device)
+    X = torch.empty((CLOSURE_ROWS, ns.value), dtype=torch.float32, device=Uf.device)
+    _torch_sync()
+    coarse._check(lib().spk_closure_samples(fine._h, Uf.data_ptr(), coarse._h, X.data_ptr(), ns.value,
+                                            scratch.data_ptr(), nbytes.value))
+    coarse.synchronize()
+    return X
+
+
+class Trainer:
+    """spk_trainer: the closure MLP trained on device samples by the
+    library's own forward/backward and Adam kernels."""
+
+    def __init__(self, params=None, stream=None):
+        h = ctypes.c_void_p()
+        rc = lib().spk_trainer_create(stream, ctypes.byref(h))
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(None).decode())
+        self._h = h
+        self._X = None
+        if params is not None:
+            self.set_params(params)
+
+    def _check(self, rc):
+        if rc != SPK_OK:
+            raise SpookyError(rc, lib().spk_last_error(None).decode())
+
+    @staticmethod
+    def _fp(a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+    def set_params(self, params):
+        w = np.ascontiguousarray(params, dtype=np.float32)
+        assert w.size == CLOSURE_NPARAM
+        self._check(lib().spk_trainer_set_params(self._h, self._fp(w)))
+
+    def get_params(self):
+        w = np.empty(CLOSURE_NPARAM, np.float32)
+        self._check(lib().spk_trainer_get_params(self._h, self._fp(w)))
+        return w
+
+    def set_samples(self, X, weights):
+        """X: torch CUDA float32 [CLOSURE_ROWS, n] (kept referenced here)."""
+        _torch_sync()
+        self._X = X
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(lib().spk_trainer_set_samples(self._h, X.data_ptr(), X.shape[1], X.stride(0), self._fp(w)))
+
+    def loss_grad(self):
+        loss = np.zeros(1, np.float32)
+        g = np.empty(CLOSURE_NPARAM, np.float32)
+        self._check(lib().spk_trainer_loss_grad(self._h, self._fp(loss), self._fp(g)))
+        return float(loss[0]), g
+
+    def train(self, nsteps, batch, lr):
+        hist = np.empty(max(int(nsteps), 1), np.float32)
+        self._check(lib().spk_trainer_train(self._h, int(nsteps), int(batch), float(lr), self._fp(hist)))
+        return hist[: int(nsteps)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().spk_trainer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

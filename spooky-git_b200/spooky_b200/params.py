@@ -39,6 +39,7 @@ class Params(ctypes.Structure):
         ("toutput_flow", ctypes.c_double),
         ("fixed_dt", ctypes.c_double), ("integrator", ctypes.c_int),
         ("sts_every_step", ctypes.c_int), ("form", ctypes.c_int),
+        ("closure", ctypes.c_int),
     ]
 
     def copy(self):
@@ -91,6 +92,7 @@ def default_params(**overrides):
     p.integrator = SPK_INT_RK3
     p.sts_every_step = 0
     p.form = SPK_FORM_PLAIN
+    p.closure = 0
     sts_vars = overrides.pop("sts_variables", None)
     if isinstance(overrides.get("sts_algorithm"), str):
         overrides["sts_algorithm"] = STS_ALGORITHMS[overrides["sts_algorithm"]]
