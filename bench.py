@@ -339,6 +339,39 @@ def run_mti(args, world, rank, local_rank):
         }), flush=True)
 
 
+def run_closure(args, world, rank, local_rank):
+    """The learned-closure configuration: a 256^3 MHD truth run (nu = eta =
+    2e-4, config-2 fields) in the plain form, closure samples every 250
+    steps, GPU training, and 64^3 runs with and without the closure to the
+    truth's final time; one JSON line with the spectral errors against the
+    filtered truth and the costs."""
+    import torch
+    from spooky_b200 import closure as C
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    nf, ncs = args.n, args.n // 4
+    r = C.run(n_fine=nf, n_coarse=ncs, steps=args.closure_steps, snap_every=max(args.closure_steps // 8, 1),
+              train_steps=3000, batch=16384, lr=2e-3, log=lambda m: print(m, file=sys.stderr, flush=True))
+    print(json.dumps({
+        "metric": f"{ncs}^3 learned-closure run vs filtered {nf}^3 truth: RMS relative shell-spectrum error",
+        "value": r["error_closure"], "unit": "relative error (shells 1..k_c)", "higher_is_better": False,
+        "n_gpus": 1, "vs_baseline": None, "dtype": "fp64 state, fp32 MLP", "data": "synthetic (seeded config-2 fields)",
+        "config": {"workload": f"MHD {nf}^3 truth (plain form, {args.closure_steps} steps, nu = eta = 2e-4) -> "
+                               f"{ncs}^3 closure run, sharp filter k_c = {r['k_cut']}",
+                   "train_steps": 3000, "batch": 16384},
+        "error_without_closure": r["error_plain"],
+        "error_u": {"closure": r["error_u_closure"], "plain": r["error_u_plain"]},
+        "error_b": {"closure": r["error_b_closure"], "plain": r["error_b_plain"]},
+        "energy": {"truth": r["energy_truth"], "closure": r["energy_closure"], "plain": r["energy_plain"]},
+        "t_end": r["t_end"], "truth_seconds": r["truth_seconds"], "closure_run_seconds": r["seconds_closure"],
+        "plain_coarse_run_seconds": r["seconds_plain"], "cost_advantage": r["cost_advantage"],
+        "train_seconds": r["train_seconds"], "loss": {"initial": r["loss_initial"], "final": r["loss_final"]},
+        "shell_spectra": {k: [float("%.5g" % v) for v in r["spectrum_" + k][: r["k_cut"] + 1]]
+                          for k in ("truth", "closure", "plain")},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,6 +385,9 @@ def main():
     ap.add_argument("--boxes", type=int, default=512)
     ap.add_argument("--mti", action="store_true",
                     help="config 3 instead: Boussinesq MHD + anisotropic conduction with RKL2 super-time-stepping")
+    ap.add_argument("--closure", action="store_true",
+                    help="learned-closure workload instead: --n truth, --n/4 closure run (config 5)")
+    ap.add_argument("--closure-steps", type=int, default=2000)
     ap.add_argument("--profile-run", action="store_true",
                     help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")
@@ -371,6 +407,9 @@ def main():
         return
     if args.mti:
         run_mti(args, world, rank, local_rank)
+        return
+    if args.closure:
+        run_closure(args, world, rank, local_rank)
         return
 
     import torch

@@ -348,12 +348,15 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     z.lines = L;
     const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
-    if (z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.zder_n > 0) {
-        cudaFuncSetAttribute(k_zpass2<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_zpass2<T, N, true><<<nblk, nthr, smem, c->stream>>>(z);
+    if (z.closure) {
+        cudaFuncSetAttribute(k_zpass2<T, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, N, 2><<<nblk, nthr, smem, c->stream>>>(z);
+    } else if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
+        cudaFuncSetAttribute(k_zpass2<T, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, N, 1><<<nblk, nthr, smem, c->stream>>>(z);
     } else {
-        cudaFuncSetAttribute(k_zpass2<T, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_zpass2<T, N, false><<<nblk, nthr, smem, c->stream>>>(z);
+        cudaFuncSetAttribute(k_zpass2<T, N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_zpass2<T, N, 0><<<nblk, nthr, smem, c->stream>>>(z);
     }
 }
 

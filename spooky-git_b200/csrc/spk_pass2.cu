@@ -200,9 +200,11 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     return z;
 }
 
-// GEN: derived gradient channels or the to-real output (the general path);
-// otherwise every input channel is a plain half spectrum.
-template <typename T, int N, bool GEN>
+// GEN: 0 -- every input channel is a plain half spectrum; 1 -- derived
+// gradient channels or the to-real output (the general path); 2 -- the
+// general path with the learned closure (its own instantiation, so that the
+// MLP's registers do not weigh on the others).
+template <typename T, int N, int GEN>
 __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, N>;
     constexpr int LTPC = F::LTPC, TPC = F::TPC;
@@ -219,12 +221,12 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     const int nl = min(L, nlines - line0);
     const int nin = a.nin;
     const int nder0 = nin + (a.derive_gz == 1 ? 1 : 0);   // first closure d/dz channel
-    const int nin_all = nder0 + (GEN ? a.zder_n : 0);
+    const int nin_all = nder0 + (GEN == 2 ? a.zder_n : 0);
     const int npin = (nin_all + 1) / 2, npout = (a.nout + 1) / 2;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
-    const bool clos = GEN && a.closure;
+    const bool clos = GEN == 2 && a.closure;
     const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots, clos ? CL_NP : 0);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             constexpr int NH = N >> 1;
             const int k = n <= NH ? n : N - n;
             C2<T> A, B;
-            if constexpr (!GEN) {
+            if constexpr (GEN == 0) {
                 A = pa[k];
                 B = pb[k];
             } else {
@@ -316,11 +318,11 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         // an idle transform (and the missing partner of an odd last pair) writes the junk row
         T* pr0 = valid ? real + (size_t)(2 * p * L + l) * RS : junk;
         T* pr1 = (valid && 2 * p + 1 < nin_all) ? pr0 + LRS : junk;
-        const bool to_real = GEN && a.mode == ZM_TO_REAL && valid && l < nl;
+        const bool to_real = GEN != 0 && a.mode == ZM_TO_REAL && valid && l < nl;
         regfft_run<T, N, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
             pr0[z] = v.x;
             pr1[z] = v.y;
-            if (GEN && to_real) {
+            if (GEN != 0 && to_real) {
                 const size_t line = (size_t)(line0 + l);
                 if (2 * p < nin) a.real_out[((size_t)(2 * p) * nlines + line) * N + z] = (double)v.x;
                 if (2 * p + 1 < nin) a.real_out[((size_t)(2 * p + 1) * nlines + line) * N + z] = (double)v.y;
