@@ -177,8 +177,12 @@ int spk_step_info(spk_ctx* ctx, int* kernels_per_step, double* bytes_per_step);
 /* Per-pass timing of one RK3 stage: each pass of stage 2 (no cleaning, no
  * dt reduction) is launched `reps` times between CUDA events on the context
  * stream.  out[i]: pass name, average ms per launch, algorithmic bytes per
- * launch.  The passes update the context state (stage-2 RK updates), so call
- * it on a context whose state may change.  No reference counterpart. */
+ * launch, launches per step.  With deferred masked modes (HD/MHD RK3: the
+ * RHS of stages 0-1 updates the kept modes only and stage 2 also moves the
+ * modes outside the 2/3 mask once) the stage-2 RHS ("rhs_rk", once per step)
+ * and the stage-1 RHS ("rhs_rk_01", twice) are reported apart.  The passes
+ * update the context state (stage updates), so call it on a context whose
+ * state may change.  No reference counterpart. */
 typedef struct spk_pass_stat {
     char   name[24];
     double ms;

@@ -63,6 +63,10 @@ struct spk_ctx {
     int nin_base;                  // u, B, theta channels (no gradient channels)
     // learned closure: d/dx and d/dy channels of u [and B] (ncl_half each),
     // parameters on the device, Delta^2; closure_on once weights are set
+    // deferred dealiased-out modes (HD/MHD RK3, no STS): kept x / y indices
+    bool defer = false;
+    int* d_keep = nullptr;
+    int nkx = 0, nky = 0;
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
     bool closure_on = false;
     float* d_cparams = nullptr;
@@ -242,7 +246,7 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
 }
 
 
-template <typename T, int N, int DIR, bool CONV>
+template <typename T, int N, int DIR, bool CONV, bool DEF = false>
 static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     constexpr int KT = axis_kt<T, N, CONV>();
     const int nthr = KT * RegFft<T, N>::TPC;
@@ -256,16 +260,26 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
     const size_t smem = fixed + (size_t)a.nst * stage;
-    cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV>, nthr, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV, DEF>, nthr, smem);
     const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
     c->launches++;
-    k_axis2<T, N, DIR, CONV><<<grid, nthr, smem, c->stream>>>(a);
+    k_axis2<T, N, DIR, CONV, DEF><<<grid, nthr, smem, c->stream>>>(a);
 }
 
 template <typename T, int N, int DIR>
 static void launch_axis_conv(spk_ctx* c, AxisArgs& a, long total) {
+    if constexpr (DIR > 0) {
+        if (a.defer_stage) {   // x inverse of a deferred stage: state input
+            if constexpr (sizeof(T) == 4) {
+                if (a.convert) { launch_axis_ln<T, N, DIR, true, true>(c, a, total); return; }
+            } else {
+                launch_axis_ln<T, N, DIR, false, true>(c, a, total);
+                return;
+            }
+        }
+    }
     if constexpr (sizeof(T) == 4 && DIR > 0) {
         if (a.convert) { launch_axis_ln<T, N, DIR, true>(c, a, total); return; }
     }
@@ -435,19 +449,31 @@ static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch,
     }
 }
 
-// first inverse pass over the state: fields in order, cleaning u and B when asked
-static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx) {
+// first inverse pass over the state: fields in order.  stage: the RK3 stage
+// (1 or 2 with deferred masked modes scales those modes to the stage's value)
+static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx, int stage = 0) {
     AxisArgs a = axis_args(c, 0);
     a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);   // scaleKernel factor
-    if (c->p.incompressible) add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_u), 3, 1, 0, 0);
-    if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, 0);
+    a.defer_stage = (c->defer && c->d_keep && U == c->U && (stage == 1 || stage == 2)) ? stage : 0;
+    a.scs = c->sc;
+    auto mark = [&](int first, int grp) {
+        for (int q = first; q < a.njobs; q++) a.job[q].defer_grp = grp;
+    };
+    if (c->p.incompressible) { const int j0 = a.njobs; add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_u), 3, 1, 0, 0); mark(j0, 1); }
+    if (c->p.mhd) { const int j0 = a.njobs; add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_b), 3, 1, 0, 0); mark(j0, 2); }
     if (c->p.boussinesq) {
         add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_th), 1, 1, 0, 0);
         if (with_gx && c->aniso_rhs) add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_gx), 1, 1, 1, 0);
     }
     if (with_gx && c->closure_on) {
+        int j0 = a.njobs;
         add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_dx), 3, 1, 1, 0);
-        if (c->p.mhd) add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_dx + 3), 3, 1, 1, 0);
+        mark(j0, 1);
+        if (c->p.mhd) {
+            j0 = a.njobs;
+            add_job(c, a, U + (size_t)c->MAG * c->nc, chan(c, c->bufA, c->ch_dx + 3), 3, 1, 1, 0);
+            mark(j0, 2);
+        }
     }
     axis(c, a, +1);
 }
@@ -554,10 +580,16 @@ static void pass_x_forward(spk_ctx* c) {
 static void rhs(spk_ctx* c, XfArgs& x) {
     const FastDiv fz = FastDiv::make((unsigned)c->nzh);
     // 128-thread CTAs, three per SM: every load of a mode is issued up front
-    const int grid = (int)std::min<size_t>((c->nc * c->nb + 127) / 128, (size_t)c->num_sms * 3 * 8);
+    const size_t modes = x.defer ? (size_t)x.nkx * x.nky * c->kz_keep : c->nc;
+    const int grid = (int)std::min<size_t>((modes * c->nb + 127) / 128, (size_t)c->num_sms * 3 * 8);
     c->launches++;
     if (c->fp32) k_rhs<float><<<grid, 128, 0, c->stream>>>(x, fz);
     else k_rhs<double><<<grid, 128, 0, c->stream>>>(x, fz);
+    if (x.defer && x.mode == XM_RK2) {
+        // the step's masked modes, once
+        c->launches++;
+        k_masked_rk<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(x, fz);
+    }
 }
 
 static void xfwd(spk_ctx* c, XfArgs& x) {
@@ -586,6 +618,14 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     x.nu = c->p.nu; x.nu_m = c->p.nu_m; x.nu_th = c->p.nu_th; x.N2 = c->p.N2;
     x.mode = mode; x.clean = clean ? 1 : 0;
     x.sc = c->sc;
+    x.defer = c->defer && c->d_keep && (mode == XM_RK0 || mode == XM_RK1 || mode == XM_RK2);
+    if (x.defer) {
+        x.kxi = c->d_keep; x.kyi = c->d_keep + c->nkx;
+        x.nkx = c->nkx; x.nky = c->nky;
+        x.fd_kzk = FastDiv::make((unsigned)c->kz_keep);
+        x.fd_nky = FastDiv::make((unsigned)c->nky);
+        x.fd_nkx = FastDiv::make((unsigned)c->nkx);
+    }
     return x;
 }
 
@@ -726,7 +766,7 @@ static void record_step(spk_ctx* c, int parity) {
     c->launches++;
     for (int s = 0; s < nst; s++) {
         const bool first = s == 0;
-        pass_x_inverse(c, c->U, true);
+        pass_x_inverse(c, c->U, true, euler ? 0 : s);
         pass_y_inverse(c, true);
         if (first) {
             if (sts_before) {
@@ -1000,6 +1040,11 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     }
     c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
     c->nin = ch;
+    c->nkx = c->nky = 0;
+    for (int i = 0; i < c->nx; i++) c->nkx += c->mx[i] != 0.0;
+    for (int j = 0; j < c->ny; j++) c->nky += c->my[j] != 0.0;
+    c->defer = p.incompressible && !p.boussinesq && c->sts_mask == 0 && p.integrator == SPK_INT_RK3 &&
+               c->nkx > 0 && c->nky > 0 && c->kz_keep > 0;
     int oc = 0;
     c->out_T = c->out_E = c->out_F = c->out_Q = -1;
     if (p.incompressible) { c->out_T = oc; oc += 5; }
@@ -1108,6 +1153,7 @@ static int ctx_alloc(spk_ctx* c) {
         c->h_sc[b].nu = c->bnu.empty() ? c->p.nu : c->bnu[b];
         c->h_sc[b].nu_m = c->bnu_m.empty() ? c->p.nu_m : c->bnu_m[b];
         c->h_sc[b].nu_th = c->bnu_th.empty() ? c->p.nu_th : c->bnu_th[b];
+        c->h_sc[b].masked_live = 1;
     }
     CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars) * nb, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
@@ -1115,6 +1161,13 @@ static int ctx_alloc(spk_ctx* c) {
     if (c->p.closure) {
         CK(cudaMalloc(&c->d_cparams, sizeof(float) * CL_NP));
         CK(cudaMemset(c->d_cparams, 0, sizeof(float) * CL_NP));
+    }
+    if (c->defer) {
+        std::vector<int> keep;
+        for (int i = 0; i < c->nx; i++) if (c->mx[i] != 0.0) keep.push_back(i);
+        for (int j = 0; j < c->ny; j++) if (c->my[j] != 0.0) keep.push_back(j);
+        CK(cudaMalloc(&c->d_keep, sizeof(int) * keep.size()));
+        CK(cudaMemcpy(c->d_keep, keep.data(), sizeof(int) * keep.size(), cudaMemcpyHostToDevice));
     }
     return SPK_OK;
 }
@@ -1125,6 +1178,7 @@ static void ctx_free(spk_ctx* c) {
     cudaFree(c->bufA); cudaFree(c->bufB); cudaFree(c->rA); cudaFree(c->rB); cudaFree(c->breal);
     cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
     cudaFree(c->d_cparams);
+    cudaFree(c->d_keep);
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->h_sums) cudaFreeHost(c->h_sums);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -1226,6 +1280,12 @@ static void launch_clean(spk_ctx* c) {
         k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc, bs, c->nb);
     if (c->p.mhd)
         k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc, bs, c->nb);
+    if (c->defer && c->d_keep) {
+        // is there content outside the 2/3 mask to carry through the steps?
+        const dim3 grid((unsigned)std::min<size_t>((c->nc + 255) / 256, (size_t)c->num_sms * 4), (unsigned)c->nb);
+        k_masked_scan<<<grid, 256, 0, c->stream>>>(c->g, c->U, c->F, bs, c->sc);
+        k_masked_flag<<<c->nb, 32, 0, c->stream>>>(c->sc);
+    }
     c->dirty = false;
 }
 
@@ -1675,7 +1735,8 @@ struct PassBytes { double x_inv, y_inv, z, y_fwd, x_fwd, rhs[3]; };
 
 // Algorithmic HBM bytes of each pass: every array the pass must read or
 // write, once; products only where the 2/3 mask keeps them.
-static PassBytes pass_bytes(const spk_ctx* c) {
+// masked_live: the deferred masked modes carry content (DevScalars::masked_live)
+static PassBytes pass_bytes(const spk_ctx* c, bool masked_live = true) {
     PassBytes b;
     const double nc = (double)c->nc, b_t = (double)csize(c), s16 = 16.0;
     int nx_keep = 0, ny_keep = 0;
@@ -1691,6 +1752,14 @@ static PassBytes pass_bytes(const spk_ctx* c) {
     b.y_fwd = c->nout * nkz * b_t + c->nout * nkyz * b_t;
     b.x_fwd = c->nout * nkyz * b_t + c->nout * nkxyz * b_t;
     const double nl = c->nout * nkxyz * b_t;
+    if (c->defer) {
+        // stages 0 and 1 touch the kept modes only; stage 2 also moves the
+        // masked modes once (U r, U w)
+        b.rhs[0] = nl + 3.0 * c->F * nkxyz * s16;
+        b.rhs[1] = nl + 4.0 * c->F * nkxyz * s16;
+        b.rhs[2] = nl + 3.0 * c->F * nkxyz * s16 + (masked_live ? 2.0 * c->F * (nc - nkxyz) * s16 : 0.0);
+        return b;
+    }
     b.rhs[0] = nl + 3.0 * c->F * nc * s16;    // U r, U w, S w
     b.rhs[1] = nl + 4.0 * c->F * nc * s16;    // U r, S r, U w, S w
     b.rhs[2] = nl + 3.0 * c->F * nc * s16;    // U r, S r, U w
@@ -1716,7 +1785,14 @@ extern "C" int spk_step_info(spk_ctx* c, int* kps, double* bytes) {
         if (c->p.heat_equation) {
             *bytes = 3.0 * 3.0 * c->F * (double)c->nc * 16.0;
         } else {
-            const PassBytes b = pass_bytes(c);
+            bool live = true;
+            if (c->defer) {
+                const int rc = pull_scalars(c);
+                if (rc) return rc;
+                live = false;
+                for (int b2 = 0; b2 < c->nb; b2++) live = live || c->h_sc[b2].masked_live != 0;
+            }
+            const PassBytes b = pass_bytes(c, live);
             *bytes = 3.0 * (b.x_inv + b.y_inv + b.z + b.y_fwd + b.x_fwd) + b.rhs[0] + b.rhs[1] + b.rhs[2];
         }
     }
@@ -1729,26 +1805,37 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    const PassBytes pb = pass_bytes(c);
-    const char* names[6] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward", "rhs_rk"};
-    const double bytes[6] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd, pb.rhs[2]};
+    bool live = true;
+    if (c->defer) {
+        const int rc = pull_scalars(c);
+        if (rc) return rc;
+        live = false;
+        for (int b2 = 0; b2 < c->nb; b2++) live = live || c->h_sc[b2].masked_live != 0;
+    }
+    const PassBytes pb = pass_bytes(c, live);
+    // with deferred masked modes the RHS of stages 0-1 (kept modes) and of
+    // stage 2 (kept modes + the step's masked modes) are timed apart
+    const char* names[7] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward", "rhs_rk", "rhs_rk_01"};
+    const double bytes[7] = {pb.x_inv, pb.y_inv, pb.z, pb.y_fwd, pb.x_fwd, pb.rhs[2], pb.rhs[1]};
+    const int npass = c->defer ? 7 : 6;
     int n = 0;
     // one warm pipeline so every buffer holds stage data
-    pass_x_inverse(c, c->U, true);
+    pass_x_inverse(c, c->U, true, 2);
     pass_y_inverse(c, true);
     pass_z_products(c, false);
     pass_y_forward(c, c->nout, c->bufA, c->bufB);
     pass_x_forward(c);
-    for (int k = 0; k < 6 && n < max_out; k++) {
+    for (int k = 0; k < npass && n < max_out; k++) {
         CK(cudaEventRecord(e0, c->stream));
         for (int r = 0; r < reps; r++) {
             switch (k) {
-                case 0: pass_x_inverse(c, c->U, true); break;
+                case 0: pass_x_inverse(c, c->U, true, 2); break;
                 case 1: pass_y_inverse(c, true); break;
                 case 2: pass_z_products(c, false); break;
                 case 3: pass_y_forward(c, c->nout, c->bufA, c->bufB); break;
                 case 4: pass_x_forward(c); break;
-                default: { XfArgs x = xf_args(c, c->U, XM_RK2, false); rhs(c, x); } break;
+                case 5: { XfArgs x = xf_args(c, c->U, XM_RK2, false); rhs(c, x); } break;
+                default: { XfArgs x = xf_args(c, c->U, XM_RK1, false); rhs(c, x); } break;
             }
         }
         CK(cudaEventRecord(e1, c->stream));
@@ -1759,7 +1846,7 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
         strncpy(out[n].name, names[k], sizeof(out[n].name) - 1);
         out[n].ms = ms / reps;
         out[n].bytes = bytes[k];
-        out[n].launches_per_step = 3;
+        out[n].launches_per_step = (c->defer && k == 5) ? 1 : (k == 6 ? 2 : 3);
         n++;
     }
     cudaEventDestroy(e0);

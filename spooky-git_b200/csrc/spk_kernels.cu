@@ -139,6 +139,49 @@ __global__ void k_clean(DevGrid g, double2* V0, size_t box_stride, int nb) {
 }
 
 // ---------------------------------------------------------------------------
+// Per box: the squared L2 norms of the nf fields from V0 over all modes and
+// over the modes outside the 2/3 mask (grid.y = box), then the flag of the
+// deferred masked modes: live unless the masked norm is below 1e-13 of the
+// whole (a masked field that small changes nothing at FP64 resolution
+// whether or not its decay is applied).
+// ---------------------------------------------------------------------------
+__global__ void k_masked_scan(DevGrid g, const double2* V0, int nf, size_t box_stride, DevScalars* scs) {
+    const int box = blockIdx.y;
+    const size_t nc = g.nc;
+    const double2* V = V0 + (size_t)box * box_stride;
+    double sa = 0.0, sm = 0.0;
+    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(gi % g.nzh);
+        const size_t r = gi / g.nzh;
+        const int j = (int)(r % g.ny), i = (int)(r / g.ny);
+        double v = 0.0;
+        for (int f = 0; f < nf; f++) {
+            const double2 x = V[(size_t)f * nc + gi];
+            v += x.x * x.x + x.y * x.y;
+        }
+        sa += v;
+        if (!(g.mx[i] != 0.0 && g.my[j] != 0.0 && g.mz[k] != 0.0)) sm += v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sm += __shfl_xor_sync(0xffffffffu, sm, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&scs[box].scan_all, sa);
+        atomicAdd(&scs[box].scan_masked, sm);
+    }
+}
+
+__global__ void k_masked_flag(DevScalars* scs) {
+    if (threadIdx.x != 0) return;
+    DevScalars& s = scs[blockIdx.x];
+    s.masked_live = (s.scan_masked <= 1e-26 * s.scan_all) ? 0 : 1;   // NaN keeps the full treatment
+    s.scan_all = 0.0;
+    s.scan_masked = 0.0;
+}
+
+// ---------------------------------------------------------------------------
 // compute_dt (compute_dt.cu:15-309) from the device maxima; the stage count
 // and stage coefficients of the super-time-stepping cycle (rkl.cu:207-591).
 // One thread per box.

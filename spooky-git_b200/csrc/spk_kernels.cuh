@@ -73,6 +73,12 @@ struct DevScalars {
     // STS: the sub-step tau in c2)
     double rkl[SPK_RKL_MAX][5];
     double nu, nu_m, nu_th;         // this box's viscosity, resistivity, thermal diffusivity
+    // deferred masked modes: 0 when the state's content outside the 2/3 mask
+    // has an L2 norm below 1e-13 of the state's (rounding noise of a round
+    // trip through real space; it only decays); set by k_masked_flag after a
+    // state is set.  scan_*: the squared norms (scratch)
+    int masked_live;
+    double scan_all, scan_masked;
 };
 
 // Classic super-time-stepping of Alexiades, Amiez & Gremaud (Commun. Numer.
@@ -128,7 +134,7 @@ struct AxisJob {
     int ch;         // channel coordinate of the input in its tensor map
     int in_state;   // input is the FP64 state (double2) instead of the pass type
     int deriv;      // multiply the input by i*k_axis(n) before the transform
-    int pad_;
+    int defer_grp;  // deferred masked modes: 1 velocity (nu), 2 magnetic field (nu_m), 0 none
 };
 
 struct AxisArgs {
@@ -150,6 +156,10 @@ struct AxisArgs {
     const DevScalars* gate; // RKL stages: skip when gate_stage > gate->s_rkl
     int gate_stage;
     int* err;       // error word (set when a TMA wait runs out)
+    // stage 1 or 2 of an RK3 step whose masked modes are deferred (XfArgs::defer):
+    // the state's masked modes enter scaled by the stage's RK3 amplification
+    int defer_stage;
+    const DevScalars* scs;
     int njobs;
     AxisJob job[SPK_MAXJOBS];
 };
@@ -210,6 +220,14 @@ struct XfArgs {
     int nb;                 // boxes side by side; sc points at nb DevScalars
     size_t box_state;       // F*nc: state elements per box (U, S, out)
     size_t box_nl;          // pass-buffer elements per box (products)
+    // Deferred dealiased-out modes (HD/MHD RK3): stages 0 and 1 update only
+    // the kept modes (a compact index over kxi x kyi x kz < kz_keep); stage 2
+    // takes every mode, the masked ones through the RK3 amplification of
+    // their linear (diffusive) right-hand side over the whole step.
+    int defer;
+    const int *kxi, *kyi;   // kept x and y indices
+    int nkx, nky;
+    FastDiv fd_kzk, fd_nky, fd_nkx;
 };
 
 struct RklArgs {

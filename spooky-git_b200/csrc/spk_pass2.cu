@@ -26,7 +26,9 @@ __host__ __device__ constexpr int axis_kt() {
     return (CONV && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
 }
 
-template <typename T, int N, int DIR, bool CONV>
+// DEF: the x inverse of RK3 stage 1 or 2 with deferred masked modes (its own
+// instantiation, so that the other passes keep their registers).
+template <typename T, int N, int DIR, bool CONV, bool DEF>
 __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
     using F = RegFft<T, N>;
     constexpr int KT = axis_kt<T, N, CONV>(), LKT = ilog2c(KT);
@@ -100,6 +102,9 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     int i = 0;
     bool aborted = false;
     C2<T> r[F::E];
+    int dbox = -1;                 // box whose deferred-mode scalars are cached
+    T dnu1 = (T)0, dnu2 = (T)0;
+    bool dlive = true;
     for (int t = blockIdx.x; t < total; t += gridDim.x, i++) {
         const int s = i % NST;
         const uint32_t par = (uint32_t)((i / NST) & 1);
@@ -117,6 +122,38 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const bool deriv = jo.deriv != 0;
         const double scale = a.scale;
         const bool skip = a.outer_filter && !okeep[o];   // uniform over the CTA
+        // Deferred masked modes (x inverse of RK3 stage 1 or 2): outside the
+        // 2/3 mask the state still holds the step's start value U, whereas
+        // the stage reads U1 = c1(z) U or U2 = c2(z) U, z = -nu k^2 dt (the
+        // recurrences of rk_value for a purely diffusive right-hand side),
+        // evaluated in the pass precision.
+        bool dfr = DEF && jo.defer_grp != 0;   // uniform over the CTA
+        T dnu = (T)0, k2yz = (T)0;
+        bool col_out = false;
+        if (dfr) {
+            if (box != dbox) {
+                const DevScalars& bs = a.scs[box];
+                dnu1 = (T)(-bs.nu * bs.dt);
+                dnu2 = (T)(-bs.nu_m * bs.dt);
+                dlive = bs.masked_live != 0;
+                dbox = box;
+            }
+            dfr = dlive;   // negligible masked content: nothing to scale
+        }
+        if (dfr) {
+            dnu = jo.defer_grp == 1 ? dnu1 : dnu2;
+            const int kc = min(k0 + c, a.g.nzh - 1);
+            const double kyo = a.g.ky[o], kzc = a.g.kz[kc];
+            k2yz = (T)(kyo * kyo + kzc * kzc);
+            col_out = !okeep[o] || k0 + c >= a.g.kz_keep;
+        }
+        auto deferred = [&](int n) -> T {   // factor of input row n (1 inside the mask)
+            const T kxn = kax[n];
+            const T z = dnu * (kxn * kxn + k2yz);
+            const T c1 = (T)1 + (T)(8.0 / 15.0) * z;
+            const T f = a.defer_stage == 1 ? c1 : c1 + (T)(-17.0 / 60.0) * z + (T)(5.0 / 12.0) * z * c1;
+            return (col_out || !keep[n]) ? f : (T)1;
+        };
         if (skip) {
         } else if constexpr (CONV) {
             const double2* src = reinterpret_cast<const double2*>(stg);
@@ -124,13 +161,18 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 double2 x = src[n * KT + c];
                 if (deriv) x = ik_mul(kd[n], x);
-                return mk<T>((T)(x.x * scale), (T)(x.y * scale));
+                C2<T> v = mk<T>((T)(x.x * scale), (T)(x.y * scale));
+                if constexpr (DEF)
+                    if (dfr) { const T f = deferred(n); v = mk<T>(f * v.x, f * v.y); }
+                return v;
             });
         } else {
             const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
             const T sc = (T)scale;
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 C2<T> v = src[n * KT + c];
+                if constexpr (DEF)
+                    if (dfr) { const T f = (T)deferred(n); v = mk<T>(f * v.x, f * v.y); }
                 if (deriv) { const T kk = kax[n]; v = mk<T>(-kk * v.y, kk * v.x); }
                 return mk<T>(v.x * sc, v.y * sc);
             });
@@ -543,20 +585,42 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
     const unsigned ny = (unsigned)a.g.ny, nlines = (unsigned)(a.g.nx * a.g.ny);
     const bool needS = a.mode == XM_RK1 || a.mode == XM_RK2;
     const double2 z0 = d2(0.0, 0.0);
-    const size_t total = nc * (size_t)a.nb;
+    // deferred masked modes: every stage visits the kept modes only
+    // (k_masked_rk moves the masked ones once per step)
+    const bool compact = a.defer != 0;
+    const int kzk = a.g.kz_keep;
+    const size_t total = (compact ? (size_t)a.nkx * a.nky * kzk : nc) * (size_t)a.nb;
     for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
-        // global line over the boxes -> box, line, k (nx*ny is a power of two)
-        const unsigned gline = fzh.div((unsigned)gb);
-        const int k = (int)(gb - (size_t)gline * nzh);
-        const unsigned ubox = a.fd_nl.div(gline);
-        const int box = (int)ubox;
-        const unsigned line = gline - ubox * nlines;
-        const unsigned ui = a.fd_ny.div(line);
-        const int i = (int)ui, j = (int)(line - ui * ny);
+        int k, i, j, box;
+        unsigned line;
+        if (compact) {
+            // compact index -> box, kept x index, kept y index, k < kz_keep
+            const unsigned r1 = a.fd_kzk.div((unsigned)gb);
+            k = (int)(gb - (size_t)r1 * kzk);
+            const unsigned r2 = a.fd_nky.div(r1);
+            const int jy = (int)(r1 - r2 * (unsigned)a.nky);
+            const unsigned r3 = a.fd_nkx.div(r2);
+            const int ix = (int)(r2 - r3 * (unsigned)a.nkx);
+            box = (int)r3;
+            i = a.kxi[ix];
+            j = a.kyi[jy];
+            line = (unsigned)i * ny + (unsigned)j;
+        } else {
+            // global line over the boxes -> box, line, k (nx*ny is a power of two)
+            const unsigned gline = fzh.div((unsigned)gb);
+            k = (int)(gb - (size_t)gline * nzh);
+            const unsigned ubox = a.fd_nl.div(gline);
+            box = (int)ubox;
+            line = gline - ubox * nlines;
+            const unsigned ui = a.fd_ny.div(line);
+            i = (int)ui;
+            j = (int)(line - ui * ny);
+        }
         const size_t gi = (size_t)line * nzh + k;                // mode within the box
         const size_t bo = (size_t)box * a.box_state;            // box offset in U, S, out
         const double dt = a.sc[box].dt, nu = a.sc[box].nu, nu_m = a.sc[box].nu_m, nu_th = a.sc[box].nu_th;
         const bool m = a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0;
+
         const C2<T>* nl = (const C2<T>*)a.nl + (size_t)box * a.box_nl;
         const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
         auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
@@ -682,6 +746,64 @@ __global__ void __launch_bounds__(128, 3) k_rhs(const __grid_constant__ XfArgs a
 // compute_cycle_RKL2 (rkl.cu:437-591).  Skipped for stages beyond the
 // cycle's stage count.
 // ---------------------------------------------------------------------------
+// Masked modes of a deferred RK3 step, once per step (with stage 2):
+// outside the 2/3 mask the right-hand side is the diffusion -nu k^2 U of a
+// divergence-free U (the nonlinear terms are masked and the Leray
+// projection leaves it unchanged), so the three stages amount to
+// U <- c(z) U, z = -nu k^2 dt, c from the recurrences of rk_value; the
+// divergence cleaning of the next step follows, as in k_rhs.  Kept modes are
+// skipped (k_rhs owns them).
+__global__ void __launch_bounds__(256) k_masked_rk(const __grid_constant__ XfArgs a, FastDiv fzh) {
+    const size_t nc = a.g.nc;
+    const int nzh = a.g.nzh;
+    const unsigned ny = (unsigned)a.g.ny, nlines = (unsigned)(a.g.nx * a.g.ny);
+    const size_t total = nc * (size_t)a.nb;
+    const double g0 = 8.0 / 15.0, g1 = 5.0 / 12.0, g2 = 3.0 / 4.0, x0 = -17.0 / 60.0, x1 = -5.0 / 12.0;
+    auto amp = [&](double z) {
+        const double c1 = 1.0 + g0 * z;
+        const double s1 = c1 + x0 * z;
+        const double c2 = s1 + g1 * z * c1;
+        const double s2 = c2 + x1 * z * c1;
+        return s2 + g2 * z * c2;
+    };
+    for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
+        const unsigned gline = fzh.div((unsigned)gb);
+        const int k = (int)(gb - (size_t)gline * nzh);
+        const unsigned ubox = a.fd_nl.div(gline);
+        const unsigned line = gline - ubox * nlines;
+        if (!a.sc[ubox].masked_live) continue;   // negligible masked content stays as it is
+        const unsigned ui = a.fd_ny.div(line);
+        const int i = (int)ui, j = (int)(line - ui * ny);
+        if (a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0) continue;
+        const size_t gi = (size_t)line * nzh + k;
+        const size_t bo = (size_t)ubox * a.box_state;
+        double2 X[6];
+#pragma unroll
+        for (int c = 0; c < 3; c++) X[c] = a.U[bo + (size_t)(a.VEL + c) * nc + gi];
+        if (a.mhd)
+#pragma unroll
+            for (int c = 0; c < 3; c++) X[3 + c] = a.U[bo + (size_t)(a.MAG + c) * nc + gi];
+        const double dt = a.sc[ubox].dt, nu = a.sc[ubox].nu, nu_m = a.sc[ubox].nu_m;
+        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double cu = amp(-nu * k2 * dt);
+        double2 Un[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) Un[c] = d2(cu * X[c].x, cu * X[c].y);
+        if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+        for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.VEL + c) * nc + gi] = Un[c];
+        if (a.mhd) {
+            const double cb = amp(-nu_m * k2 * dt);
+#pragma unroll
+            for (int c = 0; c < 3; c++) Un[c] = d2(cb * X[3 + c].x, cb * X[3 + c].y);
+            if (a.clean) clean3(Un, kx, ky, kz);
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.MAG + c) * nc + gi] = Un[c];
+        }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArgs a, double2* U, int vslot, FastDiv fzh,
                                                   FastDiv fny) {
