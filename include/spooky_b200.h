@@ -167,6 +167,19 @@ typedef struct spk_budgets {
 } spk_budgets_t;
 int spk_budgets(spk_ctx* ctx, spk_budgets_t* out);
 
+/* Shell spectrum of fields f1, f2 of the context state:
+ * InputOutput::computeSpectrum1d / Spectrum1d (src/io/spooky_output_spectrum.cu:424-442,
+ * src/cuda/cuda_kernels_generic.cu:441-472).  out[m] (m < min(max_bins, nbins)) is
+ * the sum over modes with m = (int)(|k|/deltak + 0.5) of w Re(U_f1/N conj(U_f2/N)),
+ * N = NX*NY*NZ, w = 2 for kz index > 0; deltak = 2 pi/min(lx, ly, lz) and
+ * nbins = (int)(kmax/deltak + 0.5) with the dealiased kmax (wavevector.cu:100-111).
+ * Shells m >= nbins are left out (the reference's kernel adds them past the end
+ * of its array).  *total (may be NULL): the Parseval sum with weight 1 at kz = 0
+ * and at the Nyquist plane, i.e. the grid mean of f1 f2 (twoFieldCorrelation,
+ * src/io/spooky_output_functions.cu).  Synchronises the context stream. */
+int spk_spectrum(spk_ctx* ctx, int f1, int f2, double* out, int max_bins, int* nbins, double* deltak,
+                 double* total);
+
 /* Launch accounting of one recorded main-loop step: kernels launched per
  * step (RKL stages counted at their recorded bound) and the algorithmic HBM
  * bytes of one RK3 step of this pass design (every array a pass must touch,

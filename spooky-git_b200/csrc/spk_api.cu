@@ -68,6 +68,10 @@ struct spk_ctx {
     int* d_keep = nullptr;
     int nkx = 0, nky = 0;
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
+    // shell spectra: bins (InputOutput / Wavevector, wavevector.cu:100-111)
+    int nbins = 0;
+    double deltak = 0.0;
+    double* d_spec = nullptr;
     bool closure_on = false;
     float* d_cparams = nullptr;
     double delta2 = 0.0;
@@ -1043,6 +1047,14 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     c->nkx = c->nky = 0;
     for (int i = 0; i < c->nx; i++) c->nkx += c->mx[i] != 0.0;
     for (int j = 0; j < c->ny; j++) c->nky += c->my[j] != 0.0;
+    {
+        // Wavevector: deltak = 2 pi / min(l), nbins = (int)(kmax/deltak + 0.5) (wavevector.cu:100-111)
+        double lmin = p.lx;
+        if (p.ly < lmin) lmin = p.ly;
+        if (p.lz < lmin) lmin = p.lz;
+        c->deltak = 2.0 * M_PI / lmin;
+        c->nbins = (int)(c->kmax / c->deltak + 0.5);
+    }
     c->defer = p.incompressible && !p.boussinesq && c->sts_mask == 0 && p.integrator == SPK_INT_RK3 &&
                c->nkx > 0 && c->nky > 0 && c->kz_keep > 0;
     int oc = 0;
@@ -1162,6 +1174,7 @@ static int ctx_alloc(spk_ctx* c) {
         CK(cudaMalloc(&c->d_cparams, sizeof(float) * CL_NP));
         CK(cudaMemset(c->d_cparams, 0, sizeof(float) * CL_NP));
     }
+    CK(cudaMalloc(&c->d_spec, sizeof(double) * (size_t)(c->nbins + 1)));
     if (c->defer) {
         std::vector<int> keep;
         for (int i = 0; i < c->nx; i++) if (c->mx[i] != 0.0) keep.push_back(i);
@@ -1179,6 +1192,7 @@ static void ctx_free(spk_ctx* c) {
     cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
     cudaFree(c->d_cparams);
     cudaFree(c->d_keep);
+    cudaFree(c->d_spec);
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->h_sums) cudaFreeHost(c->h_sums);
     if (c->own_stream) cudaStreamDestroy(c->stream);

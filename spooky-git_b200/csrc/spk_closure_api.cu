@@ -158,6 +158,32 @@ extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, flo
 }
 
 // ---------------------------------------------------------------------------
+// shell spectra (diagnostics)
+// ---------------------------------------------------------------------------
+extern "C" int spk_spectrum(spk_ctx* c, int f1, int f2, double* out, int max_bins, int* nbins, double* deltak,
+                            double* total) {
+    if (!c || f1 < 0 || f2 < 0 || f1 >= c->F || f2 >= c->F) return SPK_ERR_ARG;
+    if (nbins) *nbins = c->nbins;
+    if (deltak) *deltak = c->deltak;
+    if (c->nbins < 1) return fail(c, SPK_ERR_UNSUPPORTED, "no spectral bins for this grid");
+    CK(cudaMemsetAsync(c->d_spec, 0, sizeof(double) * (size_t)(c->nbins + 1), c->stream));
+    const double inv_n = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);
+    const int grid = (int)std::min<size_t>((c->nc + 255) / 256, (size_t)c->num_sms * 8);
+    k_spectrum<<<grid, 256, sizeof(double) * (size_t)c->nbins, c->stream>>>(
+        c->g, c->U + (size_t)f1 * c->nc, c->U + (size_t)f2 * c->nc, c->nbins, c->deltak, inv_n, c->d_spec);
+    c->launches++;
+    int rc = launch_status(c);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->h_sums, c->d_spec + c->nbins, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double> h((size_t)c->nbins);
+    CK(cudaMemcpyAsync(h.data(), c->d_spec, sizeof(double) * (size_t)c->nbins, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (out) for (int m = 0; m < std::min(max_bins, c->nbins); m++) out[m] = h[(size_t)m];
+    if (total) *total = c->h_sums[0];
+    return SPK_OK;
+}
+
+// ---------------------------------------------------------------------------
 // trainer
 // ---------------------------------------------------------------------------
 #define SPK_TRAIN_HIST 65536

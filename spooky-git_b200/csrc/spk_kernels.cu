@@ -182,6 +182,43 @@ __global__ void k_masked_flag(DevScalars* scs) {
 }
 
 // ---------------------------------------------------------------------------
+// Shell spectrum of two fields (Spectrum1d, cuda_kernels_generic.cu:441-472):
+// per mode p = w Re(U1/N conj(U2/N)), w = 2 for kz index > 0, into shell
+// m = (int)(|k|/dk + 0.5); shells m >= nbins are left out (the reference adds
+// them past the end of its array).  out[nbins] receives the Parseval sum
+// (weight 1 at kz = 0 and at the Nyquist plane, 2 elsewhere): the mean of
+// f1 f2 over the grid (twoFieldCorrelation).  Per-CTA shared-memory
+// histograms, then atomics into out (summation order varies).
+// ---------------------------------------------------------------------------
+__global__ void k_spectrum(DevGrid g, const double2* U1, const double2* U2, int nbins, double dk, double inv_n,
+                           double* out) {
+    extern __shared__ double hist[];
+    for (int m = threadIdx.x; m < nbins; m += blockDim.x) hist[m] = 0.0;
+    __syncthreads();
+    const size_t nc = g.nc;
+    const int nzl = g.nz / 2;   // Nyquist plane index
+    double tot = 0.0;
+    for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(gi % g.nzh);
+        const size_t r = gi / g.nzh;
+        const int j = (int)(r % g.ny), i = (int)(r / g.ny);
+        const double2 a = U1[gi], b = U2[gi];
+        const double pr = (a.x * inv_n) * (b.x * inv_n) + (a.y * inv_n) * (b.y * inv_n);
+        const double p = k > 0 ? 2.0 * pr : pr;
+        tot += (k > 0 && k != nzl) ? 2.0 * pr : pr;
+        const double kx = g.kx[i], ky = g.ky[j], kz = g.kz[k];
+        const int m = (int)(sqrt(kx * kx + ky * ky + kz * kz) / dk + 0.5);
+        if (m < nbins) atomicAdd(&hist[m], p);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&out[nbins], tot);
+    __syncthreads();
+    for (int m = threadIdx.x; m < nbins; m += blockDim.x)
+        if (hist[m] != 0.0) atomicAdd(&out[m], hist[m]);
+}
+
+// ---------------------------------------------------------------------------
 // compute_dt (compute_dt.cu:15-309) from the device maxima; the stage count
 // and stage coefficients of the super-time-stepping cycle (rkl.cu:207-591).
 // One thread per box.

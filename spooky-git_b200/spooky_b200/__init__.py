@@ -38,7 +38,7 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step",
             "spk_closure_set", "spk_products", "spk_closure_samples_size", "spk_closure_samples",
             "spk_trainer_create", "spk_trainer_destroy", "spk_trainer_set_params", "spk_trainer_get_params",
-            "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train"]
+            "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train", "spk_spectrum"]
 
 # learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
@@ -116,6 +116,7 @@ def lib():
         L.spk_trainer_set_samples.argtypes = [vp, vp, sp, sp, fp]
         L.spk_trainer_loss_grad.argtypes = [vp, fp, fp]
         L.spk_trainer_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp]
+        L.spk_spectrum.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip, dp, dp]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -307,6 +308,19 @@ class Context:
         b = Budgets()
         self._check(lib().spk_budgets(self._h, ctypes.byref(b)))
         return np.array(b.energy[: self.F]), np.array(b.dissipation[: self.F])
+
+    # -- diagnostics ---------------------------------------------------------
+    def spectrum(self, f1, f2=None):
+        """Shell spectrum of fields f1, f2 (indices or names such as "vx")
+        of the state (spk_spectrum): (E[nbins], deltak, grid mean of f1 f2)."""
+        f1 = self.var_list.index(f1) if isinstance(f1, str) else int(f1)
+        f2 = f1 if f2 is None else (self.var_list.index(f2) if isinstance(f2, str) else int(f2))
+        nb, dk, tot = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        self._check(lib().spk_spectrum(self._h, f1, f2, None, 0, ctypes.byref(nb), ctypes.byref(dk), None))
+        out = np.zeros(max(nb.value, 1))
+        self._check(lib().spk_spectrum(self._h, f1, f2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       nb.value, ctypes.byref(nb), ctypes.byref(dk), ctypes.byref(tot)))
+        return out[: nb.value], dk.value, tot.value
 
     # -- learned closure -----------------------------------------------------
     def closure_set(self, params):
