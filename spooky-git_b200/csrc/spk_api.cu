@@ -67,6 +67,7 @@ struct spk_ctx {
     bool defer = false;
     int* d_keep = nullptr;
     int nkx = 0, nky = 0;
+    bool trim_now = false;         // recording a step: the inverse passes may trim (DevScalars::masked_live)
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
     // shell spectra: bins (InputOutput / Wavevector, wavevector.cu:100-111)
     int nbins = 0;
@@ -212,6 +213,7 @@ static AxisArgs axis_args(spk_ctx* c, int ax) {
     a.scale = 1.0;
     a.nb = c->nb;
     a.out_box_ch = c->nbuf_ch;
+    a.scs = c->sc;
     return a;
 }
 
@@ -314,6 +316,15 @@ static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
     a.fd_kb = FastDiv::make((unsigned)nkb);
     a.fd_box = FastDiv::make((unsigned)(nouter * nkb));
     a.fd_job = FastDiv::make((unsigned)(a.nb * nouter * nkb));
+    if (a.trim) {
+        // kept tiles of a trimmed single-box pass (used when the state has no masked content)
+        a.tr_nkb = std::max(1, (c->kz_keep + a.kt - 1) / a.kt);
+        a.tr_nouter = a.trim == 1 ? c->nky : nouter;
+        a.tr_outer = c->d_keep + c->nkx;   // kept y indices
+        a.tr_fd_kb = FastDiv::make((unsigned)a.tr_nkb);
+        a.tr_fd_box = FastDiv::make((unsigned)(a.tr_nouter * a.tr_nkb));
+        a.tr_fd_job = FastDiv::make((unsigned)(a.nb * a.tr_nouter * a.tr_nkb));
+    }
     if (dir > 0) launch_axis_dir<T, +1>(c, a, total);
     else launch_axis_dir<T, -1>(c, a, total);
 }
@@ -459,7 +470,7 @@ static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx, int stage
     AxisArgs a = axis_args(c, 0);
     a.scale = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);   // scaleKernel factor
     a.defer_stage = (c->defer && c->d_keep && U == c->U && (stage == 1 || stage == 2)) ? stage : 0;
-    a.scs = c->sc;
+    a.trim = (c->trim_now && U == c->U) ? 1 : 0;
     auto mark = [&](int first, int grp) {
         for (int q = first; q < a.njobs; q++) a.job[q].defer_grp = grp;
     };
@@ -484,6 +495,7 @@ static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx, int stage
 
 static void pass_y_inverse(spk_ctx* c, bool with_g) {
     AxisArgs a = axis_args(c, 1);
+    a.trim = c->trim_now ? 2 : 0;
     if (with_g && c->aniso_rhs) {
         // u, B, theta and d/dx theta one to one; d/dy theta from theta
         add_job(c, a, c->bufA, c->bufB, c->ch_gx + 1, 0, 0, 0);
@@ -494,6 +506,7 @@ static void pass_y_inverse(spk_ctx* c, bool with_g) {
         add_job(c, a, c->bufA, c->bufB, c->ch_dx + c->ncl_half, 0, 0, 0);
         axis(c, a, +1);
         AxisArgs b = axis_args(c, 1);
+        b.trim = a.trim;
         add_job(c, b, chan(c, c->bufA, c->ch_u), chan(c, c->bufB, c->ch_dy), c->ncl_half, 0, 1, 0);
         axis(c, b, +1);
         return;
@@ -543,6 +556,7 @@ static void set_inputs(spk_ctx* c, ZArgs& z, bool with_g) {
 static void pass_z_products(spk_ctx* c, bool do_max) {
     ZArgs z = z_args(c);
     z.mode = ZM_PRODUCTS;
+    z.trim = c->trim_now ? 1 : 0;
     set_inputs(c, z, true);
     z.nout = c->nout;
     z.hydro = 1;
@@ -746,7 +760,19 @@ static void record_breal(spk_ctx* c) {
 // ---------------------------------------------------------------------------
 // one main-loop iteration (CleanFieldDivergence + HydroMHDAdvance)
 // ---------------------------------------------------------------------------
+static void record_step_body(spk_ctx* c, int parity);
+// The inverse passes of a recorded step trim the work of masked modes when
+// the state has none (the flag is refreshed whenever a state is set).
+struct TrimScope {   // trimming on for one recording or profiling, off again on every exit
+    spk_ctx* c;
+    explicit TrimScope(spk_ctx* cc) : c(cc) { c->trim_now = c->defer && c->d_keep; }
+    ~TrimScope() { c->trim_now = false; }
+};
 static void record_step(spk_ctx* c, int parity) {
+    TrimScope ts(c);
+    record_step_body(c, parity);
+}
+static void record_step_body(spk_ctx* c, int parity) {
     const spk_params_t& p = c->p;
     const bool sts = p.supertimestepping && c->nsts > 0;
     const bool sts_before = sts && !p.sts_every_step && parity == 1;
@@ -1763,6 +1789,15 @@ static PassBytes pass_bytes(const spk_ctx* c, bool masked_live = true) {
     b.x_inv = c->F * nc * s16 + nx_in * nc * b_t;
     b.y_inv = nx_in * nc * b_t + c->nin * nc * b_t;
     b.z = c->nin * nc * b_t + c->nout * nkz * b_t;
+    if (c->defer && !masked_live) {
+        // trimmed inverse passes: only the kept (ky, kz) columns enter and
+        // only kz < kz_keep leaves the x and y passes
+        const double nyz = (double)c->nx * ny_keep * c->kz_keep;    // x inverse in and out
+        const double nz_in = (double)c->nx * c->ny * c->kz_keep;      // y inverse out, z in
+        b.x_inv = c->F * nyz * s16 + nx_in * nyz * b_t;
+        b.y_inv = nx_in * nyz * b_t + c->nin * nz_in * b_t;
+        b.z = c->nin * nz_in * b_t + c->nout * nkz * b_t;
+    }
     b.y_fwd = c->nout * nkz * b_t + c->nout * nkyz * b_t;
     b.x_fwd = c->nout * nkyz * b_t + c->nout * nkxyz * b_t;
     const double nl = c->nout * nkxyz * b_t;
@@ -1819,6 +1854,7 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    if (c->dirty) launch_clean(c);   // refreshes the masked-content flag
     bool live = true;
     if (c->defer) {
         const int rc = pull_scalars(c);
@@ -1827,6 +1863,7 @@ extern "C" int spk_profile_passes(spk_ctx* c, int reps, spk_pass_stat_t* out, in
         for (int b2 = 0; b2 < c->nb; b2++) live = live || c->h_sc[b2].masked_live != 0;
     }
     const PassBytes pb = pass_bytes(c, live);
+    TrimScope ts(c);   // time the passes as a step runs them
     // with deferred masked modes the RHS of stages 0-1 (kept modes) and of
     // stage 2 (kept modes + the step's masked modes) are timed apart
     const char* names[7] = {"x_inverse", "y_inverse", "z_products", "y_forward", "x_forward", "rhs_rk", "rhs_rk_01"};

@@ -160,6 +160,16 @@ struct AxisArgs {
     // the state's masked modes enter scaled by the stage's RK3 amplification
     int defer_stage;
     const DevScalars* scs;
+    // trimmed inverse passes of a step whose state has no masked content
+    // (DevScalars::masked_live == 0): 1 = x inverse (skip tiles of masked y
+    // rows and of kz blocks past kz_keep), 2 = y inverse (skip kz blocks past
+    // kz_keep; masked y rows, which the x inverse left unwritten, enter as 0)
+    int trim;
+    // single-box trimmed pass: enumerate only the kept tiles (tr_outer: the
+    // kept outer indices of the x inverse, tr_nkb k blocks below kz_keep)
+    int tr_nouter, tr_nkb;
+    const int* tr_outer;
+    FastDiv tr_fd_job, tr_fd_box, tr_fd_kb;
     int njobs;
     AxisJob job[SPK_MAXJOBS];
 };
@@ -194,6 +204,7 @@ struct ZArgs {
     // learned closure: input channels ch_dx (d/dx of u [and B]) and ch_dy
     // (d/dy); d/dz derived in the pass from channels zder_src[] (appended
     // after the inputs); MLP parameters (SPK_CLOSURE_NPARAM floats)
+    int trim;               // masked content absent: the kz >= kz_keep tail of every input row enters as 0
     int closure, ch_dx, ch_dy;
     int zder_n, zder_src[6];
     const float* cparams;

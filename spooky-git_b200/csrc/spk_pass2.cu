@@ -38,8 +38,15 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const int tid = threadIdx.x;
     const int c = tid & (KT - 1), q = tid >> LKT;
     const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
-    const int nkb = (a.kcols + KT - 1) / KT;
-    const int per_box = nouter * nkb;
+    // a trimmed single-box pass with no masked content walks only the tiles
+    // it keeps (every CTA reads the same flag)
+    const bool ctile = a.trim && a.nb == 1 && !a.scs[0].masked_live;
+    const bool couter = ctile && a.trim == 1;
+    const int nkb = ctile ? a.tr_nkb : (a.kcols + KT - 1) / KT;
+    const int nouter_e = couter ? a.tr_nouter : nouter;
+    const FastDiv fdj = ctile ? a.tr_fd_job : a.fd_job, fdb = ctile ? a.tr_fd_box : a.fd_box;
+    const FastDiv fdk = ctile ? a.tr_fd_kb : a.fd_kb;
+    const int per_box = nouter_e * nkb;
     const int per_job = a.nb * per_box;
     const int total = a.njobs * per_job;   // tile t = ((job * nb + box) * nouter + o) * nkb + kb
     constexpr size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
@@ -56,16 +63,22 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     constexpr uint32_t tile_bytes = (uint32_t)((size_t)N * KT * in_elem);
     const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
+    // tiles that a trimmed pass skips (uniform: every thread decides alike)
+    auto trimmed = [&](int box, int o, int kb) -> bool {
+        if (!a.trim || a.scs[box].masked_live) return false;
+        return kb * KT >= a.g.kz_keep || (a.trim == 1 && !okeep[o]);
+    };
     auto issue = [&](int t, int s) {
-        const int jb = (int)a.fd_job.div((unsigned)t);
+        const int jb = (int)fdj.div((unsigned)t);
         const int rb = t - jb * per_job;
-        const int box = (int)a.fd_box.div((unsigned)rb);
+        const int box = (int)fdb.div((unsigned)rb);
         const int rem = rb - box * per_box;
-        const int o = (int)a.fd_kb.div((unsigned)rem), kb = rem - o * nkb;
+        const int oe = (int)fdk.div((unsigned)rem), kb = rem - oe * nkb;
+        const int o = couter ? a.tr_outer[oe] : oe;
         const AxisJob& jo = a.job[jb];
         const int ch = jo.ch + box * a.in_box_ch;
         unsigned char* dst = stages + (size_t)s * stage_bytes;
-        if (a.outer_filter && !okeep[o]) {   // skipped tile: complete the phase with no bytes
+        if ((a.outer_filter && !okeep[o]) || trimmed(box, o, kb)) {   // skipped tile: complete the phase with no bytes
             mbar_expect_tx(&bar[s], 0);
             return;
         }
@@ -110,18 +123,21 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const uint32_t par = (uint32_t)((i / NST) & 1);
         const bool ok = mbar_wait(&bar[s], par, SPK_WAIT_ITERS);
         if (__syncthreads_or(!ok)) { aborted = true; break; }
-        const int jb = (int)a.fd_job.div((unsigned)t);
+        const int jb = (int)fdj.div((unsigned)t);
         const int rb = t - jb * per_job;
-        const int box = (int)a.fd_box.div((unsigned)rb);
+        const int box = (int)fdb.div((unsigned)rb);
         const int rem = rb - box * per_box;
-        const int o = (int)a.fd_kb.div((unsigned)rem), kb = rem - o * nkb;
+        const int oe = (int)fdk.div((unsigned)rem), kb = rem - oe * nkb;
+        const int o = couter ? a.tr_outer[oe] : oe;
         const AxisJob& jo = a.job[jb];
         const int k0 = kb * KT;
         const int kt = min(KT, a.kcols - k0);
         const unsigned char* stg = stages + (size_t)s * stage_bytes;
         const bool deriv = jo.deriv != 0;
         const double scale = a.scale;
-        const bool skip = a.outer_filter && !okeep[o];   // uniform over the CTA
+        const bool skip = (a.outer_filter && !okeep[o]) || trimmed(box, o, kb);   // uniform over the CTA
+        // trimmed y inverse: masked y rows were not written by the x inverse
+        const bool zrows = a.trim == 2 && !skip && !a.scs[box].masked_live;
         // Deferred masked modes (x inverse of RK3 stage 1 or 2): outside the
         // 2/3 mask the state still holds the step's start value U, whereas
         // the stage reads U1 = c1(z) U or U2 = c2(z) U, z = -nu k^2 dt (the
@@ -171,6 +187,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             const T sc = (T)scale;
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 C2<T> v = src[n * KT + c];
+                if (zrows && !keep[n]) v = mk<T>((T)0, (T)0);
                 if constexpr (DEF)
                     if (dfr) { const T f = (T)deferred(n); v = mk<T>(f * v.x, f * v.y); }
                 if (deriv) { const T kk = kax[n]; v = mk<T>(-kk * v.y, kk * v.x); }
@@ -310,6 +327,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         return;
     }
 
+    // no masked content: the inverse passes left kz >= kz_keep unwritten, and
+    // those modes enter as zero
+    const int kzk = (a.trim && !bsc->masked_live) ? a.g.kz_keep : nzs;
     auto xaddr = [&](int Lx) { return xb + (size_t)sigma * XS + padi<1>(Lx); };
     C2<T> r[F::E];
 
@@ -322,6 +342,7 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
         const C2<T>* pa = raw + (size_t)(2 * p * L + l) * nzs;
         const C2<T>* pb = 2 * p + 1 < nin ? pa + (size_t)L * nzs : zrow;
         auto chv = [&](int ch, int k) -> C2<T> {
+            if (k >= kzk) return mk<T>((T)0, (T)0);
             if (ch < nin) {
                 C2<T> v = raw[((size_t)ch * L + l) * nzs + k];
                 if (a.derive_gz == 2 && ch == a.ch_th) {
@@ -347,8 +368,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             const int k = n <= NH ? n : N - n;
             C2<T> A, B;
             if constexpr (GEN == 0) {
-                A = pa[k];
-                B = pb[k];
+                const C2<T> zz = mk<T>((T)0, (T)0);
+                A = k < kzk ? pa[k] : zz;
+                B = k < kzk ? pb[k] : zz;
             } else {
                 A = chv(2 * p, k);
                 B = chv(2 * p + 1, k);
