@@ -316,6 +316,16 @@ static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
     a.fd_kb = FastDiv::make((unsigned)nkb);
     a.fd_box = FastDiv::make((unsigned)(nouter * nkb));
     a.fd_job = FastDiv::make((unsigned)(a.nb * nouter * nkb));
+    if (a.outer_filter && a.nb == 1 && a.axis == 0 && !a.trim && c->d_keep) {
+        // outer-filtered x forward: walk the kept ky rows only
+        a.tr_always = 1;
+        a.tr_nkb = nkb;
+        a.tr_nouter = c->nky;
+        a.tr_outer = c->d_keep + c->nkx;
+        a.tr_fd_kb = FastDiv::make((unsigned)a.tr_nkb);
+        a.tr_fd_box = FastDiv::make((unsigned)(a.tr_nouter * a.tr_nkb));
+        a.tr_fd_job = FastDiv::make((unsigned)(a.tr_nouter * a.tr_nkb));
+    }
     if (a.trim) {
         // kept tiles of a trimmed single-box pass (used when the state has no masked content)
         a.tr_nkb = std::max(1, (c->kz_keep + a.kt - 1) / a.kt);
@@ -1201,7 +1211,8 @@ static int ctx_alloc(spk_ctx* c) {
         CK(cudaMemset(c->d_cparams, 0, sizeof(float) * CL_NP));
     }
     CK(cudaMalloc(&c->d_spec, sizeof(double) * (size_t)(c->nbins + 1)));
-    if (c->defer) {
+    if (c->nkx > 0 && c->nky > 0) {
+        // kept x and y indices (deferred masked modes, compact tile walks)
         std::vector<int> keep;
         for (int i = 0; i < c->nx; i++) if (c->mx[i] != 0.0) keep.push_back(i);
         for (int j = 0; j < c->ny; j++) if (c->my[j] != 0.0) keep.push_back(j);

@@ -169,6 +169,7 @@ struct AxisArgs {
     // kept outer indices of the x inverse, tr_nkb k blocks below kz_keep)
     int tr_nouter, tr_nkb;
     const int* tr_outer;
+    int tr_always;          // enumerate the kept tiles regardless of the flag (outer-filtered x forward)
     FastDiv tr_fd_job, tr_fd_box, tr_fd_kb;
     int njobs;
     AxisJob job[SPK_MAXJOBS];

@@ -40,8 +40,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
     // a trimmed single-box pass with no masked content walks only the tiles
     // it keeps (every CTA reads the same flag)
-    const bool ctile = a.trim && a.nb == 1 && !a.scs[0].masked_live;
-    const bool couter = ctile && a.trim == 1;
+    const bool ctile = a.tr_always || (a.trim && a.nb == 1 && !a.scs[0].masked_live);
+    const bool couter = ctile && (a.trim == 1 || a.tr_always);
     const int nkb = ctile ? a.tr_nkb : (a.kcols + KT - 1) / KT;
     const int nouter_e = couter ? a.tr_nouter : nouter;
     const FastDiv fdj = ctile ? a.tr_fd_job : a.fd_job, fdb = ctile ? a.tr_fd_box : a.fd_box;
