@@ -222,15 +222,26 @@ def run_ensemble(args, world, rank, local_rank):
         b.set_state(U)
     ens.advance(args.warmup)
     ens.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ens.advance(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+
+    def timed():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ms_untuned = timed()
+    # the schedule autotuner (spk_ensemble_autotune), then the timed steps
+    t_tune = time.perf_counter()
+    ens.autotune(steps=3)
+    ens.advance(args.warmup)
+    ens.synchronize()
+    t_tune = time.perf_counter() - t_tune
+    ms = timed()
     kps = ens.kernels_per_step()
     ens.synchronize()
     finite = all(np.isfinite(b.budgets()[0]).all() for b in ens.boxes)
@@ -267,6 +278,9 @@ def run_ensemble(args, world, rank, local_rank):
                        "parallelism": f"boxes partitioned over {world} rank(s) by N^3 log N"},
             "one_box_at_a_time": {"value": nsample * args.steps / (one_ms * 1e-3), "unit": "box-steps/s",
                                   "sample_boxes": nsample, "rank": 0},
+            "untuned": {"value": args.boxes * args.steps / (ms_untuned * 1e-3), "unit": "box-steps/s",
+                        "what": "the launchers' own schedule, before spk_ensemble_autotune (rank 0)"},
+            "autotune_seconds": t_tune,
             "kernels_per_ensemble_step_rank0": kps,
             "gpu_launches": kps * args.steps,
             "all_finite": finite,

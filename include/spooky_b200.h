@@ -340,6 +340,21 @@ int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad);
  * (host, may be NULL) receives each step's minibatch loss. */
 int spk_trainer_train(spk_trainer* tr, int nsteps, int batch, float lr, float* loss_hist);
 
+/* Schedule autotuner (no reference counterpart).  Picks, by timing whole
+ * recorded steps with CUDA events, the launch choices that leave the
+ * arithmetic unchanged: the z pass's lines per CTA, the axis passes'
+ * pipeline stages and the RHS grid (CTAs per SM), by coordinate descent
+ * over candidate values; the tuned context computes the same bits as an
+ * untuned one.  `steps` timed steps per candidate.  The state and the step
+ * scalars are saved (one temporary device copy of the state, freed on
+ * return) and restored, so the call leaves the simulation where it was.
+ * Outputs (may be NULL): the chosen values (0: the launcher's own model)
+ * and the ms per step before and after. */
+int spk_autotune(spk_ctx* ctx, int steps, int* z_lines, int* axis_stages, int* rhs_ctas_per_sm, double* ms_before,
+                 double* ms_after);
+/* The same for every group of an ensemble (each group tuned on its own). */
+int spk_ensemble_autotune(spk_ensemble* ens, int steps);
+
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */
 const char* spk_last_error(const spk_ctx* ctx);

@@ -68,6 +68,10 @@ struct spk_ctx {
     int* d_keep = nullptr;
     int nkx = 0, nky = 0;
     bool trim_now = false;         // recording a step: the inverse passes may trim (DevScalars::masked_live)
+    // schedule knobs picked by spk_autotune (0: the launchers' own choice)
+    int tune_zl = 0;               // z pass: lines per CTA
+    int tune_nst = 0;              // axis passes: pipeline stages
+    int tune_rhs = 0;              // RHS: CTAs per SM
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
     // shell spectra: bins (InputOutput / Wavevector, wavevector.cu:100-111)
     int nbins = 0;
@@ -265,6 +269,8 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
+    if (c->tune_nst >= 2 && c->tune_nst <= 4 && fixed + (size_t)c->tune_nst * stage <= (size_t)227 * 1024)
+        a.nst = c->tune_nst;
     const size_t smem = fixed + (size_t)a.nst * stage;
     cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 1;
@@ -316,7 +322,7 @@ static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
     a.fd_kb = FastDiv::make((unsigned)nkb);
     a.fd_box = FastDiv::make((unsigned)(nouter * nkb));
     a.fd_job = FastDiv::make((unsigned)(a.nb * nouter * nkb));
-    if (a.outer_filter && a.nb == 1 && a.axis == 0 && !a.trim && c->d_keep) {
+    if (a.outer_filter && a.axis == 0 && !a.trim && c->d_keep) {
         // outer-filtered x forward: walk the kept ky rows only
         a.tr_always = 1;
         a.tr_nkb = nkb;
@@ -324,7 +330,7 @@ static void launch_axis(spk_ctx* c, AxisArgs& a, int dir) {
         a.tr_outer = c->d_keep + c->nkx;
         a.tr_fd_kb = FastDiv::make((unsigned)a.tr_nkb);
         a.tr_fd_box = FastDiv::make((unsigned)(a.tr_nouter * a.tr_nkb));
-        a.tr_fd_job = FastDiv::make((unsigned)(a.tr_nouter * a.tr_nkb));
+        a.tr_fd_job = FastDiv::make((unsigned)(a.nb * a.tr_nouter * a.tr_nkb));
     }
     if (a.trim) {
         // kept tiles of a trimmed single-box pass (used when the state has no masked content)
@@ -378,6 +384,9 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
         const double score = util * ctas;
         if (score >= best) { best = score; L = cand; }
     }
+    if (c->tune_zl > 0 && c->tune_zl <= nlines && need(c->tune_zl) <= (size_t)227 * 1024 &&
+        (c->nb == 1 || nlines % c->tune_zl == 0))
+        L = c->tune_zl;
     const size_t smem = need(L);
     if (smem > (size_t)227 * 1024) {
         c->err = "internal: z pass tile exceeds shared memory";
@@ -609,7 +618,8 @@ static void rhs(spk_ctx* c, XfArgs& x) {
     const FastDiv fz = FastDiv::make((unsigned)c->nzh);
     // 128-thread CTAs, three per SM: every load of a mode is issued up front
     const size_t modes = x.defer ? (size_t)x.nkx * x.nky * c->kz_keep : c->nc;
-    const int grid = (int)std::min<size_t>((modes * c->nb + 127) / 128, (size_t)c->num_sms * 3 * 8);
+    const size_t per_sm = c->tune_rhs > 0 ? (size_t)c->tune_rhs : 24;
+    const int grid = (int)std::min<size_t>((modes * c->nb + 127) / 128, (size_t)c->num_sms * per_sm);
     c->launches++;
     if (c->fp32) k_rhs<float><<<grid, 128, 0, c->stream>>>(x, fz);
     else k_rhs<double><<<grid, 128, 0, c->stream>>>(x, fz);
@@ -2049,3 +2059,4 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
 }
 
 #include "spk_closure_api.cu"
+#include "spk_tune.cu"

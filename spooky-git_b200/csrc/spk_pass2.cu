@@ -38,9 +38,11 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     const int tid = threadIdx.x;
     const int c = tid & (KT - 1), q = tid >> LKT;
     const int nouter = a.axis == 0 ? a.g.ny : a.g.nx;
-    // a trimmed single-box pass with no masked content walks only the tiles
-    // it keeps (every CTA reads the same flag)
-    const bool ctile = a.tr_always || (a.trim && a.nb == 1 && !a.scs[0].masked_live);
+    // a trimmed pass whose boxes all have no masked content walks only the
+    // tiles it keeps (every CTA reads the same flags)
+    bool all_clear = a.trim != 0;
+    for (int b = 0; all_clear && b < a.nb; b++) all_clear = !a.scs[b].masked_live;
+    const bool ctile = a.tr_always || all_clear;
     const bool couter = ctile && (a.trim == 1 || a.tr_always);
     const int nkb = ctile ? a.tr_nkb : (a.kcols + KT - 1) / KT;
     const int nouter_e = couter ? a.tr_nouter : nouter;

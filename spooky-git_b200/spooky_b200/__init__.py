@@ -38,7 +38,8 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_ensemble_synchronize", "spk_ensemble_kernels_per_step",
             "spk_closure_set", "spk_products", "spk_closure_samples_size", "spk_closure_samples",
             "spk_trainer_create", "spk_trainer_destroy", "spk_trainer_set_params", "spk_trainer_get_params",
-            "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train", "spk_spectrum"]
+            "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train", "spk_spectrum",
+            "spk_autotune", "spk_ensemble_autotune"]
 
 # learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
@@ -117,6 +118,8 @@ def lib():
         L.spk_trainer_loss_grad.argtypes = [vp, fp, fp]
         L.spk_trainer_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp]
         L.spk_spectrum.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip, dp, dp]
+        L.spk_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ip, dp, dp]
+        L.spk_ensemble_autotune.argtypes = [vp, ctypes.c_int]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
             if name not in ("spk_params_default", "spk_last_error"):
@@ -309,6 +312,16 @@ class Context:
         self._check(lib().spk_budgets(self._h, ctypes.byref(b)))
         return np.array(b.energy[: self.F]), np.array(b.dissipation[: self.F])
 
+    def autotune(self, steps=5):
+        """spk_autotune: pick the z-pass lines per CTA, axis stages and RHS
+        grid by timing; returns the choices and ms per step before/after."""
+        zl, nst, rhs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        b, a = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().spk_autotune(self._h, int(steps), ctypes.byref(zl), ctypes.byref(nst), ctypes.byref(rhs),
+                                       ctypes.byref(b), ctypes.byref(a)))
+        return dict(z_lines=zl.value, axis_stages=nst.value, rhs_ctas_per_sm=rhs.value, ms_before=b.value,
+                    ms_after=a.value)
+
     # -- diagnostics ---------------------------------------------------------
     def spectrum(self, f1, f2=None):
         """Shell spectrum of fields f1, f2 (indices or names such as "vx")
@@ -492,6 +505,10 @@ class Ensemble:
 
     def advance(self, nsteps=1):
         self._check(lib().spk_ensemble_advance(self._h, int(nsteps)))
+
+    def autotune(self, steps=5):
+        """spk_ensemble_autotune: tune every group's schedule by timing."""
+        self._check(lib().spk_ensemble_autotune(self._h, int(steps)))
 
     def synchronize(self):
         self._check(lib().spk_ensemble_synchronize(self._h))

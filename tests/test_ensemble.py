@@ -86,3 +86,37 @@ def test_ensemble_rejects_alternating_sts_and_empty_lists():
     with pytest.raises(S.SpookyError) as e:
         Ensemble([])
     assert e.value.code == 1
+
+
+@pytest.mark.gpu
+def test_autotuned_runs_compute_the_same_bits():
+    """spk_autotune changes launch choices only: a tuned context and an
+    untuned one give the same state, and the ensemble likewise."""
+    p = default_params(incompressible=1, mhd=1, gridsize=(32, 32, 32), boxsize=(L, L, L), reynolds=300.0,
+                       reynolds_magnetic=300.0, form=SPK_FORM_FP32, t_final=1e30, toutput_flow=1e30)
+    U = initial_state(p, 7)
+    a, b = Context(p), Context(p)
+    a.set_state(U)
+    b.set_state(U)
+    r = a.autotune(steps=2)
+    assert r["ms_after"] <= r["ms_before"] and a.get_time()[2] == 0
+    a.advance(5)
+    b.advance(5)
+    a.synchronize()
+    b.synchronize()
+    assert np.array_equal(a.get_state(), b.get_state())
+    params = box_params()[:4]
+    ens = Ensemble(params)
+    ref = Ensemble(params)
+    for i, q in enumerate(params):
+        ens.boxes[i].set_state(initial_state(q, 40 + i))
+        ref.boxes[i].set_state(initial_state(q, 40 + i))
+    ens.autotune(steps=2)
+    ens.advance(3)
+    ref.advance(3)
+    ens.synchronize()
+    ref.synchronize()
+    for i in range(len(params)):
+        assert np.array_equal(ens.boxes[i].get_state(), ref.boxes[i].get_state()), i
+    ens.close()
+    ref.close()
