@@ -365,9 +365,11 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int slots = std::max(1, nthr / RegFft<T, N>::TPC);
     const long nlines = (long)c->nx * c->ny;
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
+    const int gen = z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL) ? 1 : 0);
+    const int max_ctas = gen == 0 ? 5 : 4;   // the kernel's launch bounds
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
-                            slots, z.closure ? CL_NP : 0).total;
+                            slots, z.closure ? CL_NP : 0, zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots)).total;
     };
     // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
     auto rounds = [&](long n) { return (n + slots - 1) / slots; };
@@ -380,7 +382,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
         const long work = (long)(npin + npout) * cand;
         const long cap = (rounds((long)npin * cand) + rounds((long)npout * cand)) * slots;
         const double util = (double)work / (double)std::max<long>(cap, 1);
-        const int ctas = (int)std::min<size_t>(4, (size_t)(233472 / (sm + 1024)));
+        const int ctas = (int)std::min<size_t>((size_t)max_ctas, (size_t)(233472 / (sm + 1024)));
         const double score = util * ctas;
         if (score >= best) { best = score; L = cand; }
     }

@@ -245,8 +245,15 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
 // barrier, twiddle tables, input half spectra (later: the product pairs),
 // real fields, exchange slots.
 struct ZSmem { size_t tw, zero, junk, area, real, xb, cw, total; };
+// alias: the plain variant with one round of transforms in each direction
+// and at least two FFT stages keeps its exchange slots in the input/product
+// area: every slot has loaded its legs before the first exchange barrier (a
+// one-stage transform has no such barrier before its stores to the slots)
+__host__ __device__ inline bool zpass_alias(int gen, int nstages, int npin, int npout, int lines, int slots) {
+    return gen == 0 && nstages >= 2 && npin * lines <= slots && npout * lines <= slots;
+}
 __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
-                                              int nzs, int slots, int ncw) {
+                                              int nzs, int slots, int ncw, bool alias) {
     ZSmem z;
     const int rs = n + 16, xs = n + (n >> 4);
     z.tw = 128;
@@ -254,9 +261,13 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     z.junk = align16(z.zero + (size_t)nzs * csz);            // a real row that idle transforms write
     z.area = align16(z.junk + (size_t)rs * (csz / 2));
     const size_t raw = (size_t)nin * lines * nzs * csz, prod = (size_t)npout * lines * n * csz;
-    z.real = align16(z.area + (raw > prod ? raw : prod));
-    z.xb = align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
-    z.cw = align16(z.xb + (size_t)slots * xs * csz);         // closure MLP parameters (floats)
+    const size_t xbs = (size_t)slots * xs * csz;
+    size_t area = raw > prod ? raw : prod;
+    if (alias && xbs > area) area = xbs;
+    z.real = align16(z.area + area);
+    z.xb = alias ? z.area : align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
+    const size_t end = alias ? z.real + (size_t)nin_all * lines * rs * (csz / 2) : z.xb + xbs;
+    z.cw = align16(end);                                     // closure MLP parameters (floats)
     z.total = align16(z.cw + (size_t)ncw * sizeof(float));
     return z;
 }
@@ -266,7 +277,7 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
 // general path with the learned closure (its own instantiation, so that the
 // MLP's registers do not weigh on the others).
 template <typename T, int N, int GEN>
-__global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs a) {
+__global__ void __launch_bounds__(128, GEN == 0 ? 5 : 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, N>;
     constexpr int LTPC = F::LTPC, TPC = F::TPC;
     constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
@@ -288,7 +299,9 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
     const bool clos = GEN == 2 && a.closure;
-    const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots, clos ? CL_NP : 0);
+    const bool alias = zpass_alias(GEN, F::NS, npin, npout, L, slots);
+    const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots,
+                                   clos ? CL_NP : 0, alias);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
     C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
@@ -510,8 +523,13 @@ __global__ void __launch_bounds__(128, 4) k_zpass2(const __grid_constant__ ZArgs
             if (a.nout & 1) put(a.nout, (T)0);
         }
         if (a.do_max) {
-            // the exchange slots are free here: 6 x 32 block-max scratch
+            // block-max scratch (8 x 32): the exchange slots, or with aliased
+            // slots the real fields (every warp has left the point loop)
             T* red = reinterpret_cast<T*>(xb);
+            if (alias) {
+                __syncthreads();
+                red = real;
+            }
             const int nmax = clos ? 8 : 6;
             warp_block_max<T>(mu, nmax, red);
             if (tid < nmax) {
