@@ -366,7 +366,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const long nlines = (long)c->nx * c->ny;
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
     const int gen = z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL) ? 1 : 0);
-    const int max_ctas = gen == 0 ? 5 : 4;   // the kernel's launch bounds
+    const int max_ctas = gen == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4;   // the kernel's launch bounds
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
                             slots, z.closure ? CL_NP : 0, zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots)).total;

@@ -277,7 +277,7 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
 // general path with the learned closure (its own instantiation, so that the
 // MLP's registers do not weigh on the others).
 template <typename T, int N, int GEN>
-__global__ void __launch_bounds__(128, GEN == 0 ? 5 : 4) k_zpass2(const __grid_constant__ ZArgs a) {
+__global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, N>;
     constexpr int LTPC = F::LTPC, TPC = F::TPC;
     constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
