@@ -623,8 +623,9 @@ static void rhs(spk_ctx* c, XfArgs& x) {
     const size_t per_sm = c->tune_rhs > 0 ? (size_t)c->tune_rhs : 24;
     const int grid = (int)std::min<size_t>((modes * c->nb + 127) / 128, (size_t)c->num_sms * per_sm);
     c->launches++;
-    if (c->fp32) k_rhs<float><<<grid, 128, 0, c->stream>>>(x, fz);
-    else k_rhs<double><<<grid, 128, 0, c->stream>>>(x, fz);
+    if (c->fp32 && !c->p.boussinesq) k_rhs<float, 4><<<grid, 128, 0, c->stream>>>(x, fz);
+    else if (c->fp32) k_rhs<float, 3><<<grid, 128, 0, c->stream>>>(x, fz);
+    else k_rhs<double, 3><<<grid, 128, 0, c->stream>>>(x, fz);
     if (x.defer && x.mode == XM_RK2) {
         // the step's masked modes, once
         c->launches++;

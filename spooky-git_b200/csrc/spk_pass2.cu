@@ -620,8 +620,11 @@ __device__ __forceinline__ double2 rk_value(const XfArgs& a, size_t gi, double2 
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 3) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
+// MINB: resident CTAs per SM the registers are budgeted for (4 for the FP32
+// HD/MHD form, where the few spills cost less than the lost occupancy; 3 for
+// the FP64 form and for Boussinesq, which keep more values live).
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArgs a, FastDiv fzh) {
     const size_t nc = a.g.nc;
     const int nzh = a.g.nzh, nzs = a.g.nzs;
     const unsigned ny = (unsigned)a.g.ny, nlines = (unsigned)(a.g.nx * a.g.ny);
