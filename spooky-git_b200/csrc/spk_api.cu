@@ -269,7 +269,13 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
-    if (c->tune_nst >= 2 && c->tune_nst <= 4 && fixed + (size_t)c->tune_nst * stage <= (size_t)227 * 1024)
+    if (nthr < 256) {
+        // narrow tiles (128 threads): 4 CTAs per SM with fewer stages each keep
+        // as many loads in flight as 2 CTAs with more, with twice the warps
+        const long nst4 = ((long)(56 * 1024) - (long)fixed) / (long)stage;
+        if (nst4 >= 1) a.nst = (int)std::min<long>(4, nst4);
+    }
+    if (c->tune_nst >= 1 && c->tune_nst <= 4 && fixed + (size_t)c->tune_nst * stage <= (size_t)227 * 1024)
         a.nst = c->tune_nst;
     const size_t smem = fixed + (size_t)a.nst * stage;
     cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

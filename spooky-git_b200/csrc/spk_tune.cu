@@ -55,7 +55,7 @@ extern "C" int spk_autotune(spk_ctx* c, int steps, int* zl, int* nst, int* rhs, 
     const float base = time_steps(c, steps, &rc);
     float best_ms = base;
     struct Knob { int* v; std::vector<int> cand; };
-    Knob knobs[3] = {{&c->tune_zl, {1, 2, 4, 8, 16, 32, 64}}, {&c->tune_nst, {2, 3, 4}}, {&c->tune_rhs, {6, 12, 24, 48}}};
+    Knob knobs[3] = {{&c->tune_zl, {1, 2, 4, 8, 16, 32, 64}}, {&c->tune_nst, {1, 2, 3, 4}}, {&c->tune_rhs, {6, 12, 24, 48}}};
     for (int kq = 0; kq < 3 && !rc; kq++) {
         int best = *knobs[kq].v;
         for (int v : knobs[kq].cand) {
