@@ -92,8 +92,8 @@ typedef struct spk_params {
     int    integrator;      /* SPK_INT_RK3 or SPK_INT_EULER                                        */
     int    sts_every_step;  /* 1: RKL cycle after the integrator on every step (the STS test build) */
     int    form;            /* SPK_FORM_PLAIN or SPK_FORM_FP32                                     */
-    int    closure;         /* 1: reserve the learned closure's gradient channels (HD/MHD; weights
-                               from spk_closure_set)                                               */
+    int    closure;         /* 1 or 2: reserve the learned closure's gradient channels for that
+                               variant (HD/MHD; weights from spk_closure_set)                      */
 } spk_params_t;
 
 /* Fill *p with the reference's defaults (parameters.cu:77-505). */
@@ -294,6 +294,13 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
 #define SPK_CLOSURE_ROW_SCALE  16
 #define SPK_CLOSURE_ROW_TT     17
 #define SPK_CLOSURE_ROW_TE     22
+
+/* Variants (spk_params_t.closure): 1 -- the gradients of the whole
+ * resolved field; 2 -- the gradients of its small scales only, the modes with
+ * |k| > k_c/2 (k_c the smallest dealiased cut-off): features, strain and
+ * current all come from that high-passed field, so that the eddy terms act
+ * mainly near the cut-off (a variational-multiscale form).  The samples of a
+ * coarse context follow its variant. */
 
 /* Switch the closure on (params: SPK_CLOSURE_NPARAM host floats) or off
  * (params NULL) for the context's RHS, steps and dt rule.  HD and MHD

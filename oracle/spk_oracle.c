@@ -401,6 +401,15 @@ static void closure_fields(orc_ctx* c, const cpx* U) {
     const size_t nr = c->g.nr, nc = c->g.nc;
     const int mhd = c->p.mhd;
     memset(c->rgrad, 0, sizeof(double) * 18 * nr);
+    /* variant 2 (closure = 2): gradients of the small scales |k| > k_c/2 only,
+     * k_c the smallest dealiased cut-off */
+    double hp_k2 = 0.0;
+    if (c->p.closure == 2) {
+        double kc = c->kxmax;
+        if (c->kymax < kc) kc = c->kymax;
+        if (c->kzmax < kc) kc = c->kzmax;
+        hp_k2 = 0.25 * kc * kc;
+    }
     for (int b = 0; b < (mhd ? 2 : 1); b++)
         for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++) {
@@ -408,7 +417,8 @@ static void closure_fields(orc_ctx* c, const cpx* U) {
                 FOR_MODES(c) {
                     MODE_VARS(c)
                     const double kj = j == 0 ? kx : (j == 1 ? ky : kz);
-                    c->ctmp[id] = c_scale(kj, c_muli(X[id]));
+                    const int small = !(hp_k2 > 0.0) || kx * kx + ky * ky + kz * kz > hp_k2;
+                    c->ctmp[id] = small ? c_scale(kj, c_muli(X[id])) : (cpx){0.0, 0.0};
                 }
                 c2r_3d(&c->g, c->ctmp, c->rgrad + (size_t)(9 * b + 3 * i + j) * nr, c->work);
             }

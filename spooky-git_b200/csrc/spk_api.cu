@@ -73,6 +73,8 @@ struct spk_ctx {
     int tune_nst = 0;              // axis passes: pipeline stages
     int tune_rhs = 0;              // RHS: CTAs per SM
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
+    int ngrad = 0;                 // closure variant 2: gradient channels (9 or 18) from ch_dx
+    double hp_k2 = 0.0;            // closure variant 2: small scales |k|^2 > hp_k2
     // shell spectra: bins (InputOutput / Wavevector, wavevector.cu:100-111)
     int nbins = 0;
     double deltak = 0.0;
@@ -507,7 +509,7 @@ static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx, int stage
         add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_th), 1, 1, 0, 0);
         if (with_gx && c->aniso_rhs) add_job(c, a, U + (size_t)c->TH * c->nc, chan(c, c->bufA, c->ch_gx), 1, 1, 1, 0);
     }
-    if (with_gx && c->closure_on) {
+    if (with_gx && c->closure_on && c->ngrad == 0) {
         int j0 = a.njobs;
         add_job(c, a, U + (size_t)c->VEL * c->nc, chan(c, c->bufA, c->ch_dx), 3, 1, 1, 0);
         mark(j0, 1);
@@ -517,7 +519,26 @@ static void pass_x_inverse(spk_ctx* c, const double2* U, bool with_gx, int stage
             mark(j0, 2);
         }
     }
+    // closure variant 2: d/dx_j of the small scales of u (then B), channel ch_dx + 3 j + i
+    auto grad_jobs = [&](AxisArgs& g, int field, int ch0, int grp) {
+        g.hp_k2 = c->hp_k2;
+        for (int j = 0; j < 3; j++) {
+            const int j0 = g.njobs;
+            add_job(c, g, U + (size_t)field * c->nc, chan(c, c->bufA, ch0 + 3 * j), 3, 1, j + 1, 0);
+            for (int q = j0; q < g.njobs; q++) { g.job[q].defer_grp = grp; g.job[q].hp = 1; }
+        }
+    };
+    const bool grad9 = with_gx && c->closure_on && c->ngrad > 0;
+    if (grad9) grad_jobs(a, c->VEL, c->ch_dx, 1);
     axis(c, a, +1);
+    if (grad9 && c->p.mhd) {
+        AxisArgs b = axis_args(c, 0);
+        b.scale = a.scale;
+        b.defer_stage = a.defer_stage;
+        b.trim = a.trim;
+        grad_jobs(b, c->MAG, c->ch_dx + 9, 2);
+        axis(c, b, +1);
+    }
 }
 
 static void pass_y_inverse(spk_ctx* c, bool with_g) {
@@ -527,6 +548,17 @@ static void pass_y_inverse(spk_ctx* c, bool with_g) {
         // u, B, theta and d/dx theta one to one; d/dy theta from theta
         add_job(c, a, c->bufA, c->bufB, c->ch_gx + 1, 0, 0, 0);
         add_job(c, a, chan(c, c->bufA, c->ch_th), chan(c, c->bufB, c->ch_gy), 1, 0, 1, 0);
+    } else if (with_g && c->closure_on && c->ngrad > 0) {
+        // variant 2: every channel one to one, in launches of at most SPK_MAXJOBS jobs
+        const int n = c->nin_base + c->ngrad;
+        for (int c0 = 0; c0 < n; c0 += SPK_MAXJOBS) {
+            AxisArgs b = axis_args(c, 1);
+            b.trim = a.trim;
+            const int m = std::min(SPK_MAXJOBS, n - c0);
+            add_job(c, b, chan(c, c->bufA, c0), chan(c, c->bufB, c0), m, 0, 0, 0);
+            axis(c, b, +1);
+        }
+        return;
     } else if (with_g && c->closure_on) {
         // u, B and their d/dx one to one; then d/dy of u, B (a second launch:
         // the jobs of one launch are capped)
@@ -570,13 +602,19 @@ static void set_inputs(spk_ctx* c, ZArgs& z, bool with_g) {
     z.ch_u = c->ch_u; z.ch_b = c->ch_b; z.ch_th = c->ch_th;
     if (with_g && c->aniso_rhs) { z.nin += 2; z.ch_gx = c->ch_gx; z.ch_gy = c->ch_gy; z.derive_gz = 1; }
     if (with_g && c->closure_on) {
-        z.nin += 2 * c->ncl_half;
         z.closure = 1;
-        z.ch_dx = c->ch_dx; z.ch_dy = c->ch_dy;
-        z.zder_n = c->ncl_half;
-        for (int d = 0; d < c->ncl_half; d++) z.zder_src[d] = c->ch_u + d;
+        z.ch_dx = c->ch_dx;
         z.cparams = c->d_cparams;
         z.delta2 = (float)c->delta2;
+        if (c->ngrad > 0) {
+            z.nin += c->ngrad;
+            z.cl_grad9 = 1;
+        } else {
+            z.nin += 2 * c->ncl_half;
+            z.ch_dy = c->ch_dy;
+            z.zder_n = c->ncl_half;
+            for (int d = 0; d < c->ncl_half; d++) z.zder_src[d] = c->ch_u + d;
+        }
     }
 }
 
@@ -891,6 +929,7 @@ static int check_params(const spk_params_t* p, std::string& why) {
     }
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
+    if (p->closure < 0 || p->closure > 2) { why = "closure must be 0, 1 (full-field model) or 2 (small-scale model)"; return SPK_ERR_ARG; }
     if (p->closure && (!p->incompressible || p->boussinesq)) { why = "the learned closure covers the HD and MHD modules"; return SPK_ERR_UNSUPPORTED; }
     if (p->closure && p->supertimestepping) { why = "the learned closure with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
     return SPK_OK;
@@ -1092,10 +1131,16 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     if (c->aniso_rhs) { c->ch_gx = ch; c->ch_gy = ch + 1; ch += 2; }
     c->ch_dx = c->ch_dy = -1;
     c->ncl_half = 0;
-    if (p.closure) {
+    if (p.closure == 1) {
         c->ncl_half = p.mhd ? 6 : 3;
         c->ch_dx = ch; ch += c->ncl_half;
         c->ch_dy = ch; ch += c->ncl_half;
+    } else if (p.closure == 2) {
+        // every gradient component from the x inverse, of the small scales only
+        c->ngrad = p.mhd ? 18 : 9;
+        c->ch_dx = ch; ch += c->ngrad;
+        const double kc = std::min(c->kxmax, std::min(c->kymax, c->kzmax));
+        c->hp_k2 = 0.25 * kc * kc;
     }
     c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
     c->nin = ch;

@@ -240,19 +240,22 @@ __global__ void k_sub(double2* y, const double2* x, size_t n) {
         y[i] = make_double2(y[i].x - x[i].x, y[i].y - x[i].y);
 }
 
-// Spectral gradients: out[9 b + 3 i + j] = i k_j U_{field(b, i)} (b = 0: u, 1: B).
-__global__ void k_gradients(const DevGrid g, const double2* U, int VEL, int MAG, int nb, double2* out) {
+// Spectral gradients: out[9 b + 3 i + j] = i k_j U_{field(b, i)} (b = 0: u, 1: B);
+// hp_k2 > 0: only modes with |k|^2 > hp_k2 (the closure's variant 2).
+__global__ void k_gradients(const DevGrid g, const double2* U, int VEL, int MAG, int nb, double hp_k2, double2* out) {
     const size_t nc = g.nc;
     for (size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x; id < nc; id += (size_t)gridDim.x * blockDim.x) {
         const int k = (int)(id % g.nzh);
         const size_t rr = id / g.nzh;
         const int j = (int)(rr % g.ny), i = (int)(rr / g.ny);
         const double kv[3] = {g.kx[i], g.ky[j], g.kz[k]};
+        const bool keep = !(hp_k2 > 0.0) || kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2] > hp_k2;
         for (int b = 0; b < nb; b++)
             for (int c = 0; c < 3; c++) {
                 const double2 x = U[(size_t)((b ? MAG : VEL) + c) * nc + id];
                 for (int d = 0; d < 3; d++)
-                    out[(size_t)(9 * b + 3 * c + d) * nc + id] = make_double2(-kv[d] * x.y, kv[d] * x.x);
+                    out[(size_t)(9 * b + 3 * c + d) * nc + id] =
+                        keep ? make_double2(-kv[d] * x.y, kv[d] * x.x) : make_double2(0.0, 0.0);
             }
     }
 }

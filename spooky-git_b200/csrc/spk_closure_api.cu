@@ -148,7 +148,8 @@ extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, flo
     if (rc) return rc;
     // gradients of the filtered state
     CK(cudaMemsetAsync(Gs, 0, sizeof(double2) * c->nc * 18, c->stream));
-    k_gradients<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->VEL, c->MAG, c->p.mhd ? 2 : 1, Gs);
+    k_gradients<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->VEL, c->MAG, c->p.mhd ? 2 : 1,
+                                                          c->p.closure == 2 ? c->hp_k2 : 0.0, Gs);
     c->launches++;
     rc = c2r_channels(c, Gs, 18, Rg);
     if (rc) return rc;

@@ -133,8 +133,11 @@ struct AxisJob {
     void* out;
     int ch;         // channel coordinate of the input in its tensor map
     int in_state;   // input is the FP64 state (double2) instead of the pass type
-    int deriv;      // multiply the input by i*k_axis(n) before the transform
+    int deriv;      // multiply the input by i*k before the transform: 1 k along the axis (row n),
+                    // 2 k of the outer index, 3 kz of the column
     int defer_grp;  // deferred masked modes: 1 velocity (nu), 2 magnetic field (nu_m), 0 none
+    int hp;         // keep only |k|^2 > AxisArgs::hp_k2 (the small scales of the closure's variant 2)
+    int pad_;
 };
 
 struct AxisArgs {
@@ -165,6 +168,7 @@ struct AxisArgs {
     // rows and of kz blocks past kz_keep), 2 = y inverse (skip kz blocks past
     // kz_keep; masked y rows, which the x inverse left unwritten, enter as 0)
     int trim;
+    double hp_k2;           // high-pass threshold of the jobs with hp set
     // single-box trimmed pass: enumerate only the kept tiles (tr_outer: the
     // kept outer indices of the x inverse, tr_nkb k blocks below kz_keep)
     int tr_nouter, tr_nkb;
@@ -207,6 +211,7 @@ struct ZArgs {
     // after the inputs); MLP parameters (SPK_CLOSURE_NPARAM floats)
     int trim;               // masked content absent: the kz >= kz_keep tail of every input row enters as 0
     int closure, ch_dx, ch_dy;
+    int cl_grad9;           // closure variant 2: the 9 (18) gradient channels from ch_dx, [direction][component]
     int zder_n, zder_src[6];
     const float* cparams;
     float delta2;

@@ -135,8 +135,15 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         const int k0 = kb * KT;
         const int kt = min(KT, a.kcols - k0);
         const unsigned char* stg = stages + (size_t)s * stage_bytes;
-        const bool deriv = jo.deriv != 0;
+        const int deriv = jo.deriv;
         const double scale = a.scale;
+        // derivative along the outer index or the column, and the high-pass
+        // of the closure's small scales (uniform over the CTA)
+        double kout = 0.0, kcol = 0.0;
+        if (deriv >= 2 || jo.hp) {
+            kout = a.axis == 0 ? a.g.ky[o] : a.g.kx[o];
+            kcol = a.g.kz[min(k0 + c, a.g.nzh - 1)];
+        }
         const bool skip = (a.outer_filter && !okeep[o]) || trimmed(box, o, kb);   // uniform over the CTA
         // trimmed y inverse: masked y rows were not written by the x inverse
         const bool zrows = a.trim == 2 && !skip && !a.scs[box].masked_live;
@@ -178,7 +185,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 double2 x = src[n * KT + c];
-                if (deriv) x = ik_mul(kd[n], x);
+                if (deriv) x = ik_mul(deriv == 1 ? kd[n] : (deriv == 2 ? kout : kcol), x);
+                if (jo.hp && !(kd[n] * kd[n] + kout * kout + kcol * kcol > a.hp_k2)) x = make_double2(0.0, 0.0);
                 C2<T> v = mk<T>((T)(x.x * scale), (T)(x.y * scale));
                 if constexpr (DEF)
                     if (dfr) { const T f = deferred(n); v = mk<T>(f * v.x, f * v.y); }
@@ -192,7 +200,14 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
                 if (zrows && !keep[n]) v = mk<T>((T)0, (T)0);
                 if constexpr (DEF)
                     if (dfr) { const T f = (T)deferred(n); v = mk<T>(f * v.x, f * v.y); }
-                if (deriv) { const T kk = kax[n]; v = mk<T>(-kk * v.y, kk * v.x); }
+                if (deriv) {
+                    const T kk = deriv == 1 ? kax[n] : (T)(deriv == 2 ? kout : kcol);
+                    v = mk<T>(-kk * v.y, kk * v.x);
+                }
+                if (jo.hp) {
+                    const double kn = a.axis == 0 ? a.g.kx[n] : a.g.ky[n];
+                    if (!(kn * kn + kout * kout + kcol * kcol > a.hp_k2)) v = mk<T>((T)0, (T)0);
+                }
                 return mk<T>(v.x * sc, v.y * sc);
             });
         }
@@ -463,14 +478,25 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             float ctau[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, cemf[3] = {0.f, 0.f, 0.f};
             if (clos) {
                 float A[9], G[9], vn, ve;
+                if (a.cl_grad9) {
+                    // variant 2: channel ch_dx + 3 j + i holds d u_i / d x_j (B: + 9)
 #pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    A[3 * i + 0] = (float)fr[(a.ch_dx + i) * LRS];
-                    A[3 * i + 1] = (float)fr[(a.ch_dy + i) * LRS];
-                    A[3 * i + 2] = (float)fr[(nder0 + i) * LRS];
-                    G[3 * i + 0] = a.mhd ? (float)fr[(a.ch_dx + 3 + i) * LRS] : 0.f;
-                    G[3 * i + 1] = a.mhd ? (float)fr[(a.ch_dy + 3 + i) * LRS] : 0.f;
-                    G[3 * i + 2] = a.mhd ? (float)fr[(nder0 + 3 + i) * LRS] : 0.f;
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            A[3 * i + j] = (float)fr[(a.ch_dx + 3 * j + i) * LRS];
+                            G[3 * i + j] = a.mhd ? (float)fr[(a.ch_dx + 9 + 3 * j + i) * LRS] : 0.f;
+                        }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 3; i++) {
+                        A[3 * i + 0] = (float)fr[(a.ch_dx + i) * LRS];
+                        A[3 * i + 1] = (float)fr[(a.ch_dy + i) * LRS];
+                        A[3 * i + 2] = (float)fr[(nder0 + i) * LRS];
+                        G[3 * i + 0] = a.mhd ? (float)fr[(a.ch_dx + 3 + i) * LRS] : 0.f;
+                        G[3 * i + 1] = a.mhd ? (float)fr[(a.ch_dy + 3 + i) * LRS] : 0.f;
+                        G[3 * i + 2] = a.mhd ? (float)fr[(nder0 + 3 + i) * LRS] : 0.f;
+                    }
                 }
                 closure_point(cw, a.delta2, A, G, ctau, cemf, &vn, &ve);
                 if (live && a.do_max) {

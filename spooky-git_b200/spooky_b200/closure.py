@@ -105,10 +105,11 @@ def subgrid_weights(X):
 
 
 def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_steps=3000, batch=16384, lr=2e-3,
-        seed=0, form=SPK_FORM_PLAIN, log=None):
+        seed=0, form=SPK_FORM_PLAIN, variant=1, log=None):
     """Truth, samples, training and the two coarse runs; returns a dict of
     the measured quantities (spectral errors with and without the closure,
-    run costs, losses)."""
+    run costs, losses).  variant: 1 the full-field model, 2 the small-scale
+    model (gradients of the modes above half the cut-off)."""
     import torch
     say = log or (lambda *a: None)
     L = 2 * np.pi
@@ -118,7 +119,7 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     U0 = mhd_random_state(pf, 1, 2)
     fine = Context(pf)
     fine.set_state(U0)
-    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, **common)
+    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, closure=variant, **common)
     sampler = Context(pc0)
     Uf = torch.empty(fine.shape_c, dtype=torch.complex128, device="cuda")
     samples, truth_s, done = [], 0.0, 0
@@ -154,7 +155,7 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     U0c = filter_to(U0, pf, pc0)
     res = {}
     for name, cp in (("closure", params), ("plain", None)):
-        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=1, **common)
+        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=variant, **common)
         ctx = Context(pc)
         if cp is not None:
             ctx.closure_set(cp)
