@@ -365,8 +365,11 @@ def run_closure(args, world, rank, local_rank):
     if rank != 0:
         return
     nf, ncs = args.n, args.n // 4
+    # weight of the energy-transfer error in the loss (None: the workflow's
+    # per-variant default)
+    transfer = args.closure_transfer if args.closure_transfer is not None else {1: 0.0, 2: 4.0}[args.closure_variant]
     r = C.run(n_fine=nf, n_coarse=ncs, steps=args.closure_steps, snap_every=max(args.closure_steps // 8, 1),
-              train_steps=3000, batch=16384, lr=2e-3, variant=args.closure_variant,
+              train_steps=3000, batch=16384, lr=2e-3, variant=args.closure_variant, transfer=transfer,
               log=lambda m: print(m, file=sys.stderr, flush=True))
     print(json.dumps({
         "metric": f"{ncs}^3 learned-closure run vs filtered {nf}^3 truth: RMS relative shell-spectrum error",
@@ -375,7 +378,8 @@ def run_closure(args, world, rank, local_rank):
         "config": {"workload": f"MHD {nf}^3 truth (plain form, {args.closure_steps} steps, nu = eta = 2e-4) -> "
                                f"{ncs}^3 closure run, sharp filter k_c = {r['k_cut']}",
                    "train_steps": 3000, "batch": 16384,
-                   "closure_variant": {1: "full-field model", 2: "small-scale model"}[args.closure_variant]},
+                   "closure_variant": {1: "full-field model", 2: "small-scale model"}[args.closure_variant],
+                   "loss_transfer_weight": transfer},
         "error_without_closure": r["error_plain"],
         "error_u": {"closure": r["error_u_closure"], "plain": r["error_u_plain"]},
         "error_b": {"closure": r["error_b_closure"], "plain": r["error_b_plain"]},
@@ -405,6 +409,8 @@ def main():
                     help="learned-closure workload instead: --n truth, --n/4 closure run (config 5)")
     ap.add_argument("--closure-steps", type=int, default=2000)
     ap.add_argument("--closure-variant", type=int, default=1, choices=[1, 2])
+    ap.add_argument("--closure-transfer", type=float, default=None,
+                    help="weight of the energy-transfer error in the closure loss (default: 0 variant 1, 4 variant 2)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")

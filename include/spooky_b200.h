@@ -280,13 +280,18 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
  * Training samples are SoA float rows (row r of every sample contiguous,
  * rows `stride` floats apart): features[8], S[5] (xx xy xz yy yz), J[3],
  * Delta^2 n, target stress[5] (the Basdevant channels: xx xy xz yy yz),
- * target EMF[3].  The loss is the mean over samples of
- *   w0 |dT - T_target|_F^2 + w1 |dE - E_target|^2
- * (the full traceless symmetric stress in the Frobenius norm). */
+ * target EMF[3], and the strain Sf[5] and current Jf[3] of the whole
+ * resolved field (equal to S, J in variant 1).  The loss is the mean over
+ * samples of
+ *   w0 |dT - T_target|_F^2 + w1 |dE - E_target|^2 + w2 (P - P_target)^2
+ * (the full traceless symmetric stress in the Frobenius norm), where
+ * P = -dT:Sf - dE.Jf = 2 nu_t S:Sf + eta_t J.Jf is the model's transfer of
+ * resolved energy to the subgrid scales and P_target = -T_target:Sf -
+ * E_target.Jf the true one (dissipation matching). */
 #define SPK_CLOSURE_NFEAT   8
 #define SPK_CLOSURE_HIDDEN  32
 #define SPK_CLOSURE_NPARAM  (32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2)
-#define SPK_CLOSURE_ROWS    25
+#define SPK_CLOSURE_ROWS    33
 /* sample rows */
 #define SPK_CLOSURE_ROW_FEAT   0
 #define SPK_CLOSURE_ROW_S      8
@@ -294,6 +299,8 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
 #define SPK_CLOSURE_ROW_SCALE  16
 #define SPK_CLOSURE_ROW_TT     17
 #define SPK_CLOSURE_ROW_TE     22
+#define SPK_CLOSURE_ROW_SF     25
+#define SPK_CLOSURE_ROW_JF     30
 
 /* Variants (spk_params_t.closure): 1 -- the gradients of the whole
  * resolved field; 2 -- the gradients of its small scales only, the modes with
@@ -340,7 +347,7 @@ int spk_trainer_create(void* cuda_stream, spk_trainer** out);
 int spk_trainer_destroy(spk_trainer* tr);
 int spk_trainer_set_params(spk_trainer* tr, const float* params);        /* host floats; resets Adam */
 int spk_trainer_get_params(spk_trainer* tr, float* params);              /* host floats */
-int spk_trainer_set_samples(spk_trainer* tr, const float* samples, size_t n, size_t stride, const float w[2]);
+int spk_trainer_set_samples(spk_trainer* tr, const float* samples, size_t n, size_t stride, const float w[3]);
 /* Full-batch mean loss and gradient at the current parameters (host outputs). */
 int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad);
 /* nsteps Adam steps (lr) on minibatches of `batch` samples; loss_hist

@@ -74,7 +74,7 @@ def set_threads(n):
 
 # ---- learned closure (include/spooky_b200.h, SPK_CLOSURE_*) ----------------
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
-CLOSURE_ROWS = 25
+CLOSURE_ROWS = 33
 
 
 def closure_features(A, G):
@@ -95,10 +95,11 @@ def closure_mlp(params, f):
 
 
 def closure_loss_grad(samples, params, w):
-    """samples: [CLOSURE_ROWS, n] rows; returns (loss, grad)."""
+    """samples: [CLOSURE_ROWS, n] rows; w: the stress, EMF and energy-transfer
+    weights (a third weight left out is 0); returns (loss, grad)."""
     X = np.ascontiguousarray(samples, dtype=np.float64)
     params = np.ascontiguousarray(params, dtype=np.float64)
-    w = np.ascontiguousarray(w, dtype=np.float64)
+    w = np.zeros(3) + np.pad(np.asarray(w, dtype=np.float64), (0, 3 - len(w)))   # w[2] defaults to 0
     g = np.empty(CLOSURE_NPARAM)
     loss = ctypes.c_double()
     lib().orc_closure_loss_grad(_dp(X), X.shape[1], X.shape[1], _dp(params), _dp(w), _dp(g), ctypes.byref(loss))

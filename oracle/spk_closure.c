@@ -91,7 +91,9 @@ void orc_closure_loss_grad(const double* X, size_t n, size_t stride, const doubl
     memset(grad, 0, sizeof(double) * SPK_CLOSURE_NPARAM);
     double L = 0.0;
     for (size_t s = 0; s < n; s++) {
-        double f[NF], S[5], J[3], tT[5], tE[3];
+        double f[NF], S[5], J[3], tT[5], tE[3], Sf[5], Jf[3];
+        for (int r = 0; r < 5; r++) Sf[r] = X[(SPK_CLOSURE_ROW_SF + r) * stride + s];
+        for (int r = 0; r < 3; r++) Jf[r] = X[(SPK_CLOSURE_ROW_JF + r) * stride + s];
         for (int r = 0; r < NF; r++) f[r] = X[(SPK_CLOSURE_ROW_FEAT + r) * stride + s];
         for (int r = 0; r < 5; r++) S[r] = X[(SPK_CLOSURE_ROW_S + r) * stride + s];
         for (int r = 0; r < 3; r++) J[r] = X[(SPK_CLOSURE_ROW_J + r) * stride + s];
@@ -108,7 +110,15 @@ void orc_closure_loss_grad(const double* X, size_t n, size_t stride, const doubl
         const double fro = e[0] * e[0] + e[3] * e[3] + ezz * ezz + 2.0 * (e[1] * e[1] + e[2] * e[2] + e[4] * e[4]);
         double eE[3], emf = 0.0;
         for (int r = 0; r < 3; r++) { eE[r] = -eta * J[r] - tE[r]; emf += eE[r] * eE[r]; }
-        L += w[0] * fro + w[1] * emf;
+        /* dissipation matching: P = 2 nu S:Sf + eta J.Jf against -tT:Sf - tE.Jf */
+        const double SSf = S[0] * Sf[0] + S[3] * Sf[3] + (S[0] + S[3]) * (Sf[0] + Sf[3]) +
+                           2.0 * (S[1] * Sf[1] + S[2] * Sf[2] + S[4] * Sf[4]);
+        const double TSf = tT[0] * Sf[0] + tT[3] * Sf[3] + (tT[0] + tT[3]) * (Sf[0] + Sf[3]) +
+                           2.0 * (tT[1] * Sf[1] + tT[2] * Sf[2] + tT[4] * Sf[4]);
+        double JJf = 0.0, EJf = 0.0;
+        for (int r = 0; r < 3; r++) { JJf += J[r] * Jf[r]; EJf += tE[r] * Jf[r]; }
+        const double dP = (2.0 * nu * SSf + eta * JJf) - (-TSf - EJf);
+        L += w[0] * fro + w[1] * emf + w[2] * dP * dP;
         /* d fro / d e: zz enters through e0 and e3 */
         double ge[5];
         ge[0] = 2.0 * e[0] - 2.0 * ezz;
@@ -117,6 +127,8 @@ void orc_closure_loss_grad(const double* X, size_t n, size_t stride, const doubl
         double dnu = 0.0, deta = 0.0;
         for (int r = 0; r < 5; r++) dnu += w[0] * ge[r] * (-2.0 * S[r]);
         for (int r = 0; r < 3; r++) deta += w[1] * 2.0 * eE[r] * (-J[r]);
+        dnu += w[2] * 2.0 * dP * 2.0 * SSf;
+        deta += w[2] * 2.0 * dP * JJf;
         double d3[NO];
         d3[0] = dnu * scale * sigmoid(o[0]);
         d3[1] = deta * scale * sigmoid(o[1]);

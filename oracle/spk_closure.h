@@ -22,7 +22,7 @@ double orc_closure_features(const double* A, const double* G, double* feat, doub
 void orc_closure_mlp(const double* params, const double* f, double* o);
 
 /* Mean loss and its gradient over samples rows (SoA, row r at samples + r*stride);
- * w[0], w[1]: weights of the stress and EMF errors. */
+ * w[0], w[1], w[2]: weights of the stress, EMF and energy-transfer errors. */
 void orc_closure_loss_grad(const double* samples, size_t n, size_t stride, const double* params,
                            const double* w, double* grad, double* loss);
 

@@ -397,14 +397,15 @@ static void complex2real(orc_ctx* c, const cpx* Uin, double* R, int nf) {
 /* ---- learned closure terms (include/spooky_b200.h, SPK_CLOSURE_*): the
  * spectral gradients of u and B to real space, then per point the features,
  * the MLP and the terms -2 nu_t S, -eta_t J; maxima of nu_t and eta_t. */
-static void closure_fields(orc_ctx* c, const cpx* U) {
+/* The gradients A (9) and G (9) of U in real space into c->rgrad; use_hp:
+ * of the small scales |k| > k_c/2 only (variant 2), k_c the smallest
+ * dealiased cut-off. */
+static void closure_grads(orc_ctx* c, const cpx* U, int use_hp) {
     const size_t nr = c->g.nr, nc = c->g.nc;
     const int mhd = c->p.mhd;
     memset(c->rgrad, 0, sizeof(double) * 18 * nr);
-    /* variant 2 (closure = 2): gradients of the small scales |k| > k_c/2 only,
-     * k_c the smallest dealiased cut-off */
     double hp_k2 = 0.0;
-    if (c->p.closure == 2) {
+    if (use_hp) {
         double kc = c->kxmax;
         if (c->kymax < kc) kc = c->kymax;
         if (c->kzmax < kc) kc = c->kzmax;
@@ -422,6 +423,12 @@ static void closure_fields(orc_ctx* c, const cpx* U) {
                 }
                 c2r_3d(&c->g, c->ctmp, c->rgrad + (size_t)(9 * b + 3 * i + j) * nr, c->work);
             }
+}
+
+static void closure_fields(orc_ctx* c, const cpx* U) {
+    const size_t nr = c->g.nr;
+    const int mhd = c->p.mhd;
+    closure_grads(c, U, c->p.closure == 2);
     double numax = 0.0, etamax = 0.0;
     #pragma omp parallel for schedule(static) reduction(max : numax, etamax)
     for (long q = 0; q < (long)nr; q++) {
@@ -1138,7 +1145,18 @@ void orc_closure_samples(orc_ctx* f, const double* Uf, orc_ctx* c, double* X, si
         c->rgrad = (double*)calloc(nr * 18, sizeof(double));
         c->ctmp = (cpx*)calloc(nc, sizeof(cpx));
     }
-    closure_fields(c, c->U);   /* gradients (the MLP outputs are not used) */
+    /* strain and current of the whole resolved field, then the model's gradients */
+    double* full = (double*)malloc(sizeof(double) * nr * 8);
+    closure_grads(c, c->U, 0);
+    #pragma omp parallel for schedule(static)
+    for (long q = 0; q < (long)nr; q++) {
+        double A[9], G[9], fe[8], S5[5], J3[3];
+        for (int r = 0; r < 9; r++) { A[r] = c->rgrad[(size_t)r * nr + q]; G[r] = c->rgrad[(size_t)(9 + r) * nr + q]; }
+        orc_closure_features(A, G, fe, S5, J3);
+        for (int r = 0; r < 5; r++) full[(size_t)r * nr + q] = S5[r];
+        for (int r = 0; r < 3; r++) full[(size_t)(5 + r) * nr + q] = J3[r];
+    }
+    closure_grads(c, c->U, c->p.closure == 2);
     #pragma omp parallel for schedule(static)
     for (long q = 0; q < (long)nr; q++) {
         double A[9], G[9], fe[8], S5[5], J3[3];
@@ -1150,7 +1168,10 @@ void orc_closure_samples(orc_ctx* f, const double* Uf, orc_ctx* c, double* X, si
         X[(size_t)SPK_CLOSURE_ROW_SCALE * stride + q] = c->delta2 * n;
         for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_TT + r) * stride + q] = Rt[(size_t)r * nr + q];
         for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_TE + r) * stride + q] = np == 8 ? Rt[(size_t)(5 + r) * nr + q] : 0.0;
+        for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_SF + r) * stride + q] = full[(size_t)r * nr + q];
+        for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_JF + r) * stride + q] = full[(size_t)(5 + r) * nr + q];
     }
+    free(full);
     free(Pf); free(Pt); free(Pc); free(Rt);
     f->closure_on = fon;
     c->closure_on = con;

@@ -26,7 +26,7 @@ struct TrainArgs {
     int minibatch;           // 1: sample r -> (a * ((base + r) mod n) + c) mod n
     unsigned long long a, c, base;
     const float* params;
-    float w0, w1;            // loss weights (stress, EMF)
+    float w0, w1, w2;        // loss weights (stress, EMF, energy transfer)
     float* partial;          // [gridDim.x][CL_NP + 1] (last: loss)
 };
 
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(CL_CHUNK) k_closure_grad(const __grid_constant
     for (size_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         const size_t r = ch * CL_CHUNK + tid;
         const bool valid = r < a.m;
-        float f[CL_NF], S[5], J[3], tT[5], tE[3], scale = 0.f;
+        float f[CL_NF], S[5], J[3], tT[5], tE[3], Sf[5], Jf[3], scale = 0.f;
         if (valid) {
             size_t s = r;
             if (a.minibatch) s = (size_t)((a.a * ((a.base + r) % a.n) + a.c) % a.n);
@@ -67,13 +67,17 @@ __global__ void __launch_bounds__(CL_CHUNK) k_closure_grad(const __grid_constant
             for (int i = 0; i < 5; i++) tT[i] = X[(size_t)(SPK_CLOSURE_ROW_TT + i) * a.stride];
 #pragma unroll
             for (int i = 0; i < 3; i++) tE[i] = X[(size_t)(SPK_CLOSURE_ROW_TE + i) * a.stride];
+#pragma unroll
+            for (int i = 0; i < 5; i++) Sf[i] = X[(size_t)(SPK_CLOSURE_ROW_SF + i) * a.stride];
+#pragma unroll
+            for (int i = 0; i < 3; i++) Jf[i] = X[(size_t)(SPK_CLOSURE_ROW_JF + i) * a.stride];
         } else {
 #pragma unroll
             for (int i = 0; i < CL_NF; i++) f[i] = 0.f;
 #pragma unroll
-            for (int i = 0; i < 5; i++) { S[i] = 0.f; tT[i] = 0.f; }
+            for (int i = 0; i < 5; i++) { S[i] = 0.f; tT[i] = 0.f; Sf[i] = 0.f; }
 #pragma unroll
-            for (int i = 0; i < 3; i++) { J[i] = 0.f; tE[i] = 0.f; }
+            for (int i = 0; i < 3; i++) { J[i] = 0.f; tE[i] = 0.f; Jf[i] = 0.f; }
         }
         // forward
         float h1[CL_NH], h2[CL_NH];
@@ -104,10 +108,20 @@ __global__ void __launch_bounds__(CL_CHUNK) k_closure_grad(const __grid_constant
         float eE[3], emf = 0.f;
 #pragma unroll
         for (int i = 0; i < 3; i++) { eE[i] = -eta * J[i] - tE[i]; emf += eE[i] * eE[i]; }
-        if (valid) lsum += a.w0 * fro + a.w1 * emf;
+        // energy transfer into the subgrid scales: model 2 nu S:Sf + eta J.Jf
+        // against the true -T:Sf - E.Jf (Sf, Jf of the whole resolved field)
+        const float SSf = S[0] * Sf[0] + S[3] * Sf[3] + (S[0] + S[3]) * (Sf[0] + Sf[3]) +
+                          2.f * (S[1] * Sf[1] + S[2] * Sf[2] + S[4] * Sf[4]);
+        const float TSf = tT[0] * Sf[0] + tT[3] * Sf[3] + (tT[0] + tT[3]) * (Sf[0] + Sf[3]) +
+                          2.f * (tT[1] * Sf[1] + tT[2] * Sf[2] + tT[4] * Sf[4]);
+        const float JJf = J[0] * Jf[0] + J[1] * Jf[1] + J[2] * Jf[2];
+        const float EJf = tE[0] * Jf[0] + tE[1] * Jf[1] + tE[2] * Jf[2];
+        const float dP = 2.f * nu * SSf + eta * JJf + TSf + EJf;
+        if (valid) lsum += a.w0 * fro + a.w1 * emf + a.w2 * dP * dP;
         const float ge0 = 2.f * e[0] - 2.f * ezz, ge3 = 2.f * e[3] - 2.f * ezz;
-        const float dnu = a.w0 * -2.f * (ge0 * S[0] + ge3 * S[3] + 4.f * (e[1] * S[1] + e[2] * S[2] + e[4] * S[4]));
-        float deta = 0.f;
+        const float dnu = a.w0 * -2.f * (ge0 * S[0] + ge3 * S[3] + 4.f * (e[1] * S[1] + e[2] * S[2] + e[4] * S[4])) +
+                          a.w2 * 4.f * dP * SSf;
+        float deta = a.w2 * 2.f * dP * JJf;
 #pragma unroll
         for (int i = 0; i < 3; i++) deta += a.w1 * 2.f * eE[i] * -J[i];
         const float d30 = valid ? dnu * scale / (1.f + expf(-o0)) : 0.f;
@@ -260,17 +274,37 @@ __global__ void k_gradients(const DevGrid g, const double2* U, int VEL, int MAG,
     }
 }
 
-// Sample rows from the real-space gradients Rg[18][nr] and targets Rt[np][nr].
-__global__ void k_closure_rows(const double* Rg, const double* Rt, int np, size_t nr, double delta2, float* X,
-                               size_t stride) {
+// Sample rows from the real-space gradients Rg[18][nr] of the model's input,
+// the whole field's gradients Rgf[18][nr] (nullptr: the same as Rg) and the
+// targets Rt[np][nr].
+__global__ void k_closure_rows(const double* Rg, const double* Rgf, const double* Rt, int np, size_t nr,
+                               double delta2, float* X, size_t stride) {
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nr; q += (size_t)gridDim.x * blockDim.x) {
         double A[9], G[9], f[8], S5[5], J3[3];
+        if (Rgf) {
+#pragma unroll
+            for (int r = 0; r < 9; r++) {
+                A[r] = Rgf[(size_t)r * nr + q];
+                G[r] = Rgf[(size_t)(9 + r) * nr + q];
+            }
+            closure_features<double>(A, G, f, S5, J3);
+#pragma unroll
+            for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_SF + r) * stride + q] = (float)S5[r];
+#pragma unroll
+            for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_JF + r) * stride + q] = (float)J3[r];
+        }
 #pragma unroll
         for (int r = 0; r < 9; r++) {
             A[r] = Rg[(size_t)r * nr + q];
             G[r] = Rg[(size_t)(9 + r) * nr + q];
         }
         const double n = closure_features<double>(A, G, f, S5, J3);
+        if (!Rgf) {
+#pragma unroll
+            for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_SF + r) * stride + q] = (float)S5[r];
+#pragma unroll
+            for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_JF + r) * stride + q] = (float)J3[r];
+        }
 #pragma unroll
         for (int r = 0; r < 8; r++) X[(size_t)(SPK_CLOSURE_ROW_FEAT + r) * stride + q] = (float)f[r];
 #pragma unroll

@@ -70,7 +70,7 @@ static int c2r_channels(spk_ctx* c, const double2* X, int nch, double* R) {
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 static int pad_to(int n, int F) { return ((n + F - 1) / F) * F; }
 
-struct SampleScratch { size_t pf, pt, pc, gs, rt, rg, total; };
+struct SampleScratch { size_t pf, pt, pc, gs, rt, rg, rgf, total; };
 static SampleScratch sample_scratch(const spk_ctx* f, const spk_ctx* c) {
     const int np = c->p.mhd ? 8 : 5;
     SampleScratch s;
@@ -80,7 +80,9 @@ static SampleScratch sample_scratch(const spk_ctx* f, const spk_ctx* c) {
     s.gs = s.pc + al256(sizeof(double2) * c->nc * np);
     s.rt = s.gs + al256(sizeof(double2) * c->nc * pad_to(18, c->F));
     s.rg = s.rt + al256(sizeof(double) * c->nr * np);
-    s.total = s.rg + al256(sizeof(double) * c->nr * 18);
+    s.rgf = s.rg + al256(sizeof(double) * c->nr * 18);
+    // the whole field's gradients, apart from the model's input in variant 2
+    s.total = s.rgf + (c->p.closure == 2 ? al256(sizeof(double) * c->nr * 18) : 0);
     return s;
 }
 
@@ -116,6 +118,7 @@ extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, flo
     double2* Gs = (double2*)(base + sl.gs);
     double* Rt = (double*)(base + sl.rt);
     double* Rg = (double*)(base + sl.rg);
+    double* Rgf = c->p.closure == 2 ? (double*)(base + sl.rgf) : nullptr;
     const int np = c->p.mhd ? 8 : 5;
     // products of the fine state (without the closure)
     const bool fon = f->closure_on;
@@ -146,14 +149,18 @@ extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, flo
     c->launches++;
     rc = c2r_channels(c, Pt, np, Rt);
     if (rc) return rc;
-    // gradients of the filtered state
-    CK(cudaMemsetAsync(Gs, 0, sizeof(double2) * c->nc * 18, c->stream));
-    k_gradients<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->VEL, c->MAG, c->p.mhd ? 2 : 1,
-                                                          c->p.closure == 2 ? c->hp_k2 : 0.0, Gs);
-    c->launches++;
-    rc = c2r_channels(c, Gs, 18, Rg);
-    if (rc) return rc;
-    k_closure_rows<<<ew_blocks(c->nr), 256, 0, c->stream>>>(Rg, Rt, np, c->nr, c->delta2, X, stride);
+    // gradients of the filtered state: the whole field's (variant 2: and those
+    // of its small scales, the model's input)
+    for (int pass = 0; pass < (Rgf ? 2 : 1); pass++) {
+        const bool hp = Rgf && pass == 1;
+        CK(cudaMemsetAsync(Gs, 0, sizeof(double2) * c->nc * 18, c->stream));
+        k_gradients<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U, c->VEL, c->MAG, c->p.mhd ? 2 : 1,
+                                                              hp ? c->hp_k2 : 0.0, Gs);
+        c->launches++;
+        rc = c2r_channels(c, Gs, 18, Rgf && !hp ? Rgf : Rg);
+        if (rc) return rc;
+    }
+    k_closure_rows<<<ew_blocks(c->nr), 256, 0, c->stream>>>(Rg, Rgf, Rt, np, c->nr, c->delta2, X, stride);
     c->launches++;
     return launch_status(c);
 }
@@ -196,7 +203,7 @@ struct spk_trainer {
     float *hist = nullptr, *h_hist = nullptr;
     const float* X = nullptr;
     size_t n = 0, stride = 0;
-    float w0 = 1.f, w1 = 1.f;
+    float w0 = 1.f, w1 = 1.f, w2 = 0.f;
     int t = 0;                       // Adam steps taken
     unsigned long long cursor = 0;   // samples drawn so far
 };
@@ -264,9 +271,9 @@ extern "C" int spk_trainer_get_params(spk_trainer* tr, float* params) {
     return SPK_OK;
 }
 
-extern "C" int spk_trainer_set_samples(spk_trainer* tr, const float* X, size_t n, size_t stride, const float w[2]) {
+extern "C" int spk_trainer_set_samples(spk_trainer* tr, const float* X, size_t n, size_t stride, const float w[3]) {
     if (!tr || !X || n == 0 || stride < n || !w) return fail(nullptr, SPK_ERR_ARG, "bad samples");
-    tr->X = X; tr->n = n; tr->stride = stride; tr->w0 = w[0]; tr->w1 = w[1];
+    tr->X = X; tr->n = n; tr->stride = stride; tr->w0 = w[0]; tr->w1 = w[1]; tr->w2 = w[2];
     tr->cursor = 0;
     return SPK_OK;
 }
@@ -283,7 +290,7 @@ static void trainer_grad(spk_trainer* tr, size_t m, bool minibatch, float* loss_
     a.a = mult % (tr->n > 0 ? tr->n : 1);
     a.c = tr->n / 3;
     a.base = tr->cursor;
-    a.params = tr->params; a.w0 = tr->w0; a.w1 = tr->w1;
+    a.params = tr->params; a.w0 = tr->w0; a.w1 = tr->w1; a.w2 = tr->w2;
     a.partial = tr->partial;
     const int nblk = (int)std::min<size_t>(CL_MAXBLK, (m + CL_CHUNK - 1) / CL_CHUNK);
     k_closure_grad<<<nblk, CL_CHUNK, grad_smem(), tr->stream>>>(a);

@@ -43,7 +43,7 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
 
 # learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
-CLOSURE_ROWS = 25
+CLOSURE_ROWS = 33
 
 
 class Budgets(ctypes.Structure):
@@ -410,10 +410,15 @@ class Trainer:
         return w
 
     def set_samples(self, X, weights):
-        """X: torch CUDA float32 [CLOSURE_ROWS, n] (kept referenced here)."""
+        """X: torch CUDA float32 [CLOSURE_ROWS, n] (kept referenced here);
+        weights: of the stress, EMF and energy-transfer errors (a third weight
+        left out is 0)."""
         _torch_sync()
         self._X = X
-        w = np.ascontiguousarray(weights, dtype=np.float32)
+        w = np.asarray(weights, dtype=np.float32).ravel()
+        if w.size not in (2, 3):
+            raise ValueError("weights: 2 or 3 values")
+        w = np.ascontiguousarray(np.pad(w, (0, 3 - w.size)))
         self._check(lib().spk_trainer_set_samples(self._h, X.data_ptr(), X.shape[1], X.stride(0), self._fp(w)))
 
     def loss_grad(self):

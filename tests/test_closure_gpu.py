@@ -51,7 +51,7 @@ def test_trainer_loss_and_gradient_match_oracle():
     P = random_params(rng)
     P[-2:] = 0.1
     P32 = P.astype(np.float32)
-    w = np.array([2.0, 3.0])
+    w = np.array([2.0, 3.0, 1.5])
     loss_o, g_o = O.closure_loss_grad(X.astype(np.float32).astype(np.float64), P32.astype(np.float64), w)
     tr = Trainer(P32)
     tr.set_samples(torch_dev(X, np.float32), w)
@@ -69,7 +69,7 @@ def test_first_adam_step_is_signed_lr():
     rng = np.random.default_rng(22)
     X = random_samples(rng, 2048)
     P = random_params(rng).astype(np.float32)
-    w = np.array([1.0, 1.0])
+    w = np.array([1.0, 1.0, 1.0])
     tr = Trainer(P)
     tr.set_samples(torch_dev(X, np.float32), w)
     _, g_o = O.closure_loss_grad(X.astype(np.float32).astype(np.float64), P.astype(np.float64), w)
@@ -91,7 +91,7 @@ def test_trainer_fits_a_teacher_network():
         nu, eta = X[16, s] * np.log1p(np.exp(o))
         X[17:22, s] = -2 * nu * X[8:13, s]
         X[22:25, s] = -eta * X[13:16, s]
-    w = np.array([1.0, 1.0]) / np.mean(X[17:25] ** 2)
+    w = np.array([1.0, 1.0, 1.0]) / np.mean(X[17:25] ** 2)
     tr = Trainer(random_params(rng).astype(np.float32))
     tr.set_samples(torch_dev(X, np.float32), w)
     l0, _ = tr.loss_grad()
@@ -186,12 +186,17 @@ def test_samples_match_oracle(mhd, variant):
     fine, coarse = Context(pf), Context(pc)
     got = closure_samples(fine, torch_dev(Uf), coarse).cpu().numpy().astype(np.float64)
     assert rel_l2(coarse.get_state(), oc.get_state()) < 1e-14
-    groups = [(0, 8), (8, 13), (13, 16), (16, 17), (17, 22), (22, 25)]
+    groups = [(0, 8), (8, 13), (13, 16), (16, 17), (17, 22), (22, 25), (25, 30), (30, 33)]
     for a, b in groups:
-        if not mhd and a in (13, 22):
+        if not mhd and a in (13, 22, 30):
             assert np.abs(got[a:b]).max() == 0.0
             continue
         assert rel_l2(got[a:b], want[a:b]) < 1e-5, (a, b)
+    # the whole field's strain and current: the model's own in variant 1
+    if variant == 1:
+        assert np.array_equal(got[25:33], got[8:16])
+    else:
+        assert rel_l2(got[25:30], got[8:13]) > 1e-2
 
 
 def test_trained_closure_beats_the_plain_coarse_run():

@@ -68,6 +68,8 @@ def random_samples(rng, n):
         f, S, J, nn = O.closure_features(_traceless(rng), _traceless(rng))
         X[0:8, s], X[8:13, s], X[13:16, s], X[16, s] = f, S, J, 0.02 * nn
     X[17:25] = 0.05 * rng.standard_normal((8, n))
+    # whole-field strain and current: the model's plus other scales
+    X[25:33] = X[8:16] + 0.3 * np.abs(X[8:16]).mean() * rng.standard_normal((8, n))
     return X
 
 
@@ -76,7 +78,7 @@ def test_loss_gradient_matches_finite_differences():
     P = random_params(rng)
     P[-2:] = 0.2   # softplus away from its flat end
     X = random_samples(rng, 64)
-    w = np.array([3.0, 2.0])
+    w = np.array([3.0, 2.0, 1.5])
     loss, g = O.closure_loss_grad(X, P, w)
     assert loss > 0
     for idx in rng.choice(O.CLOSURE_NPARAM, 40, replace=False).tolist() + [O.CLOSURE_NPARAM - 1, O.CLOSURE_NPARAM - 2]:
@@ -100,7 +102,7 @@ def test_adam_fits_a_teacher_network():
         nu, eta = X[16, s] * np.log1p(np.exp(o))
         X[17:22, s] = -2 * nu * X[8:13, s]
         X[22:25, s] = -eta * X[13:16, s]
-    w = np.array([1.0, 1.0]) / np.mean(X[17:25] ** 2)
+    w = np.array([1.0, 1.0, 1.0]) / np.mean(X[17:25] ** 2)
     P = random_params(rng)
     m, v = np.zeros_like(P), np.zeros_like(P)
     l0 = O.closure_loss_grad(X, P, w)[0]
