@@ -313,6 +313,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
+    const int sigma_w = (tid & ~31) >> LTPC;   // the lowest slot of this warp (warp-uniform)
     const bool clos = GEN == 2 && a.closure;
     const bool alias = zpass_alias(GEN, F::NS, npin, npout, L, slots);
     const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots,
@@ -369,6 +370,9 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         const int tau = base + sigma;
         const bool valid = tau < ninv;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
+        // false: no slot of this warp has a transform, and the warp skips the
+        // math (FP64 only: in FP32 the branches cost more than they save, measured)
+        const bool act = sizeof(T) == 4 || base + sigma_w < ninv;
         const C2<T>* pa = raw + (size_t)(2 * p * L + l) * nzs;
         const C2<T>* pb = 2 * p + 1 < nin ? pa + (size_t)L * nzs : zrow;
         auto chv = [&](int ch, int k) -> C2<T> {
@@ -393,7 +397,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             }
             return mk<T>((T)0, (T)0);
         };
-        regfft_load<T, N, +1>(r, q, [&](int n) -> C2<T> {
+        if (act) regfft_load<T, N, +1>(r, q, [&](int n) -> C2<T> {
             constexpr int NH = N >> 1;
             const int k = n <= NH ? n : N - n;
             C2<T> A, B;
@@ -421,7 +425,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
                 if (2 * p < nin) a.real_out[((size_t)(2 * p) * nlines + line) * N + z] = (double)v.x;
                 if (2 * p + 1 < nin) a.real_out[((size_t)(2 * p + 1) * nlines + line) * N + z] = (double)v.y;
             }
-        });
+        }, act);
     }
     __syncthreads();
     if (a.mode == ZM_TO_REAL) return;
@@ -582,8 +586,9 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         const bool valid = tau < nfw;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
         const C2<T>* pp = prod + (size_t)(p * L + l) * N;
-        regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
-        regfft_run<T, N, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; });
+        const bool act = sizeof(T) == 4 || base + sigma_w < nfw;
+        if (act) regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
+        regfft_run<T, N, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
         __syncthreads();
         for (int s2 = warp; s2 < slots; s2 += nwarp) {
             const int tau2 = base + s2;

@@ -146,38 +146,47 @@ __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
 // of the CTA must call it: it starts with a barrier (earlier reads of the
 // buffer, including a previous tile's, are complete) and ends with one (the
 // writes are visible).
+// act = false: a thread with no transform to run (it must be false for a
+// whole warp at a time) only takes part in the barriers, which stay at the
+// same instructions for every warp of the CTA.
 template <typename T, int N, int DIR, int S, typename XA>
-__device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr) {
+__device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool act = true) {
     using F = RegFft<T, N>;
     constexpr int R = F::radix(S);
     constexpr int BPT = F::E / R;
     __syncthreads();   // earlier readers of the exchange buffer are done
+    if (act) {
 #pragma unroll
-    for (int u = 0; u < BPT; u++)
+        for (int u = 0; u < BPT; u++)
 #pragma unroll
-        for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
+            for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
+    }
     __syncthreads();
     constexpr int R1 = F::radix(S + 1);
     constexpr int BPT1 = F::E / R1;
+    if (act) {
 #pragma unroll
-    for (int u = 0; u < BPT1; u++)
+        for (int u = 0; u < BPT1; u++)
 #pragma unroll
-        for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1>(q, u, r));
+            for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1>(q, u, r));
+    }
 }
 
 // FS: barrier before the last stage's stores (when store() writes into the
-// exchange buffer that the last exchange just read).
+// exchange buffer that the last exchange just read).  act: as for
+// regfft_exchange (no math, no stores, the same barriers).
 template <typename T, int N, int DIR, int S, bool FS, typename XA, typename ST>
-__device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store) {
+__device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
     using F = RegFft<T, N>;
-    regfft_stage_math<T, N, DIR, S>(a, q, tw);
+    if (act) regfft_stage_math<T, N, DIR, S>(a, q, tw);
     if constexpr (S + 1 < F::NS) {
-        regfft_exchange<T, N, DIR, S>(a, q, xaddr);
-        regfft_from<T, N, DIR, S + 1, FS>(a, q, tw, xaddr, store);
+        regfft_exchange<T, N, DIR, S>(a, q, xaddr, act);
+        regfft_from<T, N, DIR, S + 1, FS>(a, q, tw, xaddr, store, act);
     } else {
         if constexpr (FS && S > 0) __syncthreads();
         constexpr int R = F::radix(S), P = F::P(S);
         constexpr int BPT = F::E / R;
+        if (!act) return;
 #pragma unroll
         for (int u = 0; u < BPT; u++) {
             const int g = q + u * F::TPC;   // last stage: H = 1, beta = g
@@ -200,8 +209,8 @@ __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
 }
 
 template <typename T, int N, int DIR, bool FS = false, typename XA, typename ST>
-__device__ __forceinline__ void regfft_run(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store) {
-    regfft_from<T, N, DIR, 0, FS>(a, q, tw, xaddr, store);
+__device__ __forceinline__ void regfft_run(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
+    regfft_from<T, N, DIR, 0, FS>(a, q, tw, xaddr, store, act);
 }
 
 // Host mirror of the geometry.
