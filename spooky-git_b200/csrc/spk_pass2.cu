@@ -370,9 +370,8 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         const int tau = base + sigma;
         const bool valid = tau < ninv;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
-        // false: no slot of this warp has a transform, and the warp skips the
-        // math (FP64 only: in FP32 the branches cost more than they save, measured)
-        const bool act = sizeof(T) == 4 || base + sigma_w < ninv;
+        // false: no slot of this warp has a transform, and the warp skips the math
+        const bool act = base + sigma_w < ninv;
         const C2<T>* pa = raw + (size_t)(2 * p * L + l) * nzs;
         const C2<T>* pb = 2 * p + 1 < nin ? pa + (size_t)L * nzs : zrow;
         auto chv = [&](int ch, int k) -> C2<T> {
@@ -586,6 +585,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         const bool valid = tau < nfw;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
         const C2<T>* pp = prod + (size_t)(p * L + l) * N;
+        // (forward rounds: FP64 only; in FP32 the branches cost more than they save, measured)
         const bool act = sizeof(T) == 4 || base + sigma_w < nfw;
         if (act) regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
         regfft_run<T, N, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
