@@ -94,6 +94,8 @@ typedef struct spk_params {
     int    form;            /* SPK_FORM_PLAIN or SPK_FORM_FP32                                     */
     int    closure;         /* 1 or 2: reserve the learned closure's gradient channels for that
                                variant (HD/MHD; weights from spk_closure_set)                      */
+    double closure_kc_frac; /* variant 2: the small scales are |k| > closure_kc_frac * k_c
+                               (0: 1/2)                                                            */
 } spk_params_t;
 
 /* Fill *p with the reference's defaults (parameters.cu:77-505). */
@@ -304,7 +306,8 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
 
 /* Variants (spk_params_t.closure): 1 -- the gradients of the whole
  * resolved field; 2 -- the gradients of its small scales only, the modes with
- * |k| > k_c/2 (k_c the smallest dealiased cut-off): features, strain and
+ * |k| > f k_c (k_c the smallest dealiased cut-off, f =
+ * spk_params_t.closure_kc_frac, 1/2 when 0): features, strain and
  * current all come from that high-passed field, so that the eddy terms act
  * mainly near the cut-off (a variational-multiscale form).  The samples of a
  * coarse context follow its variant. */

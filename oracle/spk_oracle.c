@@ -409,7 +409,8 @@ static void closure_grads(orc_ctx* c, const cpx* U, int use_hp) {
         double kc = c->kxmax;
         if (c->kymax < kc) kc = c->kymax;
         if (c->kzmax < kc) kc = c->kzmax;
-        hp_k2 = 0.25 * kc * kc;
+        const double f = c->p.closure_kc_frac > 0.0 ? c->p.closure_kc_frac : 0.5;
+        hp_k2 = f * f * kc * kc;
     }
     for (int b = 0; b < (mhd ? 2 : 1); b++)
         for (int i = 0; i < 3; i++)

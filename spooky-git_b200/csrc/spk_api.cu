@@ -930,6 +930,7 @@ static int check_params(const spk_params_t* p, std::string& why) {
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
     if (p->closure < 0 || p->closure > 2) { why = "closure must be 0, 1 (full-field model) or 2 (small-scale model)"; return SPK_ERR_ARG; }
+    if (!(p->closure_kc_frac >= 0.0 && p->closure_kc_frac < 1.0)) { why = "closure_kc_frac must be in [0, 1)"; return SPK_ERR_ARG; }
     if (p->closure && (!p->incompressible || p->boussinesq)) { why = "the learned closure covers the HD and MHD modules"; return SPK_ERR_UNSUPPORTED; }
     if (p->closure && p->supertimestepping) { why = "the learned closure with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
     return SPK_OK;
@@ -1140,7 +1141,8 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
         c->ngrad = p.mhd ? 18 : 9;
         c->ch_dx = ch; ch += c->ngrad;
         const double kc = std::min(c->kxmax, std::min(c->kymax, c->kzmax));
-        c->hp_k2 = 0.25 * kc * kc;
+        const double f = p.closure_kc_frac > 0.0 ? p.closure_kc_frac : 0.5;
+        c->hp_k2 = f * f * kc * kc;
     }
     c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
     c->nin = ch;

@@ -113,14 +113,15 @@ def subgrid_weights(X, transfer=1.0):
 
 
 def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_steps=3000, batch=16384, lr=2e-3,
-        seed=0, form=SPK_FORM_PLAIN, variant=1, transfer=None, log=None):
+        seed=0, form=SPK_FORM_PLAIN, variant=1, transfer=None, kc_frac=0.0, log=None):
     """Truth, samples, training and the two coarse runs; returns a dict of
     the measured quantities (spectral errors with and without the closure,
     run costs, losses).  variant: 1 the full-field model, 2 the small-scale
     model (gradients of the modes above half the cut-off); transfer: the
     relative weight of the energy-transfer error in the loss (0: stress and
     EMF errors only; None: 0 for variant 1, 4 for variant 2, the better of
-    0, 1 and 4 in the 64^3-vs-256^3 workload)."""
+    0, 1 and 4 in the 64^3-vs-256^3 workload); kc_frac: variant 2's
+    small scales are |k| > kc_frac * k_c (0: 1/2)."""
     if transfer is None:
         transfer = {1: 0.0, 2: 4.0}[variant]
     import torch
@@ -132,7 +133,7 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     U0 = mhd_random_state(pf, 1, 2)
     fine = Context(pf)
     fine.set_state(U0)
-    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, closure=variant, **common)
+    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, closure=variant, closure_kc_frac=kc_frac, **common)
     sampler = Context(pc0)
     Uf = torch.empty(fine.shape_c, dtype=torch.complex128, device="cuda")
     samples, truth_s, done = [], 0.0, 0
@@ -168,7 +169,7 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     U0c = filter_to(U0, pf, pc0)
     res = {}
     for name, cp in (("closure", params), ("plain", None)):
-        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=variant, **common)
+        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=variant, closure_kc_frac=kc_frac, **common)
         ctx = Context(pc)
         if cp is not None:
             ctx.closure_set(cp)

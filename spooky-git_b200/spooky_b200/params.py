@@ -40,6 +40,7 @@ class Params(ctypes.Structure):
         ("fixed_dt", ctypes.c_double), ("integrator", ctypes.c_int),
         ("sts_every_step", ctypes.c_int), ("form", ctypes.c_int),
         ("closure", ctypes.c_int),
+        ("closure_kc_frac", ctypes.c_double),
     ]
 
     def copy(self):

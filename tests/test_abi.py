@@ -59,3 +59,15 @@ def test_context_creation_rejects_bad_config_without_gpu():
     with pytest.raises(S.SpookyError) as e:
         S.Context(p)
     assert e.value.code == 6
+
+
+def test_closure_threshold_outside_unit_interval_is_rejected_without_gpu():
+    """closure_kc_frac (variant 2's small-scale threshold, a fraction of the
+    cut-off) must lie in [0, 1); the check runs before any CUDA call."""
+    L = 6.283185307179586
+    p = default_params(incompressible=1, mhd=1, gridsize=(16, 16, 16), boxsize=(L, L, L), closure=2,
+                       closure_kc_frac=1.2)
+    with pytest.raises(S.SpookyError) as e:
+        S.Context(p)
+    assert e.value.code == 1   # SPK_ERR_ARG
+    assert "closure_kc_frac" in str(e.value)
