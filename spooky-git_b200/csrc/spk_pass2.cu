@@ -280,8 +280,12 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     size_t area = raw > prod ? raw : prod;
     if (alias && xbs > area) area = xbs;
     z.real = align16(z.area + area);
-    z.xb = alias ? z.area : align16(z.real + (size_t)nin_all * lines * rs * (csz / 2));
-    const size_t end = alias ? z.real + (size_t)nin_all * lines * rs * (csz / 2) : z.xb + xbs;
+    const size_t realb = (size_t)nin_all * lines * rs * (csz / 2);
+    // with aliased slots the block-max scratch (8 x 32 values) moves to the
+    // real fields, which a few short lines per CTA do not cover
+    const size_t redb = (size_t)8 * 32 * (csz / 2);
+    z.xb = alias ? z.area : align16(z.real + realb);
+    const size_t end = alias ? z.real + (realb > redb ? realb : redb) : z.xb + xbs;
     z.cw = align16(end);                                     // closure MLP parameters (floats)
     z.total = align16(z.cw + (size_t)ncw * sizeof(float));
     return z;

@@ -89,6 +89,29 @@ def test_ensemble_rejects_alternating_sts_and_empty_lists():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", [SPK_FORM_FP32, SPK_FORM_PLAIN])
+@pytest.mark.parametrize("n", [24, 32])
+def test_autotuned_short_hd_boxes_compute_the_same_bits(n, form):
+    """Short HD lines at one line per CTA (an autotuner candidate) share the
+    z pass's exchange slots with its input area, and the CFL block maxima
+    then use the real-field area: it must hold them.  Tuned and untuned
+    contexts give the same state."""
+    p = default_params(incompressible=1, gridsize=(n, n, n), boxsize=(L, L, L), reynolds=300.0, form=form,
+                       t_final=1e30, toutput_flow=1e30)
+    U = initial_state(p, 11)
+    a, b = Context(p), Context(p)
+    a.set_state(U)
+    b.set_state(U)
+    r = a.autotune(steps=2)
+    assert r["ms_after"] <= r["ms_before"]
+    a.advance(4)
+    b.advance(4)
+    a.synchronize()
+    b.synchronize()
+    assert np.array_equal(a.get_state(), b.get_state())
+
+
+@pytest.mark.gpu
 def test_autotuned_runs_compute_the_same_bits():
     """spk_autotune changes launch choices only: a tuned context and an
     untuned one give the same state, and the ensemble likewise."""
