@@ -248,8 +248,10 @@ struct AxisCfg { int kt; int nthr; size_t smem; };
 static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     AxisCfg a;
     const RegFftGeom g = regfft_geom(N, c->fp32);
-    int kt = std::min(64, 256 / g.TPC);
-    if (c->fp32 && state_in && kt > 2) kt /= 2;
+    const int full = std::min(64, 256 / g.TPC);
+    const int cols = std::max(pow2_ceil(N / 2 + 1), 32 / g.TPC);   // short axes: a cubic box's kz columns
+    int kt = (N < 64 && cols < full) ? cols : full;
+    if (c->fp32 && state_in && kt == full && kt > 2) kt /= 2;
     kt = std::max(kt, 2);
     a.kt = kt;
     a.nthr = kt * g.TPC;
@@ -257,6 +259,16 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     return a;
 }
 
+
+// The dynamic shared-memory cap of a pass kernel: the opt-in maximum, set
+// alike by every launch.  One instantiation serves contexts and ensemble
+// groups with different tile sizes, and a cap set to one launch's size would
+// be too small for a recorded launch of another (a kernel node launched on
+// its own, as a profiler's replay does).  Occupancy follows each launch's
+// own size.
+template <typename K> static void allow_full_smem(K* kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
 
 template <typename T, int N, int DIR, bool CONV, bool DEF = false>
 static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
@@ -280,7 +292,7 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     if (c->tune_nst >= 1 && c->tune_nst <= 4 && fixed + (size_t)c->tune_nst * stage <= (size_t)227 * 1024)
         a.nst = c->tune_nst;
     const size_t smem = fixed + (size_t)a.nst * stage;
-    cudaFuncSetAttribute(k_axis2<T, N, DIR, CONV, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_full_smem(k_axis2<T, N, DIR, CONV, DEF>);
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV, DEF>, nthr, smem);
     const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
@@ -407,13 +419,13 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
     if (z.closure) {
-        cudaFuncSetAttribute(k_zpass2<T, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_full_smem(k_zpass2<T, N, 2>);
         k_zpass2<T, N, 2><<<nblk, nthr, smem, c->stream>>>(z);
     } else if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
-        cudaFuncSetAttribute(k_zpass2<T, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_full_smem(k_zpass2<T, N, 1>);
         k_zpass2<T, N, 1><<<nblk, nthr, smem, c->stream>>>(z);
     } else {
-        cudaFuncSetAttribute(k_zpass2<T, N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_full_smem(k_zpass2<T, N, 0>);
         k_zpass2<T, N, 0><<<nblk, nthr, smem, c->stream>>>(z);
     }
 }

@@ -19,11 +19,18 @@ namespace spk {
 // Tile width of the strided-axis pass: KT columns x TPC threads = 256
 // threads (KT <= 64); an FP64 input tile in the FP32 form (CONV) is half as
 // wide so that one pipeline stage stays at 32 KB.
+//
+// Short axes (N < 64) take the tile no wider than the kz columns of a cubic
+// box, N/2 + 1 rounded up to a power of two, and at least one warp per CTA:
+// a 64-column tile on a 16^3 box would transform 55 columns of padding.
+__host__ __device__ constexpr int pow2_ceil(int n) { return n <= 1 ? 1 : 2 * pow2_ceil((n + 1) / 2); }
 template <typename T, int N, bool CONV>
 __host__ __device__ constexpr int axis_kt() {
     constexpr int tpc = RegFft<T, N>::TPC;
-    constexpr int kt = (256 / tpc) > 64 ? 64 : (256 / tpc);
-    return (CONV && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
+    constexpr int full = (256 / tpc) > 64 ? 64 : (256 / tpc);
+    constexpr int cols = pow2_ceil(N / 2 + 1) > 32 / tpc ? pow2_ceil(N / 2 + 1) : 32 / tpc;
+    constexpr int kt = (N < 64 && cols < full) ? cols : full;
+    return (CONV && kt == full && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
 }
 
 // DEF: the x inverse of RK3 stage 1 or 2 with deferred masked modes (its own
