@@ -103,6 +103,10 @@ class ClockSampler:
             for nm, v in zip(names, parts[4:8]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
@@ -490,8 +494,9 @@ def main():
             dist.destroy_process_group()
         return
 
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    clk_path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_rank{rank}.csv")
+    import tempfile
+    clk_fd, clk_path = tempfile.mkstemp(prefix=f"spk_bench_clocks_rank{rank}_", suffix=".csv")
+    os.close(clk_fd)
     ctx32, ms32, clocks = timed_run(SPK_FORM_FP32, clk_path)
     kps, bytes_step = ctx32.step_info()
     ctx64, ms64, _ = timed_run(SPK_FORM_PLAIN)

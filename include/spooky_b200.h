@@ -233,8 +233,14 @@ int spk_profile_passes(spk_ctx* ctx, int reps, spk_pass_stat_t* out, int max_out
  *   that first call before any stream capture.
  * - Every call shares the one array and clears what must start at zero;
  *   calls whose GPU work overlaps (other streams, other threads) race on it.
+ * - Each call copies the wavevector tables, twiddles and starting scalars
+ *   from host memory that lives only while the call runs; a call made on a
+ *   stream that is being captured returns SPK_ERR_UNSUPPORTED.
+ * - The learned closure is not available here: p->closure != 0 returns
+ *   SPK_ERR_UNSUPPORTED.
  * - Calls no cudaMalloc/cudaFree and no allocating library routine; errors
- *   are reported through spk_last_error(NULL). */
+ *   are reported through spk_last_error(NULL).  The first-call set-up is
+ *   guarded by a lock, so host threads may make their first calls at once. */
 #define SPK_NOALLOC_SCRATCH_BYTES (24u << 20)
 int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U, double* dU, void* cuda_stream);
 

@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -2015,9 +2016,12 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SPK_NOALLOC_SCR
 // array's name is only a stand-in: a kernel must receive this address.
 static void* g_noalloc_ptr[SPK_NOALLOC_MAX_DEVICES];
 
+static std::mutex g_noalloc_mutex;   // host threads making their first calls at once
+
 // Once per device, with that device current: the scratch address (and,
 // once per process, the tensor-map encoder).
 static int noalloc_setup(int dev) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (g_noalloc_ptr[dev]) return SPK_OK;
     spk_ctx* c = nullptr;   // errors go to spk_last_error(NULL)
     void* ptr = nullptr;
@@ -2040,9 +2044,25 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
     std::string why;
     int rc = check_params(p, why);
     if (rc != SPK_OK) return fail(nullptr, rc, why);
+    if (p->closure)
+        return fail(nullptr, SPK_ERR_UNSUPPORTED,
+                    "spk_compute_dfield_noalloc has no learned-closure parameters: set closure = 0");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SPK_NOALLOC_MAX_DEVICES)
         return fail(nullptr, SPK_ERR_CUDA, "no usable current device");
+    // The tables and starting scalars are copied from host memory that lives
+    // only for the duration of the call, so a capture would record copies
+    // from freed memory: a call on a capturing stream is refused.
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const cudaError_t e = cudaStreamIsCapturing(cuda_stream ? (cudaStream_t)cuda_stream : cudaStreamLegacy, &cs);
+        if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            if (e != cudaSuccess) cudaGetLastError();
+            return fail(nullptr, SPK_ERR_UNSUPPORTED,
+                        "spk_compute_dfield_noalloc was called on a stream that is being captured; it copies "
+                        "host tables and cannot be recorded");
+        }
+    }
 
     // a context on the host stack, bound to the scratch array (no device
     // or pinned allocation; the caller's stream, or the legacy stream)

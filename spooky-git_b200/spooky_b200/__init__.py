@@ -152,6 +152,24 @@ def _ptr(a):
     return a.ctypes.data, 1
 
 
+def _check_state_tensor(name, a, shape, dtype="complex128"):
+    """A device array handed to an entry point: a contiguous torch CUDA
+    tensor of `dtype` and `shape` (the C ABI cannot check sizes itself, and a
+    wrong buffer would make the pass kernels read or write out of bounds)."""
+    import sys
+    torch = sys.modules.get("torch")
+    if torch is None or not isinstance(a, torch.Tensor):
+        raise TypeError(f"{name} must be a torch CUDA tensor")
+    if not a.is_cuda:
+        raise ValueError(f"{name} must be on a CUDA device")
+    if a.dtype != getattr(torch, dtype):
+        raise ValueError(f"{name} must be {dtype}, got {a.dtype}")
+    if not a.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if tuple(a.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(a.shape)}, expected {tuple(shape)}")
+
+
 def params_from_file(path):
     """Parameters of a libconfig-format spooky.cfg (spk_params_from_file):
     the reference's keys and defaults, then its module checks.  Raises
@@ -187,6 +205,9 @@ def compute_dfield_noalloc(params, U, dU, stream=None):
     call and for the device after it.  Calls that overlap on the GPU race on
     the shared scratch array."""
     p = params.copy()
+    shape = (num_fields(p), p.nx, p.ny, p.nz // 2 + 1)
+    _check_state_tensor("U", U, shape)
+    _check_state_tensor("dU", dU, shape)
     _torch_sync()
     rc = lib().spk_compute_dfield_noalloc(ctypes.byref(p), U.data_ptr(), dU.data_ptr(), stream)
     if rc != SPK_OK:
@@ -273,6 +294,8 @@ class Context:
         """U, dU: torch CUDA complex128 tensors of shape_c.  Waits for torch's
         current stream before and for the context stream after, so the
         tensors can be used on either side without further synchronisation."""
+        _check_state_tensor("U", U, self.shape_c)
+        _check_state_tensor("dU", dU, self.shape_c)
         _torch_sync()
         self._check(lib().spk_compute_dfield(self._h, U.data_ptr(), dU.data_ptr()))
         self.synchronize()
@@ -287,6 +310,7 @@ class Context:
 
     def to_real(self, R):
         """R: torch CUDA float64 tensor of shape_r (complete on return)."""
+        _check_state_tensor("R", R, self.shape_r, "float64")
         _torch_sync()
         self._check(lib().spk_to_real(self._h, R.data_ptr()))
         self.synchronize()
@@ -349,6 +373,7 @@ class Context:
         """Spectral products of the torch CUDA complex128 state U (shape_c):
         a torch complex128 tensor [nprod, nx, ny, nz//2+1] (spk_products)."""
         import torch
+        _check_state_tensor("U", U, self.shape_c)
         p = self.params
         P = torch.zeros((8, p.nx, p.ny, p.nz // 2 + 1), dtype=torch.complex128, device=U.device)
         n = ctypes.c_int()
@@ -364,6 +389,7 @@ def closure_samples(fine, Uf, coarse):
     coarse nx*ny*nz] (spk_closure_samples); coarse's state becomes the
     filtered state."""
     import torch
+    _check_state_tensor("Uf", Uf, fine.shape_c)
     nbytes, ns = ctypes.c_size_t(), ctypes.c_size_t()
     rc = lib().spk_closure_samples_size(fine._h, coarse._h, ctypes.byref(nbytes), ctypes.byref(ns))
     if rc != SPK_OK:

@@ -107,7 +107,9 @@ def mti(ref):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of a LorenzoLMP/spooky-git checkout>")
+    ref = sys.argv[1]
     _stub_plotting()
     heat_diffusion(ref)
     mti(ref)

@@ -103,3 +103,66 @@ def test_noalloc_rejects_grids_beyond_the_scratch():
         compute_dfield_noalloc(p, U, dU)
     assert e.value.code == 2
     assert "MiB" in str(e.value) and str(S.NOALLOC_SCRATCH_BYTES >> 20) in str(e.value)
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The entry point's promise: after one warm-up call (which loads the
+    library's device code and its scratch array), further calls leave the
+    device's free memory unchanged.  A context of the same 32^3 MHD case
+    allocates several MiB, so the check tells the two apart."""
+    import torch
+    p = default_params(gridsize=(32, 32, 32), form=SPK_FORM_PLAIN, **CASES["mhd"])
+    U = on_device(make_state(p, 7))
+    dU = on_device(np.zeros(tuple(U.shape), np.complex128))
+    compute_dfield_noalloc(p, U, dU)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        compute_dfield_noalloc(p, U, dU)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 >= free0, (free0, free1)
+    ctx = Context(p)
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free1 - free2 >= 4 << 20, "a context should allocate its buffers (sanity check of the measurement)"
+    ctx.close()
+
+
+def test_noalloc_rejects_bad_tensors_and_closure():
+    import torch
+    p = default_params(gridsize=(16, 16, 16), form=SPK_FORM_PLAIN, **CASES["hd"])
+    good = on_device(np.zeros((3, 16, 16, 9), np.complex128))
+    with pytest.raises(ValueError):
+        compute_dfield_noalloc(p, good[:2], good)
+    with pytest.raises(ValueError):
+        compute_dfield_noalloc(p, good.to(torch.complex64), good)
+    with pytest.raises(ValueError):
+        compute_dfield_noalloc(p, good.cpu(), good)
+    pc = default_params(gridsize=(16, 16, 16), form=SPK_FORM_PLAIN, closure=1, **CASES["hd"])
+    with pytest.raises(SpookyError) as e:
+        compute_dfield_noalloc(pc, good, torch.zeros_like(good))
+    assert e.value.code == 2
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """A call on a stream under capture is refused before anything is queued
+    (its host tables would be recorded as copies from freed memory)."""
+    import ctypes
+    import torch
+    p = default_params(gridsize=(16, 16, 16), form=SPK_FORM_PLAIN, **CASES["hd"])
+    U = on_device(make_state(p, 3))
+    dU = torch.zeros_like(U)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    rc = None
+    with torch.cuda.graph(g, stream=s):
+        rc = S.lib().spk_compute_dfield_noalloc(ctypes.byref(p.copy()), U.data_ptr(), dU.data_ptr(),
+                                                 s.cuda_stream)
+        dU.add_(0)   # keep the captured graph non-empty
+    assert rc == 2
+    assert "captur" in S.lib().spk_last_error(None).decode()
+    del g
+    # the entry point still works after the refused call
+    ref = dfield_with_context(p, U.cpu().numpy())
+    assert rel_l2(dfield_noalloc(p, U.cpu().numpy()), ref) < TOL_RHS[SPK_FORM_PLAIN]
