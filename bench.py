@@ -34,8 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "spooky-git_b200"))
 
-from spooky_b200.initial import mhd_random_state  # noqa: E402
-from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, default_params  # noqa: E402
+from spooky_b200.initial import masked_noise_state, mhd_random_state  # noqa: E402
+from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, cfg_text, default_params  # noqa: E402
 
 METRIC = "256^3 MHD RK3 steps/s, FP32 form vs plain, 1xB200, at <=1e-5 rel L2 vs FP64"
 HBM_FALLBACK = 6650.0
@@ -163,6 +163,41 @@ def cpu_baseline_sample(n):
             "sample": f"{steps} RK3 step(s) of {n}^3 MHD from the same initial state (FP64 C oracle, OpenMP)"}
 
 
+def reference_cufft_leg(p, U0, warmup, steps, U_plain, timeout=900):
+    """The reference's own CUDA build (cuFFT + cuBLAS, FP64; oracle/refbuild)
+    on the same workload and GPU: its main-loop body for `warmup` + `steps`
+    steps from U0, the timed steps between CUDA events.  Returns its rate and
+    the rel L2 of its final state against this library's plain form after
+    the same number of steps (U_plain)."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "spooky_ref")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/spooky_ref is not built (make -C oracle/refbuild REF=<reference checkout>)"}
+    with tempfile.TemporaryDirectory(prefix="spk_ref_") as d:
+        with open(os.path.join(d, "spooky.cfg"), "w") as f:
+            f.write(cfg_text(p, configname="reference timing run"))
+        u0, u1 = os.path.join(d, "u0.bin"), os.path.join(d, "u1.bin")
+        np.ascontiguousarray(U0, dtype=np.complex128).tofile(u0)
+        try:
+            r = subprocess.run([exe, d, u0, str(warmup), str(steps), u1], capture_output=True, text=True,
+                               timeout=timeout)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"reference build did not finish within {timeout} s"}
+        if r.returncode != 0:
+            return {"unavailable": f"reference build exited {r.returncode}: " + (r.stderr or r.stdout)[-300:]}
+        js = [l for l in r.stdout.splitlines() if l.startswith("{")]
+        if not js:
+            return {"unavailable": "reference build printed no result line"}
+        j = json.loads(js[-1])
+        U1 = np.fromfile(u1, dtype=np.complex128).reshape(U0.shape)
+    rel = float(np.linalg.norm((U1 - U_plain).ravel()) / np.linalg.norm(U_plain.ravel()))
+    return {"value": j["steps_per_s"], "unit": "steps/s", "ms_per_step": j["ms_per_step"], "steps": j["steps"],
+            "warmup": j["warmup"], "ffts_per_step": j["ffts_per_step"], "rel_l2_vs_plain_fp64": rel,
+            "after_steps": j["warmup"] + j["steps"],
+            "what": "the reference's own sources (cuFFT + cuBLAS, FP64) built for sm_100a by oracle/refbuild; "
+                    "main-loop body CleanFieldDivergence + HydroMHDAdvance, CUDA events on the legacy stream"}
+
+
 ENSEMBLE_SIZES = (16, 24, 32, 48, 64)
 
 
@@ -208,6 +243,45 @@ def partition_boxes(costs, world):
     return [sorted(p) for p in parts]
 
 
+def ensemble_timing(params, states, steps, warmup, stream, barrier=None):
+    """Advance one ensemble of the given boxes: `steps` timed steps with the
+    launchers' own schedule, then spk_ensemble_autotune and `steps` timed
+    steps again.  Returns (ms untuned, ms tuned, autotune seconds, kernels
+    per ensemble step, all budgets finite)."""
+    import torch
+    import spooky_b200 as S
+    ens = S.Ensemble(params, stream=stream.cuda_stream)
+    for b, U in zip(ens.boxes, states):
+        b.set_state(U)
+    ens.advance(warmup)
+    ens.synchronize()
+
+    def timed():
+        if barrier is not None:
+            barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.advance(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ms_untuned = timed()
+    # the schedule autotuner (spk_ensemble_autotune), then the timed steps
+    t_tune = time.perf_counter()
+    ens.autotune(steps=3)
+    ens.advance(warmup)
+    ens.synchronize()
+    t_tune = time.perf_counter() - t_tune
+    ms = timed()
+    kps = ens.kernels_per_step()
+    ens.synchronize()
+    finite = all(np.isfinite(b.budgets()[0]).all() for b in ens.boxes)
+    ens.close()
+    return ms_untuned, ms, t_tune, kps, finite
+
+
 def run_ensemble(args, world, rank, local_rank):
     import torch
     import torch.distributed as dist
@@ -221,35 +295,8 @@ def run_ensemble(args, world, rank, local_rank):
     params = [boxes[i][1] for i in mine]
     states = [box_state(*boxes[i]) for i in mine]
     stream = torch.cuda.Stream()
-    ens = S.Ensemble(params, stream=stream.cuda_stream)
-    for b, U in zip(ens.boxes, states):
-        b.set_state(U)
-    ens.advance(args.warmup)
-    ens.synchronize()
-
-    def timed():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ens.advance(args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
-    ms_untuned = timed()
-    # the schedule autotuner (spk_ensemble_autotune), then the timed steps
-    t_tune = time.perf_counter()
-    ens.autotune(steps=3)
-    ens.advance(args.warmup)
-    ens.synchronize()
-    t_tune = time.perf_counter() - t_tune
-    ms = timed()
-    kps = ens.kernels_per_step()
-    ens.synchronize()
-    finite = all(np.isfinite(b.budgets()[0]).all() for b in ens.boxes)
-    ens.close()
+    ms_untuned, ms, t_tune, kps, finite = ensemble_timing(params, states, args.steps, args.warmup, stream,
+                                                          dist.barrier if world > 1 else None)
     # one box at a time: each box alone through its own graph, on a sample
     nsample = min(len(mine), 64)
     one_ms = 0.0
@@ -320,29 +367,40 @@ def mti_state(p):
     return to_spectral(np.concatenate([u, B, th[None]]))
 
 
-def run_mti(args, world, rank, local_rank):
+def mti_timing(n, steps, warmup, stream):
+    """Config 3 at n^3: `warmup` steps, then `steps` steps between CUDA events.
+    Returns (ms per step, RKL2 stages per cycle, kernels per recorded step,
+    simulated time, (dt_hyp, dt_par, dt_sts, dt), energies)."""
     import torch
     import spooky_b200 as S
-    torch.cuda.set_device(local_rank)
-    p = mti_params(args.n)
-    stream = torch.cuda.Stream()
+    p = mti_params(n)
     ctx = S.Context(p, stream=stream.cuda_stream)
     ctx.set_state(mti_state(p))
-    ctx.advance(args.warmup)
+    ctx.advance(warmup)
     ctx.synchronize()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    ctx.advance(args.steps)
+    ctx.advance(steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     ctx.synchronize()
-    t, dt, step = ctx.get_time()
+    t, _, _ = ctx.get_time()
     hyp, par, sts, cur = ctx.compute_dt()
     s_rkl = int(1 + 4.0 * (1.0 + 2.0 * cur / sts) / (1.0 + np.sqrt(9.0 + 16.0 * cur / sts)))
     kps = ctx.step_info()[0]
     e, _ = ctx.budgets()
+    ctx.close()
+    return ms, s_rkl, kps, t, (hyp, par, sts, cur), e
+
+
+def run_mti(args, world, rank, local_rank):
+    import torch
+    import spooky_b200 as S
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    ms, s_rkl, kps, t, (hyp, par, sts, cur), e = mti_timing(args.n, args.steps, args.warmup, stream)
     if rank == 0:
         print(json.dumps({
             "metric": f"{args.n}^3 Boussinesq-MHD + anisotropic conduction, RK3 + RKL2 steps/s (config 3)",
@@ -404,6 +462,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the reference-build, config-3 and config-4 legs of the default line")
     ap.add_argument("--ensemble", action="store_true",
                     help="batched-ensemble workload instead: --boxes independent HD/MHD boxes (config 4)")
     ap.add_argument("--boxes", type=int, default=512)
@@ -555,6 +615,66 @@ def main():
         except Exception:
             traffic = None
 
+    # the same FP32 step on a state with content outside the 2/3 mask (1e-3 of
+    # the norm): the path that carries the dealiased-out modes through every
+    # stage, which a band-limited state lets the step skip
+    Um = masked_noise_state(workload_params(n, SPK_FORM_PLAIN), U0)
+    ctxm = S.Context(workload_params(n, SPK_FORM_FP32), stream=stream.cuda_stream)
+    ctxm.set_state(Um)
+    ctxm.advance(args.warmup)
+    ctxm.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctxm.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_masked = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    _, bytes_masked = ctxm.step_info()
+    ctxm.close()
+    del ctxm
+    torch.cuda.empty_cache()
+    untrimmed = {"value": world * 1000.0 / ms_masked, "unit": "steps/s", "ms_per_step": ms_masked,
+                 "bytes_per_step": bytes_masked,
+                 "step_hbm_frac": bytes_masked / (ms_masked * 1e-3) / 1e9 / peaks()[0],
+                 "what": "FP32 form, same workload plus solenoidal noise of 1e-3 of the state's norm on the "
+                         "modes outside the 2/3 mask: the dealiased-out modes are carried through every stage"}
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        del ctx32
+        torch.cuda.empty_cache()
+        try:
+            extras["reference_cufft"] = reference_cufft_leg(workload_params(n, SPK_FORM_PLAIN), U0, args.warmup,
+                                                            args.steps, U64)
+            rc = extras["reference_cufft"]
+            if "value" in rc:
+                rc["plain_fp64_over_reference"] = (1000.0 / ms64) / rc["value"]
+                rc["fp32_over_reference"] = (1000.0 / ms32) / rc["value"]
+        except Exception as ex:   # the extra legs never stop the headline line
+            extras["reference_cufft"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        try:
+            ms3, s3, k3, t3, dts3, _ = mti_timing(256, 10, 3, stream)
+            extras["config3_sample"] = {
+                "value": 1000.0 / ms3, "unit": "steps/s", "ms_per_step": ms3, "steps": 10, "warmup": 3,
+                "rkl2_stages_per_cycle": s3, "dt": dts3[3], "kernels_per_step": k3,
+                "workload": "256^3 Boussinesq MHD + anisotropic conduction, RKL2 on theta (bench.py --mti)"}
+        except Exception as ex:
+            extras["config3_sample"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        try:
+            boxes = ensemble_boxes(512)
+            params = [p for _, p in boxes]
+            states = [box_state(i, p) for i, p in boxes]
+            msu, ms4, tt4, k4, fin4 = ensemble_timing(params, states, 20, 3, stream)
+            extras["config4_sample"] = {
+                "value": 512 * 20 / (ms4 * 1e-3), "unit": "box-steps/s", "steps": 20, "warmup": 3,
+                "untuned_value": 512 * 20 / (msu * 1e-3), "autotune_seconds": tt4, "kernels_per_step": k4,
+                "all_finite": fin4,
+                "workload": "512 independent boxes, sizes {16,24,32,48,64}^3, HD/MHD, FP32 (bench.py --ensemble)"}
+        except Exception as ex:
+            extras["config4_sample"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(n)
@@ -589,7 +709,9 @@ def main():
             "gpu_launches": kps * args.steps,
             "kernels_per_step": kps,
             "cpu_baseline": cpu,
+            "untrimmed": untrimmed,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -628,22 +628,75 @@ class TimeStepping:
         return self._ctx.get_time()[2]
 
 
+class InputOutput:
+    """InputOutput's output schedule (src/io/inputoutput.hpp, check_output.cu:14-97).
+
+    After every main-loop step the supervisor calls CheckOutput.  A time
+    series is due when t - t_lastvar >= toutput_time, a snapshot when
+    t - t_lastsnap + 1e-8 >= toutput_flow (and both at t = 0).  As in the
+    reference, each output first cleans the divergence of the state, and a
+    snapshot advances t_lastsnap by toutput_flow -- which the dt rule reads,
+    so that steps land on the snapshot times.  The writers are callables:
+    ``on_timevar(supervisor, t)`` and ``on_snapshot(supervisor, num_save)``
+    (None: the schedule and the cleaning still run, nothing is written)."""
+
+    def __init__(self, sup, toutput_time=1.0, on_timevar=None, on_snapshot=None):
+        self.sup = sup
+        self.toutput_time = toutput_time
+        self.t_lastsnap = 0.0
+        self.t_lastvar = 0.0
+        self.num_save = 0
+        self.on_timevar = on_timevar
+        self.on_snapshot = on_snapshot
+
+    def CheckOutput(self):
+        self.CheckTimeSeries()
+        self.CheckSnapshot()
+
+    def CheckTimeSeries(self):
+        t, _, _ = self.sup.ctx.get_time()
+        if t - self.t_lastvar >= self.toutput_time or t == 0.0:
+            self.sup.fields.CleanFieldDivergence()
+            if t != 0.0:
+                self.t_lastvar += self.toutput_time
+            if self.on_timevar is not None:
+                self.on_timevar(self.sup, t)
+
+    def CheckSnapshot(self):
+        t, _, step = self.sup.ctx.get_time()
+        if t - self.t_lastsnap + 1e-8 >= self.sup.param.toutput_flow or t == 0.0:
+            self.sup.fields.CleanFieldDivergence()
+            if t != 0.0:
+                self.t_lastsnap += self.sup.param.toutput_flow
+                self.sup.ctx.set_time(t, step, self.t_lastsnap)
+            if self.on_snapshot is not None:
+                self.on_snapshot(self.sup, self.num_save)
+            self.num_save += 1
+
+
 class Supervisor:
     """Supervisor (src/supervisor/supervisor.hpp:24-84) for the hot path."""
 
-    def __init__(self, params, stream=None):
+    def __init__(self, params, stream=None, toutput_time=1.0, on_timevar=None, on_snapshot=None):
         self.param = Parameters(params)
         self.ctx = Context(self.param.p, stream)
         self.fields = Fields(self.ctx)
         self.timestep = TimeStepping(self.ctx)
+        self.inout = InputOutput(self, toutput_time, on_timevar, on_snapshot)
+
+    def initialDataDump(self):
+        """The outputs at t = 0 of a run that does not restart (supervisor.cu:215-225)."""
+        self.inout.CheckOutput()
 
     def executeMainLoop(self, max_steps=None):
-        """Advance until t_final (src/supervisor/supervisor.cu:169-213); the
+        """Advance until t_final (src/supervisor/supervisor.cu:169-213): per
+        step CleanFieldDivergence + HydroMHDAdvance, then CheckOutput; the
         host reads the device time once per step."""
         n = 0
         while self.timestep.current_time < self.param.t_final:
             self.timestep.HydroMHDAdvance(1)
             n += 1
+            self.inout.CheckOutput()
             if max_steps is not None and n >= max_steps:
                 break
         self.ctx.synchronize()

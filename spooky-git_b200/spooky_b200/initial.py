@@ -58,3 +58,32 @@ def mhd_random_state(p, seed_u=1, seed_b=2, b0=(0.0, 0.0, 0.1), kpeak=4.0):
     for c in range(3):
         B[c] += b0[c]
     return to_spectral(np.concatenate([u, B]))
+
+
+def masked_noise_state(p, U, rel=1e-3, seed=7):
+    """U plus solenoidal random content on the modes the 2/3 rule removes
+    (|k_d| > (2/3) k_d,max on any axis), with L2 norm rel * |U|: a state
+    whose dealiased-out modes carry real content, so that the step cannot
+    take the path that skips them.  Velocity and magnetic triples stay
+    divergence-free; a theta field gets scalar noise."""
+    rng = np.random.default_rng(seed)
+    KX, KY, KZ = kvectors(p)
+    kmx = 2 * np.pi / p.lx * (p.nx // 2 - 1)
+    kmy = 2 * np.pi / p.ly * (p.ny // 2 - 1)
+    kmz = 2 * np.pi / p.lz * (p.nz // 2 - 1)
+    outside = (np.abs(KX) > 2.0 / 3.0 * kmx) | (np.abs(KY) > 2.0 / 3.0 * kmy) | (np.abs(KZ) > 2.0 / 3.0 * kmz)
+    K2 = KX ** 2 + KY ** 2 + KZ ** 2
+    ik2 = np.where(K2 > 0, 1.0 / np.where(K2 > 0, K2, 1.0), 0.0)
+    F = U.shape[0]
+    N = np.zeros_like(U)
+    for f in range(F):
+        c = (rng.standard_normal(KX.shape) + 1j * rng.standard_normal(KX.shape)) * outside
+        # a real field's spectrum (Hermitian on the kz = 0 and Nyquist planes)
+        N[f] = np.fft.rfftn(np.fft.irfftn(c, s=(p.nx, p.ny, p.nz), axes=(0, 1, 2)))
+    for base in [b for b in (0, 3) if b + 3 <= F and not (p.heat_equation)]:
+        kdot = KX * N[base] + KY * N[base + 1] + KZ * N[base + 2]
+        N[base] -= KX * kdot * ik2
+        N[base + 1] -= KY * kdot * ik2
+        N[base + 2] -= KZ * kdot * ik2
+    N *= rel * np.linalg.norm(U.ravel()) / np.linalg.norm(N.ravel())
+    return U + N

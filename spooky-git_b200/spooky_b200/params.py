@@ -155,3 +155,70 @@ def check_parameters(p):
     if p.anisotropic_diffusion and not (p.mhd and p.boussinesq):
         errs.append("anisotropic_diffusion requires mhd and boussinesq module")
     return errs
+
+
+def _cfg_float(x):
+    """A float literal libconfig reads as a float (a '.' or an exponent)."""
+    s = repr(float(x))
+    if s in ("inf", "-inf", "nan"):
+        raise ValueError(f"{x} has no libconfig float form")
+    return s if ("." in s or "e" in s or "E" in s) else s + ".0"
+
+
+def cfg_text(p, configname="spooky_b200", toutput_time=None, output_dir="./"):
+    """A libconfig-format spooky.cfg that gives Parameters::Parameters
+    (src/parameters/parameters.cu:59-505) the physics, modules and time
+    controls of ``p``; keys the path does not use keep the reference's
+    defaults.  Extensions of spk_params_t without a cfg key (form, fixed_dt,
+    integrator, sts_every_step, closure) are not written."""
+    b = lambda v: "true" if v else "false"
+    names = var_list(p)
+    sts = [n for i, n in enumerate(names) if p.sts_vars_mask >> i & 1]
+    alg = {v: k for k, v in STS_ALGORITHMS.items()}[p.sts_algorithm]
+    lines = [
+        f'configname = "{configname}";',
+        "modules:", "{",
+        f"  with2d = {b(p.with2d)};",
+        f"  incompressible = {b(p.incompressible)};",
+        f"  heat_equation = {b(p.heat_equation)};",
+        f"  boussinesq = {b(p.boussinesq)};",
+        f"  stratification = {b(p.stratification)};",
+        f"  strat_direction = {int(p.strat_direction)};",
+        f"  mhd = {b(p.mhd)};",
+        f"  anisotropic_diffusion = {b(p.anisotropic_diffusion)};",
+        f"  supertimestepping = {b(p.supertimestepping)};",
+        f'  sts_algorithm = "{alg}";',
+        "  sts_variables = (" + ", ".join(f'"{n}"' for n in sts) + ");" if sts else "",
+        "};",
+        "physics:", "{",
+        f"  boxsize = ({_cfg_float(p.lx)}, {_cfg_float(p.ly)}, {_cfg_float(p.lz)});",
+        f"  gridsize = ({int(p.nx)}, {int(p.ny)}, {int(p.nz)});",
+        f"  reynolds = {_cfg_float(1.0 / p.nu)};",
+        f"  reynolds_magnetic = {_cfg_float(1.0 / p.nu_m)};",
+        f"  reynolds_thermic = {_cfg_float(1.0 / p.nu_th)};",
+        f"  reynolds_anisotropic = {_cfg_float(p.reynolds_ani)};",
+        f"  brunt_vaissala_squared = {_cfg_float(p.N2)};",
+        f"  mti_frequency_squared = {_cfg_float(p.OmegaT2)};",
+        "};",
+        "code:", "{",
+        f"  cfl = {_cfg_float(p.cfl)};",
+        f"  cfl_par = {_cfg_float(p.cfl_par)};",
+        f"  cfl_sts = {_cfg_float(p.cfl_sts)};",
+        f"  safety_sts = {int(p.safety_sts)};",
+        f"  safety_source = {_cfg_float(p.safety_source)};",
+        f"  t_initial = {_cfg_float(p.t_initial)};",
+        f"  t_final = {_cfg_float(p.t_final)};",
+        "  max_walltime_elapsed = 1e30;",
+        f"  antialiasing = {b(p.antialiasing)};",
+        "  restart = false;",
+        "};",
+        "output:", "{",
+        f"  snapshot_step = {_cfg_float(p.toutput_flow)};",
+        f"  timevar_step = {_cfg_float(p.toutput_flow if toutput_time is None else toutput_time)};",
+        f'  output_dir = "{output_dir}";',
+        "};",
+        "init:", "{",
+        "  spatial_structure = false;",
+        "};",
+    ]
+    return "\n".join(l for l in lines if l) + "\n"

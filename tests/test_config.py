@@ -5,6 +5,7 @@ typed lookups (no automatic int -> float conversion), the STS variable list
 and Parameters::checkParameters (:511-566).  No GPU call is made."""
 import os
 
+import numpy as np
 import pytest
 
 import spooky_b200 as S
@@ -168,3 +169,23 @@ def test_read_from_file(tmp_path):
     with pytest.raises(S.SpookyError) as e:
         S.params_from_file(os.path.join(str(tmp_path), "missing.cfg"))
     assert e.value.code == 1 and "cannot open" in str(e.value)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(incompressible=1, mhd=1, gridsize=(256, 256, 256), boxsize=(2 * np.pi,) * 3, reynolds=1e3,
+         reynolds_magnetic=1e3, cfl=1.5, t_final=1e30, toutput_flow=1e30),
+    dict(incompressible=1, mhd=1, boussinesq=1, stratification=1, strat_direction=2, anisotropic_diffusion=1,
+         supertimestepping=1, sts_variables=["th"], safety_sts=95, gridsize=(64, 32, 16), boxsize=(1.0, 2.0, 0.5),
+         reynolds=1e4, reynolds_magnetic=1e4, reynolds_ani=20.0, N2=1.0, OmegaT2=1.0, cfl=1.5),
+    dict(heat_equation=1, gridsize=(1024, 2, 2), reynolds_thermic=1000.0, cfl_par=1.5, antialiasing=0,
+         t_final=10.0, toutput_flow=5.0),
+])
+def test_cfg_text_round_trip(kw):
+    """params.cfg_text writes a spooky.cfg (the reference's keys) that reads
+    back to the same parameters: the file given to the reference's own build
+    when it is timed on the same workload."""
+    from spooky_b200.params import cfg_text
+    p = default_params(**kw)
+    q = S.params_from_string(cfg_text(p))
+    for name, _ in p._fields_:
+        assert getattr(q, name) == getattr(p, name), name

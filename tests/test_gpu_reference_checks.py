@@ -1,0 +1,167 @@
+"""GPU runs of the reference's own end-to-end checks, and of the headline
+configuration for as many steps as its precision claim names.
+
+  advected MHD vortex   tests/advected-mhd-vortex/check-advected-mhd-vortex.py:11-66 (ICs),
+                        :160-197 (L1 over the six fields / N < 1e-4 at the last snapshot)
+  heat diffusion, RK3   tests/heat-diffusion/check-heat-diffusion.py:157-166 (L1 < 1e-15 against
+                        the reference's own numpy RK3, tests/golden/heat_diffusion_rk3.npz)
+  256^3 MHD headline    the FP32 form within rel L2 1e-5 of the FP64 plain form after 1000 steps
+
+Each run goes through the Supervisor main loop, which keeps the reference's
+snapshot schedule (steps land on the snapshot times).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fields import grid, to_spectral
+from spooky_b200 import Context, Supervisor
+from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, default_params
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def real_fields(ctx):
+    import torch
+    R = torch.zeros(ctx.shape_r, dtype=torch.float64, device="cuda")
+    ctx.to_real(R)
+    return R.cpu().numpy()
+
+
+# ---- advected MHD vortex ------------------------------------------------------
+VORTEX = dict(n=(512, 512, 2), box=(1.0, 1.0, 1.0), nu=1e-4, eta=1e-4, u0=0.05, v0=0.05, sigma=200.0)
+
+
+def vortex_params(form, t_final=1.1):
+    return default_params(incompressible=1, mhd=1, gridsize=VORTEX["n"], boxsize=VORTEX["box"],
+                          reynolds=1.0 / VORTEX["nu"], reynolds_magnetic=1.0 / VORTEX["eta"], cfl=1.5,
+                          t_final=t_final, toutput_flow=0.2, form=form)
+
+
+def vortex_analytic(p, t):
+    """vel_analytical / mag_analytical of check-advected-mhd-vortex.py:30-62:
+    the vortex and its field loop advected by (u0, v0) without decay."""
+    X, Y, _ = grid(p)
+    Xt, Yt = X - VORTEX["u0"] * t, Y - VORTEX["v0"] * t
+    e = np.exp((1.0 - VORTEX["sigma"] * (Xt ** 2 + Yt ** 2)) / 2.0) / (2.0 * np.pi)
+    zero = np.zeros_like(X)
+    return np.stack([VORTEX["v0"] - e * Yt, VORTEX["u0"] + e * Xt, zero, -e * Yt, e * Xt, zero])
+
+
+def vortex_l1(R, p, t):
+    return float(np.abs(R - vortex_analytic(p, t)).sum() / (p.nx * p.ny * p.nz))
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+def test_advected_mhd_vortex(form):
+    """The reference's snapshots every 0.2 to t = 1.0 (t_final 1.1), L1 < 1e-4
+    against the advected profile at each; the plain form's first snapshot
+    equals the FP64 oracle's run of the same schedule to rel L2 1e-10."""
+    p = vortex_params(form)
+    U0 = to_spectral(vortex_analytic(p, 0.0))
+    snaps = []
+
+    def on_snapshot(sup, num):
+        t, _, step = sup.ctx.get_time()
+        snaps.append((num, t, step, real_fields(sup.ctx), sup.ctx.get_state() if num == 1 else None))
+
+    sup = Supervisor(p, on_snapshot=on_snapshot)
+    sup.fields.set(U0)
+    sup.fields.CleanFieldDivergence()
+    sup.inout.num_save = 1          # restart from snap0000 (-r 0): its snapshot is not rewritten
+    sup.executeMainLoop()
+    assert abs(sup.timestep.current_time - 1.1) < 1e-12
+    times = [t for _, t, _, _, _ in snaps]
+    assert np.allclose(times, [0.2, 0.4, 0.6, 0.8, 1.0], atol=1e-12), times
+    for num, t, _, R, _ in snaps:
+        assert vortex_l1(R, p, t) < 1e-4, (num, t, vortex_l1(R, p, t))
+    if form == SPK_FORM_PLAIN:
+        # the FP64 oracle through the same schedule to the first snapshot
+        O.set_threads(os.cpu_count() or 1)
+        o = O.Oracle(vortex_params(SPK_FORM_PLAIN, t_final=0.2))
+        o.set_state(U0)
+        o.clean_divergence()
+        while o.get_time()[0] < 0.2:
+            o.step(1)
+        _, t1, step1, _, U1 = snaps[0]
+        assert o.get_time()[2] == step1 and abs(o.get_time()[0] - t1) < 1e-14
+        assert rel_l2(U1, o.get_state()) < 1e-10
+
+
+# ---- heat diffusion, RK3 on the device ------------------------------------------
+def test_heat_diffusion_rk3_golden_on_gpu():
+    """The heat-equation RK3 kernel (k_heat) against the reference's own numpy
+    RK3: 1024x2x2, chi = 1e-3, cfl_par 1.5, snapshots at t = 5, 10; L1 < 1e-15
+    at both (check-heat-diffusion.py:157-166)."""
+    g = np.load(os.path.join(GOLDEN, "heat_diffusion_rk3.npz"))
+    nx = int(g["nx"])
+    p = default_params(heat_equation=1, gridsize=(nx, 2, 2), reynolds_thermic=1000.0, cfl=1.5, cfl_par=1.5,
+                       antialiasing=0, t_final=10.0, toutput_flow=5.0)
+    X, _, _ = grid(p)
+    a = 0.01
+    T0 = 1.0 + 0.5 * (np.tanh((X + 0.375) / a) - np.tanh((X + 0.125) / a)) + 0.5 * (
+        np.tanh((X - 0.125) / a) - np.tanh((X - 0.375) / a))
+    snaps = {}
+
+    def on_snapshot(sup, num):
+        t, _, _ = sup.ctx.get_time()
+        U = sup.ctx.get_state()
+        snaps[num] = (t, np.fft.irfftn(U[0], s=T0.shape, axes=(0, 1, 2)))
+
+    sup = Supervisor(p, toutput_time=100.0, on_snapshot=on_snapshot)
+    sup.fields.set(to_spectral(T0[None]))
+    sup.initialDataDump()
+    sup.executeMainLoop()
+    assert sup.timestep.current_time == 10.0
+    assert sorted(snaps) == [0, 1, 2]
+    for i in (1, 2):
+        t, T = snaps[i]
+        assert abs(t - 5.0 * i) < 1e-12
+        assert np.all(np.abs(T - T[:, :1, :1]) < 1e-14)
+        L1 = np.abs(g["T"][i] - T[:, 0, 0]).sum() / (nx * 4)
+        assert L1 < 1e-15, (t, L1)
+
+
+# ---- the headline configuration for 1000 steps -----------------------------------
+def test_mhd256_fp32_form_within_1e5_of_plain_after_1000_steps():
+    """256^3 MHD of the benchmark (box 2 pi, nu = eta = 1e-3, B0 = 0.1 z, CFL
+    1.5, random solenoidal u, B with E(k) ~ k^4 exp(-2 (k/4)^2), rms 1, seeds
+    1, 2).  The plain form's first step equals the FP64 oracle's (rel L2
+    1e-10); after 1000 steps the FP32 form is within rel L2 1e-5 of the plain
+    form, and its total energy within 1e-6."""
+    from spooky_b200.initial import mhd_random_state
+    L = 2 * np.pi
+    kw = dict(incompressible=1, mhd=1, gridsize=(256, 256, 256), boxsize=(L, L, L), reynolds=1e3,
+              reynolds_magnetic=1e3, cfl=1.5, t_final=1e30, toutput_flow=1e30)
+    p64 = default_params(form=SPK_FORM_PLAIN, **kw)
+    p32 = default_params(form=SPK_FORM_FP32, **kw)
+    U0 = mhd_random_state(p64)
+    O.set_threads(os.cpu_count() or 1)
+    o = O.Oracle(p64)
+    o.set_state(U0)
+    o.step(1)
+    U1 = o.get_state()
+    o.close()
+    c64 = Context(p64)
+    c64.set_state(U0)
+    c64.advance(1)
+    assert rel_l2(c64.get_state(), U1) < 1e-10
+    c64.advance(999)
+    c32 = Context(p32)
+    c32.set_state(U0)
+    c32.advance(1000)
+    c64.synchronize()
+    c32.synchronize()
+    assert c32.get_time()[2] == c64.get_time()[2] == 1000
+    err = rel_l2(c32.get_state(), c64.get_state())
+    assert err < 1e-5, err
+    e32, _ = c32.budgets()
+    e64, _ = c64.budgets()
+    assert abs(np.sum(e32) - np.sum(e64)) / np.sum(e64) < 1e-6

@@ -156,6 +156,33 @@ def test_heat_diffusion_rk3_golden():
     assert L1 < 1e-15, L1
 
 
+def test_advected_mhd_vortex_first_snapshot():
+    """tests/advected-mhd-vortex (512x512x2, box 1, nu = eta = 1e-4, CFL 1.5):
+    the vortex and its field loop advected by (0.05, 0.05); L1 over the six
+    fields / N against the advected profile < 1e-4 (check-advected-mhd-vortex.py:
+    11-66, 181-197), here at the first snapshot, t = 0.2."""
+    p = default_params(incompressible=1, mhd=1, gridsize=(512, 512, 2), boxsize=(1.0, 1.0, 1.0), reynolds=1e4,
+                       reynolds_magnetic=1e4, cfl=1.5, t_final=1.1, toutput_flow=0.2)
+    X, Y, _ = grid(p)
+
+    def profile(t):
+        Xt, Yt = X - 0.05 * t, Y - 0.05 * t
+        e = np.exp((1.0 - 200.0 * (Xt ** 2 + Yt ** 2)) / 2.0) / (2.0 * np.pi)
+        return np.stack([0.05 - e * Yt, 0.05 + e * Xt, 0 * X, -e * Yt, e * Xt, 0 * X])
+
+    o = O.Oracle(p)
+    o.set_state(to_spectral(profile(0.0)))
+    o.clean_divergence()
+    while True:
+        o.step(1)
+        t = o.get_time()[0]
+        if t + 1e-8 >= p.toutput_flow:
+            break
+    assert abs(t - 0.2) < 1e-14
+    L1 = np.abs(o.to_real() - profile(t)).sum() / (512 * 512 * 2)
+    assert L1 < 1e-4, L1
+
+
 def test_alfven_wave():
     n = 32
     p = default_params(incompressible=1, mhd=1, gridsize=(n, n, n), reynolds=1e4, reynolds_magnetic=1e4,
