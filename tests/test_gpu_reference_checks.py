@@ -98,8 +98,11 @@ def test_advected_mhd_vortex(form):
 # ---- heat diffusion, RK3 on the device ------------------------------------------
 def test_heat_diffusion_rk3_golden_on_gpu():
     """The heat-equation RK3 kernel (k_heat) against the reference's own numpy
-    RK3: 1024x2x2, chi = 1e-3, cfl_par 1.5, snapshots at t = 5, 10; L1 < 1e-15
-    at both (check-heat-diffusion.py:157-166)."""
+    RK3: 1024x2x2, chi = 1e-3, cfl_par 1.5, to t = 10; L1 < 1e-15 at the end
+    (check-heat-diffusion.py:157-166).  The run's snapshot at t = 5 lands on
+    5 exactly (the dt rule stops there); the numpy run does not stop for its
+    saves (its middle save is at t = 5.00012), so only the final states are
+    compared, as the reference's check does."""
     g = np.load(os.path.join(GOLDEN, "heat_diffusion_rk3.npz"))
     nx = int(g["nx"])
     p = default_params(heat_equation=1, gridsize=(nx, 2, 2), reynolds_thermic=1000.0, cfl=1.5, cfl_par=1.5,
@@ -121,12 +124,12 @@ def test_heat_diffusion_rk3_golden_on_gpu():
     sup.executeMainLoop()
     assert sup.timestep.current_time == 10.0
     assert sorted(snaps) == [0, 1, 2]
-    for i in (1, 2):
-        t, T = snaps[i]
-        assert abs(t - 5.0 * i) < 1e-12
-        assert np.all(np.abs(T - T[:, :1, :1]) < 1e-14)
-        L1 = np.abs(g["T"][i] - T[:, 0, 0]).sum() / (nx * 4)
-        assert L1 < 1e-15, (t, L1)
+    assert snaps[1][0] == 5.0 and snaps[2][0] == 10.0
+    assert g["t"][-1] == 10.0
+    T = snaps[2][1]
+    assert np.all(np.abs(T - T[:, :1, :1]) < 1e-14)
+    L1 = np.abs(g["T"][-1] - T[:, 0, 0]).sum() / (nx * 4)
+    assert L1 < 1e-15, L1
 
 
 # ---- the headline configuration for 1000 steps -----------------------------------
