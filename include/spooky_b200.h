@@ -114,6 +114,21 @@ void spk_params_default(spk_params_t* p);
 int spk_params_from_file(const char* path, spk_params_t* p);
 int spk_params_from_string(const char* text, spk_params_t* p);
 
+/* Any key of a spooky.cfg text (the keys of Parameters::Parameters that
+ * spk_params_t does not carry: output directory and lists, snapshot and
+ * time-series steps, wall-clock limit, initial conditions, ...), with
+ * libconfig's typed lookups and the same path syntax ("output.output_dir",
+ * "physics.boxsize.[0]").  Return 1 when the key exists with that type (the
+ * value is written), 0 when it is absent or of another type (nothing is
+ * written), -1 when the text does not parse or an argument is bad
+ * (spk_last_error(NULL)).  spk_cfg_setting_length: the element count of a
+ * group, array or list, 0 for a scalar, -1 when absent. */
+int spk_cfg_lookup_int(const char* text, const char* path, int* out);
+int spk_cfg_lookup_bool(const char* text, const char* path, int* out);
+int spk_cfg_lookup_float(const char* text, const char* path, double* out);
+int spk_cfg_lookup_string(const char* text, const char* path, char* buf, size_t len);
+int spk_cfg_setting_length(const char* text, const char* path);
+
 typedef struct spk_ctx spk_ctx;
 
 /* Create a context: validates the modules (checkParameters), builds the
@@ -161,6 +176,84 @@ int spk_to_real(spk_ctx* ctx, double* R);
 /* Wait for the context stream; returns the first asynchronous error seen. */
 int spk_synchronize(spk_ctx* ctx);
 
+/* ---- the same operations on the caller's state array ---------------------
+ * The reference's TimeStepping and RKLegendre members take the device
+ * mega-array d_all_fields as an argument (src/timestepping/timestepping.hpp:39-43,
+ * src/rkl/rkl.hpp:42).  These forms work in place on such an array, U
+ * ([F][Nc] complex FP64, device), with the context's scratch, time, step and
+ * dt, so that a caller keeping its own state makes no copies.  Single-box
+ * contexts only.  After any of them the context's own state is treated as
+ * set from outside (cleaned again before its next step).
+ *
+ * spk_advance_fields    nsteps x { CleanFieldDivergence; HydroMHDAdvance } on U
+ *                       (supervisor.cu:179-192; hydro_mhd_advance.cu:18-75); the
+ *                       step graph is recorded once per array and replayed.
+ * spk_compute_dt_fields TimeStepping::compute_dt(complexFields, realBuffer)
+ *                       (compute_dt.cu:15-309) on U.
+ * spk_rk3_fields        TimeStepping::RungeKutta3(complex_Fields, real_Buffer)
+ *                       (hydro_mhd_advance.cu:79-189; ForwardEuler with
+ *                       SPK_INT_EULER) on U with the dt of the last
+ *                       compute_dt: no dt reduction, no cleaning, no
+ *                       super-time-stepping.
+ * spk_rkl_cycle_fields  RKLegendre::compute_cycle(complex_Fields, real_Buffer)
+ *                       (rkl.cu:185-199) on U with the last dt and dt_sts.
+ *
+ * TimeStepping::compute_dfield's only other input in the reference, the RK
+ * stage counter stage_step (compute_dfield.cu:36-46), says whether the real
+ * buffer left by compute_dt is still current; spk_compute_dfield always
+ * transforms U itself, so it takes no stage argument. */
+int spk_advance_fields(spk_ctx* ctx, double* U, int nsteps);
+int spk_compute_dt_fields(spk_ctx* ctx, const double* U, double* dt_hyp, double* dt_par, double* dt_sts,
+                          double* dt_current);
+int spk_rk3_fields(spk_ctx* ctx, double* U);
+int spk_rkl_cycle_fields(spk_ctx* ctx, double* U, int* s_out);
+
+/* ---- real-space state and snapshot files ---------------------------------
+ * spk_get_state_real   Supervisor::Complex2RealFields + Fields::copy_back_to_host
+ *                      (supervisor.cu:261-272, check_output.cu:74-85): the real
+ *                      fields R[f][i][j][k] (unpadded, k fastest, FP64) of the
+ *                      context state, to host (where = 1) or device (0) memory.
+ * spk_set_state_real   the restart's R2C (the unnormalised transform of cuFFT's
+ *                      D2Z) of real fields in that layout into the context state,
+ *                      which is cleaned before the next step.
+ * Both transform on the device in FP64 (a direct sum per line) through the
+ * context's RK scratch; they are meant for snapshots, not for every step.
+ *
+ * spk_write_snapshot   InputOutput::WriteDataFile (src/io/hdf5_io.cu:19-111): an
+ *                      HDF5 file with f8 datasets t_start, t_save, t_lastsnap,
+ *                      t_lastvar and i4 step (1 element each) and one f8 dataset of
+ *                      NX*NY*NZ values per field, named vx vy vz bx by bz th, the
+ *                      real field in C order.  t_save and step are the context's.
+ * spk_read_snapshot    InputOutput::ReadDataFile's reading part (hdf5_io.cu:159-231):
+ *                      sets the state from the file's fields and the time, step
+ *                      and t_lastsnap from its scalars; returns t_lastsnap and
+ *                      t_lastvar (either may be NULL).  Choosing the file
+ *                      (restart -1 = the most recent snapNNNN.h5) is the
+ *                      caller's, as in Supervisor::Restart.
+ * The files use the format libhdf5 writes with default settings (superblock
+ * version 0, a symbol-table root group, version-1 object headers, contiguous
+ * data), written and read by the library itself: no HDF5 library is needed.
+ *
+ * spk_h5_write / spk_h5_read: the same file format for any list of 1-D
+ * datasets (host memory; no context, no GPU).  Reading converts the stored
+ * integer or floating-point type to the requested one; n must equal the
+ * stored element count.  Errors: spk_last_error(NULL). */
+int spk_get_state_real(spk_ctx* ctx, double* R, int where);
+int spk_set_state_real(spk_ctx* ctx, const double* R, int where);
+int spk_write_snapshot(spk_ctx* ctx, const char* path, double t_start, double t_lastsnap, double t_lastvar);
+int spk_read_snapshot(spk_ctx* ctx, const char* path, double* t_lastsnap, double* t_lastvar);
+
+#define SPK_H5_F64 0   /* IEEE double, little-endian on write */
+#define SPK_H5_I32 1   /* 32-bit signed integer, little-endian on write */
+typedef struct spk_h5_dataset {
+    const char* name;
+    int type;        /* SPK_H5_F64 or SPK_H5_I32 */
+    size_t n;        /* elements */
+    void* data;      /* write: the n values; read: room for n values */
+} spk_h5_dataset_t;
+int spk_h5_write(const char* path, const spk_h5_dataset_t* ds, int nds);
+int spk_h5_read(const char* path, spk_h5_dataset_t* ds, int nds);
+
 /* Energy budgets in FP64 with the reference's half-spectrum weighting
  * (computeEnergy: (2*sum|q|^2 - sum_{kz=0}|q|^2) / (2 N^6)) per field. */
 typedef struct spk_budgets {
@@ -168,6 +261,30 @@ typedef struct spk_budgets {
     double dissipation[8];   /* per field: <|grad q|^2> (k^2-weighted)     */
 } spk_budgets_t;
 int spk_budgets(spk_ctx* ctx, spk_budgets_t* out);
+
+/* Time-series quantities of InputOutput::WriteTimevarOutput
+ * (src/io/spooky_output_timevar.cu:18-213) beyond the energies of spk_budgets,
+ * as FP64 reductions of the context state (Parseval sums over the half
+ * spectrum, or grid means of the real magnetic field).  A quantity the
+ * modules do not define is -1, the reference's value for it.  Synchronises
+ * the context stream.
+ *   w2        computeEnstrophy(u): 1/2 <|curl u|^2>, computeEnergy's weighting
+ *             (every kz index > 0 counted twice, the Nyquist plane included)
+ *   hv        computeHelicity(u): <A . u> with A = i k x u / k^2 (the
+ *             reference's Helicity kernel, curl A = u)
+ *   j2, hm    the same of B (current, magnetic helicity <A . B>)
+ *   hc        <u . B> (twoFieldCorrelation)
+ *   thetaB    <|B_z| / |B|>;  bz2 <(B_z / |B|)^2>;  phiB <acos(|B_x| / |B_h|)>
+ *             (averagebz, averagebz2, averagephiB, with the 1e-16 guards and
+ *             the single-precision acos of user_defined_cuda_kernels.cu:17-46)
+ *   dissgradT computeDissipation(th): 1/2 <|grad th|^2> (-1 with anisotropic
+ *             conduction and MHD, where the reference reports the field-aligned
+ *             form, not computed here)
+ *   pv        <curl u . grad th> (potentialVorticity) */
+typedef struct spk_diagnostics {
+    double w2, hv, j2, hm, hc, thetaB, bz2, phiB, dissgradT, pv;
+} spk_diagnostics_t;
+int spk_diagnostics(spk_ctx* ctx, spk_diagnostics_t* out);
 
 /* Shell spectrum of fields f1, f2 of the context state:
  * InputOutput::computeSpectrum1d / Spectrum1d (src/io/spooky_output_spectrum.cu:424-442,

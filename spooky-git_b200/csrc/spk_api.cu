@@ -87,6 +87,10 @@ struct spk_ctx {
     // graphs
     cudaGraphExec_t gexec[2];
     bool have_graph[2];
+    // graphs of steps on a caller's state array (spk_advance_fields), for the array last used
+    cudaGraphExec_t fgexec[2];
+    bool have_fgraph[2] = {false, false};
+    const double2* fields_graph_ptr = nullptr;
     int h_step;
     std::string err;
     int sticky;
@@ -840,7 +844,10 @@ static void record_breal(spk_ctx* c) {
 // ---------------------------------------------------------------------------
 // one main-loop iteration (CleanFieldDivergence + HydroMHDAdvance)
 // ---------------------------------------------------------------------------
-static void record_step_body(spk_ctx* c, int parity);
+// rk_only: TimeStepping::RungeKutta3 (or ForwardEuler) alone, with the dt
+// already in the device scalars: no dt reduction, no super-time-stepping,
+// no divergence cleaning of the result.
+static void record_step_body(spk_ctx* c, int parity, bool rk_only = false);
 // The inverse passes of a recorded step trim the work of masked modes when
 // the state has none (the flag is refreshed whenever a state is set).
 struct TrimScope {   // trimming on for one recording or profiling, off again on every exit
@@ -852,17 +859,19 @@ static void record_step(spk_ctx* c, int parity) {
     TrimScope ts(c);
     record_step_body(c, parity);
 }
-static void record_step_body(spk_ctx* c, int parity) {
+static void record_step_body(spk_ctx* c, int parity, bool rk_only) {
     const spk_params_t& p = c->p;
-    const bool sts = p.supertimestepping && c->nsts > 0;
+    const bool sts = p.supertimestepping && c->nsts > 0 && !rk_only;
     const bool sts_before = sts && !p.sts_every_step && parity == 1;
     const bool sts_after = sts && (p.sts_every_step || parity == 0);
     const bool euler = p.integrator == SPK_INT_EULER;
     const int nst = euler ? 1 : 3;
     if (p.heat_equation) {
-        DtArgs d = dt_args(c, true);
-        k_dt<<<c->nb, 32, 0, c->stream>>>(d, c->sc);
-        c->launches++;
+        if (!rk_only) {
+            DtArgs d = dt_args(c, true);
+            k_dt<<<c->nb, 32, 0, c->stream>>>(d, c->sc);
+            c->launches++;
+        }
         if (sts_before) record_rkl_cycle(c);
         for (int s = 0; s < nst; s++) {
             XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, false);
@@ -872,10 +881,12 @@ static void record_step_body(spk_ctx* c, int parity) {
         if (sts_after) record_rkl_cycle(c);
         return;
     }
-    k_reset_max<<<c->nb, 32, 0, c->stream>>>(c->sc);
-    c->launches++;
+    if (!rk_only) {
+        k_reset_max<<<c->nb, 32, 0, c->stream>>>(c->sc);
+        c->launches++;
+    }
     for (int s = 0; s < nst; s++) {
-        const bool first = s == 0;
+        const bool first = s == 0 && !rk_only;
         pass_x_inverse(c, c->U, true, euler ? 0 : s);
         pass_y_inverse(c, true);
         if (first) {
@@ -897,7 +908,7 @@ static void record_step_body(spk_ctx* c, int parity) {
         }
         pass_y_forward(c, c->nout, c->bufA, c->bufB);
         // the last stage cleans the new u and B: CleanFieldDivergence of the next step
-        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, s == nst - 1);
+        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, s == nst - 1 && !rk_only);
         xfwd(c, x);
     }
     if (sts_after) {
@@ -1021,6 +1032,49 @@ static int params_from_config(const spkcfg::Setting& root, spk_params_t* p) {
     const int rc = check_params(p, why);
     if (rc == SPK_ERR_CONFIG) return fail(nullptr, rc, why);
     return SPK_OK;
+}
+
+// Any key of a configuration text, with libconfig's typed lookups (the
+// keys of Parameters::Parameters that spk_params_t does not carry: output,
+// initial conditions, shearing, ...).  1: found with that type; 0: absent or
+// of another type; -1: the text does not parse (spk_last_error(NULL)).
+static int cfg_root(const char* text, spkcfg::Setting* root) {
+    if (!text) { fail(nullptr, SPK_ERR_ARG, "null configuration text"); return -1; }
+    const std::string t(text);
+    std::string err;
+    if (!spkcfg::Parser(t).parse(*root, err)) { fail(nullptr, SPK_ERR_ARG, "configuration: " + err); return -1; }
+    return 0;
+}
+extern "C" int spk_cfg_lookup_int(const char* text, const char* path, int* out) {
+    spkcfg::Setting r;
+    if (cfg_root(text, &r) || !path || !out) return -1;
+    return spkcfg::get_int(r, path, out) ? 1 : 0;
+}
+extern "C" int spk_cfg_lookup_bool(const char* text, const char* path, int* out) {
+    spkcfg::Setting r;
+    if (cfg_root(text, &r) || !path || !out) return -1;
+    return spkcfg::get_bool(r, path, out) ? 1 : 0;
+}
+extern "C" int spk_cfg_lookup_float(const char* text, const char* path, double* out) {
+    spkcfg::Setting r;
+    if (cfg_root(text, &r) || !path || !out) return -1;
+    return spkcfg::get_float(r, path, out) ? 1 : 0;
+}
+extern "C" int spk_cfg_lookup_string(const char* text, const char* path, char* buf, size_t len) {
+    spkcfg::Setting r;
+    if (cfg_root(text, &r) || !path || !buf || len == 0) return -1;
+    std::string v;
+    if (!spkcfg::get_string(r, path, &v)) return 0;
+    if (v.size() + 1 > len) { fail(nullptr, SPK_ERR_ARG, std::string("string value of ") + path + " is too long"); return -1; }
+    memcpy(buf, v.c_str(), v.size() + 1);
+    return 1;
+}
+extern "C" int spk_cfg_setting_length(const char* text, const char* path) {
+    spkcfg::Setting r;
+    if (cfg_root(text, &r) || !path) return -1;
+    const spkcfg::Setting* st = spkcfg::lookup(r, path);
+    if (!st) return -1;
+    return (st->type == spkcfg::T_GROUP || st->type == spkcfg::T_ARRAY || st->type == spkcfg::T_LIST) ? (int)st->items.size() : 0;
 }
 
 extern "C" int spk_params_from_string(const char* text, spk_params_t* p) {
@@ -1303,6 +1357,7 @@ static int ctx_alloc(spk_ctx* c) {
 
 static void ctx_free(spk_ctx* c) {
     for (int i = 0; i < 2; i++) if (c->have_graph[i]) cudaGraphExecDestroy(c->gexec[i]);
+    for (int i = 0; i < 2; i++) if (c->have_fgraph[i]) cudaGraphExecDestroy(c->fgexec[i]);
     cudaFree(c->d_tab); cudaFree(c->d_tw); cudaFree(c->U); cudaFree(c->S);
     cudaFree(c->bufA); cudaFree(c->bufB); cudaFree(c->rA); cudaFree(c->rB); cudaFree(c->breal);
     cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
@@ -1404,19 +1459,27 @@ extern "C" int spk_get_time(spk_ctx* c, double* t, double* dt, int* step) {
     return SPK_OK;
 }
 
+static void launch_masked_scan(spk_ctx* c);
 static void launch_clean(spk_ctx* c) {
     const size_t bs = (size_t)c->F * c->nc;
     if (c->p.incompressible)
         k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->VEL * c->nc, bs, c->nb);
     if (c->p.mhd)
         k_clean<<<ew_blocks(c->nc * c->nb), 256, 0, c->stream>>>(c->g, c->U + (size_t)c->MAG * c->nc, bs, c->nb);
+    launch_masked_scan(c);
+    c->dirty = false;
+}
+
+// The masked-content flag of the deferred modes (DevScalars::masked_live)
+// for the current state array.
+static void launch_masked_scan(spk_ctx* c) {
+    const size_t bs = (size_t)c->F * c->nc;
     if (c->defer && c->d_keep) {
         // is there content outside the 2/3 mask to carry through the steps?
         const dim3 grid((unsigned)std::min<size_t>((c->nc + 255) / 256, (size_t)c->num_sms * 4), (unsigned)c->nb);
         k_masked_scan<<<grid, 256, 0, c->stream>>>(c->g, c->U, c->F, bs, c->sc);
         k_masked_flag<<<c->nb, 32, 0, c->stream>>>(c->sc);
     }
-    c->dirty = false;
 }
 
 extern "C" int spk_clean_divergence(spk_ctx* c) {
@@ -1475,6 +1538,35 @@ extern "C" int spk_compute_dfield(spk_ctx* c, const double* Uin, double* dUout) 
     return launch_status(c);
 }
 
+// Drops every recorded step graph (the pass layout or schedule changed).
+static void drop_graphs(spk_ctx* c) {
+    for (int i = 0; i < 2; i++) {
+        if (c->have_graph[i]) { cudaGraphExecDestroy(c->gexec[i]); c->have_graph[i] = false; }
+        if (c->have_fgraph[i]) { cudaGraphExecDestroy(c->fgexec[i]); c->have_fgraph[i] = false; }
+    }
+}
+
+// Records one main-loop step of the current state array (c->U) into *ge.
+static int capture_step(spk_ctx* c, int par, cudaGraphExec_t* ge) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const long l0 = c->launches;
+    record_step(c, par);
+    c->kernels_per_step[par] = (int)(c->launches - l0);
+    if (c->sticky) {
+        cudaGraph_t gbad;
+        cudaStreamEndCapture(c->stream, &gbad);
+        if (gbad) cudaGraphDestroy(gbad);
+        return c->sticky;
+    }
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail(c, SPK_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(c, SPK_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
+    return SPK_OK;
+}
+
 extern "C" int spk_advance(spk_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SPK_ERR_ARG;
     const bool alternate = c->p.supertimestepping && c->nsts > 0 && !c->p.sts_every_step;
@@ -1488,27 +1580,81 @@ extern "C" int spk_advance(spk_ctx* c, int nsteps) {
     for (int it = 0; it < nsteps; it++) {
         const int par = alternate ? (c->h_step & 1) : 0;
         if (!c->have_graph[par]) {
-            cudaGraph_t g;
-            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            const long l0 = c->launches;
-            record_step(c, par);
-            c->kernels_per_step[par] = (int)(c->launches - l0);
-            if (c->sticky) {
-                cudaGraph_t gbad;
-                cudaStreamEndCapture(c->stream, &gbad);
-                if (gbad) cudaGraphDestroy(gbad);
-                return c->sticky;
-            }
-            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-            if (e != cudaSuccess) return fail(c, SPK_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            CK(cudaGraphInstantiate(&c->gexec[par], g, 0));
-            cudaGraphDestroy(g);
+            int rc = capture_step(c, par, &c->gexec[par]);
+            if (rc) return rc;
             c->have_graph[par] = true;
         }
         CK(cudaGraphLaunch(c->gexec[par], c->stream));
         c->h_step++;
     }
     return SPK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Entry points on the caller's state array (the reference's d_all_fields)
+// ---------------------------------------------------------------------------
+// For one call the caller's array takes the place of the context's state.
+// Afterwards the context's own state is marked as set from outside, so that
+// its next step re-derives the masked-content flag the call overwrote.
+struct StateSwap {
+    spk_ctx* c;
+    double2* saved;
+    StateSwap(spk_ctx* cc, double2* U) : c(cc), saved(cc->U) { c->U = U; }
+    ~StateSwap() { c->U = saved; c->dirty = true; }
+};
+
+extern "C" int spk_advance_fields(spk_ctx* c, double* Uin, int nsteps) {
+    if (!c || !Uin || nsteps < 0) return SPK_ERR_ARG;
+    if (c->nb != 1) return fail(c, SPK_ERR_UNSUPPORTED, "spk_advance_fields acts on single-box contexts");
+    if (nsteps == 0) return SPK_OK;
+    double2* U = (double2*)Uin;
+    const bool alternate = c->p.supertimestepping && c->nsts > 0 && !c->p.sts_every_step;
+    StateSwap sw(c, U);
+    // the caller may have changed the array since the last call: clean it, as
+    // each iteration of the reference's main loop does
+    launch_clean(c);
+    int rc = launch_status(c);
+    if (rc) return rc;
+    if (c->fields_graph_ptr != U) {
+        for (int i = 0; i < 2; i++)
+            if (c->have_fgraph[i]) { cudaGraphExecDestroy(c->fgexec[i]); c->have_fgraph[i] = false; }
+        c->fields_graph_ptr = U;
+    }
+    for (int it = 0; it < nsteps; it++) {
+        const int par = alternate ? (c->h_step & 1) : 0;
+        if (!c->have_fgraph[par]) {
+            rc = capture_step(c, par, &c->fgexec[par]);
+            if (rc) return rc;
+            c->have_fgraph[par] = true;
+        }
+        CK(cudaGraphLaunch(c->fgexec[par], c->stream));
+        c->h_step++;
+    }
+    return SPK_OK;
+}
+
+extern "C" int spk_rk3_fields(spk_ctx* c, double* Uin) {
+    if (!c || !Uin) return SPK_ERR_ARG;
+    if (c->nb != 1) return fail(c, SPK_ERR_UNSUPPORTED, "spk_rk3_fields acts on single-box contexts");
+    StateSwap sw(c, (double2*)Uin);
+    launch_masked_scan(c);
+    record_step_body(c, 0, true);
+    return launch_status(c);
+}
+
+extern "C" int spk_compute_dt_fields(spk_ctx* c, const double* Uin, double* dt_hyp, double* dt_par, double* dt_sts,
+                                     double* dt_cur) {
+    if (!c || !Uin) return SPK_ERR_ARG;
+    if (c->nb != 1) return fail(c, SPK_ERR_UNSUPPORTED, "spk_compute_dt_fields acts on single-box contexts");
+    StateSwap sw(c, (double2*)Uin);
+    return spk_compute_dt(c, dt_hyp, dt_par, dt_sts, dt_cur);
+}
+
+extern "C" int spk_rkl_cycle_fields(spk_ctx* c, double* Uin, int* s_out) {
+    if (!c || !Uin) return SPK_ERR_ARG;
+    if (c->nb != 1) return fail(c, SPK_ERR_UNSUPPORTED, "spk_rkl_cycle_fields acts on single-box contexts");
+    StateSwap sw(c, (double2*)Uin);
+    return spk_rkl_cycle(c, s_out);
 }
 
 extern "C" int spk_rkl_cycle(spk_ctx* c, int* s_out) {
@@ -2148,3 +2294,4 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
 
 #include "spk_closure_api.cu"
 #include "spk_tune.cu"
+#include "spk_io.cu"

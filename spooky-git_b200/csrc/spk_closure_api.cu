@@ -13,8 +13,7 @@ extern "C" int spk_closure_set(spk_ctx* c, const float* params) {
     const bool on = params != nullptr;
     if (on != c->closure_on) {
         // the step graphs hold the pass layout: record them again
-        for (int i = 0; i < 2; i++)
-            if (c->have_graph[i]) { cudaGraphExecDestroy(c->gexec[i]); c->have_graph[i] = false; }
+        drop_graphs(c);
         c->closure_on = on;
     }
     return SPK_OK;

@@ -18,6 +18,7 @@
 // or compact layout, fixed-point and IEEE floating-point data of either byte
 // order.  Host code only.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -323,16 +324,18 @@ private:
         so_ = d_[at + 13];
         sl_ = d_[at + 14];
         if (so_ != 8 || sl_ != 8) { *why = "only 8-byte offsets and lengths are supported"; return false; }
+        // superblock fields at absolute positions, then addresses relative to the base
         size_t p = at + 24 + (ver == 1 ? 4 : 0);
         base_ = 0;
+        if (p + 4 * 8 + ENTRY > d_.size()) { *why = "truncated superblock"; return false; }
         const uint64_t base = raw(p, 8);
-        base_ = base == UNDEF ? at : base;
         p += 4 * 8;                       // base, free space, end of file, driver block
         const uint64_t root_oh = raw(p + 8, 8);
         const uint32_t cache = (uint32_t)raw(p + 16, 4);
         uint64_t btree = UNDEF, heap = UNDEF;
         if (cache == 1) { btree = raw(p + 24, 8); heap = raw(p + 32, 8); }
-        else {
+        base_ = base == UNDEF ? at : base;
+        if (cache != 1) {
             Info ri;
             if (!object(root_oh, &ri, why)) return false;
             btree = ri.stab_btree; heap = ri.stab_heap;

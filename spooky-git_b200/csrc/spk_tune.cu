@@ -31,11 +31,6 @@ static float time_steps(spk_ctx* c, int steps, int* rc) {
     return ms / (float)std::max(steps, 1);
 }
 
-static void drop_graphs(spk_ctx* c) {
-    for (int i = 0; i < 2; i++)
-        if (c->have_graph[i]) { cudaGraphExecDestroy(c->gexec[i]); c->have_graph[i] = false; }
-}
-
 extern "C" int spk_autotune(spk_ctx* c, int steps, int* zl, int* nst, int* rhs, double* ms_before, double* ms_after) {
     if (!c || steps < 1) return SPK_ERR_ARG;
     if (c->p.heat_equation) return fail(c, SPK_ERR_UNSUPPORTED, "the heat-equation mode has no tunable passes");

@@ -39,7 +39,17 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_closure_set", "spk_products", "spk_closure_samples_size", "spk_closure_samples",
             "spk_trainer_create", "spk_trainer_destroy", "spk_trainer_set_params", "spk_trainer_get_params",
             "spk_trainer_set_samples", "spk_trainer_loss_grad", "spk_trainer_train", "spk_spectrum",
-            "spk_autotune", "spk_ensemble_autotune"]
+            "spk_autotune", "spk_ensemble_autotune", "spk_advance_fields", "spk_compute_dt_fields",
+            "spk_rk3_fields", "spk_rkl_cycle_fields", "spk_get_state_real", "spk_set_state_real",
+            "spk_write_snapshot", "spk_read_snapshot", "spk_h5_write", "spk_h5_read", "spk_diagnostics",
+            "spk_cfg_lookup_int", "spk_cfg_lookup_bool", "spk_cfg_lookup_float", "spk_cfg_lookup_string",
+            "spk_cfg_setting_length"]
+
+DIAGNOSTICS = ("w2", "hv", "j2", "hm", "hc", "thetaB", "bz2", "phiB", "dissgradT", "pv")
+
+
+class Diagnostics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in DIAGNOSTICS]
 
 # learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
@@ -118,6 +128,20 @@ def lib():
         L.spk_trainer_loss_grad.argtypes = [vp, fp, fp]
         L.spk_trainer_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp]
         L.spk_spectrum.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip, dp, dp]
+        L.spk_advance_fields.argtypes = [vp, vp, ctypes.c_int]
+        L.spk_compute_dt_fields.argtypes = [vp, vp, dp, dp, dp, dp]
+        L.spk_rk3_fields.argtypes = [vp, vp]
+        L.spk_rkl_cycle_fields.argtypes = [vp, vp, ip]
+        L.spk_get_state_real.argtypes = [vp, vp, ctypes.c_int]
+        L.spk_set_state_real.argtypes = [vp, vp, ctypes.c_int]
+        L.spk_write_snapshot.argtypes = [vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.spk_read_snapshot.argtypes = [vp, ctypes.c_char_p, dp, dp]
+        L.spk_diagnostics.argtypes = [vp, ctypes.POINTER(Diagnostics)]
+        L.spk_cfg_lookup_int.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ip]
+        L.spk_cfg_lookup_bool.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ip]
+        L.spk_cfg_lookup_float.argtypes = [ctypes.c_char_p, ctypes.c_char_p, dp]
+        L.spk_cfg_lookup_string.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sp]
+        L.spk_cfg_setting_length.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.spk_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ip, dp, dp]
         L.spk_ensemble_autotune.argtypes = [vp, ctypes.c_int]
         L.spk_last_error.restype = ctypes.c_char_p
@@ -168,6 +192,31 @@ def _check_state_tensor(name, a, shape, dtype="complex128"):
         raise ValueError(f"{name} must be contiguous")
     if tuple(a.shape) != tuple(shape):
         raise ValueError(f"{name} has shape {tuple(a.shape)}, expected {tuple(shape)}")
+
+
+def cfg_lookup(text, path, kind, default=None):
+    """A key of a spooky.cfg text with libconfig's typed lookups
+    (spk_cfg_lookup_*): kind is "int", "bool", "float", "string" or
+    "strings" (a list or array of strings); the default when the key is
+    absent or of another type."""
+    L = lib()
+    t, k = text.encode(), path.encode()
+    if kind == "strings":
+        n = L.spk_cfg_setting_length(t, k)
+        if n <= 0:
+            return default
+        return [v for v in (cfg_lookup(text, f"{path}.[{i}]", "string") for i in range(n)) if v is not None]
+    if kind == "string":
+        buf = ctypes.create_string_buffer(4096)
+        rc = L.spk_cfg_lookup_string(t, k, buf, len(buf))
+        val = buf.value.decode() if rc == 1 else None
+    else:
+        box = {"int": ctypes.c_int, "bool": ctypes.c_int, "float": ctypes.c_double}[kind]()
+        rc = getattr(L, f"spk_cfg_lookup_{kind}")(t, k, ctypes.byref(box))
+        val = (bool(box.value) if kind == "bool" else box.value) if rc == 1 else None
+    if rc < 0:
+        raise SpookyError(1, L.spk_last_error(None).decode())
+    return default if val is None else val
 
 
 def params_from_file(path):
@@ -302,6 +351,66 @@ class Context:
 
     def advance(self, nsteps=1):
         self._check(lib().spk_advance(self._h, int(nsteps)))
+
+    # -- the same operations on a caller's state array (torch CUDA complex128, shape_c)
+    def advance_fields(self, U, nsteps=1):
+        """nsteps main-loop steps on U in place (spk_advance_fields; asynchronous)."""
+        _check_state_tensor("U", U, self.shape_c)
+        _torch_sync()
+        self._check(lib().spk_advance_fields(self._h, U.data_ptr(), int(nsteps)))
+
+    def compute_dt_fields(self, U):
+        """TimeStepping::compute_dt on U: (dt_hyp, dt_par, dt_sts, dt)."""
+        _check_state_tensor("U", U, self.shape_c)
+        _torch_sync()
+        o = [ctypes.c_double() for _ in range(4)]
+        self._check(lib().spk_compute_dt_fields(self._h, U.data_ptr(), *[ctypes.byref(x) for x in o]))
+        return np.array([x.value for x in o])
+
+    def rk3_fields(self, U):
+        """TimeStepping::RungeKutta3 on U with the last dt (spk_rk3_fields)."""
+        _check_state_tensor("U", U, self.shape_c)
+        _torch_sync()
+        self._check(lib().spk_rk3_fields(self._h, U.data_ptr()))
+        self.synchronize()
+
+    def rkl_cycle_fields(self, U):
+        _check_state_tensor("U", U, self.shape_c)
+        _torch_sync()
+        s = ctypes.c_int()
+        self._check(lib().spk_rkl_cycle_fields(self._h, U.data_ptr(), ctypes.byref(s)))
+        self.synchronize()
+        return s.value
+
+    def diagnostics(self):
+        """{name: value} of the time-series quantities of spk_diagnostics
+        (w2 hv j2 hm hc thetaB bz2 phiB dissgradT pv; -1 where undefined)."""
+        d = Diagnostics()
+        self._check(lib().spk_diagnostics(self._h, ctypes.byref(d)))
+        return {n: getattr(d, n) for n in DIAGNOSTICS}
+
+    # -- real-space state and snapshots
+    def get_state_real(self):
+        """Real fields [F][nx][ny][nz] (FP64, host) of the state (spk_get_state_real)."""
+        R = np.empty(self.shape_r, dtype=np.float64)
+        self._check(lib().spk_get_state_real(self._h, R.ctypes.data, 1))
+        return R
+
+    def set_state_real(self, R):
+        """State from real fields [F][nx][ny][nz] (spk_set_state_real)."""
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        if R.shape != self.shape_r:
+            raise ValueError(f"R has shape {R.shape}, expected {self.shape_r}")
+        self._check(lib().spk_set_state_real(self._h, R.ctypes.data, 1))
+
+    def write_snapshot(self, path, t_start=0.0, t_lastsnap=0.0, t_lastvar=0.0):
+        self._check(lib().spk_write_snapshot(self._h, os.fsencode(path), t_start, t_lastsnap, t_lastvar))
+
+    def read_snapshot(self, path):
+        """State, time, step and t_lastsnap from a snapshot; returns (t_lastsnap, t_lastvar)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().spk_read_snapshot(self._h, os.fsencode(path), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def rkl_cycle(self):
         s = ctypes.c_int()
@@ -628,27 +737,53 @@ class TimeStepping:
         return self._ctx.get_time()[2]
 
 
+def fileCounter(dirname):
+    """Index of the most recent snapNNNN.h5 in dirname (the count of
+    consecutive files from snap0000.h5, minus one; -1 when there is none),
+    as src/io/hdf5_io.cu:255-276 counts them."""
+    n = -1
+    while os.path.exists(os.path.join(dirname, "snap%04d.h5" % (n + 1))):
+        n += 1
+    return n
+
+
 class InputOutput:
-    """InputOutput's output schedule (src/io/inputoutput.hpp, check_output.cu:14-97).
+    """InputOutput's output schedule and files (src/io/inputoutput.hpp,
+    check_output.cu:14-97, hdf5_io.cu:19-276).
 
     After every main-loop step the supervisor calls CheckOutput.  A time
     series is due when t - t_lastvar >= toutput_time, a snapshot when
     t - t_lastsnap + 1e-8 >= toutput_flow (and both at t = 0).  As in the
     reference, each output first cleans the divergence of the state, and a
     snapshot advances t_lastsnap by toutput_flow -- which the dt rule reads,
-    so that steps land on the snapshot times.  The writers are callables:
-    ``on_timevar(supervisor, t)`` and ``on_snapshot(supervisor, num_save)``
-    (None: the schedule and the cleaning still run, nothing is written)."""
+    so that steps land on the snapshot times.
 
-    def __init__(self, sup, toutput_time=1.0, on_timevar=None, on_snapshot=None):
+    With an output directory, snapshots go to <dir>/data/snapNNNN.h5 (the
+    reference's HDF5 layout, spk_write_snapshot) and the time series to
+    <dir>/timevar.spooky and <dir>/spectrum.spooky (the reference's text
+    layouts).  ``on_timevar(supervisor, t)`` and ``on_snapshot(supervisor,
+    num_save)`` replace those writers; with neither a directory nor a
+    callable the schedule and the cleaning still run and nothing is written."""
+
+    TIMEVAR_DEFAULT = ("t", "ev", "em")
+    SPECTRA_DEFAULT = ()
+
+    def __init__(self, sup, toutput_time=1.0, on_timevar=None, on_snapshot=None, output_dir=None,
+                 timevar_vars=None, spectra_vars=None):
         self.sup = sup
         self.toutput_time = toutput_time
         self.t_lastsnap = 0.0
         self.t_lastvar = 0.0
         self.num_save = 0
-        self.on_timevar = on_timevar
-        self.on_snapshot = on_snapshot
+        self.output_dir = output_dir
+        self.timevar_vars = tuple(timevar_vars) if timevar_vars is not None else self.TIMEVAR_DEFAULT
+        self.spectra_vars = tuple(spectra_vars) if spectra_vars is not None else self.SPECTRA_DEFAULT
+        if output_dir is not None:
+            os.makedirs(os.path.join(output_dir, "data"), exist_ok=True)
+        self.on_timevar = on_timevar if on_timevar is not None else (self._write_timeseries if output_dir else None)
+        self.on_snapshot = on_snapshot if on_snapshot is not None else (self.WriteDataFile if output_dir else None)
 
+    # -- the schedule
     def CheckOutput(self):
         self.CheckTimeSeries()
         self.CheckSnapshot()
@@ -673,31 +808,105 @@ class InputOutput:
                 self.on_snapshot(self.sup, self.num_save)
             self.num_save += 1
 
+    # -- the files
+    def snapshot_path(self, num):
+        return os.path.join(self.output_dir, "data", "snap%04d.h5" % num)
+
+    def WriteDataFile(self, sup, num):
+        """InputOutput::WriteDataFile (hdf5_io.cu:19-111)."""
+        sup.ctx.write_snapshot(self.snapshot_path(num), sup.param.t_initial, self.t_lastsnap, self.t_lastvar)
+
+    def _write_timeseries(self, sup, t):
+        from . import outputs
+        tv = os.path.join(self.output_dir, "timevar.spooky")
+        sp = os.path.join(self.output_dir, "spectrum.spooky")
+        if t == 0.0:
+            outputs.write_timevar_header(tv, self.timevar_vars)
+            if self.spectra_vars:
+                outputs.write_spectrum_header(sp, sup.ctx, self.spectra_vars)
+        outputs.write_timevar(tv, sup.ctx, self.timevar_vars)
+        if self.spectra_vars:
+            outputs.write_spectrum(sp, sup.ctx, t, self.spectra_vars)
+
+    def ReadDataFile(self, restart_num):
+        """InputOutput::ReadDataFile (hdf5_io.cu:114-252): restart from
+        snap<restart_num> (-1, or a number past the last file: the most
+        recent one).  Sets the state, time, step, t_lastsnap and t_lastvar;
+        num_save becomes the file's number + 1.  Returns the number read, or
+        -1 when there is no snapshot (a new run, as the reference does)."""
+        last = fileCounter(os.path.join(self.output_dir, "data"))
+        if last < 0:
+            return -1
+        num = last if (restart_num == -1 or restart_num > last) else restart_num
+        path = self.snapshot_path(num)
+        if not os.path.exists(path):
+            raise SpookyError(1, f"restart file {path} not found")
+        self.t_lastsnap, self.t_lastvar = self.sup.ctx.read_snapshot(path)
+        self.num_save = num + 1
+        return num
+
 
 class Supervisor:
     """Supervisor (src/supervisor/supervisor.hpp:24-84) for the hot path."""
 
-    def __init__(self, params, stream=None, toutput_time=1.0, on_timevar=None, on_snapshot=None):
+    def __init__(self, params, stream=None, toutput_time=1.0, on_timevar=None, on_snapshot=None, output_dir=None,
+                 timevar_vars=None, spectra_vars=None, restart_num=-2):
+        """restart_num: -2 a new run; -1 restart from the most recent
+        snapshot in output_dir/data; n >= 0 from snap n (main.cu's -r)."""
         self.param = Parameters(params)
         self.ctx = Context(self.param.p, stream)
         self.fields = Fields(self.ctx)
         self.timestep = TimeStepping(self.ctx)
-        self.inout = InputOutput(self, toutput_time, on_timevar, on_snapshot)
+        self.inout = InputOutput(self, toutput_time, on_timevar, on_snapshot, output_dir, timevar_vars,
+                                 spectra_vars)
+        self.restart_num = restart_num
+        if restart_num >= -1:
+            self.Restart()
+
+    def Restart(self):
+        """Supervisor::Restart (supervisor.cu:241-245); with no snapshot on
+        disk the run starts anew (hdf5_io.cu:242-248)."""
+        if self.inout.output_dir is None:
+            raise SpookyError(1, "a restart needs an output directory")
+        if self.inout.ReadDataFile(self.restart_num) < 0:
+            self.restart_num = -2
 
     def initialDataDump(self):
-        """The outputs at t = 0 of a run that does not restart (supervisor.cu:215-225)."""
-        self.inout.CheckOutput()
+        """The outputs at t = 0 (supervisor.cu:215-238): every output of a new
+        run; a restart from snapshot 0 writes only the time series."""
+        if self.restart_num == -2:
+            self.inout.CheckOutput()
+        elif self.restart_num == 0:
+            self.inout.CheckTimeSeries()
 
-    def executeMainLoop(self, max_steps=None):
+    def executeMainLoop(self, max_steps=None, max_walltime_hours=None, stats_frequency=-1, log=print):
         """Advance until t_final (src/supervisor/supervisor.cu:169-213): per
         step CleanFieldDivergence + HydroMHDAdvance, then CheckOutput; the
-        host reads the device time once per step."""
+        host reads the device time once per step.  Stops early after
+        max_steps steps or max_walltime_hours of main-loop time; with
+        stats_frequency > 0 prints the cell-update rate every that many steps
+        (print_partial_stats, :75-80).  Returns the steps taken."""
+        import time
         n = 0
-        while self.timestep.current_time < self.param.t_final:
+        t_loop = t_part = 0.0
+        nr = self.param.nx * self.param.ny * self.param.nz
+        limit = None if max_walltime_hours is None else 3600.0 * max_walltime_hours
+        while self.timestep.current_time < self.param.t_final and (limit is None or t_loop < limit):
+            t0 = time.perf_counter()
             self.timestep.HydroMHDAdvance(1)
             n += 1
             self.inout.CheckOutput()
+            dt = time.perf_counter() - t0
+            t_loop += dt
+            t_part += dt
+            if stats_frequency > 0 and self.timestep.current_step % stats_frequency == 0:
+                log("---- The avg number of cell updates / sec is %.4e [cell_updates/s]" % (nr * stats_frequency / t_part))
+                t_part = 0.0
             if max_steps is not None and n >= max_steps:
                 break
+        if limit is not None and t_loop >= limit:
+            log("The maximum wallclock elapsed time was reached. Stopping now. You can later resume from the last "
+                "snapshot available.")
         self.ctx.synchronize()
+        self.time_in_main_loop = t_loop
         return n

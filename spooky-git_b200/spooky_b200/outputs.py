@@ -5,9 +5,12 @@ timevar.spooky (InputOutput::WriteTimevarOutput,
 src/io/spooky_output_timevar.cu:18-213) for the quantities of this path:
 t, the energies (ev, Kx, Ky, Kz, em, Mx, My, Mz, et -- computeEnergy through
 spk_budgets) and the two-field correlations (vxvy ... thvz --
-twoFieldCorrelation through the Parseval sum of spk_spectrum).  Other
-names are written as -1, the reference's value for a quantity it does not
-compute."""
+twoFieldCorrelation through the Parseval sum of spk_spectrum), and the
+enstrophies, helicities, field-direction means, thermal dissipation and
+potential vorticity of spk_diagnostics.  The field-aligned conduction terms
+(dissgradT with anisotropic conduction and MHD, fluxbbgradT) and the
+transfer spectra are written as -1, the reference's value for a quantity it
+does not compute."""
 
 # spectrum names -> field pairs (spooky_output_spectrum.cu:53-186)
 SPECTRA = {"Kx": ("vx", "vx"), "Ky": ("vy", "vy"), "Kz": ("vz", "vz"),
@@ -20,6 +23,11 @@ ENERGIES = {"ev": ("vx", "vy", "vz"), "Kx": ("vx",), "Ky": ("vy",), "Kz": ("vz",
 CORRELATIONS = {"vxvy": ("vx", "vy"), "vxvz": ("vx", "vz"), "vyvz": ("vy", "vz"),
                 "bxby": ("bx", "by"), "bxbz": ("bx", "bz"), "bybz": ("by", "bz"),
                 "thvx": ("th", "vx"), "thvy": ("th", "vy"), "thvz": ("th", "vz")}
+
+
+# enstrophy, helicities, field-direction means, thermal dissipation and
+# potential vorticity (spk_diagnostics)
+DIAGNOSTIC_NAMES = ("w2", "hv", "j2", "hm", "hc", "thetaB", "bz2", "phiB", "dissgradT", "pv")
 
 
 def _fmt(x):
@@ -56,6 +64,7 @@ def write_timevar_header(path, names):
 def timevar_values(ctx, names):
     t = ctx.get_time()[0]
     e, _ = ctx.budgets()
+    diag = None
     out = []
     for name in names:
         v = -1.0
@@ -65,6 +74,10 @@ def timevar_values(ctx, names):
             v = float(sum(e[ctx.var_list.index(q)] for q in ENERGIES[name]))
         elif name in CORRELATIONS and all(q in ctx.var_list for q in CORRELATIONS[name]):
             v = ctx.spectrum(*CORRELATIONS[name])[2]
+        elif name in DIAGNOSTIC_NAMES:
+            if diag is None:
+                diag = ctx.diagnostics()
+            v = diag[name]
         out.append(v)
     return out
 

@@ -12,7 +12,7 @@ from spooky_b200.params import Params, check_parameters, default_params
 
 def declared_symbols():
     src = open(S.HEADER_PATH).read()
-    return sorted(set(re.findall(r"\b(spk_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(spk_[a-z0-9_]+)\s*\(", src)))
 
 
 def test_header_declares_exactly_the_exported_list():

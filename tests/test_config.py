@@ -189,3 +189,52 @@ def test_cfg_text_round_trip(kw):
     q = S.params_from_string(cfg_text(p))
     for name, _ in p._fields_:
         assert getattr(q, name) == getattr(p, name), name
+
+
+CFG_EXTRA = """
+configname = "extras";
+modules: { incompressible = true; mhd = true; };
+physics: { boxsize = (1.0, 1.0, 1.0); gridsize = (16, 16, 8); reynolds = 100.0; };
+code: { t_final = 2.0; max_walltime_elapsed = 1.5; symmetries_step = 7; };
+output: {
+    timevar_step = 0.25;
+    snapshot_step = 0.5;
+    output_dir = "/tmp/run";
+    timevar_vars = ("t", "ev", "em", "w2", "hc");
+    spectra_vars = ["Kx", "Mx"];
+    vorticity = true;
+};
+"""
+
+
+def test_cfg_lookup_reads_any_key_with_libconfig_typing():
+    t = CFG_EXTRA
+    assert S.cfg_lookup(t, "output.timevar_step", "float") == 0.25
+    assert S.cfg_lookup(t, "output.output_dir", "string") == "/tmp/run"
+    assert S.cfg_lookup(t, "output.timevar_vars", "strings") == ["t", "ev", "em", "w2", "hc"]
+    assert S.cfg_lookup(t, "output.spectra_vars", "strings") == ["Kx", "Mx"]
+    assert S.cfg_lookup(t, "code.symmetries_step", "int") == 7
+    assert S.cfg_lookup(t, "output.vorticity", "bool") is True
+    # typed: an int key does not satisfy a float lookup, absent keys give the default
+    assert S.cfg_lookup(t, "code.symmetries_step", "float", -1.0) == -1.0
+    assert S.cfg_lookup(t, "output.nothing", "string", "dflt") == "dflt"
+    with pytest.raises(S.SpookyError):
+        S.cfg_lookup("physics: { a = ; }", "physics.a", "float")
+
+
+def test_command_line_overrides_follow_main_cu():
+    """src/main.cu:28-134: -n overrides the grid, --with-2d forces 2D,
+    --output-dir the cfg's output_dir, -t the wall-clock limit (x 0.95),
+    -r the restart number (absent: a new run)."""
+    from spooky_b200 import __main__ as M
+    a = M.parse_args(["--input-dir", "/x", "--output-dir", "/y", "-r", "3", "-t", "1", "30", "0",
+                      "-n", "32", "16", "8", "--with-2d", "--stats", "5"])
+    assert a.input_dir == "/x" and a.restart == 3 and a.ngrid == [32, 16, 8] and a.with_2d and a.stats == 5
+    rc = M.run_config(CFG_EXTRA, a)
+    assert rc["output_dir"] == "/y"
+    assert abs(rc["max_walltime_hours"] - 0.95 * 1.5) < 1e-15
+    assert rc["toutput_time"] == 0.25 and rc["timevar_vars"][3] == "w2"
+    b = M.parse_args([])
+    assert b.restart is None and b.ngrid is None and not b.with_2d
+    rc = M.run_config(CFG_EXTRA, b)
+    assert rc["output_dir"] == "/tmp/run" and rc["max_walltime_hours"] == 1.5
