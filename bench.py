@@ -395,6 +395,51 @@ def mti_timing(n, steps, warmup, stream):
     return ms, s_rkl, kps, t, (hyp, par, sts, cur), e
 
 
+def mti_sigma(k, chi, nu, eta, vA2, N2, OmegaT2):
+    """Growth rate of the magnetothermal instability for k along B0: the
+    largest real root of the dispersion cubic of the reference's MTI test
+    (tests/mti-eigenmode/mti_disp_rel.py:44-70) with omega_T^2 kept general,
+    x = chi k^2, Pr = nu/chi, q = eta/chi:
+    s^3 + x(1+q+Pr) s^2 + (N2 + k^2 vA^2 + (q+Pr+qPr) x^2) s
+    + qPr x^3 + N2 q x + k^2 vA^2 x - OmegaT2 x = 0."""
+    x, Pr, q = chi * k * k, nu / chi, eta / chi
+    c = [1.0, x * (1 + q + Pr), N2 + k * k * vA2 + (q + Pr + q * Pr) * x * x,
+         q * Pr * x ** 3 + N2 * q * x + k * k * vA2 * x - OmegaT2 * x]
+    r = np.roots(c)
+    return float(np.max(r[np.abs(r.imag) < 1e-12].real))
+
+
+def mti_growth_rates(n, ns=(6, 8, 10, 12), t_end=6.0, t_fit=4.0):
+    """Config 3 from its white-noise start to t_end: the slope of
+    log|theta(k = m x)| over [t_fit, t_end] for each m in ns, against the
+    dispersion relation."""
+    import torch
+    import spooky_b200 as S
+    p = mti_params(n)
+    ctx = S.Context(p)
+    ctx.set_state(mti_state(p))
+    buf = torch.empty(ctx.shape_c, dtype=torch.complex128, device="cuda")
+    ts, amps = [], []
+    while True:
+        ctx.advance(1)
+        t = ctx.get_time()[0]
+        ctx.get_state(buf)
+        torch.cuda.synchronize()
+        amps.append(buf[ctx.F - 1, list(ns), 0, 0].abs().cpu().numpy())
+        ts.append(t)
+        if t > t_end:
+            break
+    ctx.close()
+    ts, amps = np.array(ts), np.array(amps)
+    sel = ts >= t_fit
+    out = []
+    for i, m in enumerate(ns):
+        fit = float(np.polyfit(ts[sel], np.log(amps[sel, i]), 1)[0])
+        ana = mti_sigma(float(m), 1.0 / p.reynolds_ani, p.nu, p.nu_m, 1e-6, p.N2, p.OmegaT2)
+        out.append({"k": m, "sigma_fit": fit, "sigma_dispersion": ana, "rel_err": abs(fit - ana) / ana})
+    return {"modes": out, "fit_window": [t_fit, float(ts[-1])], "steps": int(len(ts))}
+
+
 def run_mti(args, world, rank, local_rank):
     import torch
     import spooky_b200 as S
@@ -412,6 +457,7 @@ def run_mti(args, world, rank, local_rank):
                        "rkl2_stages_per_cycle": s_rkl, "dt": cur, "dt_sts": sts, "dt_hyp": hyp},
             "mmode_steps_per_s": (1000.0 / ms) * args.n ** 3 / 1e6,
             "kernels_per_step_recorded": kps, "sim_time": t, "energies_finite": bool(np.isfinite(e).all()),
+            "growth_rates": mti_growth_rates(args.n),
         }), flush=True)
 
 

@@ -1,7 +1,9 @@
 // Prints the parameters a configuration file gives through the C++ surface
 // (spooky_b200::Parameters), one "name value" pair per line; on an error it
 // prints "error <code> <message>".  With --run N it also builds a Supervisor,
-// advances N steps on the GPU and prints the time, step count and energies.
+// advances N steps on the GPU and prints the time, step count and energies;
+// with --snap DIR it runs the main loop to t_final writing snapshots under
+// DIR/data and restarts a second Supervisor from the most recent one.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -32,6 +34,28 @@ int main(int argc, char** argv) {
             const spk_budgets_t b = sup.fields->budgets();
             std::printf("steps %ld\nstep %d\ntime %.17g\nenergy0 %.17g\n", taken, sup.timestep->current_step,
                         sup.timestep->current_time, b.energy[0]);
+        }
+        if (argc >= 4 && std::strcmp(argv[2], "--snap") == 0) {
+            // the main loop with snapshots in DIR/data, then a restart from the most recent one
+            const std::string dir = argv[3];
+            std::vector<double> U;
+            {
+                spooky_b200::Supervisor sup(p, nullptr, dir);
+                U.assign(2 * (size_t)sup.fields->num_fields * sup.fields->n_complex, 0.0);
+                const size_t kk = (size_t)p.nz / 2 + 1;
+                U[2 * (1 * kk)] = 0.25 * p.nx * p.ny * p.nz;
+                sup.fields->set(U.data(), false);
+                sup.initialDataDump();
+                const long taken = sup.executeMainLoop();
+                std::printf("steps %ld\nnum_save %d\ntime %.17g\nlast %d\n", taken, sup.inout->num_save,
+                            sup.timestep->current_time, sup.inout->fileCounter());
+            }
+            spooky_b200::Supervisor again(p, nullptr, dir, -1);
+            again.timestep->refresh();
+            const spk_budgets_t b = again.fields->budgets();
+            std::printf("restart_num_save %d\nrestart_time %.17g\nrestart_step %d\nrestart_lastsnap %.17g\n"
+                        "restart_energy0 %.17g\n", again.inout->num_save, again.timestep->current_time,
+                        again.timestep->current_step, again.inout->t_lastsnap, b.energy[0]);
         }
     } catch (const spooky_b200::Error& e) {
         std::printf("error %d %s\n", e.code, e.what());

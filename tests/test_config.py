@@ -238,3 +238,18 @@ def test_command_line_overrides_follow_main_cu():
     assert b.restart is None and b.ngrid is None and not b.with_2d
     rc = M.run_config(CFG_EXTRA, b)
     assert rc["output_dir"] == "/tmp/run" and rc["max_walltime_hours"] == 1.5
+
+
+def test_mti_dispersion_cubic_of_the_bench_matches_the_reference_golden():
+    """bench.mti_sigma (the growth rate config 3's check uses) reproduces the
+    reference's own dispersion cubic (tests/golden/mti_eigenmode.json, from
+    tests/mti-eigenmode/mti_disp_rel.py) at its parameters."""
+    import json
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import mti_sigma
+    g = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mti_eigenmode.json")))
+    s = mti_sigma(2 * np.pi * g["n_mode"], 1.0 / g["Pe"], 1.0 / g["ReNu"], 1.0 / g["ReEta"], g["B0"] ** 2, g["N2"],
+                  g["OmegaT2"])
+    assert abs(s - g["sigma_dispersion_cubic"]) < 1e-13
+    assert abs(s - g["sigma_check_script"]) < 1e-13

@@ -75,3 +75,22 @@ def test_cpp_supervisor_main_loop_matches_python(program, tmp_path):
     assert int(vals["steps"]) == 5 and int(vals["step"]) == step == 5
     assert float(vals["time"]) == pytest.approx(t, rel=1e-14)
     assert float(vals["energy0"]) == pytest.approx(e[0], rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_cpp_snapshots_and_restart(program, tmp_path):
+    """Supervisor with an output directory: snapshots every toutput_flow in the
+    reference's HDF5 layout, then Supervisor(p, 0, dir, -1) restarts from the
+    most recent one (its time, step, t_lastsnap and state)."""
+    cfg = CFG.replace("code: { cfl = 1.2; t_final = 0.75; };",
+                      "code: { cfl = 1.2; t_final = 0.75; };\noutput: { snapshot_step = 0.25; };")
+    out = tmp_path / "run"
+    (out / "data").mkdir(parents=True)
+    vals = run(program, cfg, tmp_path, "--snap", str(out))
+    assert int(vals["last"]) == 3 and int(vals["num_save"]) == 4      # t = 0, 0.25, 0.5, 0.75
+    assert float(vals["time"]) == pytest.approx(0.75, abs=1e-14)
+    assert int(vals["restart_num_save"]) == 4
+    assert float(vals["restart_time"]) == pytest.approx(0.75, abs=1e-14)
+    assert float(vals["restart_lastsnap"]) == pytest.approx(0.75, abs=1e-12)
+    assert int(vals["restart_step"]) > 0
+    assert float(vals["restart_energy0"]) > 0

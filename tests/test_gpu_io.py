@@ -128,11 +128,15 @@ def test_restart_continues_the_run(tmp_path, form):
     assert rel_l2(b.fields.get(), Ua) < (1e-12 if form == SPK_FORM_PLAIN else 1e-5)
     c = Supervisor(p, output_dir=out, restart_num=-1)
     assert c.inout.num_save == 5 and c.timestep.current_time == pytest.approx(ta, abs=1e-13)
-    # the time series: header, one line per output time, the reference's format
+    # the time series: header, one line per output time, the reference's
+    # format.  Its schedule has no tolerance (check_output.cu:31): at t = 0.2
+    # the accumulated t_lastvar (0.15000000000000002) leaves t - t_lastvar a
+    # hair under 0.05, so run a writes t = 0, 0.05, 0.1, 0.15, as the
+    # reference would, and the restarted run appends its own lines.
     lines = open(os.path.join(out, "timevar.spooky")).read().splitlines()
     assert lines[0].startswith("## This file contains") and lines[1].split() == ["##", "t", "ev", "em", "w2", "j2", "hc"]
     rows = [list(map(float, l.split())) for l in lines[2:]]
-    assert [r[0] for r in rows[:5]] == pytest.approx([0.0, 0.05, 0.1, 0.15, 0.2])
+    assert [r[0] for r in rows[:4]] == pytest.approx([0.0, 0.05, 0.1, 0.15])
     assert all(r[3] > 0 and r[4] > 0 for r in rows)
 
 
@@ -209,7 +213,12 @@ def test_entry_points_on_caller_memory(form):
     L = 2 * np.pi
     p = default_params(incompressible=1, mhd=1, gridsize=(32, 16, 16), boxsize=(L, L, L), reynolds=200.0,
                        reynolds_magnetic=200.0, form=form, t_final=100.0, toutput_flow=100.0)
-    U = mhd_state(p, 11)
+    # a divergence-free state on the grid (numpy's round trip leaves the Nyquist planes of
+    # the random fields with some divergence, which the first cleaning would remove)
+    c0 = Context(p)
+    c0.set_state(mhd_state(p, 11))
+    c0.clean_divergence()
+    U = c0.get_state()
     ref = Context(p)
     ref.set_state(U)
     ref.advance(4)
@@ -247,9 +256,9 @@ def test_entry_points_on_caller_memory(form):
 
 def test_rkl_cycle_on_caller_memory():
     p = default_params(heat_equation=1, gridsize=(128, 2, 2), boxsize=(4.0, 1.0, 1.0), reynolds_thermic=1.0,
-                       cfl_par=0.5, safety_sts=10, t_final=0.5, toutput_flow=100.0, antialiasing=0,
+                       cfl_par=0.5, safety_sts=1, t_final=0.5, toutput_flow=100.0, antialiasing=0,
                        supertimestepping=1, sts_algorithm="rkl2", sts_variables=["th"], integrator=1,
-                       sts_every_step=1)
+                       sts_every_step=1, fixed_dt=0.002 * 4.0 / 128)
     X, _, _ = grid(p)
     T0 = np.exp(-0.5 * X ** 2 / 0.01)[None]
     a = Context(p)

@@ -168,3 +168,22 @@ def test_mhd256_fp32_form_within_1e5_of_plain_after_1000_steps():
     e32, _ = c32.budgets()
     e64, _ = c64.budgets()
     assert abs(np.sum(e32) - np.sum(e64)) / np.sum(e64) < 1e-6
+
+
+# ---- config 3: MTI growth rates at 256^3 ------------------------------------------
+def test_mti256_growth_rates_match_the_dispersion_relation():
+    """Config 3 (256^3 box 2 pi, Boussinesq MHD, chi_par = 0.05, nu = eta =
+    1e-4, B0 = 1e-3 x, N2 = omega_T^2 = 1, RKL2 on theta, white noise 1e-4
+    in u and theta; FP32 form): the Fourier modes k = n x (n = 6, 8, 10, 12)
+    of theta grow in the linear phase at the rate of the dispersion relation
+    (bench.mti_sigma, pinned to the reference's cubic in tests/test_config.py).
+    The slope of log|theta_k| over t in [4, 6] is compared with the largest
+    root; the two other roots of these modes decay at rates above 1.2, so
+    their share has fallen below 1e-3 by t = 4."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import mti_growth_rates
+    r = mti_growth_rates(256)
+    assert r["steps"] >= 40
+    for m in r["modes"]:
+        assert m["rel_err"] < 5e-3, m
