@@ -284,7 +284,8 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
     const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, N>::TWN * sizeof(C2<T>) +
-                         (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
+                         (size_t)N * sizeof(T) + N + 1024 + 256 + 16;   // ... + row mask + outer mask (<= 1024)
+                                                                        // + box mask (<= 256)
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
@@ -489,6 +490,9 @@ static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch,
         while (N % d) d--;
         a.box_rows = d;
     }
+    // trimmed y inverse: 32-row boxes, so that the boxes of masked y rows
+    // (which the x inverse left unwritten) are not loaded at all
+    if (a.trim == 2 && N >= 128 && N % 32 == 0) a.box_rows = 32;
     if (in_state && c->fp32) a.convert = 1;
     a.in_box_ch = in_state ? c->F : buf_channels(c, base);
     if (c->nb > 1 && (base == c->rA || base == c->rB || base == c->user_U)) {
