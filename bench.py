@@ -342,14 +342,14 @@ def run_ensemble(args, world, rank, local_rank):
         dist.destroy_process_group()
 
 
-def mti_params(n):
+def mti_params(n, safety_sts=95):
     """Config 3: Boussinesq MHD with field-aligned anisotropic conduction in a
     2 pi box; gravity along z, N^2 = omega_T^2 = 1, chi_par = 1/20, chi_perp = 0,
     nu = eta = 1e-4, theta conducted by RKL2 super-time-stepping with dt capped
     at 95 dt_sts (s <= 20 stages), FP32 form."""
     L = 2 * np.pi
     return default_params(incompressible=1, mhd=1, boussinesq=1, stratification=1, strat_direction=2,
-                          anisotropic_diffusion=1, supertimestepping=1, sts_variables=["th"], safety_sts=95,
+                          anisotropic_diffusion=1, supertimestepping=1, sts_variables=["th"], safety_sts=safety_sts,
                           gridsize=(n, n, n), boxsize=(L, L, L), reynolds=1e4, reynolds_magnetic=1e4,
                           reynolds_ani=20.0, N2=1.0, OmegaT2=1.0, cfl=1.5, form=SPK_FORM_FP32,
                           t_final=1e30, toutput_flow=1e30)
@@ -409,13 +409,13 @@ def mti_sigma(k, chi, nu, eta, vA2, N2, OmegaT2):
     return float(np.max(r[np.abs(r.imag) < 1e-12].real))
 
 
-def mti_growth_rates(n, ns=(6, 8, 10, 12), t_end=6.0, t_fit=4.0):
+def mti_growth_rates(n, ns=(8, 10, 12, 16), t_end=7.0, t_fit=5.0, safety_sts=95):
     """Config 3 from its white-noise start to t_end: the slope of
     log|theta(k = m x)| over [t_fit, t_end] for each m in ns, against the
-    dispersion relation."""
+    dispersion relation.  safety_sts caps dt at that many dt_sts."""
     import torch
     import spooky_b200 as S
-    p = mti_params(n)
+    p = mti_params(n, safety_sts)
     ctx = S.Context(p)
     ctx.set_state(mti_state(p))
     buf = torch.empty(ctx.shape_c, dtype=torch.complex128, device="cuda")
@@ -437,7 +437,8 @@ def mti_growth_rates(n, ns=(6, 8, 10, 12), t_end=6.0, t_fit=4.0):
         fit = float(np.polyfit(ts[sel], np.log(amps[sel, i]), 1)[0])
         ana = mti_sigma(float(m), 1.0 / p.reynolds_ani, p.nu, p.nu_m, 1e-6, p.N2, p.OmegaT2)
         out.append({"k": m, "sigma_fit": fit, "sigma_dispersion": ana, "rel_err": abs(fit - ana) / ana})
-    return {"modes": out, "fit_window": [t_fit, float(ts[-1])], "steps": int(len(ts))}
+    return {"modes": out, "fit_window": [t_fit, float(ts[-1])], "steps": int(len(ts)), "dt_cap_dt_sts": safety_sts,
+            "dt_last": float(ts[-1] - ts[-2])}
 
 
 def run_mti(args, world, rank, local_rank):
@@ -458,6 +459,7 @@ def run_mti(args, world, rank, local_rank):
             "mmode_steps_per_s": (1000.0 / ms) * args.n ** 3 / 1e6,
             "kernels_per_step_recorded": kps, "sim_time": t, "energies_finite": bool(np.isfinite(e).all()),
             "growth_rates": mti_growth_rates(args.n),
+            "growth_rates_dt_over_4": mti_growth_rates(args.n, safety_sts=24),
         }), flush=True)
 
 

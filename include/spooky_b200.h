@@ -286,6 +286,30 @@ typedef struct spk_diagnostics {
 } spk_diagnostics_t;
 int spk_diagnostics(spk_ctx* ctx, spk_diagnostics_t* out);
 
+/* Transfer spectra of InputOutput::WriteSpectrumOutput
+ * (src/io/spooky_output_spectrum.cu:186-460): the shell spectrum, as
+ * spk_spectrum computes it, of a state field against a nonlinear term built
+ * as the reference builds it (real-space products, their transform, the
+ * masked wavenumber contraction):
+ *   "advec"          u_i  vs  -i mask k_j (u_i u_j)^      (NonLinearAdvection of u), i = x y z
+ *   "lorentz"        u_i  vs  -i mask k_j (B_i B_j)^      (NonLinearAdvection of B)
+ *   "emfpower"       B_i  vs  i mask (k x (u x B)^)_i    (CurlEMF)
+ *   "helicity"       B_i  vs  (i k x B / k^2)_i          (MagneticHelicity)
+ *   "th_advec"       th   vs  -i mask k.(u th)^          (AdvectTemperature)
+ *   "th_aniso_diss"  th   vs  i mask k.(b (b.grad th) / |b|^2)^   (AnisotropicDissipation, chi = 1)
+ *   "th_aniso_inj"   th   vs  i mask k.(b b_s / |b|^2)^           (AnisotropicInjection)
+ * out: [ncomp][max_bins] (ncomp 3, or 1 for the th terms); totals[ncomp]
+ * (may be NULL): the Parseval sums, i.e. the grid means of field x term --
+ * the time series' dissgradT (with anisotropic conduction and MHD: minus
+ * the th_aniso_diss total) and fluxbbgradT (the th_aniso_inj total).  The
+ * reference accumulates the dissipation term into a scratch array it does
+ * not clear (anisotropic_conduction.cu:157); here the term is the divergence
+ * alone.  SPK_ERR_UNSUPPORTED when the modules do not define the term.  Uses
+ * the pass buffers and the RK scratch; the state is unchanged.
+ * Synchronises the context stream. */
+int spk_transfer_spectra(spk_ctx* ctx, const char* kind, double* out, int max_bins, int* ncomp, int* nbins,
+                         double* deltak, double* totals);
+
 /* Shell spectrum of fields f1, f2 of the context state:
  * InputOutput::computeSpectrum1d / Spectrum1d (src/io/spooky_output_spectrum.cu:424-442,
  * src/cuda/cuda_kernels_generic.cu:441-472).  out[m] (m < min(max_bins, nbins)) is

@@ -284,8 +284,7 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
     const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, N>::TWN * sizeof(C2<T>) +
-                         (size_t)N * sizeof(T) + N + 1024 + 256 + 16;   // ... + row mask + outer mask (<= 1024)
-                                                                        // + box mask (<= 256)
+                         (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
     // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
     long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
     a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
@@ -391,7 +390,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int slots = std::max(1, nthr / RegFft<T, N>::TPC);
     const long nlines = (long)c->nx * c->ny;
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
-    const int gen = z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL) ? 1 : 0);
+    const int gen = z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.shear_part) ? 1 : 0);
     const int max_ctas = gen == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4;   // the kernel's launch bounds
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
@@ -427,7 +426,7 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     if (z.closure) {
         allow_full_smem(k_zpass2<T, N, 2>);
         k_zpass2<T, N, 2><<<nblk, nthr, smem, c->stream>>>(z);
-    } else if (z.derive_gz != 0 || z.mode == ZM_TO_REAL) {
+    } else if (z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.shear_part) {
         allow_full_smem(k_zpass2<T, N, 1>);
         k_zpass2<T, N, 1><<<nblk, nthr, smem, c->stream>>>(z);
     } else {
@@ -490,9 +489,6 @@ static void add_job(spk_ctx* c, AxisArgs& a, const void* in, void* out, int nch,
         while (N % d) d--;
         a.box_rows = d;
     }
-    // trimmed y inverse: 32-row boxes, so that the boxes of masked y rows
-    // (which the x inverse left unwritten) are not loaded at all
-    if (a.trim == 2 && N >= 128 && N % 32 == 0) a.box_rows = 32;
     if (in_state && c->fp32) a.convert = 1;
     a.in_box_ch = in_state ? c->F : buf_channels(c, base);
     if (c->nb > 1 && (base == c->rA || base == c->rB || base == c->user_U)) {
@@ -2299,3 +2295,4 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
 #include "spk_closure_api.cu"
 #include "spk_tune.cu"
 #include "spk_io.cu"
+#include "spk_transfer.cu"

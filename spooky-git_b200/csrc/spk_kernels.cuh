@@ -215,6 +215,9 @@ struct ZArgs {
     int zder_n, zder_src[6];
     const float* cparams;
     float delta2;
+    // diagnostics (general path only): 1 -- the symmetric matrix v_i v_j of
+    // the vector at ch_u, components xx xy xz; 2 -- components yy yz zz
+    int shear_part;
 };
 
 enum XMode { XM_RK0 = 0, XM_RK1 = 1, XM_RK2 = 2, XM_EULER = 3, XM_DFIELD = 4 };

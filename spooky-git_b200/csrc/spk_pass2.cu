@@ -68,11 +68,9 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     T* kax = reinterpret_cast<T*>(tw + F::TWN);                      // wavenumbers along the axis
     unsigned char* keep = reinterpret_cast<unsigned char*>(kax + N);  // row mask factor != 0
     unsigned char* okeep = keep + N;                                  // outer-index mask factor != 0
-    unsigned char* bkeep = okeep + 1024;                              // TMA box holds a kept row
     const int stride = a.axis == 0 ? a.g.ny * a.g.nzs : a.g.nzs;
     constexpr uint32_t tile_bytes = (uint32_t)((size_t)N * KT * in_elem);
-    const int nbox_rows = N / a.box_rows;
-    const uint32_t box_bytes = tile_bytes / (uint32_t)nbox_rows;
+    const uint32_t box_bytes = tile_bytes / (uint32_t)(N / a.box_rows);
 
     // tiles that a trimmed pass skips (uniform: every thread decides alike)
     auto trimmed = [&](int box, int o, int kb) -> bool {
@@ -93,16 +91,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             mbar_expect_tx(&bar[s], 0);
             return;
         }
-        // trimmed y inverse of a box without masked content: the masked rows
-        // were not written by the x inverse and enter as zero, so the TMA
-        // boxes that hold only such rows are not loaded
-        const bool zr = a.trim == 2 && !a.scs[box].masked_live;
-        uint32_t bytes = 0;
-        for (int b = 0; b < nbox_rows; b++)
-            if (!zr || bkeep[b]) bytes += box_bytes;
-        mbar_expect_tx(&bar[s], bytes);
-        for (int b = 0; b < nbox_rows; b++) {
-            if (zr && !bkeep[b]) continue;
+        mbar_expect_tx(&bar[s], tile_bytes);
+        for (int b = 0; b < N / a.box_rows; b++) {
             if (a.axis == 0) tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, o, b * a.box_rows, ch);
             else             tma_load_4d(dst + (size_t)b * box_bytes, &jo.tm, &bar[s], 2 * kb * KT, b * a.box_rows, o, ch);
         }
@@ -123,11 +113,6 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
         }
         const double* og = a.axis == 0 ? a.g.my : a.g.mx;   // mask factor of the outer index
         for (int i = tid; i < nouter; i += blockDim.x) okeep[i] = og[i] != 0.0;
-        for (int b = tid; b < nbox_rows; b += blockDim.x) {
-            bool any = false;
-            for (int n = b * a.box_rows; n < (b + 1) * a.box_rows; n++) any = any || mg[n] != 0.0;
-            bkeep[b] = any;
-        }
     }
     __syncthreads();
     if (tid == 0)
@@ -367,24 +352,10 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     }
     __syncthreads();
     if (tid == 0) {
-        // a trimmed pass of a box without masked content reads only the
-        // columns kz < kz_keep of each line (the others enter as zero): one
-        // copy per line and channel of an even number of columns (16-byte
-        // multiples), instead of one copy of whole rows per channel
-        const int kcp = (a.trim && !bsc->masked_live) ? min(nzs, (a.g.kz_keep + 1) & ~1) : nzs;
-        if (kcp < nzs) {
-            const uint32_t bytes = (uint32_t)((size_t)kcp * sizeof(C2<T>));
-            mbar_expect_tx(bar, bytes * (uint32_t)(nin * nl));
-            for (int ch = 0; ch < nin; ch++)
-                for (int l = 0; l < nl; l++)
-                    bulk_load(raw + ((size_t)ch * L + l) * nzs, in + (size_t)ch * a.cs_in + (size_t)(line0 + l) * nzs,
-                              bytes, bar);
-        } else {
-            const uint32_t bytes = (uint32_t)((size_t)nl * nzs * sizeof(C2<T>));
-            mbar_expect_tx(bar, bytes * (uint32_t)nin);
-            for (int ch = 0; ch < nin; ch++)
-                bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
-        }
+        const uint32_t bytes = (uint32_t)((size_t)nl * nzs * sizeof(C2<T>));
+        mbar_expect_tx(bar, bytes * (uint32_t)nin);
+        for (int ch = 0; ch < nin; ch++)
+            bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
     }
     regfft_fill_twiddles<T, N>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
     for (int i = tid; i < nzs; i += nthr) zrow[i] = mk<T>((T)0, (T)0);
@@ -547,6 +518,11 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
                     mu[6] = fmax(mu[6], (T)vn);
                     mu[7] = fmax(mu[7], (T)(a.mhd ? ve : 0.f));
                 }
+            }
+            if constexpr (GEN == 1) {
+                // ShearMatrix (cuda_kernels.cu:59-77) of the transfer spectra
+                if (a.shear_part == 1) { put(0, ux * ux); put(1, ux * uy); put(2, ux * uz); qc = 3; }
+                if (a.shear_part == 2) { put(0, uy * uy); put(1, uy * uz); put(2, uz * uz); qc = 3; }
             }
             if (a.mode == ZM_PRODUCTS) {
                 if (a.hydro) {

@@ -43,7 +43,7 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_rk3_fields", "spk_rkl_cycle_fields", "spk_get_state_real", "spk_set_state_real",
             "spk_write_snapshot", "spk_read_snapshot", "spk_h5_write", "spk_h5_read", "spk_diagnostics",
             "spk_cfg_lookup_int", "spk_cfg_lookup_bool", "spk_cfg_lookup_float", "spk_cfg_lookup_string",
-            "spk_cfg_setting_length"]
+            "spk_cfg_setting_length", "spk_transfer_spectra"]
 
 DIAGNOSTICS = ("w2", "hv", "j2", "hm", "hc", "thetaB", "bz2", "phiB", "dissgradT", "pv")
 
@@ -142,6 +142,7 @@ def lib():
         L.spk_cfg_lookup_float.argtypes = [ctypes.c_char_p, ctypes.c_char_p, dp]
         L.spk_cfg_lookup_string.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sp]
         L.spk_cfg_setting_length.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.spk_transfer_spectra.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_int, ip, ip, dp, dp]
         L.spk_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ip, dp, dp]
         L.spk_ensemble_autotune.argtypes = [vp, ctypes.c_int]
         L.spk_last_error.restype = ctypes.c_char_p
@@ -381,6 +382,20 @@ class Context:
         self._check(lib().spk_rkl_cycle_fields(self._h, U.data_ptr(), ctypes.byref(s)))
         self.synchronize()
         return s.value
+
+    def transfer_spectra(self, kind):
+        """(spectra [ncomp, nbins], deltak, totals [ncomp]) of a transfer
+        term (spk_transfer_spectra): "advec", "lorentz", "emfpower",
+        "helicity", "th_advec", "th_aniso_diss" or "th_aniso_inj"."""
+        maxb = 4096
+        out = np.zeros((3, maxb))
+        tot = np.zeros(3)
+        nc_, nb, dk = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(lib().spk_transfer_spectra(self._h, kind.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               maxb, ctypes.byref(nc_), ctypes.byref(nb), ctypes.byref(dk),
+                                               tot.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        n = min(nb.value, maxb)
+        return out[: nc_.value, :n].copy(), dk.value, tot[: nc_.value].copy()
 
     def diagnostics(self):
         """{name: value} of the time-series quantities of spk_diagnostics

@@ -7,10 +7,11 @@ t, the energies (ev, Kx, Ky, Kz, em, Mx, My, Mz, et -- computeEnergy through
 spk_budgets) and the two-field correlations (vxvy ... thvz --
 twoFieldCorrelation through the Parseval sum of spk_spectrum), and the
 enstrophies, helicities, field-direction means, thermal dissipation and
-potential vorticity of spk_diagnostics.  The field-aligned conduction terms
+potential vorticity of spk_diagnostics, the field-aligned conduction terms
 (dissgradT with anisotropic conduction and MHD, fluxbbgradT) and the
-transfer spectra are written as -1, the reference's value for a quantity it
-does not compute."""
+transfer spectra of spk_transfer_spectra.  A name the modules do not define
+is written as -1 (time series) or skipped (spectra), as the reference
+does."""
 
 # spectrum names -> field pairs (spooky_output_spectrum.cu:53-186)
 SPECTRA = {"Kx": ("vx", "vx"), "Ky": ("vy", "vy"), "Kz": ("vz", "vz"),
@@ -44,14 +45,36 @@ def write_spectrum_header(path, ctx, names):
         f.write("wavevector \t" + "".join(_fmt(i * dk) + "\t" for i in range(len(E))) + "\n")
 
 
+# transfer spectra: name -> (kind of spk_transfer_spectra, component)
+TRANSFER = {f"{k}_{c}": (k, i) for k in ("advec", "emfpower", "lorentz", "helicity") for i, c in enumerate("xyz")}
+TRANSFER.update({"th_advec": ("th_advec", 0), "th_aniso_diss": ("th_aniso_diss", 0),
+                 "th_aniso_inj": ("th_aniso_inj", 0)})
+
+
 def write_spectrum(path, ctx, t, names):
-    """One line per name: t, the name, the shell values (writeSpectrumHelper)."""
+    """One line per name: t, the name, the shell values (writeSpectrumHelper).
+    Names the modules do not define are skipped, as the reference skips them."""
+    from . import SpookyError
+    cache = {}
     with open(path, "a") as f:
         for name in names:
             pair = SPECTRA.get(name)
-            if pair is None or pair[0] not in ctx.var_list or pair[1] not in ctx.var_list:
+            if pair is not None:
+                if pair[0] not in ctx.var_list or pair[1] not in ctx.var_list:
+                    continue
+                E, _, _ = ctx.spectrum(pair[0], pair[1])
+            elif name in TRANSFER:
+                kind, comp = TRANSFER[name]
+                if kind not in cache:
+                    try:
+                        cache[kind] = ctx.transfer_spectra(kind)[0]
+                    except SpookyError:
+                        cache[kind] = None
+                if cache[kind] is None:
+                    continue
+                E = cache[kind][comp]
+            else:
                 continue
-            E, _, _ = ctx.spectrum(pair[0], pair[1])
             f.write("t\t" + _fmt(t) + "\t" + name + "\t" + "".join(_fmt(v) + "\t" for v in E) + "\n")
 
 
@@ -78,6 +101,11 @@ def timevar_values(ctx, names):
             if diag is None:
                 diag = ctx.diagnostics()
             v = diag[name]
+            if name == "dissgradT" and v == -1.0 and ctx.params.anisotropic_diffusion and ctx.params.mhd:
+                # computeAnisoDissipation, with the reference's sign (spooky_output_timevar.cu:171-180)
+                v = -float(ctx.transfer_spectra("th_aniso_diss")[2][0])
+        elif name == "fluxbbgradT" and ctx.params.anisotropic_diffusion and ctx.params.boussinesq and ctx.params.mhd:
+            v = float(ctx.transfer_spectra("th_aniso_inj")[2][0])
         out.append(v)
     return out
 
