@@ -252,7 +252,7 @@ struct AxisCfg { int kt; int nthr; size_t smem; };
 // the FP32 form is half as wide).
 static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     AxisCfg a;
-    const RegFftGeom g = regfft_geom(N, c->fp32, axis_lr(c->fp32, N, c->fp32 && state_in));
+    const RegFftGeom g = regfft_geom(N, c->fp32);
     const int full = std::min(64, 256 / g.TPC);
     const int cols = std::max(pow2_ceil(N / 2 + 1), 32 / g.TPC);   // short axes: a cubic box's kz columns
     int kt = (N < 64 && cols < full) ? cols : full;
@@ -278,19 +278,16 @@ template <typename K> static void allow_full_smem(K* kernel) {
 template <typename T, int N, int DIR, bool CONV, bool DEF = false>
 static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     constexpr int KT = axis_kt<T, N, CONV>();
-    using AF = RegFft<T, N, axis_lr<T, N, CONV>()>;
-    constexpr int MINB = axis_minb<T, N, CONV>();
-    const int nthr = KT * AF::TPC;
+    const int nthr = KT * RegFft<T, N>::TPC;
     if (a.kt != KT) { c->err = "internal: axis tile width mismatch"; c->sticky = SPK_ERR_ARG; return; }
     const size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
-    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)AF::TWN * sizeof(C2<T>) +
+    const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, N>::TWN * sizeof(C2<T>) +
                          (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
-    // stages: as many as keep MINB CTAs per SM (the registers' budget), 1..4
-    // (at least 2 with two CTAs per SM)
-    long nst = ((long)(MINB == 2 ? 113 * 1024 : 227 * 1024 / MINB - 1024) - (long)fixed) / (long)stage;
-    a.nst = (int)std::max<long>(MINB == 2 ? 2 : 1, std::min<long>(4, nst));
+    // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
+    long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
+    a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
     if (nthr < 256) {
         // narrow tiles (128 threads): 4 CTAs per SM with fewer stages each keep
         // as many loads in flight as 2 CTAs with more, with twice the warps

@@ -24,23 +24,9 @@ namespace spk {
 // box, N/2 + 1 rounded up to a power of two, and at least one warp per CTA:
 // a 64-column tile on a 16^3 box would transform 55 columns of padding.
 __host__ __device__ constexpr int pow2_ceil(int n) { return n <= 1 ? 1 : 2 * pow2_ceil((n + 1) / 2); }
-// Radix of the strided-axis transforms: the FP32 passes over pass buffers
-// (not the FP64 state) at power-of-two lengths from 64 up use radix 8 (8
-// elements per thread, as FP64 does), so that a CTA's threads need fewer
-// registers and more warps fit per SM; the z pass keeps radix 16.
-__host__ __device__ constexpr int axis_lr(bool fp32, int n, bool conv) {
-    return (fp32 && !conv && n >= 64 && is_pow2c(n)) ? 3 : (fp32 ? 4 : 3);
-}
-template <typename T, int N, bool CONV> __host__ __device__ constexpr int axis_lr() {
-    return axis_lr(sizeof(T) == 4, N, CONV);
-}
-// resident CTAs per SM the axis kernel's registers are budgeted for
-template <typename T, int N, bool CONV> __host__ __device__ constexpr int axis_minb() {
-    return (sizeof(T) == 4 && axis_lr<T, N, CONV>() == 3) ? 3 : 2;
-}
 template <typename T, int N, bool CONV>
 __host__ __device__ constexpr int axis_kt() {
-    constexpr int tpc = RegFft<T, N, axis_lr<T, N, CONV>()>::TPC;
+    constexpr int tpc = RegFft<T, N>::TPC;
     constexpr int full = (256 / tpc) > 64 ? 64 : (256 / tpc);
     constexpr int cols = pow2_ceil(N / 2 + 1) > 32 / tpc ? pow2_ceil(N / 2 + 1) : 32 / tpc;
     constexpr int kt = (N < 64 && cols < full) ? cols : full;
@@ -50,9 +36,8 @@ __host__ __device__ constexpr int axis_kt() {
 // DEF: the x inverse of RK3 stage 1 or 2 with deferred masked modes (its own
 // instantiation, so that the other passes keep their registers).
 template <typename T, int N, int DIR, bool CONV, bool DEF>
-__global__ void __launch_bounds__(256, axis_minb<T, N, CONV>()) k_axis2(const __grid_constant__ AxisArgs a) {
-    constexpr int LR = axis_lr<T, N, CONV>();
-    using F = RegFft<T, N, LR>;
+__global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
+    using F = RegFft<T, N>;
     constexpr int KT = axis_kt<T, N, CONV>(), LKT = ilog2c(KT);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
@@ -121,7 +106,7 @@ __global__ void __launch_bounds__(256, axis_minb<T, N, CONV>()) k_axis2(const __
         const C2<T>* twg = (const C2<T>*)a.plan.tw;
         const double* kg = a.axis == 0 ? a.g.kx : a.g.ky;
         const double* mg = a.axis == 0 ? a.g.mx : a.g.my;
-        regfft_fill_twiddles<T, N, LR>(tw, twg, tid, blockDim.x);
+        regfft_fill_twiddles<T, N>(tw, twg, tid, blockDim.x);
         for (int i = tid; i < N; i += blockDim.x) {
             kax[i] = (T)kg[i];
             keep[i] = mg[i] != 0.0;
@@ -205,7 +190,7 @@ __global__ void __launch_bounds__(256, axis_minb<T, N, CONV>()) k_axis2(const __
         } else if constexpr (CONV) {
             const double2* src = reinterpret_cast<const double2*>(stg);
             const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
-            regfft_load<T, N, DIR, LR>(r, q, [&](int n) -> C2<T> {
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 double2 x = src[n * KT + c];
                 if (deriv) x = ik_mul(deriv == 1 ? kd[n] : (deriv == 2 ? kout : kcol), x);
                 if (jo.hp && !(kd[n] * kd[n] + kout * kout + kcol * kcol > a.hp_k2)) x = make_double2(0.0, 0.0);
@@ -217,7 +202,7 @@ __global__ void __launch_bounds__(256, axis_minb<T, N, CONV>()) k_axis2(const __
         } else {
             const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
             const T sc = (T)scale;
-            regfft_load<T, N, DIR, LR>(r, q, [&](int n) -> C2<T> {
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 C2<T> v = src[n * KT + c];
                 if (zrows && !keep[n]) v = mk<T>((T)0, (T)0);
                 if constexpr (DEF)
@@ -244,7 +229,7 @@ __global__ void __launch_bounds__(256, axis_minb<T, N, CONV>()) k_axis2(const __
         const bool col_ok = c < kt;
         const bool filt = a.row_filter != 0;
         if (skip) continue;
-        regfft_run<T, N, DIR, false, LR>(
+        regfft_run<T, N, DIR>(
             r, q, tw, [&](int L) { return xbuf + (size_t)L * KT + c; },
             [&](int k, C2<T> v) {
                 if (col_ok && (!filt || keep[k])) out[k * stride + c] = v;

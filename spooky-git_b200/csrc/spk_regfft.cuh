@@ -36,14 +36,11 @@ __host__ __device__ constexpr bool regfft_length_ok(int n) {
     return n >= 2 && n <= 1024 && (is_pow2c(n) || (n >= 6 && n % 3 == 0 && is_pow2c(n / 3)));
 }
 
-// The full radix of power-of-two lengths: 16 in FP32, 8 in FP64 (log2).
-template <typename T> __host__ __device__ constexpr int regfft_lr() { return sizeof(T) == 4 ? 4 : 3; }
-
-template <typename T, int N, int LR = regfft_lr<T>()>
+template <typename T, int N>
 struct RegFft {
     static_assert(regfft_length_ok(N), "transform length must be 2^k (2..1024) or 3*2^k (6..768)");
     static constexpr bool P2 = is_pow2c(N);
-    static constexpr int LRF = LR;                                    // log2 of the full radix
+    static constexpr int LRF = sizeof(T) == 4 ? 4 : 3;                 // full radix 16 (FP32) / 8 (FP64)
     static constexpr int LN2 = P2 ? ilog2c(N) : ilog2c(N / 3);         // the power-of-two part
     static constexpr int E = P2 ? (LN2 < LRF ? N : (1 << LRF)) : (N < 12 ? N : 12);
     static constexpr int TPC = N / E;                                 // threads per transform
@@ -81,9 +78,9 @@ template <typename T, int R, int DIR> __device__ __forceinline__ void dft_r(C2<T
 }
 
 // Fill the per-stage twiddle tables from the table W_N^j (all threads call).
-template <typename T, int N, int LR = regfft_lr<T>()>
+template <typename T, int N>
 __device__ __forceinline__ void regfft_fill_twiddles(C2<T>* tws, const C2<T>* twg, int tid, int nthr) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     for (int i = tid; i < F::TWN; i += nthr) {
         int h = 1, pp = 1, tb = 0;
 #pragma unroll
@@ -105,9 +102,9 @@ template <typename T, int DIR> __device__ __forceinline__ C2<T> twd(const C2<T>*
 // Run stage S (butterflies of this thread, q = sub-index within the
 // transform) on registers a[E] whose legs are already loaded; apply the
 // twiddles from the per-stage tables.  Leg t of butterfly u ends in a[u*R + t].
-template <typename T, int N, int DIR, int S, int LR>
+template <typename T, int N, int DIR, int S>
 __device__ __forceinline__ void regfft_stage_math(C2<T>* a, int q, const C2<T>* tw) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     constexpr int R = F::radix(S), H = F::H(S);
     constexpr int BPT = F::E / R;
 #pragma unroll
@@ -125,9 +122,9 @@ __device__ __forceinline__ void regfft_stage_math(C2<T>* a, int q, const C2<T>* 
 
 // Element index (in the linear exchange layout g*M + position) of leg r of
 // butterfly u at stage S.
-template <typename T, int N, int S, int LR>
+template <typename T, int N, int S>
 __device__ __forceinline__ int regfft_in_index(int q, int u, int r) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     constexpr int H = F::H(S), M = F::M(S);
     const unsigned beta = (unsigned)q + (unsigned)(u * F::TPC);
     const int m = (int)(beta % (unsigned)H), g = (int)(beta / (unsigned)H);
@@ -135,9 +132,9 @@ __device__ __forceinline__ int regfft_in_index(int q, int u, int r) {
 }
 // Linear exchange index where output t of butterfly u of stage S goes
 // (element m of group g + P t, in a layout of groups of length H).
-template <typename T, int N, int S, int LR>
+template <typename T, int N, int S>
 __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     constexpr int H = F::H(S), P = F::P(S);
     const unsigned beta = (unsigned)q + (unsigned)(u * F::TPC);
     const int m = (int)(beta % (unsigned)H), g = (int)(beta / (unsigned)H);
@@ -152,9 +149,9 @@ __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
 // act = false: a thread with no transform to run (it must be false for a
 // whole warp at a time) only takes part in the barriers, which stay at the
 // same instructions for every warp of the CTA.
-template <typename T, int N, int DIR, int S, int LR, typename XA>
+template <typename T, int N, int DIR, int S, typename XA>
 __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool act = true) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     constexpr int R = F::radix(S);
     constexpr int BPT = F::E / R;
     __syncthreads();   // earlier readers of the exchange buffer are done
@@ -162,7 +159,7 @@ __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool 
 #pragma unroll
         for (int u = 0; u < BPT; u++)
 #pragma unroll
-            for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S, LR>(q, u, t)) = a[u * R + t];
+            for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
     }
     __syncthreads();
     constexpr int R1 = F::radix(S + 1);
@@ -171,20 +168,20 @@ __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool 
 #pragma unroll
         for (int u = 0; u < BPT1; u++)
 #pragma unroll
-            for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1, LR>(q, u, r));
+            for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1>(q, u, r));
     }
 }
 
 // FS: barrier before the last stage's stores (when store() writes into the
 // exchange buffer that the last exchange just read).  act: as for
 // regfft_exchange (no math, no stores, the same barriers).
-template <typename T, int N, int DIR, int S, bool FS, int LR, typename XA, typename ST>
+template <typename T, int N, int DIR, int S, bool FS, typename XA, typename ST>
 __device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
-    using F = RegFft<T, N, LR>;
-    if (act) regfft_stage_math<T, N, DIR, S, LR>(a, q, tw);
+    using F = RegFft<T, N>;
+    if (act) regfft_stage_math<T, N, DIR, S>(a, q, tw);
     if constexpr (S + 1 < F::NS) {
-        regfft_exchange<T, N, DIR, S, LR>(a, q, xaddr, act);
-        regfft_from<T, N, DIR, S + 1, FS, LR>(a, q, tw, xaddr, store, act);
+        regfft_exchange<T, N, DIR, S>(a, q, xaddr, act);
+        regfft_from<T, N, DIR, S + 1, FS>(a, q, tw, xaddr, store, act);
     } else {
         if constexpr (FS && S > 0) __syncthreads();
         constexpr int R = F::radix(S), P = F::P(S);
@@ -200,28 +197,28 @@ __device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA
 }
 
 // Load the first-stage legs through load(n).
-template <typename T, int N, int DIR, int LR = regfft_lr<T>(), typename LD>
+template <typename T, int N, int DIR, typename LD>
 __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
-    using F = RegFft<T, N, LR>;
+    using F = RegFft<T, N>;
     constexpr int R = F::radix(0);
     constexpr int BPT = F::E / R;
 #pragma unroll
     for (int u = 0; u < BPT; u++)
 #pragma unroll
-        for (int r = 0; r < R; r++) a[u * R + r] = load(regfft_in_index<T, N, 0, LR>(q, u, r));
+        for (int r = 0; r < R; r++) a[u * R + r] = load(regfft_in_index<T, N, 0>(q, u, r));
 }
 
-template <typename T, int N, int DIR, bool FS = false, int LR = regfft_lr<T>(), typename XA, typename ST>
+template <typename T, int N, int DIR, bool FS = false, typename XA, typename ST>
 __device__ __forceinline__ void regfft_run(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
-    regfft_from<T, N, DIR, 0, FS, LR>(a, q, tw, xaddr, store, act);
+    regfft_from<T, N, DIR, 0, FS>(a, q, tw, xaddr, store, act);
 }
 
 // Host mirror of the geometry.
 struct RegFftGeom { int E, TPC; };
-inline RegFftGeom regfft_geom(int n, bool fp32, int lr = 0) {
+inline RegFftGeom regfft_geom(int n, bool fp32) {
     RegFftGeom g;
     if (is_pow2c(n)) {
-        const int lrf = lr > 0 ? lr : (fp32 ? 4 : 3), ln = ilog2c(n);
+        const int lrf = fp32 ? 4 : 3, ln = ilog2c(n);
         g.E = ln < lrf ? n : (1 << lrf);
     } else {
         g.E = n < 12 ? n : 12;

@@ -181,7 +181,7 @@ def test_mti256_growth_rates_match_the_dispersion_relation():
     root; the two other roots of these modes decay at rates above 1.2, so
     their share has fallen below 1e-4 by t = 5.  At the configuration's dt
     (95 dt_sts, 0.088) the time discretisation -- RKL2 super-time-stepping
-    of the conduction around the RK3 step -- lowers the rates by 0.6-2%,
+    of the conduction around the RK3 step -- lowers the rates by 1-4%,
     growing with chi k^2 dt; with dt four times smaller it falls at least
     threefold, below 1%: the rates converge to the dispersion relation."""
     import sys
@@ -191,5 +191,5 @@ def test_mti256_growth_rates_match_the_dispersion_relation():
     r4 = mti_growth_rates(256, safety_sts=24)
     assert r["steps"] >= 40 and r4["steps"] >= 4 * r["steps"] - 8
     for m, m4 in zip(r["modes"], r4["modes"]):
-        assert m["rel_err"] < 0.03, m
+        assert m["rel_err"] < 0.05, m
         assert m4["rel_err"] < 0.01 and m4["rel_err"] < m["rel_err"] / 3, (m, m4)
