@@ -468,7 +468,11 @@ def run_closure(args, world, rank, local_rank):
     2e-4, config-2 fields) in the plain form, closure samples every 250
     steps, GPU training, and 64^3 runs with and without the closure to the
     truth's final time; one JSON line with the spectral errors against the
-    filtered truth and the costs."""
+    filtered truth and the costs.  The default trains both networks on the
+    same samples: the line's value is the tensor network's (variant 3, the
+    configuration's 18 -> 64 -> 64 -> 64 -> 12 BF16 network), the
+    eddy-coefficient network (variant 1) is reported beside it under
+    "models"."""
     import torch
     from spooky_b200 import closure as C
     torch.cuda.set_device(local_rank)
@@ -477,19 +481,37 @@ def run_closure(args, world, rank, local_rank):
     nf, ncs = args.n, args.n // 4
     # weight of the energy-transfer error in the loss (None: the workflow's
     # per-variant default)
-    transfer = args.closure_transfer if args.closure_transfer is not None else {1: 0.0, 2: 4.0}[args.closure_variant]
+    transfer = (args.closure_transfer if args.closure_transfer is not None
+                else C.TRANSFER_DEFAULT[args.closure_variant])
+    extra = (1,) if args.closure_variant == 3 else ()
     r = C.run(n_fine=nf, n_coarse=ncs, steps=args.closure_steps, snap_every=max(args.closure_steps // 8, 1),
               train_steps=3000, batch=16384, lr=2e-3, variant=args.closure_variant, transfer=transfer,
-              log=lambda m: print(m, file=sys.stderr, flush=True))
+              extra_variants=extra, log=lambda m: print(m, file=sys.stderr, flush=True))
+    names = {1: "eddy-coefficient network, full field (8 invariants -> 32 -> 32 -> 2, FP32)",
+             2: "eddy-coefficient network, small scales (8 invariants -> 32 -> 32 -> 2, FP32)",
+             3: "tensor network (18 gradients -> 64 -> 64 -> 64 -> 12, BF16 tensor cores)"}
+    models = {names[args.closure_variant]: {
+        "error": r["error_closure"], "error_u": r["error_u_closure"], "error_b": r["error_b_closure"],
+        "energy": r["energy_closure"], "run_seconds": r["seconds_closure"], "cost_advantage": r["cost_advantage"],
+        "train_seconds": r["train_seconds"], "loss": {"initial": r["loss_initial"], "final": r["loss_final"]}}}
+    for v in extra:
+        d = r[f"v{v}"]
+        models[names[v]] = {"error": d["error"], "error_u": d["error_u"], "error_b": d["error_b"],
+                            "energy": d["energy"], "run_seconds": d["seconds"], "cost_advantage": d["cost_advantage"],
+                            "train_seconds": d["train_seconds"], "finite": d["finite"],
+                            "loss": {"initial": d["loss_initial"], "final": d["loss_final"]}}
     print(json.dumps({
         "metric": f"{ncs}^3 learned-closure run vs filtered {nf}^3 truth: RMS relative shell-spectrum error",
         "value": r["error_closure"], "unit": "relative error (shells 1..k_c)", "higher_is_better": False,
-        "n_gpus": 1, "vs_baseline": None, "dtype": "fp64 state, fp32 MLP", "data": "synthetic (seeded config-2 fields)",
+        "n_gpus": 1, "vs_baseline": None,
+        "dtype": "fp64 state, " + ("bf16 MLP operands, fp32 accumulation" if args.closure_variant == 3 else "fp32 MLP"),
+        "data": "synthetic (seeded config-2 fields)",
         "config": {"workload": f"MHD {nf}^3 truth (plain form, {args.closure_steps} steps, nu = eta = 2e-4) -> "
                                f"{ncs}^3 closure run, sharp filter k_c = {r['k_cut']}",
                    "train_steps": 3000, "batch": 16384,
-                   "closure_variant": {1: "full-field model", 2: "small-scale model"}[args.closure_variant],
+                   "closure_variant": names[args.closure_variant],
                    "loss_transfer_weight": transfer},
+        "models": models,
         "error_without_closure": r["error_plain"],
         "error_u": {"closure": r["error_u_closure"], "plain": r["error_u_plain"]},
         "error_b": {"closure": r["error_b_closure"], "plain": r["error_b_plain"]},
@@ -497,8 +519,10 @@ def run_closure(args, world, rank, local_rank):
         "t_end": r["t_end"], "truth_seconds": r["truth_seconds"], "closure_run_seconds": r["seconds_closure"],
         "plain_coarse_run_seconds": r["seconds_plain"], "cost_advantage": r["cost_advantage"],
         "train_seconds": r["train_seconds"], "loss": {"initial": r["loss_initial"], "final": r["loss_final"]},
-        "shell_spectra": {k: [float("%.5g" % v) for v in r["spectrum_" + k][: r["k_cut"] + 1]]
-                          for k in ("truth", "closure", "plain")},
+        "shell_spectra": dict({k: [float("%.5g" % v) for v in r["spectrum_" + k][: r["k_cut"] + 1]]
+                               for k in ("truth", "closure", "plain")},
+                              **{f"variant{v}": [float("%.5g" % x) for x in r[f"v{v}"]["spectrum"][: r["k_cut"] + 1]]
+                                 for v in extra}),
     }), flush=True)
 
 
@@ -520,9 +544,11 @@ def main():
     ap.add_argument("--closure", action="store_true",
                     help="learned-closure workload instead: --n truth, --n/4 closure run (config 5)")
     ap.add_argument("--closure-steps", type=int, default=2000)
-    ap.add_argument("--closure-variant", type=int, default=1, choices=[1, 2])
+    ap.add_argument("--closure-variant", type=int, default=3, choices=[1, 2, 3],
+                    help="3 (default): the tensor network, with variant 1 trained and run beside it")
     ap.add_argument("--closure-transfer", type=float, default=None,
-                    help="weight of the energy-transfer error in the closure loss (default: 0 variant 1, 4 variant 2)")
+                    help="weight of the energy-transfer error in the closure loss (default: 0 variant 1, "
+                         "4 variant 2, 1 variant 3)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")

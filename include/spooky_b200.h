@@ -92,7 +92,7 @@ typedef struct spk_params {
     int    integrator;      /* SPK_INT_RK3 or SPK_INT_EULER                                        */
     int    sts_every_step;  /* 1: RKL cycle after the integrator on every step (the STS test build) */
     int    form;            /* SPK_FORM_PLAIN or SPK_FORM_FP32                                     */
-    int    closure;         /* 1 or 2: reserve the learned closure's gradient channels for that
+    int    closure;         /* 1, 2 or 3: reserve the learned closure's gradient channels for that
                                variant (HD/MHD; weights from spk_closure_set)                      */
     double closure_kc_frac; /* variant 2: the small scales are |k| > closure_kc_frac * k_c
                                (0: 1/2)                                                            */
@@ -451,6 +451,42 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
 #define SPK_CLOSURE_ROW_SF     25
 #define SPK_CLOSURE_ROW_JF     30
 
+/* Variant 3 (spk_params_t.closure = 3), the tensor network: the 18 raw
+ * gradients of the whole resolved field, made dimensionless,
+ *   x = (A[0..8], G[0..8]) / n                       (n as above; HD: G = 0),
+ *   h1 = tanh(W1 x + b1), h2 = tanh(W2 h1 + b2), h3 = tanh(W3 h2 + b3),
+ *   o = W4 h3 + b4                                   (18 -> 64 -> 64 -> 64 -> 12),
+ * in BF16 on the tensor cores: the weights and every layer input (x, h1,
+ * h2, h3) are rounded to BF16 (nearest even), the products summed in FP32
+ * onto the FP32 bias; tanh in FP32.  With s = Delta^2 n^2 o, s[0..5] is a
+ * symmetric stress (xx xy xz yy yz zz) whose traceless part
+ *   dT = (s0 - tr/3, s1, s2, s3 - tr/3, s4),   tr = s0 + s3 + s5,
+ * is added to the Basdevant stress, and s[6..11] are the off-diagonal
+ * entries M_xy M_xz M_yx M_yz M_zx M_zy of an induction tensor whose
+ * antisymmetric part is added to the EMF (MHD):
+ *   dE = ((M_yz - M_zy)/2, (M_zx - M_xz)/2, (M_xy - M_yx)/2).
+ * In the RHS both are multiplied by the backscatter ramp
+ *   r = clamp(P / (0.1 Pm + 1e-30), 0, 1),  P = -dT:S - dE.J,
+ *   Pm = |dT|_F |S|_F + |dE| |J|
+ * (S, J the point's own strain and current; |.|_F over the full 3x3
+ * tensors, zz = -(xx + yy) for dT), so that the terms only take energy from
+ * the resolved scales; the dt rule adds the largest |r dT|_F / (2 n) and
+ * (MHD) |r dE| / n to the parabolic rates.  Parameters are floats in the
+ * order W1[64][18] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[12][64]
+ * b4[12]; the context and the trainer round the weights to BF16 on upload
+ * (the trainer keeps FP32 masters for Adam).  Its samples carry 18 more
+ * rows, the raw gradients A (SPK_CLOSURE_ROW_A) and G (SPK_CLOSURE_ROW_G);
+ * the loss is the one above with dT, dE of this model (no ramp) and its
+ * gradient is taken through the BF16 roundings as if they were absent
+ * (straight-through). */
+#define SPK_CLOSURE3_NIN     18
+#define SPK_CLOSURE3_HIDDEN  64
+#define SPK_CLOSURE3_NOUT    12
+#define SPK_CLOSURE3_NPARAM  (64 * 18 + 64 + 2 * (64 * 64 + 64) + 12 * 64 + 12)
+#define SPK_CLOSURE3_ROWS    51
+#define SPK_CLOSURE_ROW_A      33
+#define SPK_CLOSURE_ROW_G      42
+
 /* Variants (spk_params_t.closure): 1 -- the gradients of the whole
  * resolved field; 2 -- the gradients of its small scales only, the modes with
  * |k| > f k_c (k_c the smallest dealiased cut-off, f =
@@ -459,9 +495,10 @@ int spk_ensemble_kernels_per_step(const spk_ensemble* ens, int* kernels);
  * mainly near the cut-off (a variational-multiscale form).  The samples of a
  * coarse context follow its variant. */
 
-/* Switch the closure on (params: SPK_CLOSURE_NPARAM host floats) or off
- * (params NULL) for the context's RHS, steps and dt rule.  HD and MHD
- * contexts; the next step re-records the step graph. */
+/* Switch the closure on (params: spk_closure_nparam(variant) host floats,
+ * the context's variant) or off (params NULL) for the context's RHS, steps
+ * and dt rule.  HD and MHD contexts; the next step re-records the step
+ * graph. */
 int spk_closure_set(spk_ctx* ctx, const float* params);
 
 /* The spectral products of U before their divergence / curl: the Basdevant
@@ -493,10 +530,16 @@ int spk_closure_samples(spk_ctx* fine, const double* Uf, spk_ctx* coarse, float*
  * takes samples (a * (i*batch + r) + c) mod n, r < batch, for an a coprime
  * with n: each pass over n samples visits every sample once. */
 typedef struct spk_trainer spk_trainer;
-int spk_trainer_create(void* cuda_stream, spk_trainer** out);
+int spk_trainer_create(void* cuda_stream, spk_trainer** out);                 /* variants 1, 2 */
+/* A trainer for the network of a variant (1 and 2: the eddy-coefficient
+ * network; 3: the tensor network, whose samples have SPK_CLOSURE3_ROWS rows). */
+int spk_trainer_create_variant(void* cuda_stream, int variant, spk_trainer** out);
+/* Parameters and sample rows of a variant's network (0 for another value). */
+int spk_closure_nparam(int variant);
+int spk_closure_rows(int variant);
 int spk_trainer_destroy(spk_trainer* tr);
 int spk_trainer_set_params(spk_trainer* tr, const float* params);        /* host floats; resets Adam */
-int spk_trainer_get_params(spk_trainer* tr, float* params);              /* host floats */
+int spk_trainer_get_params(spk_trainer* tr, float* params);              /* host floats (FP32 masters) */
 int spk_trainer_set_samples(spk_trainer* tr, const float* samples, size_t n, size_t stride, const float w[3]);
 /* Full-batch mean loss and gradient at the current parameters (host outputs). */
 int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad);

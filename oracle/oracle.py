@@ -53,6 +53,12 @@ def lib():
         L.orc_closure_mlp.argtypes = [dp, dp, dp]
         L.orc_closure_loss_grad.argtypes = [dp, ctypes.c_size_t, ctypes.c_size_t, dp, dp, dp, dp]
         L.orc_closure_adam.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_double]
+        L.orc_closure_adam_n.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.orc_closure3_set_rounding.argtypes = [ctypes.c_int]
+        L.orc_closure3_mlp.argtypes = [dp, dp, dp]
+        L.orc_closure3_terms.argtypes = [dp, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp, dp, dp]
+        L.orc_closure3_terms.restype = ctypes.c_double
+        L.orc_closure3_loss_grad.argtypes = [dp, ctypes.c_size_t, ctypes.c_size_t, dp, dp, dp, dp]
         _LIB = L
     return _LIB
 
@@ -75,6 +81,9 @@ def set_threads(n):
 # ---- learned closure (include/spooky_b200.h, SPK_CLOSURE_*) ----------------
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
 CLOSURE_ROWS = 33
+# variant 3, the tensor network (SPK_CLOSURE3_*)
+CLOSURE3_NPARAM = 64 * 18 + 64 + 2 * (64 * 64 + 64) + 12 * 64 + 12
+CLOSURE3_ROWS = 51
 
 
 def closure_features(A, G):
@@ -107,9 +116,45 @@ def closure_loss_grad(samples, params, w):
 
 
 def closure_adam(params, grad, m, v, t, lr):
-    """In place on float64 arrays params, m, v."""
+    """In place on float64 arrays params, m, v (either network)."""
     grad = np.ascontiguousarray(grad, dtype=np.float64)
-    lib().orc_closure_adam(_dp(params), _dp(grad), _dp(m), _dp(v), int(t), float(lr))
+    lib().orc_closure_adam_n(_dp(params), _dp(grad), _dp(m), _dp(v), int(t), float(lr), int(params.size))
+
+
+def closure3_set_rounding(on):
+    """Variant 3: 0 drops every BF16 rounding of the network (exact FP64)."""
+    lib().orc_closure3_set_rounding(1 if on else 0)
+
+
+def closure3_mlp(params, x):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    o = np.empty(12)
+    lib().orc_closure3_mlp(_dp(params), _dp(x), _dp(o))
+    return o
+
+
+def closure3_terms(params, delta2, A, G, mhd=True):
+    """Variant 3's RHS terms at one point: (tau[5], e[3], nu_eff, eta_eff, n)."""
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    A = np.ascontiguousarray(A, dtype=np.float64).reshape(9)
+    G = np.ascontiguousarray(G, dtype=np.float64).reshape(9)
+    tau, e = np.empty(5), np.empty(3)
+    nu, eta = ctypes.c_double(), ctypes.c_double()
+    n = lib().orc_closure3_terms(_dp(params), float(delta2), _dp(A), _dp(G), 1 if mhd else 0, _dp(tau), _dp(e),
+                                 ctypes.byref(nu), ctypes.byref(eta))
+    return tau, e, nu.value, eta.value, n
+
+
+def closure3_loss_grad(samples, params, w):
+    """samples: [CLOSURE3_ROWS, n]; returns (loss, grad[CLOSURE3_NPARAM])."""
+    X = np.ascontiguousarray(samples, dtype=np.float64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    w = np.zeros(3) + np.pad(np.asarray(w, dtype=np.float64), (0, 3 - len(w)))
+    g = np.empty(CLOSURE3_NPARAM)
+    loss = ctypes.c_double()
+    lib().orc_closure3_loss_grad(_dp(X), X.shape[1], X.shape[1], _dp(params), _dp(w), _dp(g), ctypes.byref(loss))
+    return loss.value, g
 
 
 class Oracle:
@@ -225,11 +270,12 @@ class Oracle:
         return out
 
     def closure_samples(self, U, coarse):
-        """Samples [CLOSURE_ROWS, nx*ny*nz of coarse] from this (fine) state U."""
+        """Samples [CLOSURE_ROWS (variant 3: CLOSURE3_ROWS), nx*ny*nz of
+        coarse] from this (fine) state U."""
         U = np.ascontiguousarray(U, dtype=np.complex128).reshape(self.shape_c)
         q = coarse.params
         n = q.nx * q.ny * q.nz
-        X = np.empty((CLOSURE_ROWS, n))
+        X = np.empty((CLOSURE3_ROWS if q.closure == 3 else CLOSURE_ROWS, n))
         lib().orc_closure_samples(self._h, _dp(U), coarse._h, _dp(X), n)
         return X
 

@@ -9,6 +9,7 @@
 #include "spk_closure.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <string.h>
 
 #include "../include/spooky_b200.h"
@@ -165,6 +166,195 @@ void orc_closure_adam(double* P, const double* g, double* m, double* v, int t, d
     const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
     const double c1 = 1.0 - pow(b1, t), c2 = 1.0 - pow(b2, t);
     for (int p = 0; p < SPK_CLOSURE_NPARAM; p++) {
+        m[p] = b1 * m[p] + (1.0 - b1) * g[p];
+        v[p] = b2 * v[p] + (1.0 - b2) * g[p] * g[p];
+        P[p] -= lr * (m[p] / c1) / (sqrt(v[p] / c2) + eps);
+    }
+}
+
+/* ---- variant 3: the tensor network (include/spooky_b200.h, SPK_CLOSURE3_*).
+ * Every operand the CUDA kernels feed to a BF16 tensor-core product is
+ * rounded here at the same place (weights, layer inputs, back-propagated
+ * errors); sums run in FP64 (the kernels: FP32).  orc_closure3_set_rounding(0)
+ * drops the roundings, which makes the loss smooth in the parameters for a
+ * finite-difference check of the gradient formulas. */
+enum { N3I = SPK_CLOSURE3_NIN, N3H = SPK_CLOSURE3_HIDDEN, N3O = SPK_CLOSURE3_NOUT };
+enum {
+    Q1 = 0, QB1 = Q1 + N3H * N3I, Q2 = QB1 + N3H, QB2 = Q2 + N3H * N3H, Q3 = QB2 + N3H,
+    QB3 = Q3 + N3H * N3H, Q4 = QB3 + N3H, QB4 = Q4 + N3O * N3H, QN = QB4 + N3O
+};
+
+static int g_bf16 = 1;
+void orc_closure3_set_rounding(int on) { g_bf16 = on; }
+
+/* x to FP32, then to BF16 with round-to-nearest-even on the 16 dropped bits */
+static double bf(double x) {
+    if (!g_bf16) return x;
+    float f = (float)x;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) {
+        u += 0x7fffu + ((u >> 16) & 1u);
+        u &= 0xffff0000u;
+    }
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+
+/* the network on x[18]: rounded input xb, rounded activations h1..h3, outputs o[12] */
+static void fwd3(const double* P, const double* x, double* xb, double* h1, double* h2, double* h3, double* o) {
+    for (int i = 0; i < N3I; i++) xb[i] = bf(x[i]);
+    for (int j = 0; j < N3H; j++) {
+        double a = P[QB1 + j];
+        for (int i = 0; i < N3I; i++) a += bf(P[Q1 + j * N3I + i]) * xb[i];
+        h1[j] = bf(tanh(a));
+    }
+    for (int j = 0; j < N3H; j++) {
+        double a = P[QB2 + j];
+        for (int i = 0; i < N3H; i++) a += bf(P[Q2 + j * N3H + i]) * h1[i];
+        h2[j] = bf(tanh(a));
+    }
+    for (int j = 0; j < N3H; j++) {
+        double a = P[QB3 + j];
+        for (int i = 0; i < N3H; i++) a += bf(P[Q3 + j * N3H + i]) * h2[i];
+        h3[j] = bf(tanh(a));
+    }
+    for (int j = 0; j < N3O; j++) {
+        double a = P[QB4 + j];
+        for (int i = 0; i < N3H; i++) a += bf(P[Q4 + j * N3H + i]) * h3[i];
+        o[j] = a;
+    }
+}
+
+/* the model's traceless stress dT[5] and EMF dE[3] from s = Delta^2 n^2 o */
+static void tensor_terms(const double* s, double* dT, double* dE) {
+    const double tr = (s[0] + s[3] + s[5]) / 3.0;
+    dT[0] = s[0] - tr; dT[1] = s[1]; dT[2] = s[2]; dT[3] = s[3] - tr; dT[4] = s[4];
+    /* M_xy M_xz M_yx M_yz M_zx M_zy = s6 .. s11 */
+    dE[0] = 0.5 * (s[9] - s[11]);
+    dE[1] = 0.5 * (s[10] - s[7]);
+    dE[2] = 0.5 * (s[6] - s[8]);
+}
+
+void orc_closure3_mlp(const double* params, const double* x, double* o) {
+    double xb[N3I], h1[N3H], h2[N3H], h3[N3H];
+    fwd3(params, x, xb, h1, h2, h3, o);
+}
+
+double orc_closure3_terms(const double* P, double delta2, const double* A, const double* G, int mhd, double* tau,
+                          double* e, double* nu_eff, double* eta_eff) {
+    double f[8], S5[5], J3[3], x[N3I], o[N3O], s[N3O], dT[5], dE[3];
+    const double n = orc_closure_features(A, G, f, S5, J3);
+    for (int i = 0; i < 9; i++) { x[i] = A[i] / n; x[9 + i] = G[i] / n; }
+    orc_closure3_mlp(P, x, o);
+    for (int i = 0; i < N3O; i++) s[i] = delta2 * n * n * o[i];
+    tensor_terms(s, dT, dE);
+    if (!mhd) dE[0] = dE[1] = dE[2] = 0.0;
+    const double Szz = A[8], dTzz = -(dT[0] + dT[3]);
+    const double TS = dT[0] * S5[0] + dT[3] * S5[3] + dTzz * Szz + 2.0 * (dT[1] * S5[1] + dT[2] * S5[2] + dT[4] * S5[4]);
+    const double T2 = dT[0] * dT[0] + dT[3] * dT[3] + dTzz * dTzz + 2.0 * (dT[1] * dT[1] + dT[2] * dT[2] + dT[4] * dT[4]);
+    const double S2 = S5[0] * S5[0] + S5[3] * S5[3] + Szz * Szz + 2.0 * (S5[1] * S5[1] + S5[2] * S5[2] + S5[4] * S5[4]);
+    double EJ = 0.0, E2 = 0.0, J2 = 0.0;
+    for (int k = 0; k < 3; k++) { EJ += dE[k] * J3[k]; E2 += dE[k] * dE[k]; J2 += J3[k] * J3[k]; }
+    const double Pt = -TS - EJ, Pm = sqrt(T2) * sqrt(S2) + sqrt(E2) * sqrt(J2);
+    double r = Pt / (0.1 * Pm + 1e-30);
+    r = r < 0.0 ? 0.0 : (r > 1.0 ? 1.0 : r);
+    for (int k = 0; k < 5; k++) tau[k] = r * dT[k];
+    for (int k = 0; k < 3; k++) e[k] = r * dE[k];
+    *nu_eff = r * sqrt(T2) / (2.0 * n);
+    *eta_eff = mhd ? r * sqrt(E2) / n : 0.0;
+    return n;
+}
+
+void orc_closure3_loss_grad(const double* X, size_t n, size_t stride, const double* P, const double* w, double* grad,
+                            double* loss) {
+    memset(grad, 0, sizeof(double) * QN);
+    double L = 0.0;
+    double W4b[N3O * N3H], W3b[N3H * N3H], W2b[N3H * N3H];
+    for (int i = 0; i < N3O * N3H; i++) W4b[i] = bf(P[Q4 + i]);
+    for (int i = 0; i < N3H * N3H; i++) { W3b[i] = bf(P[Q3 + i]); W2b[i] = bf(P[Q2 + i]); }
+    for (size_t q = 0; q < n; q++) {
+        double A[9], G[9], f[8], S5[5], J3[3], x[N3I], xb[N3I], h1[N3H], h2[N3H], h3[N3H], o[N3O];
+        double tT[5], tE[3], Sf[5], Jf[3], s[N3O], dT[5], dE[3];
+        for (int r = 0; r < 9; r++) {
+            A[r] = X[(SPK_CLOSURE_ROW_A + r) * stride + q];
+            G[r] = X[(SPK_CLOSURE_ROW_G + r) * stride + q];
+        }
+        for (int r = 0; r < 5; r++) { tT[r] = X[(SPK_CLOSURE_ROW_TT + r) * stride + q]; Sf[r] = X[(SPK_CLOSURE_ROW_SF + r) * stride + q]; }
+        for (int r = 0; r < 3; r++) { tE[r] = X[(SPK_CLOSURE_ROW_TE + r) * stride + q]; Jf[r] = X[(SPK_CLOSURE_ROW_JF + r) * stride + q]; }
+        const double nn = orc_closure_features(A, G, f, S5, J3);
+        const double sc = X[SPK_CLOSURE_ROW_SCALE * stride + q] * nn;   /* Delta^2 n^2 */
+        for (int i = 0; i < 9; i++) { x[i] = A[i] / nn; x[9 + i] = G[i] / nn; }
+        fwd3(P, x, xb, h1, h2, h3, o);
+        for (int i = 0; i < N3O; i++) s[i] = sc * o[i];
+        tensor_terms(s, dT, dE);
+        double e[5], eE[3];
+        for (int r = 0; r < 5; r++) e[r] = dT[r] - tT[r];
+        for (int r = 0; r < 3; r++) eE[r] = dE[r] - tE[r];
+        const double ezz = -(e[0] + e[3]), Sfzz = -(Sf[0] + Sf[3]);
+        const double fro = e[0] * e[0] + e[3] * e[3] + ezz * ezz + 2.0 * (e[1] * e[1] + e[2] * e[2] + e[4] * e[4]);
+        double emf = 0.0, eJ = 0.0;
+        for (int r = 0; r < 3; r++) { emf += eE[r] * eE[r]; eJ += eE[r] * Jf[r]; }
+        /* transfer error: -(dT - tT):Sf - (dE - tE).Jf */
+        const double dP = -(e[0] * Sf[0] + e[3] * Sf[3] + ezz * Sfzz + 2.0 * (e[1] * Sf[1] + e[2] * Sf[2] + e[4] * Sf[4])) - eJ;
+        L += w[0] * fro + w[1] * emf + w[2] * dP * dP;
+        /* d loss / d e (e5 independent, ezz through e0 and e3), d loss / d eE */
+        double g5[5], gE[3];
+        g5[0] = w[0] * (2.0 * e[0] - 2.0 * ezz) + w[2] * 2.0 * dP * -(Sf[0] - Sfzz);
+        g5[3] = w[0] * (2.0 * e[3] - 2.0 * ezz) + w[2] * 2.0 * dP * -(Sf[3] - Sfzz);
+        g5[1] = w[0] * 4.0 * e[1] + w[2] * 2.0 * dP * -2.0 * Sf[1];
+        g5[2] = w[0] * 4.0 * e[2] + w[2] * 2.0 * dP * -2.0 * Sf[2];
+        g5[4] = w[0] * 4.0 * e[4] + w[2] * 2.0 * dP * -2.0 * Sf[4];
+        for (int r = 0; r < 3; r++) gE[r] = w[1] * 2.0 * eE[r] + w[2] * 2.0 * dP * -Jf[r];
+        /* through dT(s), dE(s) and s = sc o */
+        double gs[N3O], d4[N3O], d3[N3H], d2[N3H], d1[N3H];
+        gs[0] = (2.0 * g5[0] - g5[3]) / 3.0;
+        gs[3] = (2.0 * g5[3] - g5[0]) / 3.0;
+        gs[5] = -(g5[0] + g5[3]) / 3.0;
+        gs[1] = g5[1]; gs[2] = g5[2]; gs[4] = g5[4];
+        gs[9] = 0.5 * gE[0]; gs[11] = -0.5 * gE[0];
+        gs[10] = 0.5 * gE[1]; gs[7] = -0.5 * gE[1];
+        gs[6] = 0.5 * gE[2]; gs[8] = -0.5 * gE[2];
+        for (int j = 0; j < N3O; j++) d4[j] = bf(sc * gs[j]);
+        for (int i = 0; i < N3H; i++) {
+            double a = 0.0;
+            for (int j = 0; j < N3O; j++) a += W4b[j * N3H + i] * d4[j];
+            d3[i] = bf(a * (1.0 - h3[i] * h3[i]));
+        }
+        for (int i = 0; i < N3H; i++) {
+            double a = 0.0;
+            for (int j = 0; j < N3H; j++) a += W3b[j * N3H + i] * d3[j];
+            d2[i] = bf(a * (1.0 - h2[i] * h2[i]));
+        }
+        for (int i = 0; i < N3H; i++) {
+            double a = 0.0;
+            for (int j = 0; j < N3H; j++) a += W2b[j * N3H + i] * d2[j];
+            d1[i] = bf(a * (1.0 - h1[i] * h1[i]));
+        }
+        for (int j = 0; j < N3O; j++) {
+            grad[QB4 + j] += d4[j];
+            for (int i = 0; i < N3H; i++) grad[Q4 + j * N3H + i] += d4[j] * h3[i];
+        }
+        for (int j = 0; j < N3H; j++) {
+            grad[QB3 + j] += d3[j];
+            grad[QB2 + j] += d2[j];
+            grad[QB1 + j] += d1[j];
+            for (int i = 0; i < N3H; i++) {
+                grad[Q3 + j * N3H + i] += d3[j] * h2[i];
+                grad[Q2 + j * N3H + i] += d2[j] * h1[i];
+            }
+            for (int i = 0; i < N3I; i++) grad[Q1 + j * N3I + i] += d1[j] * xb[i];
+        }
+    }
+    const double inv = n > 0 ? 1.0 / (double)n : 0.0;
+    for (int p = 0; p < QN; p++) grad[p] *= inv;
+    *loss = L * inv;
+}
+
+void orc_closure_adam_n(double* P, const double* g, double* m, double* v, int t, double lr, int np) {
+    const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
+    const double c1 = 1.0 - pow(b1, t), c2 = 1.0 - pow(b2, t);
+    for (int p = 0; p < np; p++) {
         m[p] = b1 * m[p] + (1.0 - b1) * g[p];
         v[p] = b2 * v[p] + (1.0 - b2) * g[p] * g[p];
         P[p] -= lr * (m[p] / c1) / (sqrt(v[p] / c2) + eps);

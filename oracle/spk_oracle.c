@@ -247,7 +247,7 @@ struct orc_ctx {
     /* learned closure (spk_closure.c): parameters, Delta^2, the real-space
      * closure terms -2 nu_t S (5) and -eta_t J (3), the gradients A, G (18) */
     int closure_on;
-    double cparams[SPK_CLOSURE_NPARAM];
+    double cparams[SPK_CLOSURE3_NPARAM];   /* variant 3's count, the larger */
     double delta2, nu_t_max, eta_t_max;
     double *rclos, *rgrad;
     cpx* ctmp;
@@ -431,6 +431,21 @@ static void closure_fields(orc_ctx* c, const cpx* U) {
     const int mhd = c->p.mhd;
     closure_grads(c, U, c->p.closure == 2);
     double numax = 0.0, etamax = 0.0;
+    if (c->p.closure == 3) {
+        #pragma omp parallel for schedule(static) reduction(max : numax, etamax)
+        for (long q = 0; q < (long)nr; q++) {
+            double A[9], G[9], tau[5], e[3], nu, eta;
+            for (int r = 0; r < 9; r++) { A[r] = c->rgrad[(size_t)r * nr + q]; G[r] = c->rgrad[(size_t)(9 + r) * nr + q]; }
+            orc_closure3_terms(c->cparams, c->delta2, A, G, mhd, tau, e, &nu, &eta);
+            for (int r = 0; r < 5; r++) c->rclos[(size_t)r * nr + q] = tau[r];
+            for (int r = 0; r < 3; r++) c->rclos[(size_t)(5 + r) * nr + q] = e[r];
+            if (nu > numax) numax = nu;
+            if (eta > etamax) etamax = eta;
+        }
+        c->nu_t_max = numax;
+        c->eta_t_max = etamax;
+        return;
+    }
     #pragma omp parallel for schedule(static) reduction(max : numax, etamax)
     for (long q = 0; q < (long)nr; q++) {
         double A[9], G[9], f[8], S5[5], J3[3], o[2];
@@ -452,7 +467,7 @@ static void closure_fields(orc_ctx* c, const cpx* U) {
 int orc_closure_set(orc_ctx* c, const double* params) {
     if (!params) { c->closure_on = 0; return 0; }
     if (!c->p.incompressible || c->p.boussinesq) return 1;
-    memcpy(c->cparams, params, sizeof(c->cparams));
+    memcpy(c->cparams, params, sizeof(double) * (c->p.closure == 3 ? SPK_CLOSURE3_NPARAM : SPK_CLOSURE_NPARAM));
     if (!c->rclos) {
         c->rclos = (double*)calloc(c->g.nr * 8, sizeof(double));
         c->rgrad = (double*)calloc(c->g.nr * 18, sizeof(double));
@@ -1123,7 +1138,7 @@ void orc_truncate(const orc_ctx* f, const orc_ctx* c, const double* Xf, int nch,
 }
 
 /* Training samples (include/spooky_b200.h, spk_closure_samples): one per
- * coarse point, rows of SPK_CLOSURE_ROWS doubles `stride` apart.  The coarse
+ * coarse point, rows of SPK_CLOSURE_ROWS doubles (variant 3: SPK_CLOSURE3_ROWS) `stride` apart.  The coarse
  * context's state becomes the filtered fine state. */
 void orc_closure_samples(orc_ctx* f, const double* Uf, orc_ctx* c, double* X, size_t stride) {
     const size_t nr = c->g.nr, nc = c->g.nc;
@@ -1171,6 +1186,11 @@ void orc_closure_samples(orc_ctx* f, const double* Uf, orc_ctx* c, double* X, si
         for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_TE + r) * stride + q] = np == 8 ? Rt[(size_t)(5 + r) * nr + q] : 0.0;
         for (int r = 0; r < 5; r++) X[(size_t)(SPK_CLOSURE_ROW_SF + r) * stride + q] = full[(size_t)r * nr + q];
         for (int r = 0; r < 3; r++) X[(size_t)(SPK_CLOSURE_ROW_JF + r) * stride + q] = full[(size_t)(5 + r) * nr + q];
+        if (c->p.closure == 3)
+            for (int r = 0; r < 9; r++) {
+                X[(size_t)(SPK_CLOSURE_ROW_A + r) * stride + q] = A[r];
+                X[(size_t)(SPK_CLOSURE_ROW_G + r) * stride + q] = G[r];
+            }
     }
     free(full);
     free(Pf); free(Pt); free(Pc); free(Rt);

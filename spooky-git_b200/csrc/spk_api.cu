@@ -82,6 +82,7 @@ struct spk_ctx {
     double* d_spec = nullptr;
     bool closure_on = false;
     float* d_cparams = nullptr;
+    unsigned char* d_cimg = nullptr;   // variant 3: the packed BF16 network
     double delta2 = 0.0;
     int out_T, out_E, out_F, out_Q;
     // graphs
@@ -390,11 +391,12 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     const int slots = std::max(1, nthr / RegFft<T, N>::TPC);
     const long nlines = (long)c->nx * c->ny;
     const int npin = (nin_all + 1) / 2, npout = (z.nout + 1) / 2;
-    const int gen = z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.shear_part) ? 1 : 0);
+    const int gen = z.closure == 3 ? 3 : (z.closure ? 2 : ((z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.shear_part) ? 1 : 0));
     const int max_ctas = gen == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4;   // the kernel's launch bounds
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
-                            slots, z.closure ? CL_NP : 0, zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots)).total;
+                            slots, z.closure == 3 ? C3_ZBYTES / 4 : (z.closure ? CL_NP : 0),
+                            zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots)).total;
     };
     // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
     auto rounds = [&](long n) { return (n + slots - 1) / slots; };
@@ -423,7 +425,10 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     z.lines = L;
     const int nblk = (int)(((nlines + L - 1) / L) * c->nb);
     c->launches++;
-    if (z.closure) {
+    if (z.closure == 3) {
+        allow_full_smem(k_zpass2<T, N, 3>);
+        k_zpass2<T, N, 3><<<nblk, nthr, smem, c->stream>>>(z);
+    } else if (z.closure) {
         allow_full_smem(k_zpass2<T, N, 2>);
         k_zpass2<T, N, 2><<<nblk, nthr, smem, c->stream>>>(z);
     } else if (z.derive_gz != 0 || z.mode == ZM_TO_REAL || z.shear_part) {
@@ -619,9 +624,9 @@ static void set_inputs(spk_ctx* c, ZArgs& z, bool with_g) {
     z.ch_u = c->ch_u; z.ch_b = c->ch_b; z.ch_th = c->ch_th;
     if (with_g && c->aniso_rhs) { z.nin += 2; z.ch_gx = c->ch_gx; z.ch_gy = c->ch_gy; z.derive_gz = 1; }
     if (with_g && c->closure_on) {
-        z.closure = 1;
+        z.closure = c->p.closure == 3 ? 3 : 1;
         z.ch_dx = c->ch_dx;
-        z.cparams = c->d_cparams;
+        z.cparams = c->p.closure == 3 ? (const float*)c->d_cimg : c->d_cparams;
         z.delta2 = (float)c->delta2;
         if (c->ngrad > 0) {
             z.nin += c->ngrad;
@@ -953,7 +958,10 @@ static int check_params(const spk_params_t* p, std::string& why) {
     }
     if (p->form != SPK_FORM_PLAIN && p->form != SPK_FORM_FP32) { why = "unknown form"; return SPK_ERR_ARG; }
     if (p->strat_direction < 0 || p->strat_direction > 2) { why = "strat_direction must be 0, 1 or 2"; return SPK_ERR_ARG; }
-    if (p->closure < 0 || p->closure > 2) { why = "closure must be 0, 1 (full-field model) or 2 (small-scale model)"; return SPK_ERR_ARG; }
+    if (p->closure < 0 || p->closure > 3) {
+        why = "closure must be 0, 1 (full-field model), 2 (small-scale model) or 3 (tensor network)";
+        return SPK_ERR_ARG;
+    }
     if (!(p->closure_kc_frac >= 0.0 && p->closure_kc_frac < 1.0)) { why = "closure_kc_frac must be in [0, 1)"; return SPK_ERR_ARG; }
     if (p->closure && (!p->incompressible || p->boussinesq)) { why = "the learned closure covers the HD and MHD modules"; return SPK_ERR_UNSUPPORTED; }
     if (p->closure && p->supertimestepping) { why = "the learned closure with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
@@ -1199,7 +1207,7 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
     if (c->aniso_rhs) { c->ch_gx = ch; c->ch_gy = ch + 1; ch += 2; }
     c->ch_dx = c->ch_dy = -1;
     c->ncl_half = 0;
-    if (p.closure == 1) {
+    if (p.closure == 1 || p.closure == 3) {
         c->ncl_half = p.mhd ? 6 : 3;
         c->ch_dx = ch; ch += c->ncl_half;
         c->ch_dy = ch; ch += c->ncl_half;
@@ -1340,8 +1348,13 @@ static int ctx_alloc(spk_ctx* c) {
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
     if (c->p.closure) {
-        CK(cudaMalloc(&c->d_cparams, sizeof(float) * CL_NP));
-        CK(cudaMemset(c->d_cparams, 0, sizeof(float) * CL_NP));
+        const size_t np = (size_t)spk_closure_nparam(c->p.closure);
+        CK(cudaMalloc(&c->d_cparams, sizeof(float) * np));
+        CK(cudaMemset(c->d_cparams, 0, sizeof(float) * np));
+        if (c->p.closure == 3) {
+            CK(cudaMalloc(&c->d_cimg, (size_t)C3_ALL_BYTES));
+            CK(cudaMemset(c->d_cimg, 0, (size_t)C3_ALL_BYTES));
+        }
     }
     CK(cudaMalloc(&c->d_spec, sizeof(double) * (size_t)(c->nbins + 1)));
     if (c->nkx > 0 && c->nky > 0) {
@@ -1362,6 +1375,7 @@ static void ctx_free(spk_ctx* c) {
     cudaFree(c->bufA); cudaFree(c->bufB); cudaFree(c->rA); cudaFree(c->rB); cudaFree(c->breal);
     cudaFree(c->Uc0); cudaFree(c->Uc1); cudaFree(c->dU0); cudaFree(c->sc); cudaFree(c->d_sums);
     cudaFree(c->d_cparams);
+    cudaFree(c->d_cimg);
     cudaFree(c->d_keep);
     cudaFree(c->d_spec);
     if (c->h_sc) cudaFreeHost(c->h_sc);

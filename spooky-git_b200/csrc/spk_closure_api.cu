@@ -3,11 +3,25 @@
 // products, training samples from a fine-grid state, and the trainer.
 // Included at the end of spk_api.cu (one translation unit).
 
+extern "C" int spk_closure_nparam(int variant) {
+    return (variant == 1 || variant == 2) ? (int)CL_NP : (variant == 3 ? (int)C3_NP : 0);
+}
+
+extern "C" int spk_closure_rows(int variant) {
+    return (variant == 1 || variant == 2) ? SPK_CLOSURE_ROWS : (variant == 3 ? SPK_CLOSURE3_ROWS : 0);
+}
+
 extern "C" int spk_closure_set(spk_ctx* c, const float* params) {
     if (!c) return SPK_ERR_ARG;
     if (!c->p.closure) return fail(c, SPK_ERR_UNSUPPORTED, "the context was created without params.closure");
     if (params) {
-        CK(cudaMemcpyAsync(c->d_cparams, params, sizeof(float) * CL_NP, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_cparams, params, sizeof(float) * (size_t)spk_closure_nparam(c->p.closure),
+                           cudaMemcpyHostToDevice, c->stream));
+        if (c->p.closure == 3) {
+            c->launches++;
+            k_closure3_pack<<<32, 256, 0, c->stream>>>(c->d_cparams, c->d_cimg);
+            CK(cudaGetLastError());
+        }
         CK(cudaStreamSynchronize(c->stream));
     }
     const bool on = params != nullptr;
@@ -159,7 +173,8 @@ extern "C" int spk_closure_samples(spk_ctx* f, const double* Uf, spk_ctx* c, flo
         rc = c2r_channels(c, Gs, 18, Rgf && !hp ? Rgf : Rg);
         if (rc) return rc;
     }
-    k_closure_rows<<<ew_blocks(c->nr), 256, 0, c->stream>>>(Rg, Rgf, Rt, np, c->nr, c->delta2, X, stride);
+    k_closure_rows<<<ew_blocks(c->nr), 256, 0, c->stream>>>(Rg, Rgf, Rt, np, c->nr, c->delta2, X, stride,
+                                                             c->p.closure == 3 ? 1 : 0);
     c->launches++;
     return launch_status(c);
 }
@@ -198,6 +213,9 @@ extern "C" int spk_spectrum(spk_ctx* c, int f1, int f2, double* out, int max_bin
 struct spk_trainer {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    int variant = 1;                 // 1 (also 2): the eddy-coefficient network; 3: the tensor network
+    int np = CL_NP;                  // parameters
+    unsigned char* img = nullptr;    // variant 3: the packed BF16 image of params
     float *params = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *partial = nullptr;
     float *hist = nullptr, *h_hist = nullptr;
     const float* X = nullptr;
@@ -215,10 +233,17 @@ static size_t grad_smem() { return sizeof(float) * (((CL_NP + 3) & ~3) + (size_t
         if (e_ != cudaSuccess) return fail(nullptr, SPK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
 
-extern "C" int spk_trainer_create(void* stream, spk_trainer** out) {
+extern "C" int spk_trainer_create(void* stream, spk_trainer** out) { return spk_trainer_create_variant(stream, 1, out); }
+
+static int train_blocks(const spk_trainer* tr) { return tr->variant == 3 ? 148 : CL_MAXBLK; }
+
+extern "C" int spk_trainer_create_variant(void* stream, int variant, spk_trainer** out) {
     if (!out) return fail(nullptr, SPK_ERR_ARG, "null argument");
     *out = nullptr;
+    if (spk_closure_nparam(variant) == 0) return fail(nullptr, SPK_ERR_ARG, "closure variant must be 1, 2 or 3");
     spk_trainer* tr = new spk_trainer();
+    tr->variant = variant == 3 ? 3 : 1;
+    tr->np = spk_closure_nparam(variant);
     auto bail = [&](int rc) { spk_trainer_destroy(tr); return rc; };
     if (stream) tr->stream = (cudaStream_t)stream;
     else {
@@ -226,18 +251,21 @@ extern "C" int spk_trainer_create(void* stream, spk_trainer** out) {
             return bail(fail(nullptr, SPK_ERR_CUDA, "stream creation failed"));
         tr->own_stream = true;
     }
-    if (cudaMalloc(&tr->params, sizeof(float) * CL_NP) != cudaSuccess ||
-        cudaMalloc(&tr->m, sizeof(float) * CL_NP) != cudaSuccess ||
-        cudaMalloc(&tr->v, sizeof(float) * CL_NP) != cudaSuccess ||
-        cudaMalloc(&tr->grad, sizeof(float) * CL_NP) != cudaSuccess ||
-        cudaMalloc(&tr->partial, sizeof(float) * (size_t)CL_MAXBLK * (CL_NP + 1)) != cudaSuccess ||
+    const size_t np = (size_t)tr->np;
+    if (cudaMalloc(&tr->params, sizeof(float) * np) != cudaSuccess ||
+        cudaMalloc(&tr->m, sizeof(float) * np) != cudaSuccess ||
+        cudaMalloc(&tr->v, sizeof(float) * np) != cudaSuccess ||
+        cudaMalloc(&tr->grad, sizeof(float) * np) != cudaSuccess ||
+        cudaMalloc(&tr->partial, sizeof(float) * (size_t)train_blocks(tr) * (np + 1)) != cudaSuccess ||
         cudaMalloc(&tr->hist, sizeof(float) * SPK_TRAIN_HIST) != cudaSuccess ||
-        cudaMallocHost(&tr->h_hist, sizeof(float) * SPK_TRAIN_HIST) != cudaSuccess)
+        cudaMallocHost(&tr->h_hist, sizeof(float) * SPK_TRAIN_HIST) != cudaSuccess ||
+        (tr->variant == 3 && cudaMalloc(&tr->img, (size_t)C3_ALL_BYTES) != cudaSuccess))
         return bail(fail(nullptr, SPK_ERR_ALLOC, "trainer allocation failed"));
-    cudaMemset(tr->params, 0, sizeof(float) * CL_NP);
-    cudaMemset(tr->m, 0, sizeof(float) * CL_NP);
-    cudaMemset(tr->v, 0, sizeof(float) * CL_NP);
-    if (cudaFuncSetAttribute(k_closure_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem()) != cudaSuccess)
+    cudaMemset(tr->params, 0, sizeof(float) * np);
+    cudaMemset(tr->m, 0, sizeof(float) * np);
+    cudaMemset(tr->v, 0, sizeof(float) * np);
+    if (cudaFuncSetAttribute(k_closure_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_closure3_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C3G_BYTES) != cudaSuccess)
         return bail(fail(nullptr, SPK_ERR_CUDA, "shared-memory opt-in of the gradient kernel failed"));
     *out = tr;
     return SPK_OK;
@@ -247,6 +275,7 @@ extern "C" int spk_trainer_destroy(spk_trainer* tr) {
     if (!tr) return SPK_OK;
     cudaFree(tr->params); cudaFree(tr->m); cudaFree(tr->v); cudaFree(tr->grad); cudaFree(tr->partial);
     cudaFree(tr->hist);
+    cudaFree(tr->img);
     if (tr->h_hist) cudaFreeHost(tr->h_hist);
     if (tr->own_stream) cudaStreamDestroy(tr->stream);
     delete tr;
@@ -255,9 +284,9 @@ extern "C" int spk_trainer_destroy(spk_trainer* tr) {
 
 extern "C" int spk_trainer_set_params(spk_trainer* tr, const float* params) {
     if (!tr || !params) return fail(nullptr, SPK_ERR_ARG, "null argument");
-    TCK(cudaMemcpyAsync(tr->params, params, sizeof(float) * CL_NP, cudaMemcpyHostToDevice, tr->stream));
-    TCK(cudaMemsetAsync(tr->m, 0, sizeof(float) * CL_NP, tr->stream));
-    TCK(cudaMemsetAsync(tr->v, 0, sizeof(float) * CL_NP, tr->stream));
+    TCK(cudaMemcpyAsync(tr->params, params, sizeof(float) * tr->np, cudaMemcpyHostToDevice, tr->stream));
+    TCK(cudaMemsetAsync(tr->m, 0, sizeof(float) * tr->np, tr->stream));
+    TCK(cudaMemsetAsync(tr->v, 0, sizeof(float) * tr->np, tr->stream));
     TCK(cudaStreamSynchronize(tr->stream));
     tr->t = 0;
     return SPK_OK;
@@ -265,7 +294,7 @@ extern "C" int spk_trainer_set_params(spk_trainer* tr, const float* params) {
 
 extern "C" int spk_trainer_get_params(spk_trainer* tr, float* params) {
     if (!tr || !params) return fail(nullptr, SPK_ERR_ARG, "null argument");
-    TCK(cudaMemcpyAsync(params, tr->params, sizeof(float) * CL_NP, cudaMemcpyDeviceToHost, tr->stream));
+    TCK(cudaMemcpyAsync(params, tr->params, sizeof(float) * tr->np, cudaMemcpyDeviceToHost, tr->stream));
     TCK(cudaStreamSynchronize(tr->stream));
     return SPK_OK;
 }
@@ -291,6 +320,19 @@ static void trainer_grad(spk_trainer* tr, size_t m, bool minibatch, float* loss_
     a.base = tr->cursor;
     a.params = tr->params; a.w0 = tr->w0; a.w1 = tr->w1; a.w2 = tr->w2;
     a.partial = tr->partial;
+    if (tr->variant == 3) {
+        // the tensor network: BF16 image of the FP32 masters, then chunks of 64 samples
+        Train3Args b;
+        b.X = a.X; b.n = a.n; b.stride = a.stride; b.m = a.m; b.minibatch = a.minibatch;
+        b.a = a.a; b.c = a.c; b.base = a.base;
+        b.img = tr->img; b.w0 = a.w0; b.w1 = a.w1; b.w2 = a.w2; b.partial = tr->partial;
+        const int nblk = (int)std::min<size_t>((size_t)train_blocks(tr), (m + C3_CH - 1) / C3_CH);
+        k_closure3_pack<<<32, 256, 0, tr->stream>>>(tr->params, tr->img);
+        k_closure3_grad<<<nblk, 128, C3G_BYTES, tr->stream>>>(b);
+        k_closure_reduce_n<<<(C3_NP + 1 + 127) / 128, 128, 0, tr->stream>>>(tr->partial, nblk, C3_NP, 1.0 / (double)m,
+                                                                            tr->grad, loss_out);
+        return;
+    }
     const int nblk = (int)std::min<size_t>(CL_MAXBLK, (m + CL_CHUNK - 1) / CL_CHUNK);
     k_closure_grad<<<nblk, CL_CHUNK, grad_smem(), tr->stream>>>(a);
     k_closure_reduce<<<(CL_NP + 1 + 127) / 128, 128, 0, tr->stream>>>(tr->partial, nblk, 1.0 / (double)m, tr->grad,
@@ -301,7 +343,7 @@ extern "C" int spk_trainer_loss_grad(spk_trainer* tr, float* loss, float* grad) 
     if (!tr || !tr->X) return fail(nullptr, SPK_ERR_ARG, "trainer without samples");
     trainer_grad(tr, tr->n, false, tr->hist);
     TCK(cudaGetLastError());
-    if (grad) TCK(cudaMemcpyAsync(grad, tr->grad, sizeof(float) * CL_NP, cudaMemcpyDeviceToHost, tr->stream));
+    if (grad) TCK(cudaMemcpyAsync(grad, tr->grad, sizeof(float) * tr->np, cudaMemcpyDeviceToHost, tr->stream));
     TCK(cudaMemcpyAsync(tr->h_hist, tr->hist, sizeof(float), cudaMemcpyDeviceToHost, tr->stream));
     TCK(cudaStreamSynchronize(tr->stream));
     if (loss) *loss = tr->h_hist[0];
@@ -316,7 +358,11 @@ extern "C" int spk_trainer_train(spk_trainer* tr, int nsteps, int batch, float l
             trainer_grad(tr, (size_t)batch, true, tr->hist + i);
             tr->t++;
             tr->cursor += (unsigned long long)batch;
-            k_closure_adam<<<(CL_NP + 255) / 256, 256, 0, tr->stream>>>(tr->params, tr->grad, tr->m, tr->v, tr->t, lr);
+            if (tr->variant == 3)
+                k_closure_adam_n<<<(C3_NP + 255) / 256, 256, 0, tr->stream>>>(tr->params, tr->grad, tr->m, tr->v, C3_NP,
+                                                                              tr->t, lr);
+            else
+                k_closure_adam<<<(CL_NP + 255) / 256, 256, 0, tr->stream>>>(tr->params, tr->grad, tr->m, tr->v, tr->t, lr);
         }
         TCK(cudaGetLastError());
         if (loss_hist) {

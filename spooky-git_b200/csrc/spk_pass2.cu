@@ -13,6 +13,7 @@
 // buffer (kept ky rows only in the y-forward pass).
 #include "spk_regfft.cuh"
 #include "spk_closure.cuh"
+#include "spk_closure3.cuh"
 
 namespace spk {
 
@@ -301,7 +302,8 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
 // GEN: 0 -- every input channel is a plain half spectrum; 1 -- derived
 // gradient channels or the to-real output (the general path); 2 -- the
 // general path with the learned closure (its own instantiation, so that the
-// MLP's registers do not weigh on the others).
+// MLP's registers do not weigh on the others); 3 -- the same with the
+// closure's tensor network (variant 3).
 template <typename T, int N, int GEN>
 __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) k_zpass2(const __grid_constant__ ZArgs a) {
     using F = RegFft<T, N>;
@@ -319,16 +321,16 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     const int nl = min(L, nlines - line0);
     const int nin = a.nin;
     const int nder0 = nin + (a.derive_gz == 1 ? 1 : 0);   // first closure d/dz channel
-    const int nin_all = nder0 + (GEN == 2 ? a.zder_n : 0);
+    const int nin_all = nder0 + (GEN >= 2 ? a.zder_n : 0);
     const int npin = (nin_all + 1) / 2, npout = (a.nout + 1) / 2;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int slots = nthr >> LTPC;
     const int sigma = tid >> LTPC, q = tid & (TPC - 1);
     const int sigma_w = (tid & ~31) >> LTPC;   // the lowest slot of this warp (warp-uniform)
-    const bool clos = GEN == 2 && a.closure;
+    const bool clos = GEN >= 2 && a.closure;
     const bool alias = zpass_alias(GEN, F::NS, npin, npout, L, slots);
     const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots,
-                                   clos ? CL_NP : 0, alias);
+                                   clos ? (GEN == 3 ? C3_ZBYTES / 4 : CL_NP) : 0, alias);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
     C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
@@ -338,8 +340,15 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
     float* cw = reinterpret_cast<float*>(smem_raw + lay.cw);
-    if (clos)
-        for (int i = tid; i < CL_NP; i += nthr) cw[i] = a.cparams[i];   // visible after the next barrier
+    if (clos) {   // visible after the next barrier
+        if constexpr (GEN == 3) {
+            // the packed BF16 network, in 16-byte words
+            const uint4* src = reinterpret_cast<const uint4*>(a.cparams);
+            for (int i = tid; i < C3_FWD_BYTES / 16; i += nthr) reinterpret_cast<uint4*>(cw)[i] = src[i];
+        } else {
+            for (int i = tid; i < CL_NP; i += nthr) cw[i] = a.cparams[i];
+        }
+    }
     const C2<T>* in = (const C2<T>*)a.in + (size_t)box * a.in_box;
     DevScalars* bsc = a.scs + box;
     const int LRS = L * RS;
@@ -450,7 +459,53 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         T* prodT = reinterpret_cast<T*>(prod);
         const T third = (T)(1.0 / 3.0);
         const size_t pstride = (size_t)L * N * 2;   // scalars between product pairs
-        for (int e = tid; e < L * N; e += nthr) {
+        // the closure's gradient components of the point at fr (variant 2: all nine
+        // of each field from ch_dx; else d/dx, d/dy and the z-derivative channels)
+        auto grads = [&](const T* fr, float* A, float* G) {
+            if (a.cl_grad9) {
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        A[3 * i + j] = (float)fr[(a.ch_dx + 3 * j + i) * LRS];
+                        G[3 * i + j] = a.mhd ? (float)fr[(a.ch_dx + 9 + 3 * j + i) * LRS] : 0.f;
+                    }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    A[3 * i + 0] = (float)fr[(a.ch_dx + i) * LRS];
+                    A[3 * i + 1] = (float)fr[(a.ch_dy + i) * LRS];
+                    A[3 * i + 2] = (float)fr[(nder0 + i) * LRS];
+                    G[3 * i + 0] = a.mhd ? (float)fr[(a.ch_dx + 3 + i) * LRS] : 0.f;
+                    G[3 * i + 1] = a.mhd ? (float)fr[(a.ch_dy + 3 + i) * LRS] : 0.f;
+                    G[3 * i + 2] = a.mhd ? (float)fr[(nder0 + 3 + i) * LRS] : 0.f;
+                }
+            }
+        };
+        // variant 3 runs its network on the tensor cores per chunk of 128
+        // points, ahead of the chunk's products; the others take all points
+        // in one chunk
+        unsigned char* c3rows = reinterpret_cast<unsigned char*>(cw) + C3_FWD_BYTES;
+        const int EPC = GEN == 3 ? C3_ZCHUNK : L * N;
+        for (int e0 = 0; e0 < L * N; e0 += EPC) {
+        if constexpr (GEN == 3) {
+            if (clos) {
+                const int e = e0 + tid;
+                float A[9], G[9];
+                if (e < L * N) {
+                    const int l = (int)((unsigned)e / (unsigned)N), z = e - l * N;
+                    grads(real + (size_t)l * RS + z, A, G);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 9; i++) A[i] = G[i] = 0.f;
+                }
+                c3_put_inputs(c3rows, tid, A, G);
+                __syncthreads();
+                c3_chunk_mlp(reinterpret_cast<const unsigned char*>(cw), c3rows, tid >> 5, tid & 31);
+                __syncthreads();
+            }
+        }
+        for (int e = e0 + tid; e < min(e0 + EPC, L * N); e += nthr) {
             const int l = (int)((unsigned)e / (unsigned)N), z = e - l * N;
             const bool live = l < nl;
             const size_t line = (size_t)(line0 + l);
@@ -492,27 +547,16 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             float ctau[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, cemf[3] = {0.f, 0.f, 0.f};
             if (clos) {
                 float A[9], G[9], vn, ve;
-                if (a.cl_grad9) {
-                    // variant 2: channel ch_dx + 3 j + i holds d u_i / d x_j (B: + 9)
-#pragma unroll
-                    for (int i = 0; i < 3; i++)
-#pragma unroll
-                        for (int j = 0; j < 3; j++) {
-                            A[3 * i + j] = (float)fr[(a.ch_dx + 3 * j + i) * LRS];
-                            G[3 * i + j] = a.mhd ? (float)fr[(a.ch_dx + 9 + 3 * j + i) * LRS] : 0.f;
-                        }
+                grads(fr, A, G);
+                if constexpr (GEN == 3) {
+                    // the network's outputs for this point, left in its row by the chunk pass
+                    float f[8], S5[5], J3[3];
+                    const float n = closure_features<float>(A, G, f, S5, J3);
+                    const float* o12 = reinterpret_cast<const float*>(c3rows + (size_t)(e - e0) * C3_ZROW);
+                    c3_terms(o12, a.delta2, n, A[8], S5, J3, a.mhd != 0, ctau, cemf, &vn, &ve);
                 } else {
-#pragma unroll
-                    for (int i = 0; i < 3; i++) {
-                        A[3 * i + 0] = (float)fr[(a.ch_dx + i) * LRS];
-                        A[3 * i + 1] = (float)fr[(a.ch_dy + i) * LRS];
-                        A[3 * i + 2] = (float)fr[(nder0 + i) * LRS];
-                        G[3 * i + 0] = a.mhd ? (float)fr[(a.ch_dx + 3 + i) * LRS] : 0.f;
-                        G[3 * i + 1] = a.mhd ? (float)fr[(a.ch_dy + 3 + i) * LRS] : 0.f;
-                        G[3 * i + 2] = a.mhd ? (float)fr[(nder0 + 3 + i) * LRS] : 0.f;
-                    }
+                    closure_point(cw, a.delta2, A, G, ctau, cemf, &vn, &ve);
                 }
-                closure_point(cw, a.delta2, A, G, ctau, cemf, &vn, &ve);
                 if (live && a.do_max) {
                     if (!isfinite(vn) || !isfinite(ve)) bad = 1;
                     mu[6] = fmax(mu[6], (T)vn);
@@ -566,6 +610,10 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
                 qc += 3;
             }
             if (a.nout & 1) put(a.nout, (T)0);
+        }
+        if constexpr (GEN == 3) {
+            if (clos) __syncthreads();   // the chunk's outputs are read before the next chunk's inputs
+        }
         }
         if (a.do_max) {
             // block-max scratch (8 x 32): the exchange slots, or with aliased

@@ -43,7 +43,8 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_rk3_fields", "spk_rkl_cycle_fields", "spk_get_state_real", "spk_set_state_real",
             "spk_write_snapshot", "spk_read_snapshot", "spk_h5_write", "spk_h5_read", "spk_diagnostics",
             "spk_cfg_lookup_int", "spk_cfg_lookup_bool", "spk_cfg_lookup_float", "spk_cfg_lookup_string",
-            "spk_cfg_setting_length", "spk_transfer_spectra"]
+            "spk_cfg_setting_length", "spk_transfer_spectra", "spk_trainer_create_variant",
+            "spk_closure_nparam", "spk_closure_rows"]
 
 DIAGNOSTICS = ("w2", "hv", "j2", "hm", "hc", "thetaB", "bz2", "phiB", "dissgradT", "pv")
 
@@ -54,6 +55,19 @@ class Diagnostics(ctypes.Structure):
 # learned closure (include/spooky_b200.h, SPK_CLOSURE_*)
 CLOSURE_NPARAM = 32 * 8 + 32 + 32 * 32 + 32 + 2 * 32 + 2
 CLOSURE_ROWS = 33
+# variant 3, the tensor network (SPK_CLOSURE3_*)
+CLOSURE3_NPARAM = 64 * 18 + 64 + 2 * (64 * 64 + 64) + 12 * 64 + 12
+CLOSURE3_ROWS = 51
+
+
+def closure_nparam(variant):
+    """Parameters of a closure variant's network."""
+    return CLOSURE3_NPARAM if variant == 3 else CLOSURE_NPARAM
+
+
+def closure_rows(variant):
+    """Sample rows of a closure variant."""
+    return CLOSURE3_ROWS if variant == 3 else CLOSURE_ROWS
 
 
 class Budgets(ctypes.Structure):
@@ -121,6 +135,9 @@ def lib():
         L.spk_closure_samples_size.argtypes = [vp, vp, ctypes.POINTER(sp), ctypes.POINTER(sp)]
         L.spk_closure_samples.argtypes = [vp, vp, vp, vp, sp, vp, sp]
         L.spk_trainer_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.spk_trainer_create_variant.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.spk_closure_nparam.argtypes = [ctypes.c_int]
+        L.spk_closure_rows.argtypes = [ctypes.c_int]
         L.spk_trainer_destroy.argtypes = [vp]
         L.spk_trainer_set_params.argtypes = [vp, fp]
         L.spk_trainer_get_params.argtypes = [vp, fp]
@@ -485,12 +502,15 @@ class Context:
 
     # -- learned closure -----------------------------------------------------
     def closure_set(self, params):
-        """Closure weights (CLOSURE_NPARAM floats) into the RHS, or None: off."""
+        """Closure weights (closure_nparam(variant) floats) into the RHS, or
+        None: off."""
         if params is None:
             self._check(lib().spk_closure_set(self._h, None))
             return
         w = np.ascontiguousarray(params, dtype=np.float32)
-        assert w.size == CLOSURE_NPARAM
+        if w.size != closure_nparam(self.params.closure):
+            raise ValueError(f"closure variant {self.params.closure} takes {closure_nparam(self.params.closure)} "
+                             f"parameters, not {w.size}")
         self._check(lib().spk_closure_set(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
 
     def products(self, U):
@@ -509,9 +529,9 @@ class Context:
 
 def closure_samples(fine, Uf, coarse):
     """Training samples of the closure from the fine context's state Uf (a
-    torch CUDA complex128 tensor): a torch float32 tensor [CLOSURE_ROWS,
-    coarse nx*ny*nz] (spk_closure_samples); coarse's state becomes the
-    filtered state."""
+    torch CUDA complex128 tensor): a torch float32 tensor
+    [closure_rows(variant of coarse), coarse nx*ny*nz] (spk_closure_samples);
+    coarse's state becomes the filtered state."""
     import torch
     _check_state_tensor("Uf", Uf, fine.shape_c)
     nbytes, ns = ctypes.c_size_t(), ctypes.c_size_t()
@@ -519,7 +539,7 @@ def closure_samples(fine, Uf, coarse):
     if rc != SPK_OK:
         raise SpookyError(rc, lib().spk_last_error(None).decode())
     scratch = torch.empty(nbytes.value, dtype=torch.uint8, device=Uf.device)
-    X = torch.empty((CLOSURE_ROWS, ns.value), dtype=torch.float32, device=Uf.device)
+    X = torch.empty((closure_rows(coarse.params.closure), ns.value), dtype=torch.float32, device=Uf.device)
     _torch_sync()
     coarse._check(lib().spk_closure_samples(fine._h, Uf.data_ptr(), coarse._h, X.data_ptr(), ns.value,
                                             scratch.data_ptr(), nbytes.value))
@@ -528,12 +548,15 @@ def closure_samples(fine, Uf, coarse):
 
 
 class Trainer:
-    """spk_trainer: the closure MLP trained on device samples by the
-    library's own forward/backward and Adam kernels."""
+    """spk_trainer: the closure network of a variant (1, 2: the
+    eddy-coefficient MLP; 3: the tensor network) trained on device samples by
+    the library's own forward/backward and Adam kernels."""
 
-    def __init__(self, params=None, stream=None):
+    def __init__(self, params=None, stream=None, variant=1):
         h = ctypes.c_void_p()
-        rc = lib().spk_trainer_create(stream, ctypes.byref(h))
+        self.variant = variant
+        self.nparam = closure_nparam(variant)
+        rc = lib().spk_trainer_create_variant(stream, int(variant), ctypes.byref(h))
         if rc != SPK_OK:
             raise SpookyError(rc, lib().spk_last_error(None).decode())
         self._h = h
@@ -551,18 +574,21 @@ class Trainer:
 
     def set_params(self, params):
         w = np.ascontiguousarray(params, dtype=np.float32)
-        assert w.size == CLOSURE_NPARAM
+        if w.size != self.nparam:
+            raise ValueError(f"the trainer takes {self.nparam} parameters, not {w.size}")
         self._check(lib().spk_trainer_set_params(self._h, self._fp(w)))
 
     def get_params(self):
-        w = np.empty(CLOSURE_NPARAM, np.float32)
+        w = np.empty(self.nparam, np.float32)
         self._check(lib().spk_trainer_get_params(self._h, self._fp(w)))
         return w
 
     def set_samples(self, X, weights):
-        """X: torch CUDA float32 [CLOSURE_ROWS, n] (kept referenced here);
+        """X: torch CUDA float32 [closure_rows(variant), n] (kept referenced here);
         weights: of the stress, EMF and energy-transfer errors (a third weight
         left out is 0)."""
+        if X.shape[0] < closure_rows(self.variant):
+            raise ValueError(f"variant {self.variant} samples have {closure_rows(self.variant)} rows")
         _torch_sync()
         self._X = X
         w = np.asarray(weights, dtype=np.float32).ravel()
@@ -573,7 +599,7 @@ class Trainer:
 
     def loss_grad(self):
         loss = np.zeros(1, np.float32)
-        g = np.empty(CLOSURE_NPARAM, np.float32)
+        g = np.empty(self.nparam, np.float32)
         self._check(lib().spk_trainer_loss_grad(self._h, self._fp(loss), self._fp(g)))
         return float(loss[0]), g
 

@@ -13,7 +13,7 @@ import time
 
 import numpy as np
 
-from . import CLOSURE_NPARAM, Context, Trainer, closure_samples
+from . import CLOSURE3_NPARAM, CLOSURE_NPARAM, Context, Trainer, closure_samples
 from .initial import mhd_random_state
 from .params import SPK_FORM_PLAIN, default_params
 
@@ -30,6 +30,25 @@ def init_params(seed=0, c0=0.02):
     p[_W2:_B2] = rng.standard_normal(_B2 - _W2) / np.sqrt(32.0)
     p[_W3:_B3] = 0.1 * rng.standard_normal(_B3 - _W3) / np.sqrt(32.0)
     p[_B3:] = np.log(np.expm1(c0))
+    return p
+
+
+# variant 3 (the tensor network): W1[64][18] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[12][64] b4[12]
+_V1, _VB1 = 0, 1152
+_V2, _VB2 = 1216, 5312
+_V3, _VB3 = 5376, 9472
+_V4, _VB4 = 9536, 10304
+
+
+def init_params3(seed=0, out=0.05):
+    """Scaled-normal hidden weights, small output weights: the network starts
+    near zero stress and EMF."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(CLOSURE3_NPARAM, np.float32)
+    p[_V1:_VB1] = rng.standard_normal(_VB1 - _V1) / np.sqrt(18.0)
+    p[_V2:_VB2] = rng.standard_normal(_VB2 - _V2) / np.sqrt(64.0)
+    p[_V3:_VB3] = rng.standard_normal(_VB3 - _V3) / np.sqrt(64.0)
+    p[_V4:_VB4] = out * rng.standard_normal(_VB4 - _V4) / np.sqrt(64.0)
     return p
 
 
@@ -112,18 +131,30 @@ def subgrid_weights(X, transfer=1.0):
     return np.array([wt, we, wp])
 
 
+TRANSFER_DEFAULT = {1: 0.0, 2: 4.0, 3: 1.0}
+
+
 def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_steps=3000, batch=16384, lr=2e-3,
-        seed=0, form=SPK_FORM_PLAIN, variant=1, transfer=None, kc_frac=0.0, log=None):
+        seed=0, form=SPK_FORM_PLAIN, variant=1, transfer=None, kc_frac=0.0, log=None, extra_variants=(),
+        lr3=1e-3):
     """Truth, samples, training and the two coarse runs; returns a dict of
     the measured quantities (spectral errors with and without the closure,
     run costs, losses).  variant: 1 the full-field model, 2 the small-scale
-    model (gradients of the modes above half the cut-off); transfer: the
-    relative weight of the energy-transfer error in the loss (0: stress and
-    EMF errors only; None: 0 for variant 1, 4 for variant 2, the better of
-    0, 1 and 4 in the 64^3-vs-256^3 workload); kc_frac: variant 2's
-    small scales are |k| > kc_frac * k_c (0: 1/2)."""
+    model (gradients of the modes above half the cut-off), 3 the tensor
+    network; transfer: the relative weight of the energy-transfer error in
+    the loss (0: stress and EMF errors only; None: TRANSFER_DEFAULT, for
+    variants 1 and 2 the better of 0, 1 and 4 in the 64^3-vs-256^3
+    workload); kc_frac: variant 2's small scales are |k| > kc_frac * k_c
+    (0: 1/2).  extra_variants: more networks (of 1 and 3) trained on the
+    same truth and run on the same coarse grid, their results under
+    "v<variant>" (a variant-3 sampler's rows hold every row variant 1
+    reads); lr3: the tensor network's learning rate."""
     if transfer is None:
-        transfer = {1: 0.0, 2: 4.0}[variant]
+        transfer = TRANSFER_DEFAULT[variant]
+    variants = [variant] + [v for v in extra_variants if v != variant]
+    if 2 in variants and len(variants) > 1:
+        raise ValueError("variant 2 samples differ from the others: run it alone")
+    sample_variant = 3 if 3 in variants else variant
     import torch
     say = log or (lambda *a: None)
     L = 2 * np.pi
@@ -133,7 +164,8 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     U0 = mhd_random_state(pf, 1, 2)
     fine = Context(pf)
     fine.set_state(U0)
-    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, closure=variant, closure_kc_frac=kc_frac, **common)
+    pc0 = default_params(gridsize=(n_coarse,) * 3, t_final=1e30, closure=sample_variant, closure_kc_frac=kc_frac,
+                         **common)
     sampler = Context(pc0)
     Uf = torch.empty(fine.shape_c, dtype=torch.complex128, device="cuda")
     samples, truth_s, done = [], 0.0, 0
@@ -153,23 +185,33 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     del fine, Uf
     X = torch.cat(samples, dim=1).contiguous()
     del samples
-    w = subgrid_weights(X, transfer)
-    tr = Trainer(init_params(seed))
-    tr.set_samples(X, w)
-    loss0, _ = tr.loss_grad()
-    t0 = time.perf_counter()
-    h1 = tr.train(int(train_steps * 2 // 3), batch, lr)
-    h2 = tr.train(train_steps - int(train_steps * 2 // 3), batch, lr / 4)
-    train_s = time.perf_counter() - t0
-    loss1, _ = tr.loss_grad()
-    params = tr.get_params()
-    say(f"training: {X.shape[1]} samples, loss {loss0:.4f} -> {loss1:.4f} in {train_s:.2f} s")
-    del tr, X
+    trained = {}
+    for v in variants:
+        wv = subgrid_weights(X, transfer if v == variant else TRANSFER_DEFAULT[v])
+        tr = Trainer(init_params3(seed) if v == 3 else init_params(seed), variant=v)
+        tr.set_samples(X, wv)
+        l0, _ = tr.loss_grad()
+        lv = lr3 if v == 3 else lr
+        t0 = time.perf_counter()
+        h1 = tr.train(int(train_steps * 2 // 3), batch, lv)
+        h2 = tr.train(train_steps - int(train_steps * 2 // 3), batch, lv / 4)
+        torch.cuda.synchronize()
+        ts = time.perf_counter() - t0
+        l1, _ = tr.loss_grad()
+        trained[v] = dict(params=tr.get_params(), loss_initial=l0, loss_final=l1, train_seconds=ts,
+                          loss_history=np.concatenate([h1, h2]))
+        say(f"training variant {v}: {X.shape[1]} samples, loss {l0:.4f} -> {l1:.4f} in {ts:.2f} s")
+        del tr
+    del X
+    params, loss0, loss1 = trained[variant]["params"], trained[variant]["loss_initial"], trained[variant]["loss_final"]
+    train_s = trained[variant]["train_seconds"]
     # coarse runs from the filtered initial state to the truth's final time
     U0c = filter_to(U0, pf, pc0)
     res = {}
-    for name, cp in (("closure", params), ("plain", None)):
-        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=variant, closure_kc_frac=kc_frac, **common)
+    runs = [("closure", variant, params), ("plain", variant, None)]
+    runs += [(f"v{v}", v, trained[v]["params"]) for v in variants[1:]]
+    for name, v, cp in runs:
+        pc = default_params(gridsize=(n_coarse,) * 3, t_final=T, closure=v, closure_kc_frac=kc_frac, **common)
         ctx = Context(pc)
         if cp is not None:
             ctx.closure_set(cp)
@@ -180,16 +222,23 @@ def run(n_fine=256, n_coarse=64, nu=2e-4, steps=2000, snap_every=250, train_step
     kc = int(np.floor(2.0 / 3.0 * (n_coarse // 2 - 1)))
     Eu_t, Eb_t = shell_spectrum(truth_filtered, pc0)
     out = dict(t_end=T, truth_steps=steps, truth_seconds=truth_s, train_seconds=train_s,
-               loss_initial=loss0, loss_final=loss1, loss_history=np.concatenate([h1, h2]), k_cut=kc,
+               loss_initial=loss0, loss_final=loss1, loss_history=trained[variant]["loss_history"], k_cut=kc,
                spectrum_truth=Eu_t + Eb_t, params=params)
     for name, (U, nst, secs) in res.items():
         Eu, Eb = shell_spectrum(U, pc0)
-        out[f"error_{name}"] = spectral_error(Eu + Eb, Eu_t + Eb_t, 1, kc)
-        out[f"error_u_{name}"] = spectral_error(Eu, Eu_t, 1, kc)
-        out[f"error_b_{name}"] = spectral_error(Eb, Eb_t, 1, kc)
-        out[f"energy_{name}"] = float((Eu + Eb).sum())
-        out[f"seconds_{name}"] = secs
-        out[f"spectrum_{name}"] = Eu + Eb
+        d = {"error": spectral_error(Eu + Eb, Eu_t + Eb_t, 1, kc), "error_u": spectral_error(Eu, Eu_t, 1, kc),
+             "error_b": spectral_error(Eb, Eb_t, 1, kc), "energy": float((Eu + Eb).sum()), "seconds": secs,
+             "spectrum": Eu + Eb, "steps": nst}
+        if name.startswith("v"):
+            v = int(name[1:])
+            d.update({k: trained[v][k] for k in ("loss_initial", "loss_final", "train_seconds")})
+            d["cost_advantage"] = truth_s / max(secs, 1e-9)
+            d["finite"] = bool(np.isfinite(U).all())
+            out[name] = d
+            continue
+        for k, val in d.items():
+            if k != "steps":
+                out[f"{k}_{name}"] = val
     out["energy_truth"] = float((Eu_t + Eb_t).sum())
     out["cost_advantage"] = truth_s / max(out["seconds_closure"], 1e-9)
     return out
