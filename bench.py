@@ -508,7 +508,7 @@ def run_closure(args, world, rank, local_rank):
         "data": "synthetic (seeded config-2 fields)",
         "config": {"workload": f"MHD {nf}^3 truth (plain form, {args.closure_steps} steps, nu = eta = 2e-4) -> "
                                f"{ncs}^3 closure run, sharp filter k_c = {r['k_cut']}",
-                   "train_steps": 3000, "batch": 16384,
+                   "train_steps": {"variant 1/2": 3000, "variant 3": 20000}, "batch": 16384,
                    "closure_variant": names[args.closure_variant],
                    "loss_transfer_weight": transfer},
         "models": models,
@@ -524,6 +524,44 @@ def run_closure(args, world, rank, local_rank):
                               **{f"variant{v}": [float("%.5g" % x) for x in r[f"v{v}"]["spectrum"][: r["k_cut"] + 1]]
                                  for v in extra}),
     }), flush=True)
+
+
+def run_closure_probe(args, world, rank, local_rank):
+    """The closure's fused inference alone, the small case for ncu captures
+    of its z pass: a --n^3 MHD context in the plain form (closure variant
+    --closure-variant, 0: none; fixed dt 1e-3; config-2 fields) with the
+    workflow's initial network (tensor network: output weights at scale 1),
+    W warm-up + K steps timed with CUDA events; one short JSON line with the
+    ms per step and the per-pass times."""
+    import torch
+    import spooky_b200 as S
+    from spooky_b200 import closure as C
+    from spooky_b200.initial import mhd_random_state
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    v, n = args.closure_variant, args.n
+    L = 2 * np.pi
+    p = default_params(gridsize=(n,) * 3, boxsize=(L, L, L), incompressible=1, mhd=1, reynolds=5000.0,
+                       reynolds_magnetic=5000.0, cfl=1.5, form=SPK_FORM_PLAIN, closure=v, t_final=1e30,
+                       toutput_flow=1e30, fixed_dt=1e-3)
+    stream = torch.cuda.Stream()
+    ctx = S.Context(p, stream=stream.cuda_stream)
+    ctx.set_state(mhd_random_state(p, 1, 2))
+    if v == 3:
+        ctx.closure_set(C.init_params3(0, out=1.0))
+    elif v in (1, 2):
+        ctx.closure_set(C.init_params(0))
+    ctx.advance(args.warmup)
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"closure_probe": True, "n": n, "closure_variant": v, "form": "plain",
+                      "ms_per_step": e0.elapsed_time(e1) / args.steps, "steps": args.steps, "warmup": args.warmup,
+                      "passes": ctx.profile_passes(5)}), flush=True)
 
 
 def main():
@@ -548,7 +586,10 @@ def main():
                     help="3 (default): the tensor network, with variant 1 trained and run beside it")
     ap.add_argument("--closure-transfer", type=float, default=None,
                     help="weight of the energy-transfer error in the closure loss (default: 0 variant 1, "
-                         "4 variant 2, 1 variant 3)")
+                         "4 variant 2, 0 variant 3)")
+    ap.add_argument("--closure-probe", action="store_true",
+                    help="the closure's fused inference alone: --n^3 MHD, plain form, --closure-variant network "
+                         "(the small case for ncu captures of its z pass)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")
@@ -568,6 +609,9 @@ def main():
         return
     if args.mti:
         run_mti(args, world, rank, local_rank)
+        return
+    if args.closure_probe:
+        run_closure_probe(args, world, rank, local_rank)
         return
     if args.closure:
         run_closure(args, world, rank, local_rank)
