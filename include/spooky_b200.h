@@ -96,6 +96,14 @@ typedef struct spk_params {
                                variant (HD/MHD; weights from spk_closure_set)                      */
     double closure_kc_frac; /* variant 2: the small scales are |k| > closure_kc_frac * k_c
                                (0: 1/2)                                                            */
+    /* shearing box with rotation (modules.shearing, modules.rotating,
+     * physics.shear, physics.omega; TimeStepping::ShiftTime / RemapField,
+     * Physics::BackgroundShear / BackgroundRotation).  The Coriolis force
+     * acts only when shearing is on too (shear_rotation.cu:47), while the dt
+     * rule counts omega whenever rotating is on (compute_dt.cu:112-118),
+     * both as in the reference. */
+    int    shearing, rotating;
+    double shear, omega;
 } spk_params_t;
 
 /* Fill *p with the reference's defaults (parameters.cu:77-505). */
@@ -224,6 +232,11 @@ int spk_rkl_cycle_fields(spk_ctx* ctx, double* U, int* s_out);
  *                      t_lastvar and i4 step (1 element each) and one f8 dataset of
  *                      NX*NY*NZ values per field, named vx vy vz bx by bz th, the
  *                      real field in C order.  t_save and step are the context's.
+ *                      With the shearing box the fields are first translated
+ *                      along y as InputOutput::UnshearOutput does
+ *                      (src/io/unshear_output.cu: exp(-i ky tvel Lx S / 2),
+ *                      tvel = fmod(t_save, 2 Ly / (S Lx))); reading applies no
+ *                      inverse, as the reference's restart does not.
  * spk_read_snapshot    InputOutput::ReadDataFile's reading part (hdf5_io.cu:159-231):
  *                      sets the state from the file's fields and the time, step
  *                      and t_lastsnap from its scalars; returns t_lastsnap and

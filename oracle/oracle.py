@@ -53,6 +53,8 @@ def lib():
         L.orc_closure_mlp.argtypes = [dp, dp, dp]
         L.orc_closure_loss_grad.argtypes = [dp, ctypes.c_size_t, ctypes.c_size_t, dp, dp, dp, dp]
         L.orc_closure_adam.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_double]
+        L.orc_get_tremap.argtypes = [vp]
+        L.orc_get_tremap.restype = ctypes.c_double
         L.orc_closure_adam_n.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.orc_closure3_set_rounding.argtypes = [ctypes.c_int]
         L.orc_closure3_mlp.argtypes = [dp, dp, dp]
@@ -244,6 +246,10 @@ class Oracle:
         C = np.empty((p.nx, p.ny, p.nz // 2 + 1), dtype=np.complex128)
         lib().orc_r2c(self._h, _dp(R), _dp(C))
         return C
+
+    def tremap(self):
+        """The shearing box's remap clock (TimeStepping::tremap)."""
+        return lib().orc_get_tremap(self._h)
 
     def closure_set(self, params):
         if params is None:

@@ -244,6 +244,9 @@ struct orc_ctx {
     cpx *rdU, *rdU0, *rUc0, *rUc1;
     double t, dt, dt_hyp, dt_par, dt_sts, t_lastsnap;
     int step;
+    /* shearing box: the remap clock and the shear of the wavevector in use,
+     * kx = kx0 + shx ky with shx = shear * (tremap of the stage) */
+    double tremap, shx;
     /* learned closure (spk_closure.c): parameters, Delta^2, the real-space
      * closure terms -2 nu_t S (5) and -eta_t J (3), the gradients A, G (18) */
     int closure_on;
@@ -269,6 +272,8 @@ static void pop_variables(orc_ctx* c) {
         } else if (p->boussinesq) { c->TH = 3; c->F += 1; }
     }
 }
+
+static double shift_time(const spk_params_t* p, double t);
 
 orc_ctx* orc_create(const spk_params_t* p) {
     orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
@@ -339,6 +344,10 @@ orc_ctx* orc_create(const spk_params_t* p) {
     c->t_lastsnap = 0.0;
     c->step = 0;
     c->delta2 = pow(M_PI / c->kxmax * M_PI / c->kymax * M_PI / c->kzmax, 2.0 / 3.0);
+    if (p->shearing) {
+        c->tremap = shift_time(p, c->t);
+        c->shx = p->shear * c->tremap;
+    }
     return c;
 }
 
@@ -353,9 +362,22 @@ void orc_destroy(orc_ctx* c) {
     free(c);
 }
 
+/* the shearing box's remap clock (0 without the module) */
+double orc_get_tremap(const orc_ctx* c) { return c->tremap; }
+
 void orc_set_state(orc_ctx* c, const double* U) { memcpy(c->U, U, sizeof(cpx) * c->g.nc * c->F); }
 void orc_get_state(const orc_ctx* c, double* U) { memcpy(U, c->U, sizeof(cpx) * c->g.nc * c->F); }
-void orc_set_time(orc_ctx* c, double t, int step, double t_lastsnap) { c->t = t; c->step = step; c->t_lastsnap = t_lastsnap; }
+/* With the shearing module a new time restarts the remap clock from it, as
+ * Supervisor::executeMainLoop does before its loop (supervisor.cu:171-175);
+ * the same time keeps the clock. */
+void orc_set_time(orc_ctx* c, double t, int step, double t_lastsnap) {
+    const int restart = t != c->t;
+    c->t = t; c->step = step; c->t_lastsnap = t_lastsnap;
+    if (c->p.shearing && restart) {
+        c->tremap = shift_time(&c->p, t);
+        c->shx = c->p.shear * c->tremap;
+    }
+}
 void orc_get_time(const orc_ctx* c, double* t, double* dt, int* step) {
     if (t) *t = c->t;
     if (dt) *dt = c->dt;
@@ -368,7 +390,7 @@ void orc_kgrid(const orc_ctx* c, double* kvec, double* mask, double* kmax4) {
         for (int j = 0; j < g->ny; j++)
             for (int k = 0; k < g->nzh; k++) {
                 size_t idx = (size_t)k + g->nzh * ((size_t)j + (size_t)i * g->ny);
-                kvec[idx] = c->kx[i];
+                kvec[idx] = c->kx[i] + c->shx * c->ky[j];   /* sheared */
                 kvec[g->nc + idx] = c->ky[j];
                 kvec[2 * g->nc + idx] = c->kz[k];
                 mask[idx] = c->mx[i] * c->my[j] * c->mz[k];
@@ -383,9 +405,11 @@ void orc_kgrid(const orc_ctx* c, double* kvec, double* mask, double* kmax4) {
         for (int j_ = 0; j_ < (c)->g.ny; j_++)                                     \
             for (int k_ = 0; k_ < (c)->g.nzh; k_++)
 
+/* kx is sheared: ShearWavevector (cuda_kernels_generic.cu:362-384), shx = 0
+ * without the shearing module */
 #define MODE_VARS(c)                                                               \
     const size_t id = (size_t)k_ + (c)->g.nzh * ((size_t)j_ + (size_t)i_ * (c)->g.ny); \
-    const double kx = (c)->kx[i_], ky = (c)->ky[j_], kz = (c)->kz[k_];                 \
+    const double kx = (c)->kx[i_] + (c)->shx * (c)->ky[j_], ky = (c)->ky[j_], kz = (c)->kz[k_]; \
     const double mask = (c)->mx[i_] * (c)->my[j_] * (c)->mz[k_];                       \
     (void)kx; (void)ky; (void)kz; (void)mask;
 
@@ -653,6 +677,98 @@ static void grad_pseudo_pressure(orc_ctx* c, cpx* dV) {
     }
 }
 
+/* ---- GradPseudoPressureShearing (src/cuda/cuda_kernels.cu:165-196): the
+ * divergence of dV carries the background shear's S ky vx ------------- */
+static void grad_pseudo_pressure_shearing(orc_ctx* c, cpx* dV, const cpx* Vx) {
+    const size_t nc = c->g.nc;
+    const double S = c->p.shear;
+    FOR_MODES(c) {
+        MODE_VARS(c)
+        cpx d0 = dV[id], d1 = dV[nc + id], d2 = dV[2 * nc + id];
+        cpx div = c_muli(c_add(c_add(c_add(c_scale(S * ky, Vx[id]), c_scale(kx, d0)), c_scale(ky, d1)), c_scale(kz, d2)));
+        double k2 = kx * kx + ky * ky + kz * kz;
+        double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
+        dV[id] = c_add(d0, c_scale(kx * ik2, c_muli(div)));
+        dV[nc + id] = c_add(d1, c_scale(ky * ik2, c_muli(div)));
+        dV[2 * nc + id] = c_add(d2, c_scale(kz * ik2, c_muli(div)));
+    }
+}
+
+/* ---- Physics::BackgroundShear / BackgroundRotation
+ * (src/physics/shear_rotation.cu:11-63; ShearingFlow and CoriolisForce,
+ * cuda_kernels.cu:332-355): dvy += S vx, dBy -= S Bx; with rotation (gated
+ * on shearing as in the reference) dvx += 2 omega vy, dvy -= 2 omega vx. */
+static void shear_rotation(orc_ctx* c, const cpx* U, cpx* dU) {
+    const size_t nc = c->g.nc;
+    const double S = c->p.shear, Om = c->p.omega;
+    const cpx *vx = U + (size_t)c->VX * nc, *vy = U + (size_t)c->VY * nc;
+    cpx *dvx = dU + (size_t)c->VX * nc, *dvy = dU + (size_t)c->VY * nc;
+    #pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nc; i++) dvy[i] = c_add(dvy[i], c_scale(S, vx[i]));
+    if (c->p.mhd) {
+        const cpx* bx = U + (size_t)c->BX * nc;
+        cpx* dby = dU + (size_t)c->BY * nc;
+        #pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)nc; i++) dby[i] = c_add(dby[i], c_scale(-S, bx[i]));
+    }
+    if (c->p.rotating) {
+        #pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)nc; i++) {
+            dvx[i] = c_add(dvx[i], c_scale(2.0 * Om, vy[i]));
+            dvy[i] = c_sub(dvy[i], c_scale(2.0 * Om, vx[i]));
+        }
+    }
+}
+
+/* ---- TimeStepping::ShiftTime (src/timestepping/shearing_remapping.cu:15-25) */
+static double shift_time(const spk_params_t* p, double t) {
+    const double h = p->ly / (2.0 * p->shear * p->lx);
+    return fmod(t + h, p->ly / (p->shear * p->lx)) - h;
+}
+
+/* ---- TimeStepping::RemapField (shearing_remapping.cu:27-46):
+ * RemapComplexVec (cuda_kernels_generic.cu:386-412) moves mode (nx, ny) to
+ * nx + ny when that lies strictly inside (-NX/2, NX/2), zero elsewhere;
+ * MaskVector (:414-423) then applies the 2/3 mask. */
+static void remap_fields(orc_ctx* c) {
+    const int NX = c->g.nx, NY = c->g.ny, nzh = c->g.nzh;
+    cpx* R = c->tmp;
+    for (int f = 0; f < c->F; f++) {
+        cpx* X = c->U + (size_t)f * c->g.nc;
+        memset(R, 0, sizeof(cpx) * c->g.nc);
+        for (int i = 0; i < NX; i++)
+            for (int j = 0; j < NY; j++) {
+                const int nx = (int)fmod((double)i + (NX / 2), (double)NX) - NX / 2;
+                const int ny = (int)fmod((double)j + (NY / 2), (double)NY) - NY / 2;
+                int nt = nx + ny;
+                if (nt > -NX / 2 && nt < NX / 2) {
+                    if (nt < 0) nt += NX;
+                    for (int k = 0; k < nzh; k++)
+                        R[(size_t)k + (size_t)nzh * ((size_t)j + (size_t)NY * nt)] =
+                            X[(size_t)k + (size_t)nzh * ((size_t)j + (size_t)NY * i)];
+                }
+            }
+        FOR_MODES(c) {
+            MODE_VARS(c)
+            X[id] = c_scale(mask, R[id]);
+        }
+    }
+}
+
+/* End of a step with the shearing module (hydro_mhd_advance.cu:167-180):
+ * the remap clock advances by dt; past half a shear period it restarts
+ * from the time and the fields are remapped; the wavevector follows. */
+static void shear_end_of_step(orc_ctx* c) {
+    const spk_params_t* p = &c->p;
+    if (!p->shearing) return;
+    c->tremap += c->dt;
+    if (c->tremap > p->ly / (2.0 * p->shear * p->lx)) {
+        c->tremap = shift_time(p, c->t);
+        remap_fields(c);
+    }
+    c->shx = p->shear * c->tremap;
+}
+
 /* ---- CleanDivergence (src/cuda/cuda_kernels_generic.cu:288-313) -------- */
 static void clean_vec(orc_ctx* c, cpx* X) {
     const size_t nc = c->g.nc;
@@ -686,6 +802,7 @@ static void compute_dfield(orc_ctx* c, const cpx* U, const double* rb, cpx* dU) 
         if (p->mhd) curl_emf(c, rb, dU + (size_t)c->MAG * nc);
         if (p->boussinesq) advect_temperature(c, rb, dU + (size_t)c->TH * nc);
         if (p->stratification) entropy_stratification(c, U, dU);
+        if (p->shearing) shear_rotation(c, U, dU);
         for (int i = 0; i < 3; i++)
             if (c->sts_pos[c->VEL + i] < 0)
                 nabla_op_scalar(c, U + (size_t)(c->VEL + i) * nc, dU + (size_t)(c->VEL + i) * nc, p->nu, 1);
@@ -697,7 +814,8 @@ static void compute_dfield(orc_ctx* c, const cpx* U, const double* rb, cpx* dU) 
             if (p->anisotropic_diffusion) anisotropic_heat_flux(c, U, rb, dU + (size_t)c->TH * nc);
             else nabla_op_scalar(c, U + (size_t)c->TH * nc, dU + (size_t)c->TH * nc, p->nu_th, 1);
         }
-        grad_pseudo_pressure(c, dU + (size_t)c->VEL * nc);
+        if (p->shearing) grad_pseudo_pressure_shearing(c, dU + (size_t)c->VEL * nc, U + (size_t)c->VX * nc);
+        else grad_pseudo_pressure(c, dU + (size_t)c->VEL * nc);
     } else if (p->heat_equation) {
         if (c->sts_pos[c->TH] < 0)
             nabla_op_scalar(c, U + (size_t)c->TH * nc, dU + (size_t)c->TH * nc, p->nu_th, 0);
@@ -723,8 +841,9 @@ static double max_abs(const double* a, size_t n) {
     return m;
 }
 
-/* ---- TimeStepping::compute_dt (src/timestepping/compute_dt.cu:15-309);
- * shearing/rotation terms (tremap, omega, shear) are zero here.  The maxima
+/* ---- TimeStepping::compute_dt (src/timestepping/compute_dt.cu:15-309),
+ * with the shearing box's |tremap| ky_max on the x rates and the rotation
+ * and shear rates over safety_source (:110-121, 158, 171, 216-220).  The maxima
  * run over the NX*NY*NZ real points (the reference's Idamax also scans the
  * two pad slots of each padded pencil, compute_dt.cu:90-95). */
 static void compute_dt(orc_ctx* c) {
@@ -747,8 +866,11 @@ static void compute_dt(orc_ctx* c) {
         double maxfx = max_abs(rb + (size_t)c->VX * nr, nr);
         double maxfy = max_abs(rb + (size_t)c->VY * nr, nr);
         double maxfz = max_abs(rb + (size_t)c->VZ * nr, nr);
-        gamma_v = ((kxmax + 0.0 * kymax) * maxfx + kymax * maxfy + kzmax * maxfz);
-        gamma_tmp = (kxmax) * (kxmax) * p->nu;
+        const double kxs = kxmax + fabs(c->tremap) * kymax;
+        gamma_v = (kxs * maxfx + kymax * maxfy + kzmax * maxfz);
+        if (p->rotating) gamma_v += fabs(p->omega) / p->safety_source;
+        if (p->shearing) gamma_v += fabs(p->shear) / p->safety_source;
+        gamma_tmp = kxs * kxs * p->nu;
         if (c->sts_pos[c->VX] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         gamma_tmp = kymax * kymax * p->nu;
         if (c->sts_pos[c->VY] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
@@ -758,9 +880,9 @@ static void compute_dt(orc_ctx* c) {
             gamma_th += pow(fabs(p->N2), 0.5) / p->safety_source;
             if (p->anisotropic_diffusion) {
                 gamma_th += pow(fabs(p->OmegaT2), 0.5) / p->safety_source;
-                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * (1. / p->reynolds_ani);
+                gamma_tmp = (kxs * kxs + kymax * kymax + kzmax * kzmax) * (1. / p->reynolds_ani);
             } else {
-                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * p->nu_th;
+                gamma_tmp = (kxs * kxs + kymax * kymax + kzmax * kzmax) * p->nu_th;
             }
             if (c->sts_pos[c->TH] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         }
@@ -768,8 +890,8 @@ static void compute_dt(orc_ctx* c) {
             double maxbx = max_abs(rb + (size_t)c->BX * nr, nr);
             double maxby = max_abs(rb + (size_t)c->BY * nr, nr);
             double maxbz = max_abs(rb + (size_t)c->BZ * nr, nr);
-            gamma_b = (kxmax) * maxbx + kymax * maxby + kzmax * maxbz;
-            gamma_tmp = (kxmax) * (kxmax) * p->nu_m;
+            gamma_b = kxs * maxbx + kymax * maxby + kzmax * maxbz;
+            gamma_tmp = kxs * kxs * p->nu_m;
             if (c->sts_pos[c->BX] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
             gamma_tmp = kymax * kymax * p->nu_m;
             if (c->sts_pos[c->BY] < 0) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
@@ -1026,17 +1148,21 @@ static void runge_kutta3(orc_ctx* c) {
     const double dt = c->dt;
     cpx *U = c->U, *dU = c->dU, *S = c->S;
     /* stage 1: real buffer from compute_dt */
+    const int sh = c->p.shearing;
     compute_dfield(c, U, c->realbuf, dU);
     axpy(U, dU, U, 1.0, gammaRK[0] * dt, n);
     axpy(U, dU, S, 1.0, xiRK[0] * dt, n);
     if (c->p.incompressible) complex2real(c, U, c->realbuf, c->F);
+    if (sh) c->shx = c->p.shear * (c->tremap + gammaRK[0] * dt);
     compute_dfield(c, U, c->realbuf, dU);
     axpy(S, dU, U, 1.0, gammaRK[1] * dt, n);
     axpy(U, dU, S, 1.0, xiRK[1] * dt, n);
     if (c->p.incompressible) complex2real(c, U, c->realbuf, c->F);
+    if (sh) c->shx = c->p.shear * (c->tremap + (gammaRK[0] + xiRK[0] + gammaRK[1]) * dt);
     compute_dfield(c, U, c->realbuf, dU);
     axpy(S, dU, U, 1.0, gammaRK[2] * dt, n);
     c->t += c->dt;
+    shear_end_of_step(c);
 }
 
 /* ---- TimeStepping::ForwardEuler (hydro_mhd_advance.cu:191-248) -------- */
@@ -1045,6 +1171,7 @@ static void forward_euler(orc_ctx* c) {
     compute_dfield(c, c->U, c->realbuf, c->dU);
     axpy(c->U, c->dU, c->U, 1.0, c->dt, n);
     c->t += c->dt;
+    shear_end_of_step(c);
 }
 
 /* ---- one main-loop iteration: Supervisor::executeMainLoop body

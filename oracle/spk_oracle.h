@@ -29,6 +29,7 @@ size_t   orc_ncomplex(const orc_ctx* c);
 void orc_set_state(orc_ctx* c, const double* U);     /* [F][Nc] complex */
 void orc_get_state(const orc_ctx* c, double* U);
 void orc_set_time(orc_ctx* c, double t, int step, double t_lastsnap);
+double orc_get_tremap(const orc_ctx* c);
 void orc_get_time(const orc_ctx* c, double* t, double* dt, int* step);
 
 /* k tables: kvec[3][Nc] and mask[Nc], plus kxmax, kymax, kzmax, kmax. */

@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -69,6 +70,7 @@ struct spk_ctx {
     int* d_keep = nullptr;
     int nkx = 0, nky = 0;
     bool trim_now = false;         // recording a step: the inverse passes may trim (DevScalars::masked_live)
+    double stage_csh = 0.0;        // shearing box: the recorded RK stage's offset of the remap clock, in dt
     // schedule knobs picked by spk_autotune (0: the launchers' own choice)
     int tune_zl = 0;               // z pass: lines per CTA
     int tune_nst = 0;              // axis passes: pipeline stages
@@ -219,6 +221,7 @@ static AxisArgs axis_args(spk_ctx* c, int ax) {
     AxisArgs a;
     memset(&a, 0, sizeof(a));
     a.g = c->g;
+    a.g.csh = c->stage_csh;
     a.plan = ax == 0 ? c->plan_x : c->plan_y;
     a.axis = ax;
     a.kcols = c->nzh;
@@ -708,6 +711,7 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     XfArgs x;
     memset(&x, 0, sizeof(x));
     x.g = c->g;
+    x.g.csh = c->stage_csh;
     x.plan = c->plan_x;
     x.nl = c->bufA; x.cs_nl = c->g.ncs;   // products after the x-forward pass
     x.fd_ny = FastDiv::make((unsigned)c->ny);
@@ -725,6 +729,7 @@ static XfArgs xf_args(spk_ctx* c, double2* U, int mode, bool clean) {
     x.nu = c->p.nu; x.nu_m = c->p.nu_m; x.nu_th = c->p.nu_th; x.N2 = c->p.N2;
     x.mode = mode; x.clean = clean ? 1 : 0;
     x.sc = c->sc;
+    x.rotating = c->p.rotating; x.omega = c->p.omega;
     x.defer = c->defer && c->d_keep && (mode == XM_RK0 || mode == XM_RK1 || mode == XM_RK2);
     if (x.defer) {
         x.kxi = c->d_keep; x.kyi = c->d_keep + c->nkx;
@@ -752,6 +757,7 @@ static DtArgs dt_args(spk_ctx* c, bool advance) {
     d.rkl_smax = c->rkl_smax;
     d.sts_alg = p.sts_algorithm;
     d.closure = c->closure_on ? 1 : 0;
+    d.shearing = p.shearing; d.rotating = p.rotating; d.shear = p.shear; d.omega = p.omega;
     return d;
 }
 
@@ -853,6 +859,7 @@ static void record_breal(spk_ctx* c) {
 // already in the device scalars: no dt reduction, no super-time-stepping,
 // no divergence cleaning of the result.
 static void record_step_body(spk_ctx* c, int parity, bool rk_only = false);
+static void launch_clean(spk_ctx* c);
 // The inverse passes of a recorded step trim the work of masked modes when
 // the state has none (the flag is refreshed whenever a state is set).
 struct TrimScope {   // trimming on for one recording or profiling, off again on every exit
@@ -886,12 +893,24 @@ static void record_step_body(spk_ctx* c, int parity, bool rk_only) {
         if (sts_after) record_rkl_cycle(c);
         return;
     }
+    const bool shear = p.shearing != 0;
     if (!rk_only) {
+        if (shear) {
+            // CleanFieldDivergence at the start of the step (supervisor.cu:184),
+            // with the wavevector of the possibly remapped state: with the
+            // shearing box it is not fused into the previous step's last stage
+            launch_clean(c);
+            c->launches += p.mhd ? 2 : 1;
+        }
         k_reset_max<<<c->nb, 32, 0, c->stream>>>(c->sc);
         c->launches++;
     }
+    // shearing box: stage s uses the wavevector at tremap + csh[s] dt
+    // (hydro_mhd_advance.cu:129-131, 148-150)
+    const double csh[3] = {0.0, 8.0 / 15.0, 8.0 / 15.0 + -17.0 / 60.0 + 5.0 / 12.0};
     for (int s = 0; s < nst; s++) {
         const bool first = s == 0 && !rk_only;
+        c->stage_csh = (shear && !euler) ? csh[s] : 0.0;
         pass_x_inverse(c, c->U, true, euler ? 0 : s);
         pass_y_inverse(c, true);
         if (first) {
@@ -913,13 +932,29 @@ static void record_step_body(spk_ctx* c, int parity, bool rk_only) {
         }
         pass_y_forward(c, c->nout, c->bufA, c->bufB);
         // the last stage cleans the new u and B: CleanFieldDivergence of the next step
-        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, s == nst - 1 && !rk_only);
+        XfArgs x = xf_args(c, c->U, euler ? XM_EULER : s, s == nst - 1 && !rk_only && !shear);
         xfwd(c, x);
+    }
+    c->stage_csh = 0.0;
+    if (shear) {
+        // the remap clock, then RemapAllFields when it passed half a period
+        k_shear_end<<<1, 32, 0, c->stream>>>(c->sc, p.lx, p.ly, p.shear);
+        const long items = (long)c->F * c->ny * ((c->nzh + SPK_REMAP_KC - 1) / SPK_REMAP_KC);
+        const int grid = (int)std::min<long>(items, (long)c->num_sms * 8);
+        k_remap<<<grid, 256, sizeof(double2) * (size_t)c->nx * SPK_REMAP_KC, c->stream>>>(c->g, c->U, c->F, c->sc);
+        c->launches += 2;
     }
     if (sts_after) {
         if (c->sts_aniso) record_breal(c);
         record_rkl_cycle(c);
     }
+}
+
+// TimeStepping::ShiftTime (src/timestepping/shearing_remapping.cu:15-25):
+// the remap clock of time t
+static double shift_time(const spk_params_t& p, double t) {
+    const double h = p.ly / (2.0 * p.shear * p.lx);
+    return fmod(t + h, p.ly / (p.shear * p.lx)) - h;
 }
 
 // ---------------------------------------------------------------------------
@@ -965,6 +1000,12 @@ static int check_params(const spk_params_t* p, std::string& why) {
     if (!(p->closure_kc_frac >= 0.0 && p->closure_kc_frac < 1.0)) { why = "closure_kc_frac must be in [0, 1)"; return SPK_ERR_ARG; }
     if (p->closure && (!p->incompressible || p->boussinesq)) { why = "the learned closure covers the HD and MHD modules"; return SPK_ERR_UNSUPPORTED; }
     if (p->closure && p->supertimestepping) { why = "the learned closure with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
+    if (p->shearing) {
+        if (!p->incompressible) { why = "the shearing box needs the incompressible module"; return SPK_ERR_UNSUPPORTED; }
+        if (!(p->shear != 0.0) || !std::isfinite(p->shear)) { why = "shearing needs a finite, nonzero shear"; return SPK_ERR_ARG; }
+        if (p->supertimestepping) { why = "the shearing box with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
+        if (p->closure) { why = "the shearing box with the learned closure is not supported"; return SPK_ERR_UNSUPPORTED; }
+    }
     return SPK_OK;
 }
 
@@ -983,6 +1024,8 @@ static int params_from_config(const spkcfg::Setting& root, spk_params_t* p) {
     get_bool(root, "modules.mhd", &p->mhd);
     get_bool(root, "modules.anisotropic_diffusion", &p->anisotropic_diffusion);
     get_bool(root, "modules.supertimestepping", &p->supertimestepping);
+    get_bool(root, "modules.shearing", &p->shearing);
+    get_bool(root, "modules.rotating", &p->rotating);
     // sts_algorithm / sts_variables (:111-156): read only with supertimestepping;
     // no (or an empty) variable list switches it off
     std::vector<std::string> sts_vars;
@@ -1015,6 +1058,8 @@ static int params_from_config(const spkcfg::Setting& root, spk_params_t* p) {
     get_float(root, "physics.reynolds_anisotropic", &p->reynolds_ani);
     get_float(root, "physics.brunt_vaissala_squared", &p->N2);
     get_float(root, "physics.mti_frequency_squared", &p->OmegaT2);
+    get_float(root, "physics.omega", &p->omega);
+    get_float(root, "physics.shear", &p->shear);
     get_float(root, "code.cfl", &p->cfl);
     get_float(root, "code.cfl_par", &p->cfl_par);
     get_float(root, "code.cfl_sts", &p->cfl_sts);
@@ -1036,6 +1081,14 @@ static int params_from_config(const spkcfg::Setting& root, spk_params_t* p) {
     for (const std::string& v : sts_vars)
         for (size_t f = 0; f < names.size(); f++)
             if (names[f] == v) p->sts_vars_mask |= 1u << f;
+    // with shearing, snapshots only where the box is exactly periodic
+    // (parameters.cu:551-562, its arithmetic kept: a step above one period
+    // becomes the whole number of periods it holds, not their length)
+    if (p->shearing) {
+        const double tperiodic = p->ly / (p->shear * p->lx);
+        if (p->toutput_flow < tperiodic) p->toutput_flow = tperiodic;
+        else p->toutput_flow = (double)(int)(p->toutput_flow / tperiodic);
+    }
     std::string why;
     const int rc = check_params(p, why);
     if (rc == SPK_ERR_CONFIG) return fail(nullptr, rc, why);
@@ -1232,8 +1285,10 @@ static int ctx_init(spk_ctx* c, const spk_params_t* pin, void* stream) {
         c->deltak = 2.0 * M_PI / lmin;
         c->nbins = (int)(c->kmax / c->deltak + 0.5);
     }
+    // (the shearing box's source terms and sheared projection act on masked
+    // modes too: no deferral)
     c->defer = p.incompressible && !p.boussinesq && c->sts_mask == 0 && p.integrator == SPK_INT_RK3 &&
-               c->nkx > 0 && c->nky > 0 && c->kz_keep > 0;
+               c->nkx > 0 && c->nky > 0 && c->kz_keep > 0 && !p.shearing;
     int oc = 0;
     c->out_T = c->out_E = c->out_F = c->out_Q = -1;
     if (p.incompressible) { c->out_T = oc; oc += 5; }
@@ -1343,8 +1398,13 @@ static int ctx_alloc(spk_ctx* c) {
         c->h_sc[b].nu_m = c->bnu_m.empty() ? c->p.nu_m : c->bnu_m[b];
         c->h_sc[b].nu_th = c->bnu_th.empty() ? c->p.nu_th : c->bnu_th[b];
         c->h_sc[b].masked_live = 1;
+        // the main loop starts the remap clock from the time (supervisor.cu:171-175)
+        c->h_sc[b].tremap = c->p.shearing ? shift_time(c->p, c->p.t_initial) : 0.0;
     }
     CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars) * nb, cudaMemcpyHostToDevice));
+    c->g.shear = c->p.shearing ? c->p.shear : 0.0;
+    c->g.csh = 0.0;
+    c->g.shsc = c->sc;
     CK(cudaMalloc(&c->d_sums, sizeof(double) * 16));
     CK(cudaMallocHost(&c->h_sums, sizeof(double) * 16));
     if (c->p.closure) {
@@ -1451,6 +1511,9 @@ extern "C" int spk_set_time(spk_ctx* c, double t, int step, double t_lastsnap) {
     if (!c) return SPK_ERR_ARG;
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaMemcpy(c->h_sc, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
+    // a new time restarts the remap clock from it (executeMainLoop's ShiftTime
+    // after a restart, supervisor.cu:171-175); the same time keeps the clock
+    if (c->p.shearing && t != c->h_sc->t) c->h_sc->tremap = shift_time(c->p, t);
     c->h_sc->t = t; c->h_sc->step = step; c->h_sc->t_lastsnap = t_lastsnap;
     CK(cudaMemcpy(c->sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice));
     c->h_step = step;
@@ -1828,6 +1891,9 @@ extern "C" int spk_ensemble_create(const spk_params_t* boxes, int nbox, void* cu
         const spk_params_t& p = boxes[i];
         if (p.closure)
             return ens_fail("ensemble box " + std::to_string(i) + ": the learned closure is not supported in ensembles",
+                            SPK_ERR_UNSUPPORTED);
+        if (p.shearing)
+            return ens_fail("ensemble box " + std::to_string(i) + ": the shearing box is not supported in ensembles",
                             SPK_ERR_UNSUPPORTED);
         if (p.supertimestepping && !p.sts_every_step)
             return ens_fail("ensemble box " + std::to_string(i) +
@@ -2207,6 +2273,9 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
     if (p->closure)
         return fail(nullptr, SPK_ERR_UNSUPPORTED,
                     "spk_compute_dfield_noalloc has no learned-closure parameters: set closure = 0");
+    if (p->shearing)
+        return fail(nullptr, SPK_ERR_UNSUPPORTED,
+                    "spk_compute_dfield_noalloc keeps no remap clock: the shearing box needs a context");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SPK_NOALLOC_MAX_DEVICES)
         return fail(nullptr, SPK_ERR_CUDA, "no usable current device");
@@ -2262,6 +2331,7 @@ extern "C" int spk_compute_dfield_noalloc(const spk_params_t* p, const double* U
     c->d_tab = t;
     c->g.kx = t; c->g.ky = t + c->nx; c->g.kz = t + c->nx + c->ny;
     c->g.mx = m; c->g.my = m + c->nx; c->g.mz = m + c->nx + c->ny;
+    c->g.shear = 0.0; c->g.csh = 0.0; c->g.shsc = nullptr;
     c->d_tw = base + o_tw;
     c->sc = (DevScalars*)(base + o_sc);
     c->bufA = c->p.incompressible ? base + o_bufA : nullptr;

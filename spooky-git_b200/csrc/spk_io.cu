@@ -104,11 +104,36 @@ static void xy_dft(spk_ctx* c, double2* A, double sign) {
     c->launches += 2;
 }
 
-extern "C" int spk_get_state_real(spk_ctx* c, double* R, int where) {
+// UnshearComplexVec (cuda_kernels_generic.cu:425-439): every mode times
+// exp(-i ky prefactor / 2), a translation along y
+__global__ void k_unshear(DevGrid g, double2* X, int F, double prefactor) {
+    const size_t n = g.nc * (size_t)F;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t gi = q % g.nc;
+        const int j = (int)((gi / g.nzh) % g.ny);
+        const double ky = g.ky[j];
+        const double cr = cos(-0.5 * ky * prefactor), ci = sin(-0.5 * ky * prefactor);
+        const double2 v = X[q];
+        X[q] = make_double2(v.x * cr - v.y * ci, v.x * ci + v.y * cr);
+    }
+}
+
+// The real fields of the state into R (host or device); with the shearing
+// box and unshear set, first InputOutput::UnshearOutput's translation at
+// time t (unshear_output.cu: tvelocity = fmod(t, 2 Ly / (S Lx)), prefactor
+// tvelocity Lx S), as the snapshots hold them.
+static int state_real_out(spk_ctx* c, double* R, int where, bool unshear, double t) {
     if (!c || !R) return SPK_ERR_ARG;
     if (c->nb != 1) return fail(c, SPK_ERR_UNSUPPORTED, "spk_get_state_real acts on single-box contexts");
     const long lines = (long)c->F * c->nx * c->ny;
     CK(cudaMemcpyAsync(c->S, c->U, sizeof(double2) * c->nc * c->F, cudaMemcpyDeviceToDevice, c->stream));
+    if (unshear && c->p.shearing) {
+        const spk_params_t& p = c->p;
+        const double tvel = fmod(t, 2.0 * p.ly / (p.shear * p.lx));
+        k_unshear<<<io_grid((long)(c->nc * c->F / 256 + 1)), 256, 0, c->stream>>>(c->g, c->S, c->F,
+                                                                                    tvel * p.lx * p.shear);
+        c->launches++;
+    }
     xy_dft(c, c->S, +1.0);
     k_z_c2r<<<io_grid(lines), 128, sizeof(double2) * 2 * c->nz, c->stream>>>(
         c->S, lines, c->nz, c->nzh, 1.0 / ((double)c->nx * c->ny * c->nz));
@@ -120,6 +145,8 @@ extern "C" int spk_get_state_real(spk_ctx* c, double* R, int where) {
     if (where) CK(cudaStreamSynchronize(c->stream));
     return SPK_OK;
 }
+
+extern "C" int spk_get_state_real(spk_ctx* c, double* R, int where) { return state_real_out(c, R, where, false, 0.0); }
 
 extern "C" int spk_set_state_real(spk_ctx* c, const double* R, int where) {
     if (!c || !R) return SPK_ERR_ARG;
@@ -198,7 +225,7 @@ extern "C" int spk_write_snapshot(spk_ctx* c, const char* path, double t_start, 
     const double t_save = c->h_sc->t;
     const int32_t step = c->h_sc->step;
     std::vector<double> R((size_t)c->F * c->nr);
-    rc = spk_get_state_real(c, R.data(), 1);
+    rc = state_real_out(c, R.data(), 1, true, t_save);
     if (rc) return rc;
     std::vector<spk_h5_dataset_t> ds;
     ds.push_back({"t_start", SPK_H5_F64, 1, &t_start});
@@ -253,12 +280,13 @@ __global__ void k_quadratics(DevGrid g, const double2* U, int VEL, int MAG, int 
                              int have_th, double* sums) {
     const size_t nc = g.nc;
     const int nzl = (g.nz % 2 == 0) ? g.nz / 2 : -1;
+    const double shx = grid_shx(g);
     double s[7] = {0, 0, 0, 0, 0, 0, 0};
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const int k = (int)(gi % g.nzh);
         const size_t r = gi / g.nzh;
         const int j = (int)(r % g.ny), i = (int)(r / g.ny);
-        const double kx = g.kx[i], ky = g.ky[j], kz = g.kz[k];
+        const double kx = g.kx[i] + shx * g.ky[j], ky = g.ky[j], kz = g.kz[k];
         const double k2 = kx * kx + ky * ky + kz * kz;
         const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
         const double we = k > 0 ? 2.0 : 1.0;

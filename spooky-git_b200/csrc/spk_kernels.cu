@@ -121,13 +121,14 @@ __global__ void k_heat(const __grid_constant__ XfArgs a) {
 // V: the vector field of box 0; box b's copy starts box_stride elements later.
 __global__ void k_clean(DevGrid g, double2* V0, size_t box_stride, int nb) {
     const size_t nc = g.nc;
+    const double shx = grid_shx(g);
     for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < nc * nb; gb += (size_t)gridDim.x * blockDim.x) {
         const size_t box = gb / nc, gi = gb - box * nc;
         double2* V = V0 + box * box_stride;
         const int k = (int)(gi % g.nzh);
         const size_t r = gi / g.nzh;
         const int j = (int)(r % g.ny), i = (int)(r / g.ny);
-        const double kx = g.kx[i], ky = g.ky[j], kz = g.kz[k];
+        const double kx = g.kx[i] + shx * g.ky[j], ky = g.ky[j], kz = g.kz[k];
         double2 X[3] = {V[gi], V[nc + gi], V[2 * nc + gi]};
         const double k2 = kx * kx + ky * ky + kz * kz;
         const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
@@ -197,6 +198,7 @@ __global__ void k_spectrum(DevGrid g, const double2* U1, const double2* U2, int 
     __syncthreads();
     const size_t nc = g.nc;
     const int nzl = g.nz / 2;   // Nyquist plane index
+    const double shx = grid_shx(g);
     double tot = 0.0;
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const int k = (int)(gi % g.nzh);
@@ -206,7 +208,7 @@ __global__ void k_spectrum(DevGrid g, const double2* U1, const double2* U2, int 
         const double pr = (a.x * inv_n) * (b.x * inv_n) + (a.y * inv_n) * (b.y * inv_n);
         const double p = k > 0 ? 2.0 * pr : pr;
         tot += (k > 0 && k != nzl) ? 2.0 * pr : pr;
-        const double kx = g.kx[i], ky = g.ky[j], kz = g.kz[k];
+        const double kx = g.kx[i] + shx * g.ky[j], ky = g.ky[j], kz = g.kz[k];
         const int m = (int)(sqrt(kx * kx + ky * ky + kz * kz) / dk + 0.5);
         if (m < nbins) atomicAdd(&hist[m], p);
     }
@@ -244,8 +246,12 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
         const double maxfx = __longlong_as_double((long long)sc->maxbits[0]);
         const double maxfy = __longlong_as_double((long long)sc->maxbits[1]);
         const double maxfz = __longlong_as_double((long long)sc->maxbits[2]);
-        gamma_v = ((kxmax + 0.0 * kymax) * maxfx + kymax * maxfy + kzmax * maxfz);
-        gamma_tmp = (kxmax) * (kxmax) * nu;
+        // x rates with the shearing box's |tremap| ky_max (0 without it)
+        const double kxs = kxmax + fabs(sc->tremap) * kymax;
+        gamma_v = (kxs * maxfx + kymax * maxfy + kzmax * maxfz);
+        if (a.rotating) gamma_v += fabs(a.omega) / a.safety_source;
+        if (a.shearing) gamma_v += fabs(a.shear) / a.safety_source;
+        gamma_tmp = kxs * kxs * nu;
         if (!in_sts(a.VX)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         gamma_tmp = kymax * kymax * nu;
         if (!in_sts(a.VY)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
@@ -255,9 +261,9 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
             gamma_th += sqrt(fabs(a.N2)) / a.safety_source;
             if (a.aniso) {
                 gamma_th += sqrt(fabs(a.OmegaT2)) / a.safety_source;
-                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * (1. / a.reynolds_ani);
+                gamma_tmp = (kxs * kxs + kymax * kymax + kzmax * kzmax) * (1. / a.reynolds_ani);
             } else {
-                gamma_tmp = ((kxmax) * (kxmax) + kymax * kymax + kzmax * kzmax) * nu_th;
+                gamma_tmp = (kxs * kxs + kymax * kymax + kzmax * kzmax) * nu_th;
             }
             if (!in_sts(a.TH)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
         }
@@ -265,8 +271,8 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
             const double maxbx = __longlong_as_double((long long)sc->maxbits[3]);
             const double maxby = __longlong_as_double((long long)sc->maxbits[4]);
             const double maxbz = __longlong_as_double((long long)sc->maxbits[5]);
-            gamma_b = (kxmax) * maxbx + kymax * maxby + kzmax * maxbz;
-            gamma_tmp = (kxmax) * (kxmax) * nu_m;
+            gamma_b = kxs * maxbx + kymax * maxby + kzmax * maxbz;
+            gamma_tmp = kxs * kxs * nu_m;
             if (!in_sts(a.BX)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
             gamma_tmp = kymax * kymax * nu_m;
             if (!in_sts(a.BY)) gamma_par += gamma_tmp; else gamma_sts += gamma_tmp;
@@ -364,6 +370,68 @@ __global__ void k_dt(const __grid_constant__ DtArgs a, DevScalars* scs) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Shearing box, end of a step (hydro_mhd_advance.cu:167-180): the remap
+// clock advances by dt; past half a shear period it restarts from the new
+// time (ShiftTime, shearing_remapping.cu:15-25) and the fields are remapped.
+// ---------------------------------------------------------------------------
+__global__ void k_shear_end(DevScalars* sc, double lx, double ly, double shear) {
+    if (threadIdx.x != 0) return;
+    double tr = sc->tremap + sc->dt;
+    int remap = 0;
+    if (tr > ly / (2.0 * shear * lx)) {
+        tr = fmod(sc->t + ly / (2.0 * shear * lx), ly / (shear * lx)) - ly / (2.0 * shear * lx);
+        remap = 1;
+    }
+    sc->tremap = tr;
+    sc->remap = remap;
+}
+
+// RemapField (shearing_remapping.cu:27-46) of every field when the step
+// remapped: mode (nx, ny) moves to nx + ny when that lies strictly inside
+// (-NX/2, NX/2) (RemapComplexVec, cuda_kernels_generic.cu:386-412), every
+// other destination is zero, then the 2/3 mask (MaskVector, :414-423).  A
+// work item is one (field, y index, pair of kz columns): its x columns go to
+// shared memory, then back gathered (destination nt takes source nt - ny),
+// in place.
+#define SPK_REMAP_KC 2
+__global__ void k_remap(DevGrid g, double2* U, int F, const DevScalars* sc) {
+    if (!sc->remap) return;
+    extern __shared__ double2 col[];   // [nx][SPK_REMAP_KC]
+    const int nx = g.nx, ny = g.ny, nzh = g.nzh;
+    const int ngk = (nzh + SPK_REMAP_KC - 1) / SPK_REMAP_KC;
+    const long items = (long)F * ny * ngk;
+    const int lo = -(nx / 2), hi = nx - 1 - nx / 2;   // signed x indices
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int kg = (int)(it % ngk);
+        const long r = it / ngk;
+        const int j = (int)(r % ny), f = (int)(r / ny);
+        const int k0 = kg * SPK_REMAP_KC;
+        double2* X = U + (size_t)f * g.nc;
+        __syncthreads();   // the previous item's writes have read the columns
+        for (int e = threadIdx.x; e < nx * SPK_REMAP_KC; e += blockDim.x) {
+            const int i = e / SPK_REMAP_KC, k = k0 + e % SPK_REMAP_KC;
+            if (k < nzh) col[e] = X[(size_t)k + (size_t)nzh * ((size_t)j + (size_t)ny * i)];
+        }
+        __syncthreads();
+        const int nyv = (int)fmod((double)j + (ny / 2), (double)ny) - ny / 2;
+        for (int e = threadIdx.x; e < nx * SPK_REMAP_KC; e += blockDim.x) {
+            const int i = e / SPK_REMAP_KC, kk = e % SPK_REMAP_KC, k = k0 + kk;
+            if (k >= nzh) continue;
+            const int nt = (int)fmod((double)i + (nx / 2), (double)nx) - nx / 2;
+            const int ns = nt - nyv;
+            double2 v = make_double2(0.0, 0.0);
+            if (nt > -(nx / 2) && nt < nx / 2 && ns >= lo && ns <= hi) {
+                const int is = ns < 0 ? ns + nx : ns;
+                const double m = g.mx[i] * g.my[j] * g.mz[k];
+                const double2 s = col[is * SPK_REMAP_KC + kk];
+                v = make_double2(s.x * m, s.y * m);
+            }
+            X[(size_t)k + (size_t)nzh * ((size_t)j + (size_t)ny * i)] = v;
+        }
+    }
+}
+
 // reset the dt maxima before the first stage of a step
 __global__ void k_reset_max(DevScalars* sc) {
     if (threadIdx.x < 8) sc[blockIdx.x].maxbits[threadIdx.x] = 0ull;   // one block per box
@@ -430,6 +498,7 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
 // FP64 energy / dissipation sums with the half-spectrum weights
 // (computeEnergy, spooky_output_functions.cu:23-55).
 __global__ void k_budgets(DevGrid g, const double2* U, int F, double* sums) {
+    const double shx = grid_shx(g);
     const size_t nc = g.nc;
     __shared__ double red[2][32];
     for (int f = 0; f < F; f++) {
@@ -441,7 +510,8 @@ __global__ void k_budgets(DevGrid g, const double2* U, int F, double* sums) {
             const double2 q = U[(size_t)f * nc + gi];
             const double w = k == 0 ? 1.0 : 2.0;
             const double a2 = q.x * q.x + q.y * q.y;
-            const double k2 = g.kx[i] * g.kx[i] + g.ky[j] * g.ky[j] + g.kz[k] * g.kz[k];
+            const double kxs = g.kx[i] + shx * g.ky[j];
+            const double k2 = kxs * kxs + g.ky[j] * g.ky[j] + g.kz[k] * g.kz[k];
             e += w * a2;
             d += w * k2 * a2;
         }

@@ -46,6 +46,7 @@ struct FastDiv {
     }
 };
 
+struct DevScalars;
 struct DevGrid {
     int nx, ny, nz, nzh;
     int nzs;                        // row length of the pass buffers (nzh rounded up to even)
@@ -54,6 +55,10 @@ struct DevGrid {
     size_t ncs;                     // nx*ny*nzs (pass-buffer elements per channel)
     const double *kx, *ky, *kz;     // wavevector tables (exact reference expressions)
     const double *mx, *my, *mz;     // separable mask factors, 0.0 or 1.0
+    // shearing box: kx of mode (i, j) is kx[i] + shear * (tremap + csh * dt) * ky[j]
+    // with tremap and dt from *shsc (csh: the RK stage's offset; shear 0: off)
+    double shear, csh;
+    const DevScalars* shsc;
 };
 
 #define SPK_RKL_MAX 128
@@ -79,7 +84,18 @@ struct DevScalars {
     // state is set.  scan_*: the squared norms (scratch)
     int masked_live;
     double scan_all, scan_masked;
+    // shearing box: the remap clock (TimeStepping::tremap) and whether the
+    // step that just ended remapped the fields
+    double tremap;
+    int remap;
 };
+
+// ShearWavevector's tremap * shear (cuda_kernels_generic.cu:362-384) for
+// the wavevector of the launch's stage; 0 without the shearing module.
+__device__ __forceinline__ double grid_shx(const DevGrid& g) {
+    if (g.shear == 0.0) return 0.0;
+    return g.shear * (g.csh != 0.0 ? g.shsc->tremap + g.csh * g.shsc->dt : g.shsc->tremap);
+}
 
 // Classic super-time-stepping of Alexiades, Amiez & Gremaud (Commun. Numer.
 // Meth. Eng. 12, 31, 1996) as the reference states it (rkl.cu:594-664).
@@ -248,6 +264,9 @@ struct XfArgs {
     const int *kxi, *kyi;   // kept x and y indices
     int nkx, nky;
     FastDiv fd_kzk, fd_nky, fd_nkx;
+    // shearing box (g.shear != 0): Coriolis force with rotating on
+    int rotating;
+    double omega;
 };
 
 struct RklArgs {
@@ -276,6 +295,8 @@ struct DtArgs {
     int rkl_smax;
     int sts_alg;             // STS_ALG_*
     int closure;             // add the closure's max eddy viscosity / resistivity (maxbits[6], [7])
+    int shearing, rotating;  // the shearing box's rates (compute_dt.cu:110-121)
+    double shear, omega;
 };
 
 }  // namespace spk

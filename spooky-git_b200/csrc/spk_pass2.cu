@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     int dbox = -1;                 // box whose deferred-mode scalars are cached
     T dnu1 = (T)0, dnu2 = (T)0;
     bool dlive = true;
+    const double shx_x = grid_shx(a.g);   // the shearing box's wavevector shear (0 without it)
     for (int t = blockIdx.x; t < total; t += gridDim.x, i++) {
         const int s = i % NST;
         const uint32_t par = (uint32_t)((i / NST) & 1);
@@ -152,6 +153,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             kout = a.axis == 0 ? a.g.ky[o] : a.g.kx[o];
             kcol = a.g.kz[min(k0 + c, a.g.nzh - 1)];
         }
+        // shearing box: on x lines kx(n, o) = kx[n] + shx ky[o]
+        const double kshift = a.axis == 0 ? shx_x * a.g.ky[o] : 0.0;
         const bool skip = (a.outer_filter && !okeep[o]) || trimmed(box, o, kb);   // uniform over the CTA
         // trimmed y inverse: masked y rows were not written by the x inverse
         const bool zrows = a.trim == 2 && !skip && !a.scs[box].masked_live;
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 double2 x = src[n * KT + c];
-                if (deriv) x = ik_mul(deriv == 1 ? kd[n] : (deriv == 2 ? kout : kcol), x);
+                if (deriv) x = ik_mul(deriv == 1 ? kd[n] + kshift : (deriv == 2 ? kout : kcol), x);
                 if (jo.hp && !(kd[n] * kd[n] + kout * kout + kcol * kcol > a.hp_k2)) x = make_double2(0.0, 0.0);
                 C2<T> v = mk<T>((T)(x.x * scale), (T)(x.y * scale));
                 if constexpr (DEF)
@@ -209,7 +212,8 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
                 if constexpr (DEF)
                     if (dfr) { const T f = (T)deferred(n); v = mk<T>(f * v.x, f * v.y); }
                 if (deriv) {
-                    const T kk = deriv == 1 ? kax[n] : (T)(deriv == 2 ? kout : kcol);
+                    const T kk = deriv == 1 ? (kshift != 0.0 ? (T)(a.g.kx[n] + kshift) : kax[n])
+                                            : (T)(deriv == 2 ? kout : kcol);
                     v = mk<T>(-kk * v.y, kk * v.x);
                 }
                 if (jo.hp) {
@@ -730,6 +734,7 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
     const bool compact = a.defer != 0;
     const int kzk = a.g.kz_keep;
     const size_t total = (compact ? (size_t)a.nkx * a.nky * kzk : nc) * (size_t)a.nb;
+    const double shx = grid_shx(a.g);   // shearing box: kx = kx0 + shx ky
     for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
         int k, i, j, box;
         unsigned line;
@@ -795,7 +800,7 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
             if (a.bous && a.nl_F >= 0) { f0 = P(a.nl_F); f1 = P(a.nl_F + 1); f2 = P(a.nl_F + 2); }
             if (a.bous && a.aniso_rhs && a.nl_Q >= 0) { q0 = P(a.nl_Q); q1 = P(a.nl_Q + 1); q2 = P(a.nl_Q + 2); }
         }
-        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
         const double k2 = kx * kx + ky * ky + kz * kz;
         double2 usd = z0;
 
@@ -813,6 +818,17 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
                 else if (a.sd == 1) { R[1] = d2(R[1].x - Xt.x, R[1].y - Xt.y); usd = Xu[1]; }
                 else                { R[2] = d2(R[2].x - Xt.x, R[2].y - Xt.y); usd = Xu[2]; }
             }
+            if (a.g.shear != 0.0) {
+                // BackgroundShear / BackgroundRotation (shear_rotation.cu:11-63):
+                // dvy += S vx; with rotation dvx += 2 omega vy, dvy -= 2 omega vx
+                const double S = a.g.shear;
+                R[1] = d2(R[1].x + S * Xu[0].x, R[1].y + S * Xu[0].y);
+                if (a.rotating) {
+                    const double w2 = 2.0 * a.omega;
+                    R[0] = d2(R[0].x + w2 * Xu[1].x, R[0].y + w2 * Xu[1].y);
+                    R[1] = d2(R[1].x - w2 * Xu[0].x, R[1].y - w2 * Xu[0].y);
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 if (!((a.sts_mask >> (a.VEL + c)) & 1u)) {
@@ -820,10 +836,18 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
                     R[c] = d2(R[c].x + f * Xu[c].x, R[c].y + f * Xu[c].y);
                 }
             }
-            // Leray: dU += i k (i k.dU)/k^2
+            // Leray: dU += i k (i k.dU)/k^2; the shearing box adds S ky vx to
+            // k.dU (GradPseudoPressureShearing, cuda_kernels.cu:165-196)
             const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
-            const double sx = kx * R[0].x + ky * R[1].x + kz * R[2].x;
-            const double sy = kx * R[0].y + ky * R[1].y + kz * R[2].y;
+            double sx, sy;
+            if (a.g.shear != 0.0) {
+                const double Sky = a.g.shear * ky;
+                sx = Sky * Xu[0].x + kx * R[0].x + ky * R[1].x + kz * R[2].x;
+                sy = Sky * Xu[0].y + kx * R[0].y + ky * R[1].y + kz * R[2].y;
+            } else {
+                sx = kx * R[0].x + ky * R[1].x + kz * R[2].x;
+                sy = kx * R[0].y + ky * R[1].y + kz * R[2].y;
+            }
             const double kk[3] = {kx, ky, kz};
 #pragma unroll
             for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
@@ -846,6 +870,8 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 double2 R = d2(-S3[c].y, S3[c].x);
+                // shearing box: dBy -= S Bx (ShearingFlow with -shear)
+                if (c == 1 && a.g.shear != 0.0) R = d2(R.x + (-a.g.shear) * Xb[0].x, R.y + (-a.g.shear) * Xb[0].y);
                 if (!((a.sts_mask >> (a.MAG + c)) & 1u)) {
                     const double f = -nu_m * k2;
                     R = d2(R.x + f * Xb[c].x, R.y + f * Xb[c].y);

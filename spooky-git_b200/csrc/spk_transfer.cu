@@ -30,11 +30,12 @@ struct TermArgs {
 template <typename T>
 __global__ void k_term(const __grid_constant__ TermArgs a) {
     const size_t nc = a.g.nc;
+    const double shx = grid_shx(a.g);
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const int k = (int)(gi % a.g.nzh);
         const size_t r = gi / a.g.nzh;
         const int j = (int)(r % a.g.ny), i = (int)(r / a.g.ny);
-        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
         if (a.kind == TR_HEL) {
             const double k2 = kx * kx + ky * ky + kz * kz;
             const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;

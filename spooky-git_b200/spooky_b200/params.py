@@ -41,6 +41,8 @@ class Params(ctypes.Structure):
         ("sts_every_step", ctypes.c_int), ("form", ctypes.c_int),
         ("closure", ctypes.c_int),
         ("closure_kc_frac", ctypes.c_double),
+        ("shearing", ctypes.c_int), ("rotating", ctypes.c_int),
+        ("shear", ctypes.c_double), ("omega", ctypes.c_double),
     ]
 
     def copy(self):
@@ -94,6 +96,10 @@ def default_params(**overrides):
     p.sts_every_step = 0
     p.form = SPK_FORM_PLAIN
     p.closure = 0
+    p.shearing = 0
+    p.rotating = 0
+    p.shear = 0.0
+    p.omega = 0.0
     sts_vars = overrides.pop("sts_variables", None)
     if isinstance(overrides.get("sts_algorithm"), str):
         overrides["sts_algorithm"] = STS_ALGORITHMS[overrides["sts_algorithm"]]
@@ -170,7 +176,9 @@ def cfg_text(p, configname="spooky_b200", toutput_time=None, output_dir="./"):
     (src/parameters/parameters.cu:59-505) the physics, modules and time
     controls of ``p``; keys the path does not use keep the reference's
     defaults.  Extensions of spk_params_t without a cfg key (form, fixed_dt,
-    integrator, sts_every_step, closure) are not written."""
+    integrator, sts_every_step, closure) are not written.  With shearing on,
+    the reader moves snapshot_step to a multiple of the shear period as the
+    reference does (parameters.cu:551-562)."""
     b = lambda v: "true" if v else "false"
     names = var_list(p)
     sts = [n for i, n in enumerate(names) if p.sts_vars_mask >> i & 1]
@@ -187,6 +195,8 @@ def cfg_text(p, configname="spooky_b200", toutput_time=None, output_dir="./"):
         f"  mhd = {b(p.mhd)};",
         f"  anisotropic_diffusion = {b(p.anisotropic_diffusion)};",
         f"  supertimestepping = {b(p.supertimestepping)};",
+        f"  shearing = {b(p.shearing)};",
+        f"  rotating = {b(p.rotating)};",
         f'  sts_algorithm = "{alg}";',
         "  sts_variables = (" + ", ".join(f'"{n}"' for n in sts) + ");" if sts else "",
         "};",
@@ -199,6 +209,8 @@ def cfg_text(p, configname="spooky_b200", toutput_time=None, output_dir="./"):
         f"  reynolds_anisotropic = {_cfg_float(p.reynolds_ani)};",
         f"  brunt_vaissala_squared = {_cfg_float(p.N2)};",
         f"  mti_frequency_squared = {_cfg_float(p.OmegaT2)};",
+        f"  shear = {_cfg_float(p.shear)};",
+        f"  omega = {_cfg_float(p.omega)};",
         "};",
         "code:", "{",
         f"  cfl = {_cfg_float(p.cfl)};",

@@ -1,0 +1,144 @@
+"""The shearing box with rotation on the GPU against its CPU oracle
+(oracle/spk_oracle.c: ShiftTime, RemapField, BackgroundShear,
+BackgroundRotation, GradPseudoPressureShearing, the sheared wavevector and
+the dt rule), and the reference's shearing-wave test
+(tests/shearing-wave/check-shearing-wave.py): 64^3 HD, S = 1.5, omega = 1,
+vz = cos(ky0 y), snapshots every shear period to t = 10 through the command
+line, each against the sheared, viscously decayed analytic wave (L1 < 1e-7)."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fields import random_solenoidal, to_spectral
+from spooky_b200 import Context, fileCounter
+from spooky_b200.params import SPK_FORM_FP32, SPK_FORM_PLAIN, cfg_text, default_params
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+S, OM = 1.5, 1.0
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def _params(mhd, n=16, form=SPK_FORM_PLAIN, **kw):
+    base = dict(incompressible=1, gridsize=(n, n, n), boxsize=(1.0, 1.5, 1.0), reynolds=2000.0, shearing=1,
+                rotating=1, shear=S, omega=OM, t_final=1e9, toutput_flow=1e9, form=form)
+    if mhd:
+        base.update(mhd=1, reynolds_magnetic=1000.0)
+    base.update(kw)
+    return default_params(**base)
+
+
+def _state(p, seed):
+    fields = list(random_solenoidal(p, seed, kpeak=3.0))
+    if p.mhd:
+        fields += list(random_solenoidal(p, seed + 7, kpeak=3.0, rms=0.6))
+    return to_spectral(np.stack(fields))
+
+
+def _torch(U):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(U)).cuda()
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+@pytest.mark.parametrize("mhd", [False, True])
+def test_sheared_rhs_matches_oracle(mhd, form):
+    import torch
+    p = _params(mhd, form=form)
+    U = _state(p, 3)
+    o = O.Oracle(p)
+    o.set_time(0.31)                       # a sheared wavevector
+    want = o.compute_dfield(U)
+    ctx = Context(p)
+    ctx.set_time(0.31)
+    dU = torch.zeros(ctx.shape_c, dtype=torch.complex128, device="cuda")
+    ctx.compute_dfield(_torch(U), dU)
+    got = dU.cpu().numpy()
+    assert rel_l2(got, want) < (1e-12 if form == SPK_FORM_PLAIN else 2e-5), rel_l2(got, want)
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+@pytest.mark.parametrize("mhd", [False, True])
+def test_steps_across_a_remap_match_oracle(mhd, form):
+    """Ten steps from t = 0.45 at dt = 0.01: the remap clock passes half a
+    shear period (0.5) at the fifth step and the fields are remapped."""
+    p = _params(mhd, form=form, fixed_dt=0.01)
+    U = _state(p, 5)
+    o = O.Oracle(p)
+    o.set_time(0.45)
+    o.set_state(U)
+    o.step(10)
+    ctx = Context(p)
+    ctx.set_state(U)
+    ctx.set_time(0.45)
+    ctx.advance(10)
+    ctx.synchronize()
+    got, want = ctx.get_state(), o.get_state()
+    assert abs(ctx.get_time()[0] - o.get_time()[0]) < 1e-14
+    assert rel_l2(got, want) < (1e-11 if form == SPK_FORM_PLAIN else 1e-5), rel_l2(got, want)
+
+
+def test_cfl_dt_matches_oracle():
+    p = _params(True)
+    U = _state(p, 7)
+    o = O.Oracle(p)
+    o.set_time(0.7)
+    o.set_state(U)
+    o.clean_divergence()
+    want = o.compute_dt()
+    ctx = Context(p)
+    ctx.set_state(U)
+    ctx.set_time(0.7)
+    ctx.clean_divergence()
+    got = ctx.compute_dt()
+    for g, w in zip(got, want):
+        assert abs(g - w) < 1e-12 * abs(w), (got, want)
+
+
+def test_reference_shearing_wave(tmp_path):
+    import test_hdf5 as H
+    n = 64
+    p = default_params(incompressible=1, gridsize=(n, n, n), boxsize=(1.0, 1.5, 1.0), reynolds=2000.0, shearing=1,
+                       rotating=1, shear=S, omega=OM, cfl=1.5, cfl_par=0.5, safety_source=0.2, t_final=10.0,
+                       toutput_flow=1.0, antialiasing=1)
+    lx, ly, lz = 1.0, 1.5, 1.0
+    x = -lx / 2 + lx * np.arange(n) / n
+    y = -ly / 2 + ly * np.arange(n) / n
+    X, Y, _ = np.meshgrid(x, y, -lz / 2 + lz * np.arange(n) / n, indexing="ij")
+    ky0 = 2 * np.pi / ly
+    vz0 = np.cos(ky0 * Y)
+    d = tmp_path
+    (d / "data").mkdir()
+    (d / "spooky.cfg").write_text(cfg_text(p, toutput_time=0.1).replace('output_dir = "./"', f'output_dir = "{d}"'))
+    items = {"t_start": np.array([0.0]), "t_save": np.array([0.0]), "t_lastsnap": np.array([0.0]),
+             "t_lastvar": np.array([0.0]), "step": np.array([0], dtype=np.int32),
+             "vx": 0 * vz0.ravel(), "vy": 0 * vz0.ravel(), "vz": vz0.ravel()}
+    H.h5_write(d / "data" / "snap0000.h5", items)
+    env = dict(os.environ, PYTHONPATH=os.path.join(ROOT, "spooky-git_b200"))
+    r = subprocess.run([sys.executable, "-m", "spooky_b200", "--input-dir", str(d), "-r", "0"], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    nsnap = fileCounter(str(d / "data"))
+    assert nsnap == 10                     # t = 1, 2, ..., 10: one per shear period
+    kyv = 2.0 * np.pi * np.fft.fftfreq(n, d=ly / n)
+    KY = np.broadcast_to(kyv[None, :, None], X.shape)
+    nu = 1.0 / 2000.0
+    errs = []
+    for i in range(1, nsnap + 1):
+        R = H.h5_read(d / "data" / f"snap{i:04d}.h5", {k: (np.float64, n ** 3) for k in ("vx", "vy", "vz")} |
+                      {"t_save": (np.float64, 1)})
+        t = R["t_save"][0]
+        assert abs(t - i) < 1e-12
+        # check-shearing-wave.py:135-140, 166-180
+        vz_an = np.real(np.fft.ifft(np.fft.fft(vz0, axis=1) * np.exp(1j * KY * X * S * t), axis=1))
+        vz_an *= np.exp(-nu * (ky0 ** 2 * t + (1. / 3.) * S ** 2 * ky0 ** 2 * t ** 3))
+        L1 = (np.abs(R["vx"]).sum() + np.abs(R["vy"]).sum() + np.abs(R["vz"] - vz_an.ravel()).sum()) / n ** 3
+        errs.append(L1)
+    assert max(errs) < 1e-7, errs
