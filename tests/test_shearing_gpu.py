@@ -142,3 +142,61 @@ def test_reference_shearing_wave(tmp_path):
         L1 = (np.abs(R["vx"]).sum() + np.abs(R["vy"]).sum() + np.abs(R["vz"] - vz_an.ravel()).sum()) / n ** 3
         errs.append(L1)
     assert max(errs) < 1e-7, errs
+
+
+def test_reference_mri_eigenmode(tmp_path):
+    """tests/mri-eigenmode/check-mri-eigenmode.py: 64^3 MHD shearing box
+    (S = 1.5, omega = 1, Re = Rm = 3000) with a mean field B0z = 0.1 and the
+    axisymmetric MRI eigenmode kX = 2 pi, kZ = 4 pi of amplitude 1e-4,
+    through the command line to t = 1; every field against the eigenmode
+    grown at its viscous-resistive rate (L1 < 1e-7)."""
+    import test_hdf5 as H
+    n = 64
+    lx, ly, lz = 1.0, 1.5, 1.0
+    p = default_params(incompressible=1, mhd=1, gridsize=(n, n, n), boxsize=(lx, ly, lz), reynolds=3000.0,
+                       reynolds_magnetic=3000.0, shearing=1, rotating=1, shear=S, omega=OM, cfl=1.5, cfl_par=0.5,
+                       safety_source=0.2, t_final=1.0, toutput_flow=1.0, antialiasing=1)
+    # the eigenmode (check-mri-eigenmode.py:27-74)
+    B0z, a = 0.1, 1e-4
+    kZ, kX = 2.0 * 2.0 * np.pi / lz, 1.0 * 2.0 * np.pi / lx
+    gamma2 = kZ * kZ / (kZ * kZ + kX * kX)
+    kappa2 = 2 * OM * (2 * OM - S)
+    omegaA2 = B0z * B0z * kZ * kZ
+    omega_nu2 = omegaA2 + 0.5 * kappa2 * gamma2 * (1. - np.sqrt(1. + 16. * omegaA2 * OM * OM / (kappa2 * kappa2 * gamma2)))
+    sigma_nu = np.sqrt(-omega_nu2)
+    sigma = sigma_nu - (kX * kX + kZ * kZ) / 3000.0
+    sigma_eta = sigma + (kX * kX + kZ * kZ) / 3000.0
+    ax = [-l / 2 + l * np.arange(n) / n for l in (lx, ly, lz)]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    ph = kX * X + kZ * Z
+    vx0 = a * np.cos(ph)
+    vy0 = vx0 * (S * omegaA2 / (sigma_eta * sigma_eta) - (2 * OM - S)) / (sigma_nu + omegaA2 / sigma_eta)
+    vz0 = -(kX / kZ) * a * np.cos(ph)
+    bx0 = -a * np.sin(ph) * B0z * kZ / sigma_eta
+    by0 = bx0 * (-S / sigma_eta + (S * omegaA2 / (sigma_eta * sigma_eta) - (2 * OM - S)) / (sigma_nu + omegaA2 / sigma_eta))
+    bz0 = B0z * (1.0 + (kX / kZ) * a * np.sin(ph) * kZ / sigma_eta)
+    f0 = {"vx": vx0, "vy": vy0, "vz": vz0, "bx": bx0, "by": by0, "bz": bz0}
+    d = tmp_path
+    (d / "data").mkdir()
+    (d / "spooky.cfg").write_text(cfg_text(p, toutput_time=0.1).replace('output_dir = "./"', f'output_dir = "{d}"'))
+    items = {"t_start": np.array([0.0]), "t_save": np.array([0.0]), "t_lastsnap": np.array([0.0]),
+             "t_lastvar": np.array([0.0]), "step": np.array([0], dtype=np.int32)}
+    items.update({k: v.ravel() for k, v in f0.items()})
+    H.h5_write(d / "data" / "snap0000.h5", items)
+    env = dict(os.environ, PYTHONPATH=os.path.join(ROOT, "spooky-git_b200"))
+    r = subprocess.run([sys.executable, "-m", "spooky_b200", "--input-dir", str(d), "-r", "0"], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert fileCounter(str(d / "data")) == 1
+    R = H.h5_read(d / "data" / "snap0001.h5", {k: (np.float64, n ** 3) for k in f0} | {"t_save": (np.float64, 1)})
+    t = R["t_save"][0]
+    assert abs(t - 1.0) < 1e-12
+    L1 = 0.0
+    for k, v in f0.items():
+        want = (v - (B0z if k == "bz" else 0.0)) * np.exp(sigma * t)   # ky = 0: shear_quantity is the identity
+        got = R[k].reshape(n, n, n) - (B0z if k == "bz" else 0.0)
+        L1 += np.abs(got - want).sum()
+    L1 /= n ** 3
+    assert L1 < 1e-7, L1
+    # the mode grew: the check is not passed by a decayed field
+    assert np.abs(R["vx"]).max() > 1.5 * a
