@@ -253,3 +253,24 @@ def test_mti_dispersion_cubic_of_the_bench_matches_the_reference_golden():
                   g["OmegaT2"])
     assert abs(s - g["sigma_dispersion_cubic"]) < 1e-13
     assert abs(s - g["sigma_check_script"]) < 1e-13
+
+
+SHEARING = """
+modules: { incompressible = true; mhd = true; shearing = true; rotating = true; };
+physics: { boxsize = (1.0, 3.0, 1.0); gridsize = (16, 16, 16); omega = 1.0; shear = 1.5; };
+output: { snapshot_step = %s; };
+"""
+
+
+# shear period ly / (S lx) = 2
+@pytest.mark.parametrize("step, want", [(0.5, 2.0), (2.0, 1.0), (7.5, 3.0)])
+def test_shearing_keys_and_snapshot_step(step, want):
+    """modules.shearing / rotating and physics.shear / omega; with shearing
+    the snapshot step becomes the shear period ly / (S lx) when shorter, else
+    int(step / period) -- the reference's arithmetic (parameters.cu:551-562),
+    kept as written: a count of periods, not their length."""
+    p = S.params_from_string(SHEARING % step)
+    assert (p.shearing, p.rotating, p.shear, p.omega) == (1, 1, 1.5, 1.0)
+    assert p.toutput_flow == want
+    q = S.params_from_string((SHEARING % step).replace("shearing = true", "shearing = false"))
+    assert q.shearing == 0 and q.toutput_flow == step
