@@ -40,6 +40,27 @@ template <int DIR, typename V, typename T> __device__ __forceinline__ V rotc(V a
     return r;
 }
 
+// FP32 complex arithmetic on Blackwell's paired FP32 instructions (FADD2,
+// FMUL2, FFMA2: one instruction for both lanes, each lane rounded as the
+// scalar operation).  Sums, differences and real scalings give the same bits
+// as the scalar forms; the products round a.x b (both lanes) first and fuse
+// the a.y terms, the same single-FMA accuracy as the scalar contraction.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 cscale(float s, float2 a) { return __fmul2_rn(make_float2(s, s), a); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    // (a.x b.x - a.y b.y, a.x b.y + a.y b.x)
+    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+template <int DIR> __device__ __forceinline__ float2 rotc(float2 a, float c, float s) {
+    // DIR < 0: (a.x c + a.y s, a.y c - a.x s); DIR > 0: (a.x c - a.y s, a.y c + a.x s)
+    const float2 t = __fmul2_rn(a, make_float2(c, c));
+    return DIR < 0 ? __ffma2_rn(make_float2(a.y, -a.x), make_float2(s, s), t)
+                   : __ffma2_rn(make_float2(-a.y, a.x), make_float2(s, s), t);
+}
+#endif
+
 // ---- in-register DFTs (natural-order input and output) -------------------
 template <typename T, int DIR> __device__ __forceinline__ void dft2(C2<T>* a) {
     C2<T> t = a[0]; a[0] = cadd(t, a[1]); a[1] = csub(t, a[1]);

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
     int dbox = -1;                 // box whose deferred-mode scalars are cached
     T dnu1 = (T)0, dnu2 = (T)0;
     bool dlive = true;
-    const double shx_x = CONV ? grid_shx(a.g) : 0.0;   // the shearing box's wavevector shear (0 without it)
+    const double shx_x = DIR > 0 ? grid_shx(a.g) : 0.0;   // the shearing box's wavevector shear (0 without it)
     for (int t = blockIdx.x; t < total; t += gridDim.x, i++) {
         const int s = i % NST;
         const uint32_t par = (uint32_t)((i / NST) & 1);
@@ -153,9 +153,9 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
             kout = a.axis == 0 ? a.g.ky[o] : a.g.kx[o];
             kcol = a.g.kz[min(k0 + c, a.g.nzh - 1)];
         }
-        // shearing box: on x lines kx(n, o) = kx[n] + shx ky[o]; the x inverse
-        // (CONV: it reads the FP64 state) is the only pass with x derivatives
-        const double kshift = (CONV && a.axis == 0 && shx_x != 0.0) ? shx_x * a.g.ky[o] : 0.0;
+        // shearing box: on x lines kx(n, o) = kx[n] + shx ky[o] (0 without it;
+        // only the x inverse, which reads the state, takes x derivatives)
+        const double kshift = (DIR > 0 && a.axis == 0 && shx_x != 0.0) ? shx_x * a.g.ky[o] : 0.0;
         const bool skip = (a.outer_filter && !okeep[o]) || trimmed(box, o, kb);   // uniform over the CTA
         // trimmed y inverse: masked y rows were not written by the x inverse
         const bool zrows = a.trim == 2 && !skip && !a.scs[box].masked_live;
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisAr
                 if constexpr (DEF)
                     if (dfr) { const T f = (T)deferred(n); v = mk<T>(f * v.x, f * v.y); }
                 if (deriv) {
-                    const T kk = deriv == 1 ? kax[n] : (T)(deriv == 2 ? kout : kcol);
+                    const T kk = deriv == 1 ? kax[n] + (T)kshift : (T)(deriv == 2 ? kout : kcol);
                     v = mk<T>(-kk * v.y, kk * v.x);
                 }
                 if (jo.hp) {
