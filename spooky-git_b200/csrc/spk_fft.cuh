@@ -47,7 +47,8 @@ template <int DIR, typename V, typename T> __device__ __forceinline__ V rotc(V a
 // the a.y terms, the same single-FMA accuracy as the scalar contraction.
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+// a - b as fma(-1, b, a): exact product, one rounding -- the bits of a - b
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
 __device__ __forceinline__ float2 cscale(float s, float2 a) { return __fmul2_rn(make_float2(s, s), a); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     // (a.x b.x - a.y b.y, a.x b.y + a.y b.x)
