@@ -399,7 +399,8 @@ static void launch_zpass_ln(spk_ctx* c, ZArgs& z, int nin_all) {
     auto need = [&](int lines) {
         return zsmem_layout(N, RegFft<T, N>::TWN, (int)sizeof(C2<T>), z.nin, nin_all, npout, lines, c->g.nzs,
                             slots, z.closure == 3 ? C3_ZBYTES / 4 : (z.closure ? CL_NP : 0),
-                            zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots)).total;
+                            zpass_alias(gen, RegFft<T, N>::NS, npin, npout, lines, slots),
+                            (gen == 1 && z.load_breal && zpass_stage_b<T, N>()) ? 3 : 0).total;
     };
     // lines per CTA: best (busy transform slots) x (resident CTAs per SM, <= 4)
     auto rounds = [&](long n) { return (n + slots - 1) / slots; };

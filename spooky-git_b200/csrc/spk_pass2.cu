@@ -271,7 +271,7 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
 // Shared-memory carve of k_zpass2 (host and device agree through this):
 // barrier, twiddle tables, input half spectra (later: the product pairs),
 // real fields, exchange slots.
-struct ZSmem { size_t tw, zero, junk, area, real, xb, cw, total; };
+struct ZSmem { size_t tw, zero, junk, area, real, xb, cw, bre, total; };
 // alias: the plain variant with one round of transforms in each direction
 // and at least two FFT stages keeps its exchange slots in the input/product
 // area: every slot has loaded its legs before the first exchange barrier (a
@@ -280,7 +280,7 @@ __host__ __device__ inline bool zpass_alias(int gen, int nstages, int npin, int 
     return gen == 0 && nstages >= 2 && npin * lines <= slots && npout * lines <= slots;
 }
 __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
-                                              int nzs, int slots, int ncw, bool alias) {
+                                              int nzs, int slots, int ncw, bool alias, int nbre = 0) {
     ZSmem z;
     const int rs = n + 16, xs = n + (n >> 4);
     z.tw = 128;
@@ -299,9 +299,15 @@ __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, 
     z.xb = alias ? z.area : align16(z.real + realb);
     const size_t end = alias ? z.real + (realb > redb ? realb : redb) : z.xb + xbs;
     z.cw = align16(end);                                     // closure MLP parameters (floats)
-    z.total = align16(z.cw + (size_t)ncw * sizeof(float));
+    // the flux mode's real B lines (nbre components), bulk-copied with the inputs
+    z.bre = align16(z.cw + (size_t)ncw * sizeof(float));
+    z.total = align16(z.bre + (size_t)nbre * lines * n * (csz / 2));
     return z;
 }
+
+// The flux mode stages the CTA's lines of the cached real B in shared memory
+// when a line's bytes keep every bulk copy 16-byte aligned.
+template <typename T, int N> __host__ __device__ constexpr bool zpass_stage_b() { return (N * sizeof(T)) % 16 == 0; }
 
 // GEN: 0 -- every input channel is a plain half spectrum; 1 -- derived
 // gradient channels or the to-real output (the general path); 2 -- the
@@ -333,8 +339,10 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     const int sigma_w = (tid & ~31) >> LTPC;   // the lowest slot of this warp (warp-uniform)
     const bool clos = GEN >= 2 && a.closure;
     const bool alias = zpass_alias(GEN, F::NS, npin, npout, L, slots);
+    // flux mode: the CTA's real B lines arrive with the inputs, off the point loop's path
+    const bool stage_b = GEN == 1 && zpass_stage_b<T, N>() && a.load_breal;
     const ZSmem lay = zsmem_layout(N, F::TWN, (int)sizeof(C2<T>), nin, nin_all, npout, L, nzs, slots,
-                                   clos ? (GEN == 3 ? C3_ZBYTES / 4 : CL_NP) : 0, alias);
+                                   clos ? (GEN == 3 ? C3_ZBYTES / 4 : CL_NP) : 0, alias, stage_b ? 3 : 0);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     C2<T>* tw = reinterpret_cast<C2<T>*>(smem_raw + lay.tw);
     C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
@@ -344,6 +352,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
     float* cw = reinterpret_cast<float*>(smem_raw + lay.cw);
+    T* bre = reinterpret_cast<T*>(smem_raw + lay.bre);
     if (clos) {   // visible after the next barrier
         if constexpr (GEN == 3) {
             // the packed BF16 network, in 16-byte words
@@ -366,9 +375,13 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     __syncthreads();
     if (tid == 0) {
         const uint32_t bytes = (uint32_t)((size_t)nl * nzs * sizeof(C2<T>));
-        mbar_expect_tx(bar, bytes * (uint32_t)nin);
+        const uint32_t bbytes = stage_b ? (uint32_t)((size_t)nl * N * sizeof(T)) : 0u;
+        mbar_expect_tx(bar, bytes * (uint32_t)nin + 3u * bbytes);
         for (int ch = 0; ch < nin; ch++)
             bulk_load(raw + (size_t)ch * L * nzs, in + (size_t)ch * a.cs_in + (size_t)line0 * nzs, bytes, bar);
+        if (stage_b)
+            for (int cb = 0; cb < 3; cb++)
+                bulk_load(bre + (size_t)cb * L * N, (const T*)a.breal + ((size_t)cb * nlines + line0) * N, bbytes, bar);
     }
     regfft_fill_twiddles<T, N>(tw, (const C2<T>*)a.plan.tw, tid, nthr);
     for (int i = tid; i < nzs; i += nthr) zrow[i] = mk<T>((T)0, (T)0);
@@ -517,7 +530,11 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             T ux = 0, uy = 0, uz = 0, bx = 0, by = 0, bz = 0, th = 0, gx = 0, gy = 0, gz = 0;
             if (a.ch_u >= 0) { ux = fr[a.ch_u * LRS]; uy = fr[(a.ch_u + 1) * LRS]; uz = fr[(a.ch_u + 2) * LRS]; }
             if (a.load_breal) {
-                if (live) {
+                if (live && stage_b) {
+                    bx = bre[(size_t)(0 * L + l) * N + z];
+                    by = bre[(size_t)(1 * L + l) * N + z];
+                    bz = bre[(size_t)(2 * L + l) * N + z];
+                } else if (live) {
                     bx = breal[(0 * (size_t)nlines + line) * N + z];
                     by = breal[(1 * (size_t)nlines + line) * N + z];
                     bz = breal[(2 * (size_t)nlines + line) * N + z];
