@@ -1004,7 +1004,6 @@ static int check_params(const spk_params_t* p, std::string& why) {
     if (p->shearing) {
         if (!p->incompressible) { why = "the shearing box needs the incompressible module"; return SPK_ERR_UNSUPPORTED; }
         if (!(p->shear != 0.0) || !std::isfinite(p->shear)) { why = "shearing needs a finite, nonzero shear"; return SPK_ERR_ARG; }
-        if (p->supertimestepping) { why = "the shearing box with super-time-stepping is not supported"; return SPK_ERR_UNSUPPORTED; }
         if (p->closure) { why = "the shearing box with the learned closure is not supported"; return SPK_ERR_UNSUPPORTED; }
     }
     return SPK_OK;

@@ -475,11 +475,12 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
     if (a.stage > a.sc->s_rkl) return;
     const double* c = a.sc->rkl[a.stage];
     const size_t nc = a.g.nc;
+    const double shx = grid_shx(a.g);   // shearing box: the wavevector of the current remap clock
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const int k = (int)(gi % a.g.nzh);
         const size_t r = gi / a.g.nzh;
         const int j = (int)(r % a.g.ny), i = (int)(r / a.g.ny);
-        const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+        const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
         const double k2 = kx * kx + ky * ky + kz * kz;
         for (int v = 0; v < a.nsts; v++) {
             if (a.kind[v] == 3) continue;

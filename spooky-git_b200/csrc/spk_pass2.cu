@@ -996,6 +996,7 @@ __global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArg
     const int nzh = a.g.nzh, nzs = a.g.nzs;
     const C2<T>* nl = (const C2<T>*)a.nl;
     double2* Uc = U + (size_t)a.fields[vslot] * nc;
+    const double shx = grid_shx(a.g);   // shearing box: the wavevector of the current remap clock
     for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
         const unsigned line = fzh.div((unsigned)gi);
         const int k = (int)(gi - (size_t)line * nzh);
@@ -1005,7 +1006,7 @@ __global__ void __launch_bounds__(256) k_rkl_flux(const __grid_constant__ RklArg
         if (a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0) {
             const size_t li = (size_t)line * nzs + k;
             const double2 q0 = to_d2(nl[li]), q1 = to_d2(nl[a.cs_nl + li]), q2 = to_d2(nl[2 * a.cs_nl + li]);
-            const double kx = a.g.kx[i], ky = a.g.ky[j], kz = a.g.kz[k];
+            const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
             const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
             dU = d2(-sq.y, sq.x);   // i * mask * k.q
         }

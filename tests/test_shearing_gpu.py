@@ -229,3 +229,48 @@ def test_reference_mri_eigenmode(tmp_path):
     assert L1 < 1e-7, L1
     # the mode grew: the check is not passed by a decayed field
     assert np.abs(R["vx"]).max() > 1.5 * a
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+def test_super_time_stepped_shearing_box_matches_oracle(form):
+    """MHD with RKL2 super-time-stepping of all six fields, alternating
+    before and after the RK3 step, ten steps across a remap: the cycles run
+    at the wavevector of the remap clock they meet."""
+    p = _params(True, form=form, fixed_dt=0.01, supertimestepping=1, sts_algorithm="rkl2",
+                sts_variables=["vx", "vy", "vz", "bx", "by", "bz"], safety_sts=50)
+    U = _state(p, 21)
+    o = O.Oracle(p)
+    o.set_time(0.45)
+    o.set_state(U)
+    o.step(10)
+    ctx = Context(p)
+    ctx.set_state(U)
+    ctx.set_time(0.45)
+    ctx.advance(10)
+    ctx.synchronize()
+    got, want = ctx.get_state(), o.get_state()
+    assert rel_l2(got, want) < (1e-11 if form == SPK_FORM_PLAIN else 1e-5), rel_l2(got, want)
+
+
+@pytest.mark.parametrize("form", [SPK_FORM_PLAIN, SPK_FORM_FP32])
+def test_anisotropic_conduction_cycle_in_the_shearing_box_matches_oracle(form):
+    """Boussinesq MHD with anisotropic conduction, theta on an RKL2 cycle (the
+    flux chain: sheared x derivative, staged real B, flux divergence with the
+    sheared kx), ten steps across a remap."""
+    p = _aniso_params(form)
+    p.supertimestepping = 1
+    p.sts_vars_mask = 1 << 6            # theta
+    p.fixed_dt = 0.01
+    p.safety_sts = 50
+    U = _bous_state(p, 23)
+    o = O.Oracle(p)
+    o.set_time(0.45)
+    o.set_state(U)
+    o.step(10)
+    ctx = Context(p)
+    ctx.set_state(U)
+    ctx.set_time(0.45)
+    ctx.advance(10)
+    ctx.synchronize()
+    got, want = ctx.get_state(), o.get_state()
+    assert rel_l2(got, want) < (1e-10 if form == SPK_FORM_PLAIN else 2e-5), rel_l2(got, want)
