@@ -590,8 +590,10 @@ def main():
     ap.add_argument("--closure-probe", action="store_true",
                     help="the closure's fused inference alone: --n^3 MHD, plain form, --closure-variant network "
                          "(the small case for ncu captures of its z pass)")
+    ap.add_argument("--profile-form", default="fp32", choices=["fp32", "plain"],
+                    help="the form of --profile-run")
     ap.add_argument("--profile-run", action="store_true",
-                    help="only the FP32 form, W warm-up + K timed steps, one short JSON line "
+                    help="one form only (--profile-form), W warm-up + K timed steps, one short JSON line "
                          "(the small case for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -660,10 +662,11 @@ def main():
         return ctx, max_over_ranks(ms), clocks
 
     if args.profile_run:
-        ctxp, msp, _ = timed_run(SPK_FORM_FP32)
+        ctxp, msp, _ = timed_run(SPK_FORM_PLAIN if args.profile_form == "plain" else SPK_FORM_FP32)
         kps, bytes_step = ctxp.step_info()
         if rank == 0:
-            print(json.dumps({"profile_run": True, "n": n, "ms_per_step": msp, "steps": args.steps,
+            print(json.dumps({"profile_run": True, "form": args.profile_form, "n": n, "ms_per_step": msp,
+                              "steps": args.steps,
                               "warmup": args.warmup, "kernels_per_step": kps, "step_bytes": bytes_step}),
                   flush=True)
         del ctxp
