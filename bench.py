@@ -1,7 +1,7 @@
 """Benchmark: 256^3 incompressible MHD, low-storage RK3 steps per second on B200.
 
-Workload (the reference's headline metric, BASELINE "256^3 MHD RK3 steps/s,
-FP32 form vs plain"): 256^3 box [0, 2 pi)^3, u and B independent random
+Workload (the headline metric: 256^3 MHD RK3 steps/s, FP32 form beside the
+plain FP64 form): 256^3 box [0, 2 pi)^3, u and B independent random
 solenoidal Gaussian fields with shell spectrum E(k) ~ k^4 exp(-2 (k/4)^2),
 rms 1 per component, B0 = 0.1 z added to the k=0 mode of B, nu = eta = 1e-3,
 CFL 1.5, 2/3 dealiasing, dt from the reference's CFL rule every step.
