@@ -562,8 +562,9 @@ int spk_trainer_train(spk_trainer* tr, int nsteps, int batch, float lr, float* l
 
 /* Schedule autotuner (no reference counterpart).  Picks, by timing whole
  * recorded steps with CUDA events, the launch choices that leave the
- * arithmetic unchanged: the z pass's lines per CTA, the axis passes'
- * pipeline stages and the RHS grid (CTAs per SM), by coordinate descent
+ * arithmetic unchanged: the axis tile width of short axes, the z pass's
+ * lines per CTA, the axis passes' pipeline stages and the RHS grid (CTAs
+ * per SM), by coordinate descent
  * over candidate values; the tuned context computes the same bits as an
  * untuned one.  `steps` timed steps per candidate.  The state and the step
  * scalars are saved (one temporary device copy of the state, freed on
@@ -574,6 +575,15 @@ int spk_autotune(spk_ctx* ctx, int steps, int* z_lines, int* axis_stages, int* r
                  double* ms_after);
 /* The same for every group of an ensemble (each group tuned on its own). */
 int spk_ensemble_autotune(spk_ensemble* ens, int steps);
+/* The context's launch schedule: the three knobs above (0: the launcher's
+ * own model) and the axis tile divisor -- 2 gives the axis passes of axes up
+ * to 64 long half-width tiles (a 64^3 box has 33 kz columns, 21 below the
+ * 2/3 cut-off, in a 64-column tile), 1 the full tiles; the autotuner tries
+ * both where an axis is that short.  Setting it (e.g. a schedule tuned on
+ * another context of the same grid) re-records the step graph; the values
+ * computed do not change. */
+int spk_get_schedule(const spk_ctx* ctx, int* z_lines, int* axis_stages, int* rhs_ctas_per_sm, int* axis_tile_div);
+int spk_set_schedule(spk_ctx* ctx, int z_lines, int axis_stages, int rhs_ctas_per_sm, int axis_tile_div);
 
 /* Human-readable text of the last error on this context (or of the last
  * failed spk_ctx_create when ctx is NULL). */

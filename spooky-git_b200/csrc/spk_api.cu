@@ -74,6 +74,7 @@ struct spk_ctx {
     // schedule knobs picked by spk_autotune (0: the launchers' own choice)
     int tune_zl = 0;               // z pass: lines per CTA
     int tune_nst = 0;              // axis passes: pipeline stages
+    int tune_kt = 0;               // axis passes of short axes: 2 = half-width tiles
     int tune_rhs = 0;              // RHS: CTAs per SM
     int ch_dx = -1, ch_dy = -1, ncl_half = 0;
     int ngrad = 0;                 // closure variant 2: gradient channels (9 or 18) from ch_dx
@@ -262,6 +263,8 @@ static AxisCfg axis_cfg(const spk_ctx* c, int N, bool state_in) {
     int kt = (N < 64 && cols < full) ? cols : full;
     if (c->fp32 && state_in && kt == full && kt > 2) kt /= 2;
     kt = std::max(kt, 2);
+    // the autotuner's half tiles of short axes (axis_half_ok)
+    if (c->tune_kt == 2 && N <= 64 && kt / 2 >= 2 && (kt / 2) * g.TPC >= 32) kt /= 2;
     a.kt = kt;
     a.nthr = kt * g.TPC;
     a.smem = 0;
@@ -279,11 +282,10 @@ template <typename K> static void allow_full_smem(K* kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
-template <typename T, int N, int DIR, bool CONV, bool DEF = false>
-static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
-    constexpr int KT = axis_kt<T, N, CONV>();
+template <typename T, int N, int DIR, bool CONV, bool DEF, int KTD>
+static void launch_axis_kt(spk_ctx* c, AxisArgs& a, long total) {
+    constexpr int KT = axis_kt<T, N, CONV, KTD>();
     const int nthr = KT * RegFft<T, N>::TPC;
-    if (a.kt != KT) { c->err = "internal: axis tile width mismatch"; c->sticky = SPK_ERR_ARG; return; }
     const size_t in_elem = CONV ? sizeof(double2) : sizeof(C2<T>);
     const size_t stage = (((size_t)N * KT * in_elem) + 127) & ~(size_t)127;
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
@@ -301,12 +303,23 @@ static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
     if (c->tune_nst >= 1 && c->tune_nst <= 4 && fixed + (size_t)c->tune_nst * stage <= (size_t)227 * 1024)
         a.nst = c->tune_nst;
     const size_t smem = fixed + (size_t)a.nst * stage;
-    allow_full_smem(k_axis2<T, N, DIR, CONV, DEF>);
+    allow_full_smem(k_axis2<T, N, DIR, CONV, DEF, KTD>);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV, DEF>, nthr, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_axis2<T, N, DIR, CONV, DEF, KTD>, nthr, smem);
     const int grid = (int)std::min<long>(total, (long)c->num_sms * std::max(per_sm, 1));
     c->launches++;
-    k_axis2<T, N, DIR, CONV, DEF><<<grid, nthr, smem, c->stream>>>(a);
+    k_axis2<T, N, DIR, CONV, DEF, KTD><<<grid, nthr, smem, c->stream>>>(a);
+}
+
+// the tile width the arguments carry (axis_cfg) picks the instantiation
+template <typename T, int N, int DIR, bool CONV, bool DEF = false>
+static void launch_axis_ln(spk_ctx* c, AxisArgs& a, long total) {
+    if (a.kt == axis_kt<T, N, CONV, 1>()) { launch_axis_kt<T, N, DIR, CONV, DEF, 1>(c, a, total); return; }
+    if constexpr (axis_half_ok<T, N, CONV>()) {
+        if (a.kt == axis_kt<T, N, CONV, 2>()) { launch_axis_kt<T, N, DIR, CONV, DEF, 2>(c, a, total); return; }
+    }
+    c->err = "internal: axis tile width mismatch";
+    c->sticky = SPK_ERR_ARG;
 }
 
 template <typename T, int N, int DIR>

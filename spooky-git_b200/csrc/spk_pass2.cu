@@ -26,20 +26,33 @@ namespace spk {
 // a 64-column tile on a 16^3 box would transform 55 columns of padding.
 __host__ __device__ constexpr int pow2_ceil(int n) { return n <= 1 ? 1 : 2 * pow2_ceil((n + 1) / 2); }
 template <typename T, int N, bool CONV>
-__host__ __device__ constexpr int axis_kt() {
+__host__ __device__ constexpr int axis_kt_base() {
     constexpr int tpc = RegFft<T, N>::TPC;
     constexpr int full = (256 / tpc) > 64 ? 64 : (256 / tpc);
     constexpr int cols = pow2_ceil(N / 2 + 1) > 32 / tpc ? pow2_ceil(N / 2 + 1) : 32 / tpc;
     constexpr int kt = (N < 64 && cols < full) ? cols : full;
     return (CONV && kt == full && kt > 2) ? kt / 2 : (kt < 2 ? 2 : kt);
 }
+// Short axes (N <= 64) also come in half-width tiles (KTD = 2), an
+// autotuner choice: a 64^3 box has 33 kz columns (21 below the 2/3 cut-off)
+// in a 64-column tile.  The half tile keeps at least one warp per CTA.
+template <typename T, int N, bool CONV>
+__host__ __device__ constexpr bool axis_half_ok() {
+    return N <= 64 && axis_kt_base<T, N, CONV>() / 2 >= 2 &&
+           (axis_kt_base<T, N, CONV>() / 2) * RegFft<T, N>::TPC >= 32;
+}
+template <typename T, int N, bool CONV, int KTD = 1>
+__host__ __device__ constexpr int axis_kt() {
+    return axis_kt_base<T, N, CONV>() / KTD;
+}
 
 // DEF: the x inverse of RK3 stage 1 or 2 with deferred masked modes (its own
-// instantiation, so that the other passes keep their registers).
-template <typename T, int N, int DIR, bool CONV, bool DEF>
+// instantiation, so that the other passes keep their registers).  KTD: tile
+// width divisor (1, or 2 for the half tiles of short axes).
+template <typename T, int N, int DIR, bool CONV, bool DEF, int KTD>
 __global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
     using F = RegFft<T, N>;
-    constexpr int KT = axis_kt<T, N, CONV>(), LKT = ilog2c(KT);
+    constexpr int KT = axis_kt<T, N, CONV, KTD>(), LKT = ilog2c(KT);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
     const int NST = a.nst;

@@ -8,7 +8,9 @@
 //             busy transform slots: the launcher's own choice is a model);
 //   tune_nst  pipeline stages of the axis passes (TMA loads in flight against
 //             CTAs per SM);
-//   tune_rhs  CTAs per SM of the RHS grid (loads in flight against tail).
+//   tune_rhs  CTAs per SM of the RHS grid (loads in flight against tail);
+//   tune_kt   half-width tiles for the axis passes of axes up to 64 long
+//             (fewer idle columns against fewer threads per CTA).
 // Coordinate descent over the knobs, each candidate timed with CUDA events
 // over whole recorded steps; the state and the step scalars are restored
 // afterwards.
@@ -50,8 +52,11 @@ extern "C" int spk_autotune(spk_ctx* c, int steps, int* zl, int* nst, int* rhs, 
     const float base = time_steps(c, steps, &rc);
     float best_ms = base;
     struct Knob { int* v; std::vector<int> cand; };
-    Knob knobs[3] = {{&c->tune_zl, {1, 2, 4, 8, 16, 32, 64}}, {&c->tune_nst, {1, 2, 3, 4}}, {&c->tune_rhs, {6, 12, 24, 48}}};
-    for (int kq = 0; kq < 3 && !rc; kq++) {
+    // the tile width first: the stage count depends on it
+    const bool short_axis = c->nx <= 64 || c->ny <= 64;
+    Knob knobs[4] = {{&c->tune_kt, short_axis ? std::vector<int>{0, 2} : std::vector<int>{}},
+                     {&c->tune_zl, {1, 2, 4, 8, 16, 32, 64}}, {&c->tune_nst, {1, 2, 3, 4}}, {&c->tune_rhs, {6, 12, 24, 48}}};
+    for (int kq = 0; kq < 4 && !rc; kq++) {
         int best = *knobs[kq].v;
         for (int v : knobs[kq].cand) {
             *knobs[kq].v = v;
@@ -77,6 +82,28 @@ extern "C" int spk_autotune(spk_ctx* c, int steps, int* zl, int* nst, int* rhs, 
     if (ms_before) *ms_before = base;
     if (ms_after) *ms_after = best_ms;
     return launch_status(c);
+}
+
+extern "C" int spk_get_schedule(const spk_ctx* c, int* zl, int* nst, int* rhs, int* tile_div) {
+    if (!c) return SPK_ERR_ARG;
+    if (zl) *zl = c->tune_zl;
+    if (nst) *nst = c->tune_nst;
+    if (rhs) *rhs = c->tune_rhs;
+    if (tile_div) *tile_div = c->tune_kt == 2 ? 2 : 1;
+    return SPK_OK;
+}
+
+extern "C" int spk_set_schedule(spk_ctx* c, int zl, int nst, int rhs, int tile_div) {
+    if (!c) return SPK_ERR_ARG;
+    if (zl < 0 || nst < 0 || nst > 4 || rhs < 0 || (tile_div != 0 && tile_div != 1 && tile_div != 2))
+        return fail(c, SPK_ERR_ARG, "schedule: z_lines >= 0, axis_stages 0..4, rhs_ctas_per_sm >= 0, axis_tile_div 0, 1 or 2");
+    CK(cudaStreamSynchronize(c->stream));
+    c->tune_zl = zl;
+    c->tune_nst = nst;
+    c->tune_rhs = rhs;
+    c->tune_kt = tile_div == 2 ? 2 : 0;
+    drop_graphs(c);   // the next step records the new schedule
+    return SPK_OK;
 }
 
 extern "C" int spk_ensemble_autotune(spk_ensemble* e, int steps) {

@@ -44,7 +44,7 @@ EXPORTED = ["spk_params_default", "spk_ctx_create", "spk_ctx_destroy", "spk_size
             "spk_write_snapshot", "spk_read_snapshot", "spk_h5_write", "spk_h5_read", "spk_diagnostics",
             "spk_cfg_lookup_int", "spk_cfg_lookup_bool", "spk_cfg_lookup_float", "spk_cfg_lookup_string",
             "spk_cfg_setting_length", "spk_transfer_spectra", "spk_trainer_create_variant",
-            "spk_closure_nparam", "spk_closure_rows"]
+            "spk_closure_nparam", "spk_closure_rows", "spk_get_schedule", "spk_set_schedule"]
 
 DIAGNOSTICS = ("w2", "hv", "j2", "hm", "hc", "thetaB", "bz2", "phiB", "dissgradT", "pv")
 
@@ -161,6 +161,8 @@ def lib():
         L.spk_cfg_setting_length.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.spk_transfer_spectra.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_int, ip, ip, dp, dp]
         L.spk_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ip, dp, dp]
+        L.spk_get_schedule.argtypes = [vp, ip, ip, ip, ip]
+        L.spk_set_schedule.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.spk_ensemble_autotune.argtypes = [vp, ctypes.c_int]
         L.spk_last_error.restype = ctypes.c_char_p
         for name in EXPORTED:
@@ -478,14 +480,28 @@ class Context:
         return np.array(b.energy[: self.F]), np.array(b.dissipation[: self.F])
 
     def autotune(self, steps=5):
-        """spk_autotune: pick the z-pass lines per CTA, axis stages and RHS
-        grid by timing; returns the choices and ms per step before/after."""
+        """spk_autotune: pick the axis tile width of short axes, the z-pass
+        lines per CTA, axis stages and RHS grid by timing; returns the choices
+        and ms per step before/after."""
         zl, nst, rhs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         b, a = ctypes.c_double(), ctypes.c_double()
         self._check(lib().spk_autotune(self._h, int(steps), ctypes.byref(zl), ctypes.byref(nst), ctypes.byref(rhs),
                                        ctypes.byref(b), ctypes.byref(a)))
-        return dict(z_lines=zl.value, axis_stages=nst.value, rhs_ctas_per_sm=rhs.value, ms_before=b.value,
-                    ms_after=a.value)
+        out = dict(z_lines=zl.value, axis_stages=nst.value, rhs_ctas_per_sm=rhs.value, ms_before=b.value,
+                   ms_after=a.value)
+        out["axis_tile_div"] = self.get_schedule()["axis_tile_div"]
+        return out
+
+    def get_schedule(self):
+        """spk_get_schedule: the launch schedule (0: the launcher's model)."""
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(lib().spk_get_schedule(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(z_lines=v[0].value, axis_stages=v[1].value, rhs_ctas_per_sm=v[2].value, axis_tile_div=v[3].value)
+
+    def set_schedule(self, z_lines=0, axis_stages=0, rhs_ctas_per_sm=0, axis_tile_div=1):
+        """spk_set_schedule: set the launch schedule (same values computed)."""
+        self._check(lib().spk_set_schedule(self._h, int(z_lines), int(axis_stages), int(rhs_ctas_per_sm),
+                                           int(axis_tile_div)))
 
     # -- diagnostics ---------------------------------------------------------
     def spectrum(self, f1, f2=None):
