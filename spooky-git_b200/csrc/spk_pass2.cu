@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         T* pr0 = valid ? real + (size_t)(2 * p * L + l) * RS : junk;
         T* pr1 = (valid && 2 * p + 1 < nin_all) ? pr0 + LRS : junk;
         const bool to_real = GEN != 0 && a.mode == ZM_TO_REAL && valid && l < nl;
-        regfft_run<T, N, +1>(r, q, tw, xaddr, [&](int z, C2<T> v) {
+        regfft_run<T, N, +1, false, true>(r, q, tw, xaddr, [&](int z, C2<T> v) {
             pr0[z] = v.x;
             pr1[z] = v.y;
             if (GEN != 0 && to_real) {
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         // (forward rounds: FP64 only; in FP32 the branches cost more than they save, measured)
         const bool act = sizeof(T) == 4 || base + sigma_w < nfw;
         if (act) regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
-        regfft_run<T, N, -1, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
+        regfft_run<T, N, -1, true, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
         __syncthreads();
         for (int s2 = warp; s2 < slots; s2 += nwarp) {
             const int tau2 = base + s2;

@@ -149,7 +149,11 @@ __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
 // act = false: a thread with no transform to run (it must be false for a
 // whole warp at a time) only takes part in the barriers, which stay at the
 // same instructions for every warp of the CTA.
-template <typename T, int N, int DIR, int S, typename XA>
+// XP: xaddr(L) is a fixed base plus padi<1>(L) = L + L/16.  Where the legs
+// of a butterfly step through L by a multiple of 16, or stay inside one
+// aligned block of 16, their padded positions are the first leg's plus a
+// compile-time offset, and the exchange addresses them from one pointer.
+template <typename T, int N, int DIR, int S, bool XP = false, typename XA>
 __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool act = true) {
     using F = RegFft<T, N>;
     constexpr int R = F::radix(S);
@@ -157,31 +161,54 @@ __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool 
     __syncthreads();   // earlier readers of the exchange buffer are done
     if (act) {
 #pragma unroll
-        for (int u = 0; u < BPT; u++)
+        for (int u = 0; u < BPT; u++) {
+            // leg t of the writes is at L0 + P H t
+            constexpr int DL = F::P(S) * F::H(S);
+            if constexpr (XP && DL % 16 == 0) {
+                C2<T>* p0 = xaddr(regfft_out_index<T, N, S>(q, u, 0));
 #pragma unroll
-            for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
+                for (int t = 0; t < R; t++) p0[t * (DL + DL / 16)] = a[u * R + t];
+            } else {
+#pragma unroll
+                for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
+            }
+        }
     }
     __syncthreads();
     constexpr int R1 = F::radix(S + 1);
     constexpr int BPT1 = F::E / R1;
+    constexpr int H1 = F::H(S + 1);
     if (act) {
 #pragma unroll
-        for (int u = 0; u < BPT1; u++)
+        for (int u = 0; u < BPT1; u++) {
+            // leg r of the reads is at L0 + H1 r; with H1 = 1 the legs lie in one
+            // aligned block of 16 when R1 is a power of two up to 16
+            if constexpr (XP && H1 % 16 == 0) {
+                const C2<T>* p0 = xaddr(regfft_in_index<T, N, S + 1>(q, u, 0));
 #pragma unroll
-            for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1>(q, u, r));
+                for (int r = 0; r < R1; r++) a[u * R1 + r] = p0[r * (H1 + H1 / 16)];
+            } else if constexpr (XP && H1 == 1 && is_pow2c(R1) && R1 <= 16) {
+                const C2<T>* p0 = xaddr(regfft_in_index<T, N, S + 1>(q, u, 0));
+#pragma unroll
+                for (int r = 0; r < R1; r++) a[u * R1 + r] = p0[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R1; r++) a[u * R1 + r] = *xaddr(regfft_in_index<T, N, S + 1>(q, u, r));
+            }
+        }
     }
 }
 
 // FS: barrier before the last stage's stores (when store() writes into the
 // exchange buffer that the last exchange just read).  act: as for
 // regfft_exchange (no math, no stores, the same barriers).
-template <typename T, int N, int DIR, int S, bool FS, typename XA, typename ST>
+template <typename T, int N, int DIR, int S, bool FS, bool XP, typename XA, typename ST>
 __device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
     using F = RegFft<T, N>;
     if (act) regfft_stage_math<T, N, DIR, S>(a, q, tw);
     if constexpr (S + 1 < F::NS) {
-        regfft_exchange<T, N, DIR, S>(a, q, xaddr, act);
-        regfft_from<T, N, DIR, S + 1, FS>(a, q, tw, xaddr, store, act);
+        regfft_exchange<T, N, DIR, S, XP>(a, q, xaddr, act);
+        regfft_from<T, N, DIR, S + 1, FS, XP>(a, q, tw, xaddr, store, act);
     } else {
         if constexpr (FS && S > 0) __syncthreads();
         constexpr int R = F::radix(S), P = F::P(S);
@@ -208,9 +235,10 @@ __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
         for (int r = 0; r < R; r++) a[u * R + r] = load(regfft_in_index<T, N, 0>(q, u, r));
 }
 
-template <typename T, int N, int DIR, bool FS = false, typename XA, typename ST>
+// XP: see regfft_exchange (xaddr is a fixed base plus padi<1>(L)).
+template <typename T, int N, int DIR, bool FS = false, bool XP = false, typename XA, typename ST>
 __device__ __forceinline__ void regfft_run(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
-    regfft_from<T, N, DIR, 0, FS>(a, q, tw, xaddr, store, act);
+    regfft_from<T, N, DIR, 0, FS, XP>(a, q, tw, xaddr, store, act);
 }
 
 // Host mirror of the geometry.
