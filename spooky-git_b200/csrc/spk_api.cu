@@ -291,9 +291,16 @@ static void launch_axis_kt(spk_ctx* c, AxisArgs& a, long total) {
     // barriers + stages + exchange + twiddles + wavenumbers + row mask (+ alignment)
     const size_t fixed = 256 + (size_t)N * KT * sizeof(C2<T>) + (size_t)RegFft<T, N>::TWN * sizeof(C2<T>) +
                          (size_t)N * sizeof(T) + N + 1024 + 16;   // ... + row mask + outer mask (<= 1024)
-    // stages: as many as keep two CTAs per SM (<= 113 KB each), 2..4
-    long nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
-    a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
+    // stages: as many as keep axis_minb CTAs per SM (228 KB per SM, 1 KB
+    // reserved per CTA): three CTAs of <= 75 KB with 1..4 stages, or two of
+    // <= 113 KB with 2..4 (also when one stage does not fit the three-CTA size)
+    long nst = ((long)(75 * 1024) - (long)fixed) / (long)stage;
+    if (axis_minb<T, N>() == 3 && nst >= 1) {
+        a.nst = (int)std::min<long>(4, nst);
+    } else {
+        nst = ((long)(113 * 1024) - (long)fixed) / (long)stage;
+        a.nst = (int)std::max<long>(2, std::min<long>(4, nst));
+    }
     if (nthr < 256) {
         // narrow tiles (128 threads): 4 CTAs per SM with fewer stages each keep
         // as many loads in flight as 2 CTAs with more, with twice the warps

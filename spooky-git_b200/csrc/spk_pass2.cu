@@ -46,11 +46,22 @@ __host__ __device__ constexpr int axis_kt() {
     return axis_kt_base<T, N, CONV>() / KTD;
 }
 
+// CTAs per SM the strided-axis pass is compiled for.  FP64 transforms of
+// up to 256 points hold at most 8 elements per thread and fit 80 registers
+// with little spilling, so three CTAs (one pipeline stage each) keep more
+// warps resident (256^3 plain form: 6.00 -> 5.75 ms per step).  The FP32
+// form's 16 elements per thread, and the longer FP64 transforms, spill at 80
+// registers and keep two CTAs (512^3 plain form: 59.8 ms with two, 69.9 ms
+// with three).
+template <typename T, int N> __host__ __device__ constexpr int axis_minb() {
+    return (sizeof(T) == 8 && N <= 256 && RegFft<T, N>::E <= 8) ? 3 : 2;
+}
+
 // DEF: the x inverse of RK3 stage 1 or 2 with deferred masked modes (its own
 // instantiation, so that the other passes keep their registers).  KTD: tile
 // width divisor (1, or 2 for the half tiles of short axes).
 template <typename T, int N, int DIR, bool CONV, bool DEF, int KTD>
-__global__ void __launch_bounds__(256, 2) k_axis2(const __grid_constant__ AxisArgs a) {
+__global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_constant__ AxisArgs a) {
     using F = RegFft<T, N>;
     constexpr int KT = axis_kt<T, N, CONV, KTD>(), LKT = ilog2c(KT);
     extern __shared__ __align__(128) unsigned char smem_raw[];
