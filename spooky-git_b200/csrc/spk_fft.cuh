@@ -110,6 +110,8 @@ struct FftPlan {
 // Element n of a column at n (PAD = 0) or n + n/16 (PAD = 1: one pad slot
 // per 16 elements breaks the stride-R bank conflicts of contiguous columns).
 template <int PAD> __device__ __forceinline__ int padi(int n) { return PAD ? n + (n >> 4) : n; }
+// n plus one pad element per block of B (a power of two), n >= 0
+template <int B> __device__ __forceinline__ int padb(int n) { return n + (int)((unsigned)n / (unsigned)B); }
 __host__ __device__ inline int padded_len(int n) { return n + (n >> 4); }
 
 __host__ __device__ inline int ilog2(int n) { int l = 0; while ((1 << l) < n) l++; return l; }

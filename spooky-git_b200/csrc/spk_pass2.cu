@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
 //     STS flux, and the products -- TracelessShearMatrix[MHD]
 //     (cuda_kernels.cu:39-55, 216-234), MagneticEmf (:240-252),
 //     EnergyFluxVector (:277-289), ComputeBGradTheta +
-//     ComputeAnisotropicHeatFlux (:360-383) -- as complex pairs in the input
-//     area, which is free by then;
+//     ComputeAnisotropicHeatFlux (:360-383) -- as pairs (two real planes in
+//     FP64, complex pairs in FP32) in the input area, which is free by then;
 //  4. the product pairs are forward-transformed and unpacked into the half
 //     spectra of each product (their D2Z), kz < kz_keep.
 // ---------------------------------------------------------------------------
@@ -303,10 +303,14 @@ struct ZSmem { size_t tw, zero, junk, area, real, xb, cw, bre, total; };
 __host__ __device__ inline bool zpass_alias(int gen, int nstages, int npin, int npout, int lines, int slots) {
     return gen == 0 && nstages >= 2 && npin * lines <= slots && npout * lines <= slots;
 }
+// Exchange slots of the z pass pad one element per 128-byte row of complex
+// elements (16 in FP32, 8 in FP64), which keeps the exchanges of the
+// register FFT free of bank conflicts in both precisions.
+__host__ __device__ constexpr int zpass_xblock(int csz) { return 128 / csz; }
 __host__ __device__ inline ZSmem zsmem_layout(int n, int twn, int csz, int nin, int nin_all, int npout, int lines,
                                               int nzs, int slots, int ncw, bool alias, int nbre = 0) {
     ZSmem z;
-    const int rs = n + 16, xs = n + (n >> 4);
+    const int rs = n + 16, xs = n + n / zpass_xblock(csz);
     z.tw = 128;
     z.zero = align16(z.tw + (size_t)twn * csz);              // a zero half spectrum (missing pair partner)
     z.junk = align16(z.zero + (size_t)nzs * csz);            // a real row that idle transforms write
@@ -343,7 +347,8 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     using F = RegFft<T, N>;
     constexpr int LTPC = F::LTPC, TPC = F::TPC;
     constexpr int RS = N + 16;            // real rows: consecutive lines start 16 words apart in bank
-    constexpr int XS = N + (N >> 4);      // exchange slot (one pad element per 16)
+    constexpr int XB = zpass_xblock((int)sizeof(C2<T>));
+    constexpr int XS = N + N / XB;        // exchange slot (one pad element per XB)
     if (a.gate && a.gate_stage > a.gate->s_rkl) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int L = a.lines, nzs = a.g.nzs;
@@ -372,7 +377,15 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     C2<T>* zrow = reinterpret_cast<C2<T>*>(smem_raw + lay.zero);
     T* junk = reinterpret_cast<T*>(smem_raw + lay.junk);
     C2<T>* raw = reinterpret_cast<C2<T>*>(smem_raw + lay.area);
-    C2<T>* prod = raw;                    // the product pairs reuse the input area
+    // the product pairs reuse the input area: pair p of line l takes the 2N
+    // reals at (p*L + l)*2N.  FP64: two planes (channel 2p, then 2p+1), whose
+    // 8-byte stores from the point loop are free of bank conflicts (the
+    // plain pass is bound by shared-memory wavefronts).  FP32: interleaved
+    // complex pairs, one load per leg of the forward transform (the FP32
+    // pass is bound by instruction issue).
+    constexpr bool PLANES = sizeof(T) == 8;
+    constexpr int CS = PLANES ? N : 1;    // reals from channel 2p to 2p+1
+    T* prodT = reinterpret_cast<T*>(raw);
     T* real = reinterpret_cast<T*>(smem_raw + lay.real);
     C2<T>* xb = reinterpret_cast<C2<T>*>(smem_raw + lay.xb);
     float* cw = reinterpret_cast<float*>(smem_raw + lay.cw);
@@ -422,7 +435,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     // no masked content: the inverse passes left kz >= kz_keep unwritten, and
     // those modes enter as zero
     const int kzk = (a.trim && !bsc->masked_live) ? a.g.kz_keep : nzs;
-    auto xaddr = [&](int Lx) { return xb + (size_t)sigma * XS + padi<1>(Lx); };
+    auto xaddr = [&](int Lx) { return xb + (size_t)sigma * XS + padb<XB>(Lx); };
     C2<T> r[F::E];
 
     // 2. inverse transforms of the input pairs
@@ -477,7 +490,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         T* pr0 = valid ? real + (size_t)(2 * p * L + l) * RS : junk;
         T* pr1 = (valid && 2 * p + 1 < nin_all) ? pr0 + LRS : junk;
         const bool to_real = GEN != 0 && a.mode == ZM_TO_REAL && valid && l < nl;
-        regfft_run<T, N, +1, false, true>(r, q, tw, xaddr, [&](int z, C2<T> v) {
+        regfft_run<T, N, +1, false, XB>(r, q, tw, xaddr, [&](int z, C2<T> v) {
             pr0[z] = v.x;
             pr1[z] = v.y;
             if (GEN != 0 && to_real) {
@@ -497,7 +510,6 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
     {
         T mu[8] = {(T)0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
         int bad = 0;
-        T* prodT = reinterpret_cast<T*>(prod);
         const T third = (T)(1.0 / 3.0);
         const size_t pstride = (size_t)L * N * 2;   // scalars between product pairs
         // the closure's gradient components of the point at fr (variant 2: all nine
@@ -585,8 +597,8 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             if (a.ch_gy >= 0) gy = fr[a.ch_gy * LRS];
             if (a.derive_gz == 1) gz = fr[nin * LRS];
             else if (a.derive_gz == 2) gz = fr[a.ch_th * LRS];
-            T* pp = prodT + ((size_t)l * N + z) * 2;
-            auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1)] = v; };
+            T* pp = prodT + (PLANES ? (size_t)l * 2 * N + z : ((size_t)l * N + z) * 2);
+            auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1) * CS] = v; };
             int qc = 0;
             // learned closure: -2 nu_t S into the stress, -eta_t J into the EMF
             float ctau[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, cemf[3] = {0.f, 0.f, 0.f};
@@ -630,7 +642,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
                     }
                     if (clos)
 #pragma unroll
-                        for (int r = 0; r < 5; r++) pp[(size_t)(r >> 1) * pstride + (r & 1)] += (T)ctau[r];
+                        for (int r = 0; r < 5; r++) pp[(size_t)(r >> 1) * pstride + (r & 1) * CS] += (T)ctau[r];
                     qc = 5;
                 }
                 if (a.mhd) {
@@ -693,11 +705,14 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         const int tau = base + sigma;
         const bool valid = tau < nfw;
         const int p = valid ? tau / L : 0, l = valid ? tau - p * L : 0;
-        const C2<T>* pp = prod + (size_t)(p * L + l) * N;
+        const T* pp = prodT + (size_t)(p * L + l) * 2 * N;
         // (forward rounds: FP64 only; in FP32 the branches cost more than they save, measured)
         const bool act = sizeof(T) == 4 || base + sigma_w < nfw;
-        if (act) regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> { return pp[z]; });
-        regfft_run<T, N, -1, true, true>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
+        if (act) regfft_load<T, N, -1>(r, q, [&](int z) -> C2<T> {
+            if constexpr (PLANES) return mk<T>(pp[z], pp[N + z]);
+            else return reinterpret_cast<const C2<T>*>(pp)[z];
+        });
+        regfft_run<T, N, -1, true, XB>(r, q, tw, xaddr, [&](int k, C2<T> v) { *xaddr(k) = v; }, act);
         __syncthreads();
         for (int s2 = warp; s2 < slots; s2 += nwarp) {
             const int tau2 = base + s2;
@@ -710,7 +725,7 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
             C2<T>* o1 = out + (size_t)(2 * p2 + 1) * a.cs_out + off0;
             const bool two = 2 * p2 + 1 < a.nout;
             for (int k = lane; k < kk; k += 32) {
-                const C2<T> zk = Z[padi<1>(k)], zm = Z[padi<1>(k ? N - k : 0)];
+                const C2<T> zk = Z[padb<XB>(k)], zm = Z[padb<XB>(k ? N - k : 0)];
                 o0[k] = mk<T>(half * (zk.x + zm.x), half * (zk.y - zm.y));
                 if (two) o1[k] = mk<T>(half * (zk.y + zm.y), half * (zm.x - zk.x));
             }

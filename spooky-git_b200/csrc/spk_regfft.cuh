@@ -149,25 +149,27 @@ __device__ __forceinline__ int regfft_out_index(int q, int u, int t) {
 // act = false: a thread with no transform to run (it must be false for a
 // whole warp at a time) only takes part in the barriers, which stay at the
 // same instructions for every warp of the CTA.
-// XP: xaddr(L) is a fixed base plus padi<1>(L) = L + L/16.  Where the legs
-// of a butterfly step through L by a multiple of 16, or stay inside one
-// aligned block of 16, their padded positions are the first leg's plus a
-// compile-time offset, and the exchange addresses them from one pointer.
-template <typename T, int N, int DIR, int S, bool XP = false, typename XA>
+// XB: 0, or the pad block of the caller's layout: xaddr(L) is a fixed base
+// plus L + L/XB (XB a power of two).  Where the legs of a butterfly step
+// through L by a multiple of XB, or stay inside one aligned block of XB,
+// their padded positions are the first leg's plus a compile-time offset,
+// and the exchange addresses them from one pointer.
+template <typename T, int N, int DIR, int S, int XB = 0, typename XA>
 __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool act = true) {
     using F = RegFft<T, N>;
     constexpr int R = F::radix(S);
     constexpr int BPT = F::E / R;
+    constexpr int XBD = XB > 0 ? XB : 1;   // a nonzero divisor for the XB = 0 branches
     __syncthreads();   // earlier readers of the exchange buffer are done
     if (act) {
 #pragma unroll
         for (int u = 0; u < BPT; u++) {
             // leg t of the writes is at L0 + P H t
             constexpr int DL = F::P(S) * F::H(S);
-            if constexpr (XP && DL % 16 == 0) {
+            if constexpr (XB > 0 && DL % XBD == 0) {
                 C2<T>* p0 = xaddr(regfft_out_index<T, N, S>(q, u, 0));
 #pragma unroll
-                for (int t = 0; t < R; t++) p0[t * (DL + DL / 16)] = a[u * R + t];
+                for (int t = 0; t < R; t++) p0[t * (DL + DL / XBD)] = a[u * R + t];
             } else {
 #pragma unroll
                 for (int t = 0; t < R; t++) *xaddr(regfft_out_index<T, N, S>(q, u, t)) = a[u * R + t];
@@ -182,12 +184,12 @@ __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool 
 #pragma unroll
         for (int u = 0; u < BPT1; u++) {
             // leg r of the reads is at L0 + H1 r; with H1 = 1 the legs lie in one
-            // aligned block of 16 when R1 is a power of two up to 16
-            if constexpr (XP && H1 % 16 == 0) {
+            // aligned block of XB when R1 is a power of two up to XB
+            if constexpr (XB > 0 && H1 % XBD == 0) {
                 const C2<T>* p0 = xaddr(regfft_in_index<T, N, S + 1>(q, u, 0));
 #pragma unroll
-                for (int r = 0; r < R1; r++) a[u * R1 + r] = p0[r * (H1 + H1 / 16)];
-            } else if constexpr (XP && H1 == 1 && is_pow2c(R1) && R1 <= 16) {
+                for (int r = 0; r < R1; r++) a[u * R1 + r] = p0[r * (H1 + H1 / XBD)];
+            } else if constexpr (XB > 0 && H1 == 1 && is_pow2c(R1) && R1 <= XB) {
                 const C2<T>* p0 = xaddr(regfft_in_index<T, N, S + 1>(q, u, 0));
 #pragma unroll
                 for (int r = 0; r < R1; r++) a[u * R1 + r] = p0[r];
@@ -202,13 +204,13 @@ __device__ __forceinline__ void regfft_exchange(C2<T>* a, int q, XA xaddr, bool 
 // FS: barrier before the last stage's stores (when store() writes into the
 // exchange buffer that the last exchange just read).  act: as for
 // regfft_exchange (no math, no stores, the same barriers).
-template <typename T, int N, int DIR, int S, bool FS, bool XP, typename XA, typename ST>
+template <typename T, int N, int DIR, int S, bool FS, int XB, typename XA, typename ST>
 __device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
     using F = RegFft<T, N>;
     if (act) regfft_stage_math<T, N, DIR, S>(a, q, tw);
     if constexpr (S + 1 < F::NS) {
-        regfft_exchange<T, N, DIR, S, XP>(a, q, xaddr, act);
-        regfft_from<T, N, DIR, S + 1, FS, XP>(a, q, tw, xaddr, store, act);
+        regfft_exchange<T, N, DIR, S, XB>(a, q, xaddr, act);
+        regfft_from<T, N, DIR, S + 1, FS, XB>(a, q, tw, xaddr, store, act);
     } else {
         if constexpr (FS && S > 0) __syncthreads();
         constexpr int R = F::radix(S), P = F::P(S);
@@ -235,10 +237,10 @@ __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
         for (int r = 0; r < R; r++) a[u * R + r] = load(regfft_in_index<T, N, 0>(q, u, r));
 }
 
-// XP: see regfft_exchange (xaddr is a fixed base plus padi<1>(L)).
-template <typename T, int N, int DIR, bool FS = false, bool XP = false, typename XA, typename ST>
+// XB: see regfft_exchange (0, or the pad block of xaddr's layout).
+template <typename T, int N, int DIR, bool FS = false, int XB = 0, typename XA, typename ST>
 __device__ __forceinline__ void regfft_run(C2<T>* a, int q, const C2<T>* tw, XA xaddr, ST store, bool act = true) {
-    regfft_from<T, N, DIR, 0, FS, XP>(a, q, tw, xaddr, store, act);
+    regfft_from<T, N, DIR, 0, FS, XB>(a, q, tw, xaddr, store, act);
 }
 
 // Host mirror of the geometry.
