@@ -404,6 +404,11 @@ static void axis(spk_ctx* c, AxisArgs& a, int dir) {
         return;
     }
     if (a.njobs == 0) return;
+    if (a.row_filter && dir > 0) {   // the three-CTA k_axis2 filters the rows of forward passes only
+        c->err = "internal: row filter on an inverse axis pass";
+        c->sticky = SPK_ERR_ARG;
+        return;
+    }
     if (c->fp32) launch_axis<float>(c, a, dir);
     else launch_axis<double>(c, a, dir);
 }

@@ -140,6 +140,14 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
         for (int i = tid; i < nouter; i += blockDim.x) okeep[i] = og[i] != 0.0;
     }
     __syncthreads();
+    // The kept rows among this thread's outputs, one bit per store of the
+    // last stage (the row filter of the forward passes), and a load path for
+    // tiles with no per-row factor: in the forward passes, and in every pass
+    // of the two-CTA instantiations.  The three-CTA (FP64) inverse passes
+    // keep the plain forms, which spill less at their 80 registers.
+    constexpr bool LEAN = DIR < 0 || axis_minb<T, N>() == 2;
+    uint32_t keepm = ~0u;
+    if constexpr (LEAN) keepm = regfft_store_mask<T, N>(q, [&](int k) { return keep[k] != 0; });
     if (tid == 0)
         for (int s = 0; s < NST; s++) {
             const int t = blockIdx.x + s * gridDim.x;
@@ -228,6 +236,14 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
                     if (dfr) { const T f = deferred(n); v = mk<T>(f * v.x, f * v.y); }
                 return v;
             });
+        } else if (LEAN && !zrows && !deriv && !jo.hp && !(DEF && dfr)) {
+            // no per-row factor: the flags stay off the element loop
+            const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
+            const T sc = (T)scale;
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
+                const C2<T> v = src[n * KT + c];
+                return mk<T>(v.x * sc, v.y * sc);
+            });
         } else {
             const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
             const T sc = (T)scale;
@@ -255,13 +271,22 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
         }
         const size_t base = a.axis == 0 ? (size_t)o * a.g.nzs : (size_t)o * a.g.ny * a.g.nzs;
         C2<T>* out = (C2<T>*)jo.out + (size_t)box * a.out_box_ch * a.g.ncs + base + k0;
+        // outputs this thread stores: its column inside the box, and in a
+        // row-filtered pass the kept rows (bit e: the e-th store of the last
+        // stage)
         const bool col_ok = c < kt;
-        const bool filt = a.row_filter != 0;
+        const uint32_t smask = !col_ok ? 0u : (a.row_filter ? keepm : ~0u);
         if (skip) continue;
+        int e = 0;   // store counter: a constant per call once the stores are unrolled
         regfft_run<T, N, DIR>(
             r, q, tw, [&](int L) { return xbuf + (size_t)L * KT + c; },
             [&](int k, C2<T> v) {
-                if (col_ok && (!filt || keep[k])) out[k * stride + c] = v;
+                if constexpr (LEAN) {
+                    if ((smask >> e) & 1u) out[k * stride + c] = v;
+                    e++;
+                } else if (col_ok) {
+                    out[k * stride + c] = v;
+                }
             });
     }
     if (aborted) {

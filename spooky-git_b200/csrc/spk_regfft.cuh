@@ -225,6 +225,25 @@ __device__ __forceinline__ void regfft_from(C2<T>* a, int q, const C2<T>* tw, XA
     }
 }
 
+// Bit u*R + t set where pred(k) holds for the output k that thread q hands
+// to store() as its (u, t)-th call of the last stage (the order of
+// regfft_from's stores), so that a caller can test a per-output condition
+// from one register.
+template <typename T, int N, typename PR>
+__device__ __forceinline__ uint32_t regfft_store_mask(int q, PR pred) {
+    using F = RegFft<T, N>;
+    static_assert(F::E <= 32, "one bit per element");
+    constexpr int S = F::NS - 1, R = F::radix(S), P = F::P(S);
+    constexpr int BPT = F::E / R;
+    uint32_t m = 0;
+#pragma unroll
+    for (int u = 0; u < BPT; u++)
+#pragma unroll
+        for (int t = 0; t < R; t++)
+            if (pred((q + u * F::TPC) + P * t)) m |= 1u << (u * R + t);
+    return m;
+}
+
 // Load the first-stage legs through load(n).
 template <typename T, int N, int DIR, typename LD>
 __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
