@@ -140,14 +140,20 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
         for (int i = tid; i < nouter; i += blockDim.x) okeep[i] = og[i] != 0.0;
     }
     __syncthreads();
-    // The kept rows among this thread's outputs, one bit per store of the
-    // last stage (the row filter of the forward passes), and a load path for
-    // tiles with no per-row factor: in the forward passes, and in every pass
-    // of the two-CTA instantiations.  The three-CTA (FP64) inverse passes
-    // keep the plain forms, which spill less at their 80 registers.
+    // The kept rows among this thread's outputs (forward passes: one bit per
+    // store of the last stage, the row filter) or inputs (inverse passes: one
+    // bit per load of the first stage, the zero rows of the trimmed y
+    // inverse), and load paths with the per-tile flags off the element loop:
+    // in the forward passes, and in every pass of the two-CTA
+    // instantiations.  The three-CTA (FP64) inverse passes keep the plain
+    // forms, which spill less at their 80 registers.
     constexpr bool LEAN = DIR < 0 || axis_minb<T, N>() == 2;
     uint32_t keepm = ~0u;
-    if constexpr (LEAN) keepm = regfft_store_mask<T, N>(q, [&](int k) { return keep[k] != 0; });
+    if constexpr (LEAN) {
+        auto kept = [&](int k) { return keep[k] != 0; };
+        if constexpr (DIR < 0) keepm = regfft_store_mask<T, N>(q, kept);
+        else keepm = regfft_load_mask<T, N>(q, kept);
+    }
     if (tid == 0)
         for (int s = 0; s < NST; s++) {
             const int t = blockIdx.x + s * gridDim.x;
@@ -224,6 +230,13 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
             return (col_out || !keep[n]) ? f : (T)1;
         };
         if (skip) {
+        } else if (CONV && !deriv && !jo.hp && !(DEF && dfr)) {
+            // FP64 input, no per-row factor
+            const double2* src = reinterpret_cast<const double2*>(stg);
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
+                const double2 x = src[n * KT + c];
+                return mk<T>((T)(x.x * scale), (T)(x.y * scale));
+            });
         } else if constexpr (CONV) {
             const double2* src = reinterpret_cast<const double2*>(stg);
             const double* kd = a.axis == 0 ? a.g.kx : a.g.ky;   // FP64 derivative on the FP64 input
@@ -242,6 +255,17 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
             const T sc = (T)scale;
             regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
                 const C2<T> v = src[n * KT + c];
+                return mk<T>(v.x * sc, v.y * sc);
+            });
+        } else if (LEAN && DIR > 0 && zrows && !deriv && !jo.hp && !(DEF && dfr)) {
+            // the trimmed y inverse: masked rows read as zero (bit e: the e-th load)
+            const C2<T>* src = reinterpret_cast<const C2<T>*>(stg);
+            const T sc = (T)scale;
+            int e = 0;   // load counter: a constant per call once the loads are unrolled
+            regfft_load<T, N, DIR>(r, q, [&](int n) -> C2<T> {
+                C2<T> v = src[n * KT + c];
+                if (!((keepm >> e) & 1u)) v = mk<T>((T)0, (T)0);
+                e++;
                 return mk<T>(v.x * sc, v.y * sc);
             });
         } else {
@@ -275,7 +299,7 @@ __global__ void __launch_bounds__(256, axis_minb<T, N>()) k_axis2(const __grid_c
         // row-filtered pass the kept rows (bit e: the e-th store of the last
         // stage)
         const bool col_ok = c < kt;
-        const uint32_t smask = !col_ok ? 0u : (a.row_filter ? keepm : ~0u);
+        const uint32_t smask = !col_ok ? 0u : (DIR < 0 && a.row_filter ? keepm : ~0u);
         if (skip) continue;
         int e = 0;   // store counter: a constant per call once the stores are unrolled
         regfft_run<T, N, DIR>(

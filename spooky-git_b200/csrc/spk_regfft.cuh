@@ -244,6 +244,23 @@ __device__ __forceinline__ uint32_t regfft_store_mask(int q, PR pred) {
     return m;
 }
 
+// Bit u*R + r set where pred(n) holds for the input n that thread q reads
+// as its (u, r)-th call of load() in regfft_load.
+template <typename T, int N, typename PR>
+__device__ __forceinline__ uint32_t regfft_load_mask(int q, PR pred) {
+    using F = RegFft<T, N>;
+    static_assert(F::E <= 32, "one bit per element");
+    constexpr int R = F::radix(0);
+    constexpr int BPT = F::E / R;
+    uint32_t m = 0;
+#pragma unroll
+    for (int u = 0; u < BPT; u++)
+#pragma unroll
+        for (int r = 0; r < R; r++)
+            if (pred(regfft_in_index<T, N, 0>(q, u, r))) m |= 1u << (u * R + r);
+    return m;
+}
+
 // Load the first-stage legs through load(n).
 template <typename T, int N, int DIR, typename LD>
 __device__ __forceinline__ void regfft_load(C2<T>* a, int q, LD load) {
