@@ -589,6 +589,54 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
         // in one chunk
         unsigned char* c3rows = reinterpret_cast<unsigned char*>(cw) + C3_FWD_BYTES;
         const int EPC = GEN == 3 ? C3_ZCHUNK : L * N;
+        // The products of incompressible HD and MHD alone (the RK3 step):
+        // the general loop's arithmetic, in the same order, with its
+        // per-point flag tests hoisted (one loop per field set).
+        const bool hdmhd = GEN == 0 && want_prod && a.mode == ZM_PRODUCTS && a.hydro && !a.bous && !a.aniso &&
+                           !a.load_breal && !a.store_breal && a.ch_u >= 0 && (!a.mhd || a.ch_b >= 0);
+        auto hdmhd_loop = [&](auto mhd_c) {
+            constexpr bool MHD = decltype(mhd_c)::value;
+            const int cu = a.ch_u * LRS, cb = MHD ? a.ch_b * LRS : 0;
+            const bool dmax = a.do_max != 0, odd = (a.nout & 1) != 0;
+            for (int e = tid; e < L * N; e += nthr) {
+                const int l = (int)((unsigned)e / (unsigned)N), z = e - l * N;
+                const T* fr = real + (size_t)l * RS + z;
+                const T ux = fr[cu], uy = fr[cu + LRS], uz = fr[cu + 2 * LRS];
+                T bx = 0, by = 0, bz = 0;
+                if constexpr (MHD) { bx = fr[cb]; by = fr[cb + LRS]; bz = fr[cb + 2 * LRS]; }
+                if (dmax && l < nl) {
+                    const T av[6] = {fabs(ux), fabs(uy), fabs(uz), fabs(bx), fabs(by), fabs(bz)};
+#pragma unroll
+                    for (int c = 0; c < 6; c++) {
+                        if (!isfinite(av[c])) bad = 1;
+                        mu[c] = fmax(mu[c], av[c]);
+                    }
+                }
+                T* pp = prodT + (PLANES ? (size_t)l * 2 * N + z : ((size_t)l * N + z) * 2);
+                auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1) * CS] = v; };
+                if constexpr (!MHD) {
+                    put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz) * third);
+                    put(1, ux * uy);
+                    put(2, ux * uz);
+                    put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz) * third);
+                    put(4, uy * uz);
+                } else {
+                    put(0, ((T)2.0 * ux * ux - uy * uy - uz * uz - (T)2.0 * bx * bx + by * by + bz * bz) * third);
+                    put(1, ux * uy - bx * by);
+                    put(2, ux * uz - bx * bz);
+                    put(3, (-ux * ux + (T)2.0 * uy * uy - uz * uz + bx * bx - (T)2.0 * by * by + bz * bz) * third);
+                    put(4, uy * uz - by * bz);
+                    put(5, -by * uz + bz * uy + (T)0.f);
+                    put(6, bx * uz - bz * ux + (T)0.f);
+                    put(7, -bx * uy + by * ux + (T)0.f);
+                }
+                if (odd) put(a.nout, (T)0);
+            }
+        };
+        if (hdmhd) {
+            if (a.mhd) hdmhd_loop(std::integral_constant<bool, true>());
+            else hdmhd_loop(std::integral_constant<bool, false>());
+        } else
         for (int e0 = 0; e0 < L * N; e0 += EPC) {
         if constexpr (GEN == 3) {
             if (clos) {
