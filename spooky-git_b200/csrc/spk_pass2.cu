@@ -633,9 +633,40 @@ __global__ void __launch_bounds__(128, GEN == 0 ? (sizeof(T) == 4 ? 6 : 5) : 4) 
                 if (odd) put(a.nout, (T)0);
             }
         };
+        // The anisotropic heat flux of an RKL2 stage (ZM_RKL_FLUX with the real
+        // B lines staged): the general loop's arithmetic, in the same order,
+        // with its per-point flag tests hoisted.
+        const bool flux = GEN == 1 && stage_b && want_prod && a.mode == ZM_RKL_FLUX && a.aniso && !a.store_breal &&
+                          !a.do_max && a.ch_u < 0 && a.derive_gz == 2 && a.ch_gx >= 0 && a.ch_gy >= 0 &&
+                          a.shear_part == 0 && !clos;
         if (hdmhd) {
             if (a.mhd) hdmhd_loop(std::integral_constant<bool, true>());
             else hdmhd_loop(std::integral_constant<bool, false>());
+        } else if (flux) {
+            const int cgx = a.ch_gx * LRS, cgy = a.ch_gy * LRS, cgz = a.ch_th * LRS;
+            const int sd = a.sd;
+            const bool odd = (a.nout & 1) != 0;
+            const T chi = (T)a.chi, W = (T)a.omegaT2;
+            for (int e = tid; e < L * N; e += nthr) {
+                const int l = (int)((unsigned)e / (unsigned)N), z = e - l * N;
+                const T* fr = real + (size_t)l * RS + z;
+                T bx = 0, by = 0, bz = 0;
+                if (l < nl) {
+                    bx = bre[(size_t)(0 * L + l) * N + z];
+                    by = bre[(size_t)(1 * L + l) * N + z];
+                    bz = bre[(size_t)(2 * L + l) * N + z];
+                }
+                const T gx = fr[cgx], gy = fr[cgy], gz = fr[cgz];
+                T* pp = prodT + (PLANES ? (size_t)l * 2 * N + z : ((size_t)l * N + z) * 2);
+                auto put = [&](int ch, T v) { pp[(size_t)(ch >> 1) * pstride + (ch & 1) * CS] = v; };
+                const T bgt = bx * gx + by * gy + bz * gz;
+                const T b2 = bx * bx + by * by + bz * bz;
+                const T bs = sd == 0 ? bx : (sd == 1 ? by : bz);
+                put(0, chi * bx * (bgt + W * bs) / b2);
+                put(1, chi * by * (bgt + W * bs) / b2);
+                put(2, chi * bz * (bgt + W * bs) / b2);
+                if (odd) put(a.nout, (T)0);
+            }
         } else
         for (int e0 = 0; e0 < L * N; e0 += EPC) {
         if constexpr (GEN == 3) {
