@@ -919,173 +919,190 @@ __global__ void __launch_bounds__(128, MINB) k_rhs(const __grid_constant__ XfArg
     const int kzk = a.g.kz_keep;
     const size_t total = (compact ? (size_t)a.nkx * a.nky * kzk : nc) * (size_t)a.nb;
     const double shx = grid_shx(a.g);   // shearing box: kx = kx0 + shx ky
-    for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
-        int k, i, j, box;
-        unsigned line;
-        if (compact) {
-            // compact index -> box, kept x index, kept y index, k < kz_keep
-            const unsigned r1 = a.fd_kzk.div((unsigned)gb);
-            k = (int)(gb - (size_t)r1 * kzk);
-            const unsigned r2 = a.fd_nky.div(r1);
-            const int jy = (int)(r1 - r2 * (unsigned)a.nky);
-            const unsigned r3 = a.fd_nkx.div(r2);
-            const int ix = (int)(r2 - r3 * (unsigned)a.nkx);
-            box = (int)r3;
-            i = a.kxi[ix];
-            j = a.kyi[jy];
-            line = (unsigned)i * ny + (unsigned)j;
-        } else {
-            // global line over the boxes -> box, line, k (nx*ny is a power of two)
-            const unsigned gline = fzh.div((unsigned)gb);
-            k = (int)(gb - (size_t)gline * nzh);
-            const unsigned ubox = a.fd_nl.div(gline);
-            box = (int)ubox;
-            line = gline - ubox * nlines;
-            const unsigned ui = a.fd_ny.div(line);
-            i = (int)ui;
-            j = (int)(line - ui * ny);
-        }
-        const size_t gi = (size_t)line * nzh + k;                // mode within the box
-        const size_t bo = (size_t)box * a.box_state;            // box offset in U, S, out
-        const double dt = a.sc[box].dt, nu = a.sc[box].nu, nu_m = a.sc[box].nu_m, nu_th = a.sc[box].nu_th;
-        const bool m = a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0;
-
-        const C2<T>* nl = (const C2<T>*)a.nl + (size_t)box * a.box_nl;
-        const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
-        auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
-
-        // every load of the mode first (state, RK scratch, products), so that
-        // they are all in flight together
-        double2 Xu[3] = {z0, z0, z0}, Xb[3] = {z0, z0, z0}, Xt = z0;
-        double2 Su[3] = {z0, z0, z0}, Sb[3] = {z0, z0, z0}, St = z0;
-        double2 t0 = z0, t1 = z0, t2 = z0, t3 = z0, t4 = z0, e0 = z0, e1 = z0, e2 = z0;
-        double2 f0 = z0, f1 = z0, f2 = z0, q0 = z0, q1 = z0, q2 = z0;
-        if (a.incompressible) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                Xu[c] = a.U[bo + (size_t)(a.VEL + c) * nc + gi];
-                if (needS) Su[c] = a.S[bo + (size_t)(a.VEL + c) * nc + gi];
-            }
-        }
-        if (a.mhd) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                Xb[c] = a.U[bo + (size_t)(a.MAG + c) * nc + gi];
-                if (needS) Sb[c] = a.S[bo + (size_t)(a.MAG + c) * nc + gi];
-            }
-        }
-        if (a.bous) {
-            Xt = a.U[bo + (size_t)a.TH * nc + gi];
-            if (needS) St = a.S[bo + (size_t)a.TH * nc + gi];
-        }
-        if (m) {
-            if (a.incompressible && a.nl_T >= 0) { t0 = P(a.nl_T); t1 = P(a.nl_T + 1); t2 = P(a.nl_T + 2); t3 = P(a.nl_T + 3); t4 = P(a.nl_T + 4); }
-            if (a.mhd && a.nl_E >= 0) { e0 = P(a.nl_E); e1 = P(a.nl_E + 1); e2 = P(a.nl_E + 2); }
-            if (a.bous && a.nl_F >= 0) { f0 = P(a.nl_F); f1 = P(a.nl_F + 1); f2 = P(a.nl_F + 2); }
-            if (a.bous && a.aniso_rhs && a.nl_Q >= 0) { q0 = P(a.nl_Q); q1 = P(a.nl_Q + 1); q2 = P(a.nl_Q + 2); }
-        }
-        const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
-        const double k2 = kx * kx + ky * ky + kz * kz;
-        double2 usd = z0;
-
-        if (a.incompressible) {
-            double2 R[3];
-            // -i * mask * k_j T_ij with T = [[t0 t1 t2] [t1 t3 t4] [t2 t4 -t0-t3]]
-            const double2 s0 = d2(kx * t0.x + ky * t1.x + kz * t2.x, kx * t0.y + ky * t1.y + kz * t2.y);
-            const double2 s1 = d2(kx * t1.x + ky * t3.x + kz * t4.x, kx * t1.y + ky * t3.y + kz * t4.y);
-            const double2 s2 = d2(kx * t2.x + ky * t4.x - kz * (t0.x + t3.x), kx * t2.y + ky * t4.y - kz * (t0.y + t3.y));
-            R[0] = d2(s0.y, -s0.x);
-            R[1] = d2(s1.y, -s1.x);
-            R[2] = d2(s2.y, -s2.x);
-            if (a.strat) {
-                if (a.sd == 0)      { R[0] = d2(R[0].x - Xt.x, R[0].y - Xt.y); usd = Xu[0]; }
-                else if (a.sd == 1) { R[1] = d2(R[1].x - Xt.x, R[1].y - Xt.y); usd = Xu[1]; }
-                else                { R[2] = d2(R[2].x - Xt.x, R[2].y - Xt.y); usd = Xu[2]; }
-            }
-            if (a.g.shear != 0.0) {
-                // BackgroundShear / BackgroundRotation (shear_rotation.cu:11-63):
-                // dvy += S vx; with rotation dvx += 2 omega vy, dvy -= 2 omega vx
-                const double S = a.g.shear;
-                R[1] = d2(R[1].x + S * Xu[0].x, R[1].y + S * Xu[0].y);
-                if (a.rotating) {
-                    const double w2 = 2.0 * a.omega;
-                    R[0] = d2(R[0].x + w2 * Xu[1].x, R[0].y + w2 * Xu[1].y);
-                    R[1] = d2(R[1].x - w2 * Xu[0].x, R[1].y - w2 * Xu[0].y);
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                if (!((a.sts_mask >> (a.VEL + c)) & 1u)) {
-                    const double f = -nu * k2;
-                    R[c] = d2(R[c].x + f * Xu[c].x, R[c].y + f * Xu[c].y);
-                }
-            }
-            // Leray: dU += i k (i k.dU)/k^2; the shearing box adds S ky vx to
-            // k.dU (GradPseudoPressureShearing, cuda_kernels.cu:165-196)
-            const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
-            double sx, sy;
-            if (a.g.shear != 0.0) {
-                const double Sky = a.g.shear * ky;
-                sx = Sky * Xu[0].x + kx * R[0].x + ky * R[1].x + kz * R[2].x;
-                sy = Sky * Xu[0].y + kx * R[0].y + ky * R[1].y + kz * R[2].y;
+    // One copy of the mode loop with the flags of incompressible MHD (no
+    // Boussinesq, stratification, shearing box or super-time-stepping) fixed
+    // at compile time, which keeps the unused fields' registers out of it;
+    // the general copy serves every other configuration.  Same arithmetic.
+    auto modes = [&](auto mhd_only) {
+        constexpr bool ONLY = decltype(mhd_only)::value;
+        const bool INC = ONLY || a.incompressible, MHD = ONLY || a.mhd, BOUS = !ONLY && a.bous;
+        const bool STRAT = !ONLY && a.strat, SHEAR = !ONLY && a.g.shear != 0.0;
+        const unsigned stsm = ONLY ? 0u : a.sts_mask;
+        for (size_t gb = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gb < total; gb += (size_t)gridDim.x * blockDim.x) {
+            int k, i, j, box;
+            unsigned line;
+            if (compact) {
+                // compact index -> box, kept x index, kept y index, k < kz_keep
+                const unsigned r1 = a.fd_kzk.div((unsigned)gb);
+                k = (int)(gb - (size_t)r1 * kzk);
+                const unsigned r2 = a.fd_nky.div(r1);
+                const int jy = (int)(r1 - r2 * (unsigned)a.nky);
+                const unsigned r3 = a.fd_nkx.div(r2);
+                const int ix = (int)(r2 - r3 * (unsigned)a.nkx);
+                box = (int)r3;
+                i = a.kxi[ix];
+                j = a.kyi[jy];
+                line = (unsigned)i * ny + (unsigned)j;
             } else {
-                sx = kx * R[0].x + ky * R[1].x + kz * R[2].x;
-                sy = kx * R[0].y + ky * R[1].y + kz * R[2].y;
+                // global line over the boxes -> box, line, k (nx*ny is a power of two)
+                const unsigned gline = fzh.div((unsigned)gb);
+                k = (int)(gb - (size_t)gline * nzh);
+                const unsigned ubox = a.fd_nl.div(gline);
+                box = (int)ubox;
+                line = gline - ubox * nlines;
+                const unsigned ui = a.fd_ny.div(line);
+                i = (int)ui;
+                j = (int)(line - ui * ny);
             }
-            const double kk[3] = {kx, ky, kz};
-#pragma unroll
-            for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
-            double2 Un[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) Un[c] = rk_value(a, bo + (size_t)(a.VEL + c) * nc + gi, Xu[c], Su[c], R[c], dt);
-            if (a.mode != XM_DFIELD) {
-                if (a.clean) clean3(Un, kx, ky, kz);
-#pragma unroll
-                for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.VEL + c) * nc + gi] = Un[c];
-            }
-        }
+            const size_t gi = (size_t)line * nzh + k;                // mode within the box
+            const size_t bo = (size_t)box * a.box_state;            // box offset in U, S, out
+            const double dt = a.sc[box].dt, nu = a.sc[box].nu, nu_m = a.sc[box].nu_m, nu_th = a.sc[box].nu_th;
+            // compact: every visited mode is kept (kxi and kyi list the indices of
+            // nonzero mask factors, and the kz mask is the prefix k < kz_keep), so
+            // the product loads need not wait for the mask tables
+            const bool m = compact || (a.g.mx[i] != 0.0 && a.g.my[j] != 0.0 && a.g.mz[k] != 0.0);
 
-        if (a.mhd) {
-            // i * mask * (k x E)
-            const double2 S3[3] = {d2(ky * e2.x - kz * e1.x, ky * e2.y - kz * e1.y),
-                                   d2(kz * e0.x - kx * e2.x, kz * e0.y - kx * e2.y),
-                                   d2(kx * e1.x - ky * e0.x, kx * e1.y - ky * e0.y)};
-            double2 Un[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                double2 R = d2(-S3[c].y, S3[c].x);
-                // shearing box: dBy -= S Bx (ShearingFlow with -shear)
-                if (c == 1 && a.g.shear != 0.0) R = d2(R.x + (-a.g.shear) * Xb[0].x, R.y + (-a.g.shear) * Xb[0].y);
-                if (!((a.sts_mask >> (a.MAG + c)) & 1u)) {
-                    const double f = -nu_m * k2;
-                    R = d2(R.x + f * Xb[c].x, R.y + f * Xb[c].y);
+            const C2<T>* nl = (const C2<T>*)a.nl + (size_t)box * a.box_nl;
+            const size_t li = (size_t)line * nzs + k;   // products: [ch][line][nzs]
+            auto P = [&](int ch) -> double2 { return to_d2(nl[(size_t)ch * a.cs_nl + li]); };
+
+            // every load of the mode first (state, RK scratch, products), so that
+            // they are all in flight together
+            double2 Xu[3] = {z0, z0, z0}, Xb[3] = {z0, z0, z0}, Xt = z0;
+            double2 Su[3] = {z0, z0, z0}, Sb[3] = {z0, z0, z0}, St = z0;
+            double2 t0 = z0, t1 = z0, t2 = z0, t3 = z0, t4 = z0, e0 = z0, e1 = z0, e2 = z0;
+            double2 f0 = z0, f1 = z0, f2 = z0, q0 = z0, q1 = z0, q2 = z0;
+            if (INC) {
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    Xu[c] = a.U[bo + (size_t)(a.VEL + c) * nc + gi];
+                    if (needS) Su[c] = a.S[bo + (size_t)(a.VEL + c) * nc + gi];
                 }
-                Un[c] = rk_value(a, bo + (size_t)(a.MAG + c) * nc + gi, Xb[c], Sb[c], R, dt);
             }
-            if (a.mode != XM_DFIELD) {
-                if (a.clean) clean3(Un, kx, ky, kz);
-#pragma unroll
-                for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.MAG + c) * nc + gi] = Un[c];
+            if (MHD) {
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    Xb[c] = a.U[bo + (size_t)(a.MAG + c) * nc + gi];
+                    if (needS) Sb[c] = a.S[bo + (size_t)(a.MAG + c) * nc + gi];
+                }
             }
-        }
+            if (BOUS) {
+                Xt = a.U[bo + (size_t)a.TH * nc + gi];
+                if (needS) St = a.S[bo + (size_t)a.TH * nc + gi];
+            }
+            if (m) {
+                if (INC && a.nl_T >= 0) { t0 = P(a.nl_T); t1 = P(a.nl_T + 1); t2 = P(a.nl_T + 2); t3 = P(a.nl_T + 3); t4 = P(a.nl_T + 4); }
+                if (MHD && a.nl_E >= 0) { e0 = P(a.nl_E); e1 = P(a.nl_E + 1); e2 = P(a.nl_E + 2); }
+                if (BOUS && a.nl_F >= 0) { f0 = P(a.nl_F); f1 = P(a.nl_F + 1); f2 = P(a.nl_F + 2); }
+                if (BOUS && a.aniso_rhs && a.nl_Q >= 0) { q0 = P(a.nl_Q); q1 = P(a.nl_Q + 1); q2 = P(a.nl_Q + 2); }
+            }
+            const double kx = a.g.kx[i] + shx * a.g.ky[j], ky = a.g.ky[j], kz = a.g.kz[k];
+            const double k2 = kx * kx + ky * ky + kz * kz;
+            double2 usd = z0;
 
-        if (a.bous) {
-            const double2 s = d2(kx * f0.x + ky * f1.x + kz * f2.x, kx * f0.y + ky * f1.y + kz * f2.y);
-            double2 R = d2(s.y, -s.x);   // -i * mask * k.(u theta)
-            if (a.strat) R = d2(R.x + a.N2 * usd.x, R.y + a.N2 * usd.y);
-            if (!((a.sts_mask >> a.TH) & 1u)) {
-                if (a.aniso_rhs) {
-                    const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
-                    R = d2(R.x - sq.y, R.y + sq.x);   // += i * mask * k.q
+            if (INC) {
+                double2 R[3];
+                // -i * mask * k_j T_ij with T = [[t0 t1 t2] [t1 t3 t4] [t2 t4 -t0-t3]]
+                const double2 s0 = d2(kx * t0.x + ky * t1.x + kz * t2.x, kx * t0.y + ky * t1.y + kz * t2.y);
+                const double2 s1 = d2(kx * t1.x + ky * t3.x + kz * t4.x, kx * t1.y + ky * t3.y + kz * t4.y);
+                const double2 s2 = d2(kx * t2.x + ky * t4.x - kz * (t0.x + t3.x), kx * t2.y + ky * t4.y - kz * (t0.y + t3.y));
+                R[0] = d2(s0.y, -s0.x);
+                R[1] = d2(s1.y, -s1.x);
+                R[2] = d2(s2.y, -s2.x);
+                if (STRAT) {
+                    if (a.sd == 0)      { R[0] = d2(R[0].x - Xt.x, R[0].y - Xt.y); usd = Xu[0]; }
+                    else if (a.sd == 1) { R[1] = d2(R[1].x - Xt.x, R[1].y - Xt.y); usd = Xu[1]; }
+                    else                { R[2] = d2(R[2].x - Xt.x, R[2].y - Xt.y); usd = Xu[2]; }
+                }
+                if (SHEAR) {
+                    // BackgroundShear / BackgroundRotation (shear_rotation.cu:11-63):
+                    // dvy += S vx; with rotation dvx += 2 omega vy, dvy -= 2 omega vx
+                    const double S = a.g.shear;
+                    R[1] = d2(R[1].x + S * Xu[0].x, R[1].y + S * Xu[0].y);
+                    if (a.rotating) {
+                        const double w2 = 2.0 * a.omega;
+                        R[0] = d2(R[0].x + w2 * Xu[1].x, R[0].y + w2 * Xu[1].y);
+                        R[1] = d2(R[1].x - w2 * Xu[0].x, R[1].y - w2 * Xu[0].y);
+                    }
+                }
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    if (!((stsm >> (a.VEL + c)) & 1u)) {
+                        const double f = -nu * k2;
+                        R[c] = d2(R[c].x + f * Xu[c].x, R[c].y + f * Xu[c].y);
+                    }
+                }
+                // Leray: dU += i k (i k.dU)/k^2; the shearing box adds S ky vx to
+                // k.dU (GradPseudoPressureShearing, cuda_kernels.cu:165-196)
+                const double ik2 = k2 > 0.0 ? 1.0 / k2 : 1.0;
+                double sx, sy;
+                if (SHEAR) {
+                    const double Sky = a.g.shear * ky;
+                    sx = Sky * Xu[0].x + kx * R[0].x + ky * R[1].x + kz * R[2].x;
+                    sy = Sky * Xu[0].y + kx * R[0].y + ky * R[1].y + kz * R[2].y;
                 } else {
-                    const double f = -nu_th * k2;
-                    R = d2(R.x + f * Xt.x, R.y + f * Xt.y);
+                    sx = kx * R[0].x + ky * R[1].x + kz * R[2].x;
+                    sy = kx * R[0].y + ky * R[1].y + kz * R[2].y;
+                }
+                const double kk[3] = {kx, ky, kz};
+    #pragma unroll
+                for (int c = 0; c < 3; c++) R[c] = d2(R[c].x - kk[c] * ik2 * sx, R[c].y - kk[c] * ik2 * sy);
+                double2 Un[3];
+    #pragma unroll
+                for (int c = 0; c < 3; c++) Un[c] = rk_value(a, bo + (size_t)(a.VEL + c) * nc + gi, Xu[c], Su[c], R[c], dt);
+                if (a.mode != XM_DFIELD) {
+                    if (a.clean) clean3(Un, kx, ky, kz);
+    #pragma unroll
+                    for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.VEL + c) * nc + gi] = Un[c];
                 }
             }
-            const double2 Un = rk_value(a, bo + (size_t)a.TH * nc + gi, Xt, St, R, dt);
-            if (a.mode != XM_DFIELD) a.U[bo + (size_t)a.TH * nc + gi] = Un;
+
+            if (MHD) {
+                // i * mask * (k x E)
+                const double2 S3[3] = {d2(ky * e2.x - kz * e1.x, ky * e2.y - kz * e1.y),
+                                       d2(kz * e0.x - kx * e2.x, kz * e0.y - kx * e2.y),
+                                       d2(kx * e1.x - ky * e0.x, kx * e1.y - ky * e0.y)};
+                double2 Un[3];
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    double2 R = d2(-S3[c].y, S3[c].x);
+                    // shearing box: dBy -= S Bx (ShearingFlow with -shear)
+                    if (c == 1 && SHEAR) R = d2(R.x + (-a.g.shear) * Xb[0].x, R.y + (-a.g.shear) * Xb[0].y);
+                    if (!((stsm >> (a.MAG + c)) & 1u)) {
+                        const double f = -nu_m * k2;
+                        R = d2(R.x + f * Xb[c].x, R.y + f * Xb[c].y);
+                    }
+                    Un[c] = rk_value(a, bo + (size_t)(a.MAG + c) * nc + gi, Xb[c], Sb[c], R, dt);
+                }
+                if (a.mode != XM_DFIELD) {
+                    if (a.clean) clean3(Un, kx, ky, kz);
+    #pragma unroll
+                    for (int c = 0; c < 3; c++) a.U[bo + (size_t)(a.MAG + c) * nc + gi] = Un[c];
+                }
+            }
+
+            if (BOUS) {
+                const double2 s = d2(kx * f0.x + ky * f1.x + kz * f2.x, kx * f0.y + ky * f1.y + kz * f2.y);
+                double2 R = d2(s.y, -s.x);   // -i * mask * k.(u theta)
+                if (STRAT) R = d2(R.x + a.N2 * usd.x, R.y + a.N2 * usd.y);
+                if (!((stsm >> a.TH) & 1u)) {
+                    if (a.aniso_rhs) {
+                        const double2 sq = d2(kx * q0.x + ky * q1.x + kz * q2.x, kx * q0.y + ky * q1.y + kz * q2.y);
+                        R = d2(R.x - sq.y, R.y + sq.x);   // += i * mask * k.q
+                    } else {
+                        const double f = -nu_th * k2;
+                        R = d2(R.x + f * Xt.x, R.y + f * Xt.y);
+                    }
+                }
+                const double2 Un = rk_value(a, bo + (size_t)a.TH * nc + gi, Xt, St, R, dt);
+                if (a.mode != XM_DFIELD) a.U[bo + (size_t)a.TH * nc + gi] = Un;
+            }
         }
-    }
+    };
+    if (a.incompressible && a.mhd && !a.bous && !a.strat && a.g.shear == 0.0 && a.sts_mask == 0)
+        modes(std::integral_constant<bool, true>());
+    else
+        modes(std::integral_constant<bool, false>());
 }
 
 // ---------------------------------------------------------------------------
