@@ -1804,7 +1804,9 @@ extern "C" int spk_synchronize(spk_ctx* c) {
 // Energy budgets of box b (0 for a single-box context).
 static int box_budgets(spk_ctx* c, int b, spk_budgets_t* out) {
     CK(cudaMemsetAsync(c->d_sums, 0, sizeof(double) * 16, c->stream));
-    k_budgets<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)b * c->F * c->nc, c->F, c->d_sums);
+    if (c->nc >= (1ull << 31)) return fail(c, SPK_ERR_UNSUPPORTED, "budgets: more than 2^31 modes per box");
+    k_budgets<<<ew_blocks(c->nc), 256, 0, c->stream>>>(c->g, c->U + (size_t)b * c->F * c->nc, c->F, c->d_sums,
+                                                         FastDiv::make((unsigned)c->nzh), FastDiv::make((unsigned)c->ny));
     CK(cudaMemcpyAsync(c->h_sums, c->d_sums, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const double n2 = (double)c->nr * (double)c->nr;

@@ -498,16 +498,20 @@ __global__ void k_rkl_spectral(const __grid_constant__ RklArgs a, double2* U) {
 
 // FP64 energy / dissipation sums with the half-spectrum weights
 // (computeEnergy, spooky_output_functions.cu:23-55).
-__global__ void k_budgets(DevGrid g, const double2* U, int F, double* sums) {
+// fzh, fny: 32-bit dividers by nzh and ny (a box's modes, nx*ny*nzh, stay
+// below 2^31 for every supported size), in place of 64-bit divisions that
+// would bound the kernel by instruction issue
+__global__ void k_budgets(DevGrid g, const double2* U, int F, double* sums, FastDiv fzh, FastDiv fny) {
     const double shx = grid_shx(g);
     const size_t nc = g.nc;
     __shared__ double red[2][32];
     for (int f = 0; f < F; f++) {
         double e = 0.0, d = 0.0;
         for (size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gi < nc; gi += (size_t)gridDim.x * blockDim.x) {
-            const int k = (int)(gi % g.nzh);
-            const size_t r = gi / g.nzh;
-            const int j = (int)(r % g.ny), i = (int)(r / g.ny);
+            const unsigned r = fzh.div((unsigned)gi);
+            const int k = (int)((unsigned)gi - r * (unsigned)g.nzh);
+            const unsigned ui = fny.div(r);
+            const int i = (int)ui, j = (int)(r - ui * (unsigned)g.ny);
             const double2 q = U[(size_t)f * nc + gi];
             const double w = k == 0 ? 1.0 : 2.0;
             const double a2 = q.x * q.x + q.y * q.y;
